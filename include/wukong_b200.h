@@ -1,0 +1,296 @@
+/*
+ * wukong_b200.h — C ABI of the B200-native triple-pattern exploration step.
+ *
+ * This is the boundary a Wukong host binds to in place of the reference's src/gpu path.
+ * Every call returns an int status: 0..13 keep the numbering of Wukong's
+ * src/core/common/errors.hpp:30-45 (SUCCESS, UNKNOWN_ERROR, ... FILE_NOT_FOUND); codes from
+ * 100 up are new (the reference aborts instead: gpu_utils.hpp:28-37, assertion.hpp:89-100).
+ * No call takes or returns a torch type; pointers are plain host pointers unless a parameter
+ * says "device".
+ *
+ * Threading: one wk_ctx per host thread (the reference runs one GPUAgent thread per GPU,
+ * gpu_agent.hpp:248).  Calls on one context are serialised by an internal mutex.
+ */
+#ifndef WUKONG_B200_H
+#define WUKONG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status codes */
+enum {
+    WK_SUCCESS = 0,             /* errors.hpp:31 */
+    WK_UNKNOWN_ERROR = 1,
+    WK_SYNTAX_ERROR = 2,
+    WK_UNKNOWN_PATTERN = 3,     /* unsupported pattern shape / operator */
+    WK_ATTR_DISABLE = 4,        /* attribute (non-SID) predicate */
+    WK_NO_REQUIRED_VAR = 5,
+    WK_UNSUPPORT_UNION = 6,
+    WK_OBJ_ERROR = 7,           /* index pattern whose predicate is not TYPE/PREDICATE */
+    WK_VERTEX_INVALID = 8,      /* variable id out of range */
+    WK_UNKNOWN_SUB = 9,         /* pattern starts from an unknown variable */
+    WK_SETTING_ERROR = 10,
+    WK_FIRST_PATTERN_ERROR = 11,/* const/index start that is not the first pattern */
+    WK_UNKNOWN_FILTER = 12,
+    WK_FILE_NOT_FOUND = 13,
+    WK_E_OOM = 100,             /* device allocation failed */
+    WK_E_CAPACITY = 101,        /* a result or working set would exceed a configured cap */
+    WK_E_TIMEOUT = 102,         /* a bounded device-side wait gave up */
+    WK_E_BADARG = 103,          /* null pointer, bad column, bad direction, ... */
+    WK_E_CUDA = 104,            /* a CUDA runtime call failed (see wk_last_error) */
+    WK_E_NOSTORE = 105,         /* no GStore uploaded yet */
+    WK_E_CORRUPT = 106,         /* key table chain out of range or too long */
+    WK_E_UNSUPPORTED = 107      /* legal in Wukong but outside this path (e.g. versatile) */
+};
+
+/* Directions (type.hpp:50) and reserved ids (vertex.hpp:52-53). */
+#define WK_IN 0
+#define WK_OUT 1
+#define WK_PREDICATE_ID 0
+#define WK_TYPE_ID 1
+#define WK_NO_RESULT 0xFFFF      /* v2c_map entry of an unbound variable (query.hpp:63) */
+
+/* Execution modes of wk_query_execute. */
+#define WK_MODE_PLAIN 0     /* one launch per pattern, host sync + size read-back per step */
+#define WK_MODE_RESIDENT 1  /* all steps enqueued back to back, sizes stay on the device */
+#define WK_MODE_GRAPH 2     /* as RESIDENT, replayed from a cached CUDA graph per plan shape */
+
+typedef struct wk_ctx wk_ctx;
+typedef struct wk_table wk_table;
+typedef struct wk_gstore wk_gstore;
+typedef struct wk_serve wk_serve;
+
+/* ---------------------------------------------------------------- plain data types */
+
+/* Device context configuration.  Zero fields take defaults. */
+typedef struct wk_config {
+    int32_t device;                   /* CUDA device ordinal */
+    int32_t max_cols;                 /* widest result table accepted (default 64) */
+    uint64_t rbuf_bytes;              /* initial size of each of the two ping-pong result
+                                         buffers (GPUMem rbuf, gpu_mem.hpp:53-60); they grow */
+    uint64_t working_set_cap_bytes;   /* serving admission cap (default 40 GiB) */
+    int32_t tune;                     /* 1 = run the tile autotuner at store upload */
+    int32_t reserved[7];
+} wk_config;
+
+/* One segment: segid_t (segment_meta.hpp:159-178) + rdf_seg_meta_t (:87-154), GPU build
+ * with one ext-bucket extent (EXT_BUCKET_LIST_CAPACITY 1, :43-45). */
+typedef struct wk_seg_meta {
+    int32_t index;          /* 0 = normal segment [vid|pid|dir]; 1 = index segment [0|*|dir] */
+    uint32_t pid;           /* predicate id (PREDICATE_ID for index segments) */
+    int32_t dir;            /* WK_IN / WK_OUT */
+    uint32_t reserved;
+    uint64_t num_keys;
+    uint64_t num_buckets;   /* main-header buckets of the segment (hash space) */
+    uint64_t bucket_start;  /* absolute bucket id of its first main-header bucket */
+    uint64_t num_edges;
+    uint64_t edge_start;
+    uint64_t ext_start;     /* ext_bucket_list[0].start (absolute bucket id) */
+    uint64_t ext_num;       /* ext_bucket_list[0].num_ext_buckets */
+} wk_seg_meta;
+
+/* SPARQLQuery::Pattern (query.hpp:145-170).  Variables are negative (-1, -2, ...),
+ * constants are ids >= 0.  pred_type must be 0 (SID_t). */
+typedef struct wk_pattern {
+    int32_t subject;
+    int32_t predicate;
+    int32_t object;
+    int32_t direction;
+    int32_t pred_type;
+} wk_pattern;
+
+/* A planned basic graph pattern: SPARQLQuery::pattern_group.patterns after
+ * Planner::set_direction (planner.hpp:667-699), plus Result::nvars and the mt_factor split
+ * of an index start (sparql.hpp:213-224). */
+typedef struct wk_query {
+    const wk_pattern* patterns;
+    int32_t n_patterns;
+    int32_t nvars;
+    int32_t mt_tid;         /* 0 unless the caller splits an index start */
+    int32_t mt_factor;      /* 1 unless the caller splits an index start */
+} wk_query;
+
+/* Synthetic LUBM-shaped graph generator parameters. */
+typedef struct wk_synth_params {
+    uint64_t seed;
+    uint32_t n_orgs;
+    int32_t zipf;           /* 0 = uniform degreeFrom targets / course choice, 1 = Zipf */
+    double zipf_s;          /* Zipf exponent when zipf = 1 (default 1.1) */
+} wk_synth_params;
+
+/* Ids the generator assigned; entity classes are written in this order per org. */
+typedef struct wk_synth_vocab {
+    uint32_t t_org, t_unit, t_person_a, t_person_b, t_person_c, t_course, t_doc;
+    uint32_t p_sub_org_of, p_member_of, p_takes, p_degree_from, p_author;
+    uint32_t first_vid;     /* first vertex id (2^17) */
+    uint32_t next_vid;      /* one past the last vertex id */
+} wk_synth_vocab;
+
+/* Serving configuration (wk_serve_run_open_loop). */
+typedef struct wk_serve_config {
+    uint64_t working_set_cap_bytes;   /* admission cap on projected table bytes (40 GiB) */
+    uint64_t light_arena_bytes;       /* bytes of each light ping-pong arena (default 1 GiB) */
+    uint32_t max_inflight;            /* light queries resident at once (default 65536) */
+    uint32_t heavy_rows_per_iter;     /* heavy-step input rows per iteration (default 1<<20) */
+    int32_t reserved[6];
+} wk_serve_config;
+
+/* Per-query outcome of a batch or a serving run. */
+typedef struct wk_qresult {
+    uint64_t rows;           /* rows of the final table */
+    uint64_t elem_offset;    /* where its table starts in the caller's output buffer */
+    int32_t cols;            /* Result::col_num */
+    int32_t status;          /* WK_* status of this query */
+    double t_arrive_us;      /* serving: arrival time (open-loop schedule) */
+    double t_done_us;        /* serving: completion time (result on the host) */
+} wk_qresult;
+
+/* ---------------------------------------------------------------- errors */
+const char* wk_strerror(int code);                 /* message for a status (errors.hpp:48-62) */
+const char* wk_last_error(const wk_ctx* ctx);      /* detail of the context's last failure */
+
+/* ---------------------------------------------------------------- synthetic data + host store */
+
+/* Generate the seeded LUBM-shaped triple set as n x (s, p, o) uint32 rows.  *triples is
+ * allocated by the library and released with wk_free.  (Stands in for the loader's id
+ * files, base_loader.hpp:236-280.) */
+int wk_synth_generate(const wk_synth_params* p, uint32_t** triples, uint64_t* n_triples,
+                      wk_synth_vocab* vocab);
+void wk_free(void* p);
+
+/* Build the static segment store on the host from id triples, as
+ * SegmentRDFGraph::init_gstore does (segment_rdf_dgraph.hpp:1182-1269) after the loader's
+ * sort + dedup (base_loader.hpp:481-496).  pso and pos are the triples to insert in the OUT
+ * and IN directions (normally the same array; n x 3 uint32 each).  load_factor is the mean
+ * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.5). */
+int wk_gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
+                    double load_factor, wk_gstore** out);
+void wk_gstore_free(wk_gstore* g);
+int wk_gstore_info(const wk_gstore* g, uint64_t* n_slots, uint64_t* n_edges, uint32_t* n_segs,
+                   uint64_t* n_keys);
+/* Borrowed views of the built arrays (valid until wk_gstore_free). */
+int wk_gstore_arrays(const wk_gstore* g, const void** slots, const uint32_t** edges,
+                     const wk_seg_meta** segs);
+/* Host-side DGraph::get_triples / get_index (segment_rdf_dgraph.hpp:1114-1129):
+ * *sz = 0 and *edges = NULL on a miss. */
+int wk_gstore_get_triples(const wk_gstore* g, uint32_t vid, uint32_t pid, int32_t dir,
+                          const uint32_t** edges, uint64_t* sz);
+int wk_gstore_get_index(const wk_gstore* g, uint32_t tpid, int32_t dir, const uint32_t** edges,
+                        uint64_t* sz);
+
+/* ---------------------------------------------------------------- device context */
+int wk_ctx_create(const wk_config* cfg, wk_ctx** out);
+int wk_ctx_destroy(wk_ctx* ctx);
+int wk_ctx_sync(wk_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work on it. */
+int wk_ctx_stream(wk_ctx* ctx, void** stream);
+/* Read and clear the sticky device-side error bits of the context stream (syncs); returns
+ * WK_E_CORRUPT / WK_E_TIMEOUT / WK_E_CAPACITY or 0. */
+int wk_ctx_check(wk_ctx* ctx);
+
+/* Upload a static segment store in Wukong's layout: slots = vertex_t[n_slots] (16 B each),
+ * edges = edge_t[n_edges] (uint32), segs = one entry per segment.  Replaces
+ * GPUCache::load_segment paging (gpu_cache.hpp:341-425): the whole store stays resident. */
+int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_segs, const void* slots,
+                    uint64_t n_slots, const uint32_t* edges, uint64_t n_edges);
+int wk_store_upload_gstore(wk_ctx* ctx, const wk_gstore* g);
+/* Device bytes held by the store (slots + edges + segment table). */
+int wk_store_bytes(const wk_ctx* ctx, uint64_t* bytes);
+
+/* ---------------------------------------------------------------- result tables */
+/* A device result table: row-major uint32, col_num * r + c (query.hpp:501-509). */
+int wk_table_alloc(wk_ctx* ctx, uint64_t capacity_elems, wk_table** out);
+int wk_table_free(wk_ctx* ctx, wk_table* t);
+/* GPUEngineCuda::load_result_buf (gpu_engine_cuda.hpp:90-106). */
+int wk_table_upload(wk_ctx* ctx, wk_table* t, const uint32_t* host, uint64_t rows, int32_t cols);
+/* The final thrust::copy D2H (gpu_engine_cuda.hpp:189-193); cap_elems bounds the copy. */
+int wk_table_download(wk_ctx* ctx, const wk_table* t, uint32_t* host, uint64_t cap_elems);
+int wk_table_shape(wk_ctx* ctx, const wk_table* t, uint64_t* rows, int32_t* cols);
+/* Device address of the table's first element (for callers that keep data on the GPU). */
+int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dptr);
+
+/* ---------------------------------------------------------------- one exploration step
+ * Each call runs one planned pattern over `in` and writes the next table to `out`
+ * (grown if needed), then synchronises.  Column indices are Result::var2col values. */
+
+/* IDX P ?X — GPUEngine::index_to_unknown (gpu_engine.hpp:65-100; CPU-only in the reference,
+ * GPU stub gpu_engine_cuda.hpp:108-111).  dir picks [0|tpid|dir]. */
+int wk_step_index_to_unknown(wk_ctx* ctx, uint32_t tpid, int32_t dir, int32_t mt_tid,
+                             int32_t mt_factor, wk_table* out);
+/* C P ?X — GPUEngine::const_to_unknown (gpu_engine.hpp:102-125). */
+int wk_step_const_to_unknown(wk_ctx* ctx, uint32_t vid, uint32_t pid, int32_t dir, wk_table* out);
+/* ?X P ?Y — GPUEngineCuda::known_to_unknown (gpu_engine_cuda.hpp:113-198). */
+int wk_step_known_to_unknown(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t pid,
+                             int32_t dir, wk_table* out);
+/* ?X P ?Y, both known — GPUEngineCuda::known_to_known (gpu_engine_cuda.hpp:200-282). */
+int wk_step_known_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_start, int32_t col_end,
+                           uint32_t pid, int32_t dir, wk_table* out);
+/* ?X P C — GPUEngineCuda::known_to_const (gpu_engine_cuda.hpp:284-363). */
+int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t end_vid,
+                           uint32_t pid, int32_t dir, wk_table* out);
+
+/* ---------------------------------------------------------------- whole query
+ * GPUAgent::execute_sparql_query's pattern loop (gpu_agent.hpp:173-246) driving
+ * GPUEngine::execute_one_pattern (gpu_engine.hpp:265-338).  On success *out_table holds the
+ * final table (owned by the context until the next query on it, or pass a table of your
+ * own via wk_query_execute_into), v2c_map[nvars] and *col_num describe its columns. */
+int wk_query_execute(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_table** out_table,
+                     int32_t* v2c_map, int32_t* col_num, uint64_t* rows);
+/* Check a plan without a device: the dispatch of GPUEngine::execute_one_pattern
+ * (gpu_engine.hpp:265-338) over var_stat (query.hpp:409-416) for every pattern.  Returns the
+ * status the query would end with for a malformed plan, else 0 with the final v2c_map[nvars]
+ * and *col_num. */
+int wk_query_validate(const wk_query* q, int32_t max_cols, int32_t* v2c_map, int32_t* col_num);
+/* Same, with the final table copied to host memory (the reference's new_table vector). */
+int wk_query_execute_host(wk_ctx* ctx, const wk_query* q, int32_t mode, uint32_t* host_out,
+                          uint64_t cap_elems, int32_t* v2c_map, int32_t* col_num, uint64_t* rows);
+/* Enqueue a query on the context stream and return without waiting (RESIDENT or GRAPH mode).
+ * The result buffers must already be large enough for it, i.e. the same plan has completed
+ * once through wk_query_execute; device-side errors surface through wk_ctx_check. */
+int wk_query_enqueue(wk_ctx* ctx, const wk_query* q, int32_t mode);
+
+/* Per-step profile of one query: each step runs alone between CUDA events on the context
+ * stream, `iters` times after one warm-up run; kind is 0 index, 1 const, 2 known_to_unknown,
+ * 3 known_to_known, 4 known_to_const.  sum_deg = total neighbour-list length the step's
+ * probes found (the edges an exhaustive list scan reads). */
+typedef struct wk_step_prof {
+    int32_t kind;
+    int32_t cols_in;
+    int32_t cols_out;
+    int32_t reserved;
+    uint64_t rows_in;
+    uint64_t rows_out;
+    uint64_t sum_deg;
+    double ms;               /* mean kernel time of the step */
+} wk_step_prof;
+int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof* out,
+                     int32_t max_steps, int32_t* n_steps);
+
+/* ---------------------------------------------------------------- batching
+ * Run n planned queries together: all queries advance one pattern per level inside one
+ * persistent kernel fed by a device work queue, levels replayed from a CUDA graph.  No
+ * counterpart in the reference (it runs one query per GPU agent at a time). */
+int wk_batch_execute(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t* host_out,
+                     uint64_t cap_elems, wk_qresult* results);
+/* Device-only variant: results stay on the device (for throughput timing).  *total_rows
+ * receives the sum of final rows. */
+int wk_batch_execute_device(wk_ctx* ctx, const wk_query* queries, uint32_t n,
+                            uint64_t* total_rows);
+
+/* ---------------------------------------------------------------- serving
+ * Continuous batching over an open-loop arrival schedule (no reference counterpart; shaped
+ * like ConsoleProxy::run_query_emu, console_proxy.hpp:287-439).  arrival_us[i] is when
+ * query i arrives, relative to the start of the run; results are copied to host_out. */
+int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg, const wk_query* queries,
+                           uint32_t n, const double* arrival_us, uint32_t* host_out,
+                           uint64_t cap_elems, wk_qresult* results);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WUKONG_B200_H */

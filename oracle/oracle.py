@@ -1,0 +1,144 @@
+"""ORACLE — test infrastructure only: ctypes wrapper of oracle/liboracle.so.
+
+The C++ restatement of the reference CPU engine (oracle/wukong_oracle.cpp).  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline / reference arm import this module; the
+product library never does.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.orc_store_build.restype = P
+        L.orc_store_build.argtypes = [P, C.c_uint64, P, C.c_uint64]
+        L.orc_store_free.argtypes = [P]
+        L.orc_get_triples.argtypes = [P, C.c_uint32, C.c_uint32, C.c_int,
+                                      C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]
+        L.orc_get_index.argtypes = [P, C.c_uint32, C.c_int,
+                                    C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]
+        L.orc_store_sizes.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                      C.POINTER(C.c_uint64)]
+        L.orc_store_export.argtypes = [P, P, P, P]
+        L.orc_query_run.argtypes = [P, P, C.c_int, C.c_int, C.c_int,
+                                    C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_int), P]
+        L.orc_queries_run_parallel.argtypes = [P, P, P, P, C.c_uint32, C.c_int, P, P]
+        L.orc_step.argtypes = [P, C.c_int, P, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                               C.c_uint32, C.c_int, C.POINTER(C.POINTER(C.c_uint32)),
+                               C.POINTER(C.c_uint64), C.POINTER(C.c_int)]
+        L.orc_free.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+class OracleStore:
+    """Store built by the reference's construction rules from (s, p, o) triples."""
+
+    def __init__(self, pso, pos=None):
+        pso = np.ascontiguousarray(pso, dtype=np.uint32)
+        pos = pso if pos is None else np.ascontiguousarray(pos, dtype=np.uint32)
+        self.h = lib().orc_store_build(_p(pso), pso.shape[0], _p(pos), pos.shape[0])
+        if not self.h:
+            raise RuntimeError("oracle store build failed")
+
+    def close(self):
+        if self.h:
+            lib().orc_store_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def get_triples(self, vid, pid, d):
+        p = C.POINTER(C.c_uint32)()
+        n = C.c_uint64()
+        rc = lib().orc_get_triples(self.h, vid, pid, d, C.byref(p), C.byref(n))
+        if rc:
+            raise RuntimeError("oracle lookup status %d" % rc)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.zeros(0, np.uint32)
+
+    def get_index(self, pid, d):
+        return self.get_triples(0, pid, d)
+
+    def export(self):
+        """(slots uint64[n,2], edges uint32[m], segs uint64[k,10]) in the store's own layout."""
+        ns, ne, ng = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib().orc_store_sizes(self.h, C.byref(ns), C.byref(ne), C.byref(ng))
+        slots = np.zeros((ns.value, 2), np.uint64)
+        edges = np.zeros(max(ne.value, 1), np.uint32)
+        segs = np.zeros((ng.value, 10), np.uint64)
+        lib().orc_store_export(self.h, _p(slots), _p(edges), _p(segs))
+        return slots, edges[:ne.value], segs
+
+    def run(self, query_flat, nvars, mt_factor=1):
+        """Run one planned query (n x 5 int32 patterns).  Returns (status, table, v2c)."""
+        q = np.ascontiguousarray(query_flat, dtype=np.int32)
+        tab = C.POINTER(C.c_uint32)()
+        rows = C.c_uint64()
+        cols = C.c_int()
+        v2c = np.zeros(max(nvars, 1), np.int32)
+        rc = lib().orc_query_run(self.h, _p(q), q.shape[0], nvars, mt_factor, C.byref(tab),
+                                 C.byref(rows), C.byref(cols), _p(v2c))
+        if rc:
+            return rc, None, None
+        n = rows.value * cols.value
+        try:
+            t = np.ctypeslib.as_array(tab, shape=(max(n, 1),))[:n].copy().reshape(rows.value, cols.value)
+        finally:
+            lib().orc_free(tab)
+        return 0, t, list(v2c[:nvars])
+
+    def step(self, op, table, cs, pid, d, ce=0, end_const=0):
+        """One known_to_* operator over an input table; op 0 = k2u, 1 = k2k, 2 = k2c."""
+        t = np.ascontiguousarray(table, dtype=np.uint32)
+        out = C.POINTER(C.c_uint32)()
+        rows = C.c_uint64()
+        cols = C.c_int()
+        rc = lib().orc_step(self.h, op, _p(t), t.shape[0], t.shape[1], cs, ce, end_const, pid, d,
+                            C.byref(out), C.byref(rows), C.byref(cols))
+        if rc:
+            raise RuntimeError("oracle step status %d" % rc)
+        n = rows.value * cols.value
+        try:
+            r = np.ctypeslib.as_array(out, shape=(max(n, 1),))[:n].copy().reshape(rows.value, cols.value)
+        finally:
+            lib().orc_free(out)
+        return r
+
+    def run_many(self, flat_list, nvars_list, threads):
+        """Run many queries, one per thread at a time; returns (rows, status) arrays."""
+        offs = np.zeros(len(flat_list) + 1, np.int32)
+        for i, f in enumerate(flat_list):
+            offs[i + 1] = offs[i] + f.shape[0]
+        pats = np.ascontiguousarray(np.concatenate(flat_list) if flat_list else np.zeros((0, 5)),
+                                    dtype=np.int32)
+        nv = np.ascontiguousarray(nvars_list, dtype=np.int32)
+        rows = np.zeros(len(flat_list), np.uint64)
+        status = np.zeros(len(flat_list), np.int32)
+        lib().orc_queries_run_parallel(self.h, _p(pats), _p(offs), _p(nv), len(flat_list), threads,
+                                       _p(rows), _p(status))
+        return rows, status
+
+
+def sorted_rows(t):
+    """Rows of a result table in lexicographic order (the multiset used for parity)."""
+    if t is None or t.size == 0:
+        return np.zeros((0, 0 if t is None else t.shape[1]), np.uint32)
+    idx = np.lexsort(t.T[::-1])
+    return t[idx]

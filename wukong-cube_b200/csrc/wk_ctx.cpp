@@ -1,0 +1,842 @@
+// C ABI: context, resident store, result tables, single steps and whole queries.
+//
+// Stands in for the reference's GPUEngine / GPUEngineCuda / GPUMem / GPUCache
+// (src/gpu/gpu_engine.hpp, gpu_engine_cuda.hpp, gpu_mem.hpp, gpu_cache.hpp).  The whole store
+// is uploaded once and stays resident, so there is no segment paging, no per-step mapping
+// upload and no per-step host sync unless the caller asks for the plain mode.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "wk_ctx.h"
+
+#define WK_CUDA(ctx, call)                                   \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return (ctx)->cuda_fail(e_, #call); \
+    } while (0)
+
+namespace {
+
+const char* kMessages[] = {
+    "Everything is ok",
+    "Something wrong happened",
+    "Something wrong in the query syntax, fail to parse!",
+    "Unsupported triple pattern.",
+    "MUST enable attribute support!",
+    "NO required variables!",
+    "Unsupport UNION on attribute results",
+    "Object should not be an index",
+    "Subject or object is not valid",
+    "Tripple pattern should not start from unknown subject.",
+    "You may change SETTING files to avoid this error. (e.g. global.hpp/config/...)",
+    "Const_X_X or index_X_X must be the first pattern.",
+    "Unsupported filter type.",
+    "Query file not found.",
+};
+
+constexpr uint64_t kPadWords = 16;
+
+}  // namespace
+
+extern "C" const char* wk_strerror(int code) {
+    if (code >= 0 && code < (int)(sizeof(kMessages) / sizeof(kMessages[0]))) return kMessages[code];
+    switch (code) {
+    case WK_E_OOM: return "device allocation failed";
+    case WK_E_CAPACITY: return "result or working set exceeds a configured capacity";
+    case WK_E_TIMEOUT: return "a bounded device-side wait gave up";
+    case WK_E_BADARG: return "invalid argument";
+    case WK_E_CUDA: return "CUDA runtime error";
+    case WK_E_NOSTORE: return "no GStore uploaded";
+    case WK_E_CORRUPT: return "key table chain out of range";
+    case WK_E_UNSUPPORTED: return "unsupported on this path";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char* wk_last_error(const wk_ctx* ctx) {
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+// ---------------------------------------------------------------- context helpers
+int wk_ctx::blocks_per_sm(int op, int cols) {
+    long long k = (long long)op * 1000 + cols;
+    auto it = bps_cache.find(k);
+    if (it != bps_cache.end()) return it->second;
+    int nb = wk::step_blocks_per_sm(cols, op);
+    bps_cache[k] = nb;
+    return nb;
+}
+
+int wk_ctx::ensure_status(uint64_t tiles) {
+    if (tiles <= status_cap) return WK_SUCCESS;
+    uint64_t cap = std::max<uint64_t>(tiles + tiles / 2, 1 << 14);
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    if (d_status) WK_CUDA(this, cudaFree(d_status));
+    d_status = nullptr;
+    if (cudaMalloc(&d_status, cap * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        status_cap = 0;
+        return fail(WK_E_OOM, "status array");
+    }
+    WK_CUDA(this, cudaMemsetAsync(d_status, 0, cap * sizeof(unsigned long long), stream));
+    unsigned long long c = cap;
+    WK_CUDA(this, cudaMemcpyAsync(&d_ctl->status_cap, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    status_cap = cap;
+    drop_graphs();   // captured launches hold the old status pointer
+    return WK_SUCCESS;
+}
+
+void wk_ctx::drop_graphs() {
+    for (auto& g : graphs)
+        if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+    graphs.clear();
+}
+
+int wk_ctx::table_reserve(wk_table* t, uint64_t elems) {
+    if (t->cap >= elems && t->d) return WK_SUCCESS;
+    if (t == &rbuf[0] || t == &rbuf[1]) drop_graphs();
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    if (t->d) cudaFree(t->d);
+    t->d = nullptr;
+    t->cap = 0;
+    if (cudaMalloc(&t->d, (elems + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WK_E_OOM, "result table of " + std::to_string(elems) + " elements");
+    }
+    t->cap = elems;
+    if (!t->d_rows) {
+        if (cudaMalloc(&t->d_rows, sizeof(uint64_t)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(WK_E_OOM, "row counter");
+        }
+        WK_CUDA(this, cudaMemsetAsync(t->d_rows, 0, sizeof(uint64_t), stream));
+    }
+    return WK_SUCCESS;
+}
+
+int wk_ctx::read_ctl(uint32_t* err, uint64_t* need) {
+    WK_CUDA(this, cudaMemcpyAsync(h_ctl, d_ctl, sizeof(wk::StepCtl), cudaMemcpyDeviceToHost, stream));
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    *err = h_ctl->err;
+    *need = h_ctl->need;
+    return WK_SUCCESS;
+}
+
+int wk_ctx::clear_ctl_err() {
+    WK_CUDA(this, cudaMemsetAsync(&d_ctl->err, 0, sizeof(unsigned), stream));
+    WK_CUDA(this, cudaMemsetAsync(&d_ctl->need, 0, sizeof(unsigned long long), stream));
+    return WK_SUCCESS;
+}
+
+// ---------------------------------------------------------------- plan resolution
+namespace wk {
+
+int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm) {
+    steps.clear();
+    if (q.n_patterns < 0 || q.nvars < 0 || (q.n_patterns > 0 && !q.patterns)) return WK_E_BADARG;
+    for (int i = 0; i < q.n_patterns; ++i) {
+        const wk_pattern& p = q.patterns[i];
+        if (p.direction != WK_IN && p.direction != WK_OUT) return WK_E_BADARG;
+        PlanStep st{};
+        st.dir = p.direction;
+        if (i == 0 && is_tpid(p.subject)) {
+            // start_from_index (query.hpp:816-838) -> index_to_unknown (gpu_engine.hpp:65-100)
+            if (p.predicate != WK_PREDICATE_ID && p.predicate != WK_TYPE_ID) return WK_OBJ_ERROR;
+            if (p.pred_type != 0) return WK_UNKNOWN_PATTERN;
+            int vs = cm.var_stat(p.object);
+            if (vs < 0 || vs == 2) return WK_VERTEX_INVALID;
+            if (vs == 0) return WK_UNKNOWN_PATTERN;   // index_to_known: not on the GPU path
+            st.kind = PlanStep::kIndex;
+            st.start_const = (uint32_t)p.subject;
+            st.in_cols = 0;
+            st.out_cols = 1;
+            cm.col_num = 1;
+            cm.bind(p.object, 0);
+            steps.push_back(st);
+            continue;
+        }
+        if (p.predicate < 0) return WK_UNKNOWN_PATTERN;   // versatile (unknown predicate)
+        if (p.pred_type != 0) return WK_ATTR_DISABLE;
+        st.pid = (uint32_t)p.predicate;
+        const int vs = cm.var_stat(p.subject), ve = cm.var_stat(p.object);
+        if (vs < 0 || ve < 0) return WK_VERTEX_INVALID;
+        if (vs == 2 && ve == 1) {
+            if (cm.col_num != 0) return WK_FIRST_PATTERN_ERROR;
+            st.kind = PlanStep::kConst;
+            st.start_const = (uint32_t)p.subject;
+            st.in_cols = 0;
+            st.out_cols = 1;
+            cm.bind(p.object, 0);
+            cm.col_num = 1;
+        } else if (vs == 0 && ve == 2) {
+            st.kind = PlanStep::kK2C;
+            st.cs = cm.col(p.subject);
+            st.end_const = (uint32_t)p.object;
+            st.in_cols = st.out_cols = cm.col_num;
+        } else if (vs == 0 && ve == 0) {
+            st.kind = PlanStep::kK2K;
+            st.cs = cm.col(p.subject);
+            st.ce = cm.col(p.object);
+            st.in_cols = st.out_cols = cm.col_num;
+        } else if (vs == 0 && ve == 1) {
+            st.kind = PlanStep::kK2U;
+            st.cs = cm.col(p.subject);
+            st.in_cols = cm.col_num;
+            st.out_cols = cm.col_num + 1;
+            if (st.out_cols > max_cols) return WK_E_CAPACITY;
+            cm.bind(p.object, cm.col_num);
+            cm.col_num += 1;
+        } else if (vs == 1) {
+            return WK_UNKNOWN_SUB;
+        } else {
+            return WK_UNKNOWN_PATTERN;   // CONST|CONST, CONST|KNOWN
+        }
+        steps.push_back(st);
+    }
+    return WK_SUCCESS;
+}
+
+int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* out,
+                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override) {
+    out->cols = st.out_cols;
+    if (st.kind == PlanStep::kIndex || st.kind == PlanStep::kConst) {
+        ListArgs a{};
+        a.store = ctx->dev_store();
+        if (st.kind == PlanStep::kIndex) {
+            a.key = make_key(0, st.start_const, st.dir);
+            a.seg = ctx->seg_of(0, st.start_const, st.dir);
+            a.mt_tid = mt_tid;
+            a.mt_factor = mt_factor > 0 ? mt_factor : 1;
+        } else {
+            a.key = make_key(st.start_const, st.pid, st.dir);
+            a.seg = ctx->seg_of(st.start_const, st.pid, st.dir);
+            a.mt_tid = 0;
+            a.mt_factor = 1;
+        }
+        a.out = out->d;
+        a.out_rows = out->d_rows;
+        a.out_cap = out->cap;
+        a.ctl = ctx->d_ctl;
+        int grid = grid_override > 0 ? grid_override : std::min(ctx->sm_count * 2, 512);
+        cudaError_t e = launch_list(a, grid, s);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "list kernel launch");
+        return WK_SUCCESS;
+    }
+    if (!in) return WK_E_BADARG;
+    StepArgs a{};
+    a.store = ctx->dev_store();
+    a.seg = ctx->seg_of(1, st.pid, st.dir);   // any nonzero vid: the normal segment
+    a.seg_index = ctx->seg_of(0, 0, st.dir);
+    a.in = in->d;
+    a.in_rows = in->d_rows;
+    a.in_cap = in->cap;
+    a.out = out->d;
+    a.out_rows = out->d_rows;
+    a.out_cap = out->cap;
+    a.ctl = ctx->d_ctl;
+    a.status = ctx->d_status;
+    a.cols = st.in_cols;
+    a.col_start = st.cs;
+    a.col_end = st.ce;
+    a.end_const = st.end_const;
+    a.pid = st.pid;
+    a.dir = st.dir;
+    a.type_index = 0;
+    switch (st.kind) {
+    case PlanStep::kK2U:
+        a.op = kOpK2U;
+        a.type_index = (st.pid == kTypeId && st.dir == kIn) ? 1 : 0;
+        break;
+    case PlanStep::kK2K: a.op = kOpK2K; break;
+    default: a.op = kOpK2C; break;
+    }
+    if (st.in_cols <= 0) return WK_E_BADARG;
+    int grid = grid_override > 0 ? grid_override : ctx->blocks_per_sm(a.op, st.in_cols) * ctx->sm_count;
+    cudaError_t e = launch_step(a, grid, s);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "step kernel launch");
+    return WK_SUCCESS;
+}
+
+}  // namespace wk
+
+// ---------------------------------------------------------------- context
+extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
+    if (!out) return WK_E_BADARG;
+    wk_ctx* ctx = nullptr;
+    try {
+        ctx = new wk_ctx();
+    } catch (const std::bad_alloc&) {
+        return WK_E_OOM;
+    }
+    if (cfg) ctx->cfg = *cfg;
+    if (ctx->cfg.max_cols <= 0) ctx->cfg.max_cols = 32;
+    if (ctx->cfg.max_cols > 32) {
+        delete ctx;
+        return WK_E_BADARG;   // shared-memory staging holds at most 32 columns per row
+    }
+    if (ctx->cfg.rbuf_bytes == 0) ctx->cfg.rbuf_bytes = 64ull << 20;
+    if (ctx->cfg.working_set_cap_bytes == 0) ctx->cfg.working_set_cap_bytes = 40ull << 30;
+    ctx->device = ctx->cfg.device;
+    auto bail = [&](cudaError_t e, const char* what) {
+        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+        delete ctx;
+        (void)m;
+        return WK_E_CUDA;
+    };
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return bail(e, "cudaSetDevice");
+    e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (e != cudaSuccess) return bail(e, "sm count");
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(e, "stream");
+    e = wk::step_kernel_attrs(ctx->cfg.max_cols);
+    if (e != cudaSuccess) return bail(e, "kernel attributes");
+    e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
+    if (e != cudaSuccess) return bail(e, "control block");
+    e = cudaMallocHost(&ctx->h_ctl, sizeof(wk::StepCtl));
+    if (e != cudaSuccess) return bail(e, "pinned control block");
+    e = cudaMallocHost(&ctx->h_rows, sizeof(uint64_t) * 4);
+    if (e != cudaSuccess) return bail(e, "pinned rows");
+    wk::StepCtl init{};
+    init.epoch = 1;
+    e = cudaMemcpy(ctx->d_ctl, &init, sizeof(init), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bail(e, "control init");
+    int rc = ctx->ensure_status(1 << 14);
+    if (rc) {
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return WK_SUCCESS;
+}
+
+void wk_batch_release(wk_ctx* ctx);   // wk_batch.cu
+
+extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
+    if (!ctx) return WK_E_BADARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    wk_batch_release(ctx);
+    ctx->drop_graphs();
+    for (auto& t : ctx->rbuf) {
+        if (t.d) cudaFree(t.d);
+        if (t.d_rows) cudaFree(t.d_rows);
+    }
+    if (ctx->d_slots) cudaFree(ctx->d_slots);
+    if (ctx->d_edges) cudaFree(ctx->d_edges);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+    if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+    if (ctx->h_rows) cudaFreeHost(ctx->h_rows);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_ctx_sync(wk_ctx* ctx) {
+    if (!ctx) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_ctx_stream(wk_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return WK_E_BADARG;
+    *stream = (void*)ctx->stream;
+    return WK_SUCCESS;
+}
+
+// ---------------------------------------------------------------- store
+extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_segs,
+                               const void* slots, uint64_t n_slots, const uint32_t* edges,
+                               uint64_t n_edges) {
+    if (!ctx || (!segs && n_segs) || (!slots && n_slots) || (!edges && n_edges)) return WK_E_BADARG;
+    if (n_slots % wk::kAssoc) return ctx->fail(WK_E_BADARG, "slot count is not a multiple of 8");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const uint64_t nb = n_slots / wk::kAssoc;
+    for (uint32_t i = 0; i < n_segs; ++i) {
+        const wk_seg_meta& m = segs[i];
+        if (m.dir != WK_IN && m.dir != WK_OUT)
+            return ctx->fail(WK_E_BADARG, "segment direction");
+        if (m.bucket_start + m.num_buckets > nb)
+            return ctx->fail(WK_E_CORRUPT, "segment buckets outside the slot array");
+        if (m.edge_start + m.num_edges > n_edges)
+            return ctx->fail(WK_E_CORRUPT, "segment edges outside the edge array");
+    }
+    WK_CUDA(ctx, cudaSetDevice(ctx->device));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->d_slots) cudaFree(ctx->d_slots);
+    if (ctx->d_edges) cudaFree(ctx->d_edges);
+    ctx->d_slots = nullptr;
+    ctx->d_edges = nullptr;
+    ctx->has_store = false;
+    if (cudaMalloc(&ctx->d_slots, std::max<uint64_t>(n_slots, wk::kAssoc) * sizeof(wk::Slot)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_edges, (n_edges + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return ctx->fail(WK_E_OOM, "store upload");
+    }
+    if (n_slots)
+        WK_CUDA(ctx, cudaMemcpy(ctx->d_slots, slots, n_slots * sizeof(wk::Slot), cudaMemcpyHostToDevice));
+    if (n_edges)
+        WK_CUDA(ctx, cudaMemcpy(ctx->d_edges, edges, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ctx->n_slots = n_slots;
+    ctx->n_edges = n_edges;
+    ctx->segs.assign(segs, segs + n_segs);
+    ctx->index.build(ctx->segs.data(), n_segs);
+    ctx->has_store = true;
+    ctx->drop_graphs();
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_store_upload_gstore(wk_ctx* ctx, const wk_gstore* g) {
+    if (!ctx || !g) return WK_E_BADARG;
+    return wk_store_upload(ctx, g->segs.data(), (uint32_t)g->segs.size(), g->slots.data(),
+                           g->slots.size(), g->edges.data(), g->edges.size());
+}
+
+extern "C" int wk_store_bytes(const wk_ctx* ctx, uint64_t* bytes) {
+    if (!ctx || !bytes) return WK_E_BADARG;
+    *bytes = ctx->n_slots * sizeof(wk::Slot) + ctx->n_edges * sizeof(uint32_t) +
+             ctx->segs.size() * sizeof(wk_seg_meta);
+    return WK_SUCCESS;
+}
+
+// ---------------------------------------------------------------- tables
+extern "C" int wk_table_alloc(wk_ctx* ctx, uint64_t capacity_elems, wk_table** out) {
+    if (!ctx || !out) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    wk_table* t = new (std::nothrow) wk_table();
+    if (!t) return WK_E_OOM;
+    int rc = ctx->table_reserve(t, std::max<uint64_t>(capacity_elems, 1));
+    if (rc) {
+        delete t;
+        return rc;
+    }
+    *out = t;
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_table_free(wk_ctx* ctx, wk_table* t) {
+    if (!ctx || !t) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStreamSynchronize(ctx->stream);
+    if (t->d) cudaFree(t->d);
+    if (t->d_rows) cudaFree(t->d_rows);
+    delete t;
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_table_upload(wk_ctx* ctx, wk_table* t, const uint32_t* host, uint64_t rows,
+                               int32_t cols) {
+    if (!ctx || !t || (!host && rows && cols) || cols < 0) return WK_E_BADARG;
+    if (cols > ctx->cfg.max_cols) return ctx->fail(WK_E_CAPACITY, "too many columns");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const uint64_t n = rows * (uint64_t)cols;
+    int rc = ctx->table_reserve(t, std::max<uint64_t>(n, 1));
+    if (rc) return rc;
+    if (n) WK_CUDA(ctx, cudaMemcpyAsync(t->d, host, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->h_rows[0] = cols ? rows : 0;
+    WK_CUDA(ctx, cudaMemcpyAsync(t->d_rows, ctx->h_rows, 8, cudaMemcpyHostToDevice, ctx->stream));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    t->cols = cols;
+    return WK_SUCCESS;
+}
+
+static int table_rows(wk_ctx* ctx, const wk_table* t, uint64_t* rows) {
+    WK_CUDA(ctx, cudaMemcpyAsync(ctx->h_rows, t->d_rows, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *rows = ctx->h_rows[0];
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_table_shape(wk_ctx* ctx, const wk_table* t, uint64_t* rows, int32_t* cols) {
+    if (!ctx || !t) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    uint64_t r = 0;
+    int rc = table_rows(ctx, t, &r);
+    if (rc) return rc;
+    if (rows) *rows = r;
+    if (cols) *cols = t->cols;
+    return WK_SUCCESS;
+}
+
+static int table_download(wk_ctx* ctx, const wk_table* t, uint32_t* host, uint64_t cap_elems,
+                          uint64_t* rows_out) {
+    uint64_t r = 0;
+    int rc = table_rows(ctx, t, &r);
+    if (rc) return rc;
+    if (rows_out) *rows_out = r;
+    const uint64_t n = r * (uint64_t)t->cols;
+    if (n > cap_elems) return ctx->fail(WK_E_CAPACITY, "host buffer too small");
+    if (n > t->cap) return ctx->fail(WK_E_CORRUPT, "row count beyond table capacity");
+    if (n) WK_CUDA(ctx, cudaMemcpyAsync(host, t->d, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_table_download(wk_ctx* ctx, const wk_table* t, uint32_t* host, uint64_t cap_elems) {
+    if (!ctx || !t || (!host && cap_elems)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return table_download(ctx, t, host, cap_elems, nullptr);
+}
+
+extern "C" int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dptr) {
+    if (!ctx || !t || !dptr) return WK_E_BADARG;
+    *dptr = t->d;
+    return WK_SUCCESS;
+}
+
+// ---------------------------------------------------------------- single steps (plain)
+// Run one step with a host sync; grow the output and rerun if it did not fit.
+static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in, wk_table* out,
+                         int32_t mt_tid, int32_t mt_factor) {
+    if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    if (in && in->cols > 0) {
+        int rc = ctx->ensure_status(in->cap / in->cols / wk::kTileRows + 2);
+        if (rc) return rc;
+    }
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int rc = wk::enqueue_step(ctx, st, in, out, mt_tid, mt_factor, ctx->stream, 0);
+        if (rc) return rc;
+        uint32_t err = 0;
+        uint64_t need = 0;
+        rc = ctx->read_ctl(&err, &need);
+        if (rc) return rc;
+        if (!err) return WK_SUCCESS;
+        rc = ctx->clear_ctl_err();
+        if (rc) return rc;
+        if (err & wk::kErrCorrupt) return ctx->fail(WK_E_CORRUPT, "key table chain out of range");
+        if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "tile look-back timed out");
+        if (err & wk::kErrStatus) return ctx->fail(WK_E_CAPACITY, "status array too small");
+        if (err & wk::kErrOverflow) {
+            rc = ctx->table_reserve(out, need + need / 8 + 1024);
+            if (rc) return rc;
+        }
+    }
+    return ctx->fail(WK_E_CAPACITY, "output kept overflowing");
+}
+
+static int check_in(wk_ctx* ctx, const wk_table* in, int32_t cs, int32_t ce) {
+    if (!in || in->cols <= 0) return ctx->fail(WK_E_BADARG, "input table has no columns");
+    if (cs < 0 || cs >= in->cols || ce < 0 || ce >= in->cols)
+        return ctx->fail(WK_E_BADARG, "column out of range");
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_step_index_to_unknown(wk_ctx* ctx, uint32_t tpid, int32_t dir, int32_t mt_tid,
+                                        int32_t mt_factor, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || mt_factor < 1 || mt_tid < 0)
+        return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kIndex;
+    st.start_const = tpid;
+    st.dir = dir;
+    st.out_cols = 1;
+    return run_step_sync(ctx, st, nullptr, out, mt_tid, mt_factor);
+}
+
+extern "C" int wk_step_const_to_unknown(wk_ctx* ctx, uint32_t vid, uint32_t pid, int32_t dir,
+                                        wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kConst;
+    st.start_const = vid;
+    st.pid = pid;
+    st.dir = dir;
+    st.out_cols = 1;
+    return run_step_sync(ctx, st, nullptr, out, 0, 1);
+}
+
+extern "C" int wk_step_known_to_unknown(wk_ctx* ctx, const wk_table* in, int32_t col_start,
+                                        uint32_t pid, int32_t dir, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || in == out) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc = check_in(ctx, in, col_start, col_start);
+    if (rc) return rc;
+    if (in->cols + 1 > ctx->cfg.max_cols) return ctx->fail(WK_E_CAPACITY, "too many columns");
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kK2U;
+    st.pid = pid;
+    st.dir = dir;
+    st.cs = col_start;
+    st.in_cols = in->cols;
+    st.out_cols = in->cols + 1;
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+extern "C" int wk_step_known_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_start,
+                                      int32_t col_end, uint32_t pid, int32_t dir, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || in == out) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc = check_in(ctx, in, col_start, col_end);
+    if (rc) return rc;
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kK2K;
+    st.pid = pid;
+    st.dir = dir;
+    st.cs = col_start;
+    st.ce = col_end;
+    st.in_cols = st.out_cols = in->cols;
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+extern "C" int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t col_start,
+                                      uint32_t end_vid, uint32_t pid, int32_t dir, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || in == out) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc = check_in(ctx, in, col_start, col_start);
+    if (rc) return rc;
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kK2C;
+    st.pid = pid;
+    st.dir = dir;
+    st.cs = col_start;
+    st.end_const = end_vid;
+    st.in_cols = st.out_cols = in->cols;
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+// ---------------------------------------------------------------- whole queries
+static std::string plan_key(const std::vector<wk::PlanStep>& steps, const wk_query& q,
+                            const wk_ctx* ctx) {
+    std::string k;
+    auto put = [&](const void* p, size_t n) { k.append((const char*)p, n); };
+    for (auto& s : steps) put(&s, sizeof(s));
+    put(&q.mt_tid, 4);
+    put(&q.mt_factor, 4);
+    for (auto& t : ctx->rbuf) {
+        put(&t.d, sizeof(t.d));
+        put(&t.cap, sizeof(t.cap));
+    }
+    put(&ctx->d_status, sizeof(ctx->d_status));
+    return k;
+}
+
+static int enqueue_plan(wk_ctx* ctx, const std::vector<wk::PlanStep>& steps, const wk_query& q) {
+    for (size_t i = 0; i < steps.size(); ++i) {
+        const wk_table* in = i ? &ctx->rbuf[(i - 1) & 1] : nullptr;
+        wk_table* out = &ctx->rbuf[i & 1];
+        int rc = wk::enqueue_step(ctx, steps[i], in, out, q.mt_tid, q.mt_factor, ctx->stream, 0);
+        if (rc) return rc;
+    }
+    return WK_SUCCESS;
+}
+
+static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_table** out_table,
+                     int32_t* v2c_map, int32_t* col_num) {
+    if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    std::vector<wk::PlanStep> steps;
+    wk::ColMap cm(q->nvars);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    if (rc) return ctx->fail(rc, wk_strerror(rc));
+    if (q->mt_factor < 1 || q->mt_tid < 0) return ctx->fail(WK_E_BADARG, "mt_factor");
+    for (auto& t : ctx->rbuf) {
+        rc = ctx->table_reserve(&t, std::max<uint64_t>(t.cap, ctx->cfg.rbuf_bytes / 4));
+        if (rc) return rc;
+    }
+    if (steps.empty()) {
+        WK_CUDA(ctx, cudaMemsetAsync(ctx->rbuf[0].d_rows, 0, 8, ctx->stream));
+        ctx->rbuf[0].cols = 0;
+        *out_table = &ctx->rbuf[0];
+    } else if (mode == WK_MODE_PLAIN) {
+        // one launch per pattern, host sync + size read-back after each (the reference's shape)
+        for (size_t i = 0; i < steps.size(); ++i) {
+            const wk_table* in = i ? &ctx->rbuf[(i - 1) & 1] : nullptr;
+            rc = run_step_sync(ctx, steps[i], in, &ctx->rbuf[i & 1], q->mt_tid, q->mt_factor);
+            if (rc) return rc;
+        }
+        *out_table = &ctx->rbuf[(steps.size() - 1) & 1];
+    } else {
+        for (int attempt = 0;; ++attempt) {
+            if (attempt >= 8) return ctx->fail(WK_E_CAPACITY, "results kept overflowing");
+            uint64_t mx = std::max(ctx->rbuf[0].cap, ctx->rbuf[1].cap);
+            rc = ctx->ensure_status(mx / wk::kTileRows + 2);
+            if (rc) return rc;
+            if (mode == WK_MODE_GRAPH) {
+                std::string key = plan_key(steps, *q, ctx);
+                auto it = ctx->graphs.find(key);
+                if (it == ctx->graphs.end()) {
+                    if (ctx->graphs.size() > 256) ctx->drop_graphs();
+                    cudaGraph_t graph;
+                    WK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                    int erc = enqueue_plan(ctx, steps, *q);
+                    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+                    if (erc) return erc;
+                    if (ce != cudaSuccess) return ctx->cuda_fail(ce, "end capture");
+                    wk_ctx::GraphEntry ge;
+                    ce = cudaGraphInstantiate(&ge.exec, graph, 0);
+                    cudaGraphDestroy(graph);
+                    if (ce != cudaSuccess) return ctx->cuda_fail(ce, "graph instantiate");
+                    it = ctx->graphs.emplace(key, ge).first;
+                }
+                WK_CUDA(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+            } else {
+                rc = enqueue_plan(ctx, steps, *q);
+                if (rc) return rc;
+            }
+            uint32_t err = 0;
+            uint64_t need = 0;
+            rc = ctx->read_ctl(&err, &need);
+            if (rc) return rc;
+            if (!err) break;
+            rc = ctx->clear_ctl_err();
+            if (rc) return rc;
+            if (err & wk::kErrCorrupt) return ctx->fail(WK_E_CORRUPT, "key table chain out of range");
+            if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "tile look-back timed out");
+            if (err & (wk::kErrOverflow | wk::kErrStatus)) {
+                uint64_t want = std::max<uint64_t>(need + need / 4, mx * 2);
+                for (auto& t : ctx->rbuf) {
+                    rc = ctx->table_reserve(&t, want);
+                    if (rc) return rc;
+                }
+            }
+        }
+        *out_table = &ctx->rbuf[(steps.size() - 1) & 1];
+    }
+    if (col_num) *col_num = cm.col_num;
+    if (v2c_map)
+        for (int i = 0; i < q->nvars; ++i) v2c_map[i] = cm.v2c[i];
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_query_execute(wk_ctx* ctx, const wk_query* q, int32_t mode,
+                                const wk_table** out_table, int32_t* v2c_map, int32_t* col_num,
+                                uint64_t* rows) {
+    if (!ctx || !q || mode < 0 || mode > 2) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const wk_table* t = nullptr;
+    int rc = query_run(ctx, q, mode, &t, v2c_map, col_num);
+    if (rc) return rc;
+    if (out_table) *out_table = t;
+    if (rows) {
+        rc = table_rows(ctx, t, rows);
+        if (rc) return rc;
+    }
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_query_execute_host(wk_ctx* ctx, const wk_query* q, int32_t mode, uint32_t* host_out,
+                                     uint64_t cap_elems, int32_t* v2c_map, int32_t* col_num,
+                                     uint64_t* rows) {
+    if (!ctx || !q || mode < 0 || mode > 2 || (!host_out && cap_elems)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const wk_table* t = nullptr;
+    int rc = query_run(ctx, q, mode, &t, v2c_map, col_num);
+    if (rc) return rc;
+    return table_download(ctx, t, host_out, cap_elems, rows);
+}
+
+// Enqueue a query on the context stream without waiting (for device-side timing).  Buffers
+// must already be large enough: run wk_query_execute on the same plan first.
+extern "C" int wk_query_enqueue(wk_ctx* ctx, const wk_query* q, int32_t mode) {
+    if (!ctx || !q || (mode != WK_MODE_RESIDENT && mode != WK_MODE_GRAPH)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    std::vector<wk::PlanStep> steps;
+    wk::ColMap cm(q->nvars);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    if (rc) return rc;
+    if (mode == WK_MODE_GRAPH) {
+        auto it = ctx->graphs.find(plan_key(steps, *q, ctx));
+        if (it == ctx->graphs.end()) return ctx->fail(WK_E_BADARG, "plan not captured yet");
+        WK_CUDA(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+        return WK_SUCCESS;
+    }
+    return enqueue_plan(ctx, steps, *q);
+}
+
+// Sticky device-side error bits of the context stream (0 = none); clears them.
+extern "C" int wk_ctx_check(wk_ctx* ctx) {
+    if (!ctx) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    uint32_t err = 0;
+    uint64_t need = 0;
+    int rc = ctx->read_ctl(&err, &need);
+    if (rc) return rc;
+    if (!err) return WK_SUCCESS;
+    ctx->clear_ctl_err();
+    if (err & wk::kErrCorrupt) return WK_E_CORRUPT;
+    if (err & wk::kErrTimeout) return WK_E_TIMEOUT;
+    return WK_E_CAPACITY;
+}
+
+extern "C" int wk_query_validate(const wk_query* q, int32_t max_cols, int32_t* v2c_map,
+                                 int32_t* col_num) {
+    if (!q) return WK_E_BADARG;
+    if (max_cols <= 0) max_cols = 32;
+    std::vector<wk::PlanStep> steps;
+    wk::ColMap cm(q->nvars);
+    int rc = wk::resolve_plan(*q, max_cols, steps, cm);
+    if (rc) return rc;
+    if (col_num) *col_num = cm.col_num;
+    if (v2c_map)
+        for (int i = 0; i < q->nvars; ++i) v2c_map[i] = cm.v2c[i];
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof* out,
+                                int32_t max_steps, int32_t* n_steps) {
+    if (!ctx || !q || iters < 1 || (!out && max_steps)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    std::vector<wk::PlanStep> steps;
+    wk::ColMap cm(q->nvars);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    if (rc) return ctx->fail(rc, wk_strerror(rc));
+    if ((int)steps.size() > max_steps) return ctx->fail(WK_E_CAPACITY, "profile array too small");
+    const wk_table* t = nullptr;
+    rc = query_run(ctx, q, WK_MODE_PLAIN, &t, nullptr, nullptr);   // sizes the buffers
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    WK_CUDA(ctx, cudaEventCreate(&e0));
+    WK_CUDA(ctx, cudaEventCreate(&e1));
+    std::vector<double> acc(steps.size(), 0.0);
+    for (int it = 0; it <= iters; ++it) {
+        for (size_t i = 0; i < steps.size(); ++i) {
+            const wk_table* in = i ? &ctx->rbuf[(i - 1) & 1] : nullptr;
+            wk_table* o = &ctx->rbuf[i & 1];
+            WK_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 8, ctx->stream));
+            WK_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+            rc = wk::enqueue_step(ctx, steps[i], in, o, q->mt_tid, q->mt_factor, ctx->stream, 0);
+            if (rc) return rc;
+            WK_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+            WK_CUDA(ctx, cudaEventSynchronize(e1));
+            float ms = 0;
+            WK_CUDA(ctx, cudaEventElapsedTime(&ms, e0, e1));
+            if (it > 0) acc[i] += ms;
+            if (it == 0) {
+                wk_step_prof& p = out[i];
+                std::memset(&p, 0, sizeof(p));
+                p.kind = (int)steps[i].kind;
+                p.cols_in = steps[i].in_cols;
+                p.cols_out = steps[i].out_cols;
+                uint64_t r = 0;
+                if (in) {
+                    rc = table_rows(ctx, in, &r);
+                    if (rc) return rc;
+                }
+                p.rows_in = r;
+                rc = table_rows(ctx, o, &r);
+                if (rc) return rc;
+                p.rows_out = r;
+                WK_CUDA(ctx, cudaMemcpy(&p.sum_deg, &ctx->d_ctl->sum_deg, 8, cudaMemcpyDeviceToHost));
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (size_t i = 0; i < steps.size(); ++i) out[i].ms = acc[i] / iters;
+    if (n_steps) *n_steps = (int32_t)steps.size();
+    uint32_t err = 0;
+    uint64_t need = 0;
+    rc = ctx->read_ctl(&err, &need);
+    if (rc) return rc;
+    if (err) {
+        ctx->clear_ctl_err();
+        return ctx->fail(WK_E_CAPACITY, "profile run reported device errors");
+    }
+    return WK_SUCCESS;
+}

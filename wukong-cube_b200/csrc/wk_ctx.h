@@ -1,0 +1,131 @@
+// Device context, tables and plan resolution shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "wk_internal.h"
+#include "wk_kernels.h"
+
+// A device result table (the reference's rbuf + GPUResult, query.hpp:311-362).
+struct wk_table {
+    uint32_t* d = nullptr;     // row-major elements
+    uint64_t cap = 0;          // elements held
+    uint64_t* d_rows = nullptr;// row count, written by the kernels
+    int32_t cols = 0;
+};
+
+namespace wk {
+
+// Host mirror of SPARQLQuery::Result's column bookkeeping (query.hpp:409-459).
+struct ColMap {
+    int nvars = 0;
+    int col_num = 0;
+    std::vector<int32_t> v2c;   // NO_RESULT (0xFFFF) when unbound
+    explicit ColMap(int n) : nvars(n), v2c(n > 0 ? n : 0, WK_NO_RESULT) {}
+    // 0 = KNOWN, 1 = UNKNOWN, 2 = CONST; -1 = invalid variable id (VERTEX_INVALID)
+    int var_stat(int32_t id) const {
+        if (id >= 0) return 2;
+        int idx = -(id + 1);
+        if (idx >= nvars) return -1;
+        return v2c[idx] == WK_NO_RESULT ? 1 : 0;
+    }
+    int col(int32_t id) const { return v2c[-(id + 1)]; }
+    void bind(int32_t id, int c) { v2c[-(id + 1)] = c; }
+};
+
+// One resolved exploration step of a plan.
+struct PlanStep {
+    enum Kind { kIndex, kConst, kK2U, kK2K, kK2C } kind;
+    uint32_t pid = 0;
+    int32_t dir = 0;
+    uint32_t start_const = 0;   // kIndex: tpid; kConst: start vertex
+    int32_t cs = 0, ce = 0;     // input columns
+    uint32_t end_const = 0;     // kK2C
+    int32_t in_cols = 0, out_cols = 0;
+};
+
+// Resolve a planned pattern list into steps, as GPUEngine::execute_one_pattern dispatches
+// (gpu_engine.hpp:265-338).  Returns a WK_* status; fills v2c_map / col_num of the result.
+int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm);
+
+}  // namespace wk
+
+struct wk_ctx {
+    std::mutex mu;
+    wk_config cfg{};
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+
+    // resident store
+    wk::Slot* d_slots = nullptr;
+    uint64_t n_slots = 0;
+    uint32_t* d_edges = nullptr;
+    uint64_t n_edges = 0;
+    std::vector<wk_seg_meta> segs;
+    wk::SegIndex index;
+    bool has_store = false;
+
+    // scan control of the context stream
+    wk::StepCtl* d_ctl = nullptr;
+    unsigned long long* d_status = nullptr;
+    uint64_t status_cap = 0;
+    wk::StepCtl* h_ctl = nullptr;     // pinned
+    uint64_t* h_rows = nullptr;       // pinned
+
+    // ping-pong result buffers for whole queries (GPUMem rbuf pair, gpu_mem.hpp:53-60)
+    wk_table rbuf[2];
+
+    // CUDA graphs of resident query plans
+    struct GraphEntry {
+        cudaGraphExec_t exec = nullptr;
+        const wk_table* final_table = nullptr;
+        uint64_t cap0 = 0, cap1 = 0;
+    };
+    std::map<std::string, GraphEntry> graphs;
+
+    std::map<long long, int> bps_cache;   // (op, cols) -> blocks per SM
+    std::string last_error;
+
+    // batch / serving state (wk_batch.cu)
+    void* batch = nullptr;
+
+    wk::DevStore dev_store() const {
+        wk::DevStore s;
+        s.slots = d_slots;
+        s.n_buckets = n_slots / wk::kAssoc;
+        s.edges = d_edges;
+        s.n_edges = n_edges;
+        return s;
+    }
+    wk::SegDesc seg_of(uint64_t vid, uint32_t pid, int dir) const {
+        int32_t i = index.find(vid, pid, dir);
+        wk::SegDesc d{0, 0, 0, 0};
+        if (i >= 0 && pid < (1u << wk::kNbitsIdx)) d = wk::to_desc(segs[i]);
+        return d;
+    }
+    int fail(int code, const std::string& msg) {
+        last_error = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        last_error = std::string(what) + ": " + cudaGetErrorString(e);
+        return WK_E_CUDA;
+    }
+    int blocks_per_sm(int op, int cols);
+    void drop_graphs();
+    int ensure_status(uint64_t tiles);
+    int table_reserve(wk_table* t, uint64_t elems);
+    int read_ctl(uint32_t* err, uint64_t* need);
+    int clear_ctl_err();
+};
+
+namespace wk {
+// Enqueue one resolved step reading `in` (may be null for index/const starts) into `out`.
+int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* out,
+                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override);
+}  // namespace wk

@@ -1,0 +1,75 @@
+"""Build recipe for libwukong_b200.so (CUDA for sm_100a + C++ host) and the oracle.
+
+Compiles in-tree so the shared objects travel with the repository snapshot:
+  wukong-cube_b200/libwukong_b200.so   the product: kernels + C ABI (include/wukong_b200.h)
+  oracle/liboracle.so                  the CPU checker (test infrastructure only)
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libwukong_b200.so")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+CXX = os.environ.get("CXX", "g++")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["wk_kernels.cu", "wk_batch.cu"]
+CPP_SOURCES = ["wk_ctx.cpp", "wk_gstore.cpp", "wk_synth.cpp"]
+HEADERS = ["wk_format.h", "wk_internal.h", "wk_kernels.h", "wk_ctx.h", "wk_batch.h"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout)
+        raise RuntimeError("build step failed: " + cmd[0])
+    return r.stdout
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def build_lib(verbose=False, force=False):
+    os.makedirs(OBJ, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "wukong_b200.h")]
+    objs = []
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                        "-Xptxas", "-v", "-c", s, "-o", o])
+            if verbose:
+                print(out)
+    for src in CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if force or _stale(o, [s] + hdrs):
+            _run([CXX, "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-function",
+                  "-I" + os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o])
+    if force or _stale(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
+    return LIB
+
+
+def build_oracle():
+    _run(["make", "-s", "-C", ORACLE_DIR])
+    return os.path.join(ORACLE_DIR, "liboracle.so")
+
+
+if __name__ == "__main__":
+    print(build_lib(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    print(build_oracle())
