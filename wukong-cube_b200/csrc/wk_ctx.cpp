@@ -60,11 +60,11 @@ extern "C" const char* wk_last_error(const wk_ctx* ctx) {
 }
 
 // ---------------------------------------------------------------- context helpers
-int wk_ctx::blocks_per_sm(int op, int cols) {
-    long long k = (long long)op * 1000 + cols;
+int wk_ctx::blocks_per_sm(int op, int cols, int lanes) {
+    long long k = ((long long)op * 1000 + cols) * 16 + lanes;
     auto it = bps_cache.find(k);
     if (it != bps_cache.end()) return it->second;
-    int nb = wk::step_blocks_per_sm(cols, op);
+    int nb = wk::step_blocks_per_sm(cols, op, lanes);
     bps_cache[k] = nb;
     return nb;
 }
@@ -245,6 +245,7 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
     a.pid = st.pid;
     a.dir = st.dir;
     a.type_index = 0;
+    a.sorted_lists = ctx->sorted_lists;
     switch (st.kind) {
     case PlanStep::kK2U:
         a.op = kOpK2U;
@@ -254,7 +255,9 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
     default: a.op = kOpK2C; break;
     }
     if (st.in_cols <= 0) return WK_E_BADARG;
-    int grid = grid_override > 0 ? grid_override : ctx->blocks_per_sm(a.op, st.in_cols) * ctx->sm_count;
+    a.lanes = ctx->lanes_for(a.op, st.in_cols);
+    int grid = grid_override > 0 ? grid_override
+                                 : ctx->blocks_per_sm(a.op, st.in_cols, a.lanes) * ctx->sm_count;
     cudaError_t e = launch_step(a, grid, s);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "step kernel launch");
     return WK_SUCCESS;
@@ -387,6 +390,23 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
     ctx->segs.assign(segs, segs + n_segs);
     ctx->index.build(ctx->segs.data(), n_segs);
     ctx->has_store = true;
+    {
+        // are all lists ascending + unique?  (lets the filters binary-search long lists)
+        unsigned* d_flag = nullptr;
+        WK_CUDA(ctx, cudaMalloc(&d_flag, sizeof(unsigned)));
+        WK_CUDA(ctx, cudaMemsetAsync(d_flag, 0, sizeof(unsigned), ctx->stream));
+        cudaError_t e = wk::launch_sorted_check(ctx->dev_store(), d_flag, ctx->stream);
+        unsigned flag = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, d_flag, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        cudaFree(d_flag);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "sorted-list check");
+        if (flag & 2u) {
+            ctx->has_store = false;
+            return ctx->fail(WK_E_CORRUPT, "a key's list lies outside the edge array");
+        }
+        ctx->sorted_lists = (flag & 1u) ? 0 : 1;
+    }
     ctx->drop_graphs();
     return WK_SUCCESS;
 }
@@ -698,6 +718,8 @@ static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
         }
         *out_table = &ctx->rbuf[(steps.size() - 1) & 1];
     }
+    // a replayed graph does not run enqueue_step, so set the final table's width here
+    if (!steps.empty()) ctx->rbuf[(steps.size() - 1) & 1].cols = steps.back().out_cols;
     if (col_num) *col_num = cm.col_num;
     if (v2c_map)
         for (int i = 0; i < q->nvars; ++i) v2c_map[i] = cm.v2c[i];
@@ -744,6 +766,7 @@ extern "C" int wk_query_enqueue(wk_ctx* ctx, const wk_query* q, int32_t mode) {
         auto it = ctx->graphs.find(plan_key(steps, *q, ctx));
         if (it == ctx->graphs.end()) return ctx->fail(WK_E_BADARG, "plan not captured yet");
         WK_CUDA(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+        if (!steps.empty()) ctx->rbuf[(steps.size() - 1) & 1].cols = steps.back().out_cols;
         return WK_SUCCESS;
     }
     return enqueue_plan(ctx, steps, *q);

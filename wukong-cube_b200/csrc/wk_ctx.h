@@ -69,6 +69,9 @@ struct wk_ctx {
     std::vector<wk_seg_meta> segs;
     wk::SegIndex index;
     bool has_store = false;
+    int sorted_lists = 0;
+    int default_lanes = 2;
+    std::map<int, int> tuned_lanes;
 
     // scan control of the context stream
     wk::StepCtl* d_ctl = nullptr;
@@ -116,7 +119,12 @@ struct wk_ctx {
         last_error = std::string(what) + ": " + cudaGetErrorString(e);
         return WK_E_CUDA;
     }
-    int blocks_per_sm(int op, int cols);
+    int blocks_per_sm(int op, int cols, int lanes);
+    // lanes per probe group for (op, cols): the tuned choice, else 2 (one 32-byte sector)
+    int lanes_for(int op, int cols) const {
+        auto it = tuned_lanes.find(op * 1000 + cols);
+        return it != tuned_lanes.end() ? it->second : default_lanes;
+    }
     void drop_graphs();
     int ensure_status(uint64_t tiles);
     int table_reserve(wk_table* t, uint64_t elems);

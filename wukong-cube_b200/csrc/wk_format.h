@@ -80,8 +80,26 @@ static_assert(sizeof(Slot) == 16, "slot must be 16 bytes");
 struct SegDesc {
     uint64_t bucket_start;   // absolute bucket id of the segment's main-header region
     uint64_t num_buckets;    // hash space of the segment (0 = segment absent / empty)
-    uint64_t edge_start;     // first edge of the segment (informational)
+    uint64_t magic;          // floor((2^64 - 1) / num_buckets): Barrett reciprocal of the modulo
     uint64_t num_edges;      // number of edges of the segment (informational)
 };
+
+WK_HD uint64_t barrett_magic(uint64_t nb) { return nb ? ~0ull / nb : 0; }
+
+// hash % nb without a 64-bit division (Barrett, "Implementing the Rivest Shamir and Adleman
+// public key encryption algorithm on a standard digital signal processor", CRYPTO 1986):
+// with m = floor((2^64 - 1) / nb) the estimate q = floor(h * m / 2^64) is at most one short of
+// floor(h / nb), so one conditional subtraction gives the exact remainder.
+WK_HD uint64_t mod_barrett(uint64_t h, uint64_t nb, uint64_t m) {
+#if defined(__CUDA_ARCH__)
+    uint64_t q = __umul64hi(h, m);
+#else
+    uint64_t q = (uint64_t)(((unsigned __int128)h * m) >> 64);
+#endif
+    uint64_t r = h - q * nb;
+    if (r >= nb) r -= nb;
+    if (r >= nb) r -= nb;
+    return r;
+}
 
 }  // namespace wk

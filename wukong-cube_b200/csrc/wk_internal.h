@@ -16,7 +16,7 @@ int synth_generate(const wk_synth_params& p, std::vector<uint32_t>& out, wk_synt
 inline uint64_t host_probe(const Slot* slots, uint64_t n_buckets_total, const SegDesc& seg,
                            uint64_t key, int* corrupt) {
     if (seg.num_buckets == 0) return 0;
-    uint64_t b = seg.bucket_start + hash_u64(key) % seg.num_buckets;
+    uint64_t b = seg.bucket_start + mod_barrett(hash_u64(key), seg.num_buckets, seg.magic);
     for (uint64_t hop = 0; hop <= n_buckets_total; ++hop) {
         if (b >= n_buckets_total) {
             if (corrupt) *corrupt = 1;
@@ -50,7 +50,7 @@ inline SegDesc to_desc(const wk_seg_meta& m) {
     SegDesc d;
     d.bucket_start = m.bucket_start;
     d.num_buckets = m.num_buckets;
-    d.edge_start = m.edge_start;
+    d.magic = barrett_magic(m.num_buckets);
     d.num_edges = m.num_edges;
     return d;
 }

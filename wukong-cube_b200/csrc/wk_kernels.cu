@@ -2,16 +2,20 @@
 //
 // One launch runs one planned pattern over a whole result table (the reference chains five
 // kernels, a Thrust scan and two host syncs per pattern: gpu_engine_cuda.hpp:169-177,
-// gpu_hash.cu:96-836).  Each CTA claims 512-row tiles from a device counter and, per tile:
-//   1. stages the tile's rows in shared memory with coalesced loads;
-//   2. probes the key table with 8-lane groups: one 16-byte slot per lane, so a group reads
-//      one 128-byte bucket in a single coalesced request, four keys per group in flight;
-//      chains through slot 7 are followed until a hit or an empty link;
-//   3. counts its output rows (neighbour count for known_to_unknown, a 0/1 membership flag
-//      for known_to_known / known_to_const, found by a group-wide ballot over the list);
-//   4. turns the counts into output positions with a block scan plus a decoupled look-back
+// gpu_hash.cu:96-836).  CTAs claim 512-row tiles from a device counter and, per tile:
+//   1. start a TMA bulk copy (cp.async.bulk + mbarrier) of the tile's rows into shared memory
+//      and, while it is in flight, read each row's start column straight from global memory;
+//   2. probe the key table with groups of LANES lanes: each lane loads one 16-byte slot, so a
+//      group reads a 32/64/128-byte slice of a bucket in one coalesced request, four rows per
+//      group in flight.  Because the static store only ever inserts into the first empty slot
+//      (kvstore.hpp:163-180, segment_rdf_dgraph.hpp:216-233), an empty slot before a hit ends
+//      the search, so most probes read only the bucket's first 32-byte sector;
+//   3. count its output rows: the neighbour count for known_to_unknown, a 0/1 membership flag
+//      for known_to_known / known_to_const (a group-wide ballot over the first 8 entries, then a
+//      binary search of the rest when lists are sorted, as the loader leaves them);
+//   4. turn the counts into output positions with a block scan plus a decoupled look-back
 //      across tiles (single pass, 64-bit offsets);
-//   5. writes its output rows through shared memory with 16-byte stores: known_to_unknown
+//   5. write its output rows through shared memory with 16-byte stores: known_to_unknown
 //      expands each row once per neighbour in row-major, edge order (what the CPU engine
 //      appends, sparql.hpp:328-370); the filters compact the surviving rows in order.
 // Sizes are read from device memory, so steps chain without a host round trip; an output that
@@ -24,18 +28,16 @@ namespace wk {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kGroup = 8;                                 // lanes per bucket probe
-constexpr int kGroups = kStepThreads / kGroup;            // groups per CTA
-constexpr int kUnroll = 4;                                // keys per group in flight
-constexpr int kRowsPerGroup = kTileRows / kGroups;        // 16
-constexpr int kMaxHops = 1 << 16;                         // chain walk limit
+constexpr int kUnroll = 4;                                // rows per lane group in flight
+constexpr int kMaxProbeIters = 1 << 14;                   // chain walk limit
 constexpr unsigned long long kFlagAgg = 1, kFlagPrefix = 2;
 constexpr unsigned long long kValMask = (1ull << 46) - 1;
 constexpr unsigned long long kSpinLimit = 1ull << 24;     // look-back polls before giving up
+constexpr unsigned kTmaWaitLimit = 1u << 24;              // mbarrier polls before giving up
 constexpr int kChunkBytes = 32 * 1024;                    // staging of one output chunk
+constexpr int kLinear = 8;                                // list entries checked by ballot
 
 static_assert(kTileRows % kStepThreads == 0, "rows per thread");
-static_assert(kRowsPerGroup % kUnroll == 0, "unroll");
 
 __device__ __forceinline__ unsigned long long pack_status(unsigned epoch, unsigned long long flag,
                                                           unsigned long long v) {
@@ -46,62 +48,128 @@ __device__ __forceinline__ ulonglong2 load_slot(const Slot* p) {
     return __ldg(reinterpret_cast<const ulonglong2*>(p));
 }
 
-// Probe kUnroll keys per 8-lane group.  Every lane of the warp must call this (the ballots and
-// shuffles are warp-wide).  On return ptr[u] is the slot's pointer word in every lane of the
-// group, or 0 when the key is absent.
-__device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&bstart)[kUnroll],
-                                            const uint64_t (&nbk)[kUnroll],
-                                            const uint64_t (&key)[kUnroll],
-                                            const bool (&valid)[kUnroll],
+// ---------------------------------------------------------------- mbarrier + TMA bulk copy
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Global -> shared bulk copy; both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes,
+                                            uint64_t* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Bounded wait for the current phase; a timeout sets kErrTimeout and waits once more (bounded)
+// so no copy is left in flight when the CTA moves on.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err) {
+    unsigned n = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++n > kTmaWaitLimit) {
+            if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+            for (unsigned m = 0; m < kTmaWaitLimit && !mbar_try_wait(bar, parity); ++m) __nanosleep(256);
+            return;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- probe
+__device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
+    return s.bucket_start + mod_barrett(hash_u64(key), s.num_buckets, s.magic);
+}
+
+// Probe kUnroll keys per group of L lanes.  Every lane of the warp must call this (ballots and
+// shuffles are warp-wide).  On entry bucket[u] is the key's home bucket and pending[u] says
+// whether to look; on return ptr[u] is the slot's pointer word in every lane of the group, or 0
+// when the key is absent.
+template <int L>
+__device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&key)[kUnroll],
+                                            uint64_t (&bucket)[kUnroll], bool (&pending)[kUnroll],
                                             uint64_t (&ptr)[kUnroll], unsigned* err) {
     const int lane = threadIdx.x & 31;
-    const int gl = lane & (kGroup - 1);
-    const int gbase = lane & ~(kGroup - 1);
-    uint64_t bucket[kUnroll];
-    bool pending[kUnroll];
+    const int h = lane & (L - 1);
+    const int gbase = lane & ~(L - 1);
+    const unsigned gmask = (1u << L) - 1;
+    int round[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
         ptr[u] = 0;
-        pending[u] = valid[u] && nbk[u] != 0 && key[u] != 0;
-        bucket[u] = pending[u] ? bstart[u] + hash_u64(key[u]) % nbk[u] : 0;
+        round[u] = 0;
     }
-    for (int hop = 0;; ++hop) {
+    for (int it = 0;; ++it) {
         bool any = false;
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) any |= pending[u];
         if (!__any_sync(kFull, any)) break;
-        if (hop >= kMaxHops) {
-            if (any && gl == 0) atomicOr(err, kErrCorrupt);
+        if (it >= kMaxProbeIters) {
+            if (any && h == 0) atomicOr(err, kErrCorrupt);
             break;
         }
         ulonglong2 s[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            s[u] = make_ulonglong2(0, 0);
+            s[u] = make_ulonglong2(~0ull, 0);
             if (pending[u]) {
                 if (bucket[u] >= st.n_buckets) {
                     pending[u] = false;
-                    if (gl == 0) atomicOr(err, kErrCorrupt);
+                    if (h == 0) atomicOr(err, kErrCorrupt);
                 } else {
-                    s[u] = load_slot(st.slots + bucket[u] * kAssoc + gl);
+                    s[u] = load_slot(st.slots + bucket[u] * kAssoc + round[u] * L + h);
                 }
             }
         }
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
-            const bool hit = pending[u] && gl < kAssoc - 1 && s[u].x == key[u];
-            const unsigned m = (__ballot_sync(kFull, hit) >> gbase) & 0x7Fu;
-            const int src = m ? gbase + __ffs(m) - 1 : gbase + kAssoc - 1;
+            const bool data = round[u] * L + h < kAssoc - 1;
+            const bool hit = pending[u] && data && s[u].x == key[u];
+            const bool emp = pending[u] && data && s[u].x == 0;
+            const unsigned hm = (__ballot_sync(kFull, hit) >> gbase) & gmask;
+            const unsigned em = (__ballot_sync(kFull, emp) >> gbase) & gmask;
+            const int src = hm ? gbase + __ffs(hm) - 1 : gbase + L - 1;
             const uint64_t kx = __shfl_sync(kFull, s[u].x, src);
             const uint64_t py = __shfl_sync(kFull, s[u].y, src);
             if (pending[u]) {
-                if (m) {
+                if (hm) {
                     ptr[u] = py;
                     pending[u] = false;
-                } else if (kx == 0) {
-                    pending[u] = false;   // empty chain link: key absent
+                } else if (em) {
+                    pending[u] = false;           // first empty slot: the key is absent
+                } else if ((round[u] + 1) * L >= kAssoc) {
+                    if (kx == 0) {
+                        pending[u] = false;       // no extension bucket
+                    } else {
+                        bucket[u] = key_vid(kx);  // follow slot 7 (kvstore.hpp:303-310)
+                        round[u] = 0;
+                    }
                 } else {
-                    bucket[u] = key_vid(kx);
+                    round[u]++;
                 }
             }
         }
@@ -234,11 +302,66 @@ __device__ void exit_protocol(StepCtl* ctl, unsigned long long* status, unsigned
     }
 }
 
-template <int OP>
-__global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, int chunk_rows) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// Membership of target[u] in the (ascending, unique when `sorted`) list edges[off, off+deg):
+// the first kLinear entries by a group ballot, the rest by binary search (sorted) or a scan.
+template <int L>
+__device__ __forceinline__ void group_member(const uint32_t* edges, const uint64_t (&off)[kUnroll],
+                                             const uint64_t (&deg)[kUnroll],
+                                             const uint32_t (&target)[kUnroll],
+                                             const bool (&valid)[kUnroll], bool sorted,
+                                             bool (&found)[kUnroll]) {
+    const int lane = threadIdx.x & 31;
+    const int h = lane & (L - 1);
+    const int gbase = lane & ~(L - 1);
+    const unsigned gmask = (1u << L) - 1;
+    constexpr int per = kLinear / L;
+    uint32_t v[kUnroll][per];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+        for (int j = 0; j < per; ++j) {
+            const uint64_t k = (uint64_t)j * L + h;
+            v[u][j] = (valid[u] && k < deg[u]) ? __ldg(edges + off[u] + k) : ~target[u];
+        }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        bool hit = false;
+#pragma unroll
+        for (int j = 0; j < per; ++j) hit |= (v[u][j] == target[u]);
+        found[u] = ((__ballot_sync(kFull, hit && valid[u]) >> gbase) & gmask) != 0;
+    }
+    // long lists: one lane per group continues
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        bool more = valid[u] && !found[u] && deg[u] > (uint64_t)kLinear;
+        bool f = false;
+        if (more && h == 0) {
+            const uint32_t* p = edges + off[u];
+            if (sorted) {
+                uint64_t lo = kLinear, hi = deg[u];
+                while (lo < hi) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (__ldg(p + mid) < target[u]) lo = mid + 1; else hi = mid;
+                }
+                f = lo < deg[u] && __ldg(p + lo) == target[u];
+            } else {
+                for (uint64_t k = kLinear; k < deg[u] && !f; ++k) f = __ldg(p + k) == target[u];
+            }
+        }
+        f = __shfl_sync(kFull, f, gbase);
+        found[u] = found[u] || f;
+    }
+}
+
+template <int OP, int L>
+__global__ void __launch_bounds__(kStepThreads, 4) step_kernel(const StepArgs a, int chunk_rows) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t s_bar;
     __shared__ unsigned long long s_tile, s_excl, s_deg;
     __shared__ uint64_t s_warp[kStepThreads / 32];
+    constexpr int kGroups = kStepThreads / L;            // rows per pass
+    constexpr int kBatches = kTileRows / (kGroups * kUnroll);
+    static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
 
     const int C = a.cols;
     const int outc = (OP == kOpK2U) ? C + 1 : C;
@@ -257,10 +380,12 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
         ntiles = 0;
     }
     if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = 0;
+    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
 
-    const int gid = threadIdx.x / kGroup;
-    const int gl = threadIdx.x & (kGroup - 1);
-    const int gbase = (threadIdx.x & 31) & ~(kGroup - 1);
+    const int grp = threadIdx.x / L;
+    const int h = threadIdx.x & (L - 1);
+    unsigned phase = 0;
 
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl->tile_counter, 1ull);
@@ -269,25 +394,32 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
         if (tile >= ntiles) break;
         const uint64_t r0 = tile * kTileRows;
         const int n = (int)min((uint64_t)kTileRows, R - r0);
-
-        // 1. stage the tile's rows
         const uint32_t* src = a.in + r0 * C;
-        for (int e = threadIdx.x; e < n * C; e += kStepThreads) s_in[e] = __ldg(src + e);
+
+        // 1. rows -> shared memory, asynchronously (tables carry >= 64 bytes of tail padding)
+        if (threadIdx.x == 0) {
+            const unsigned bytes = (unsigned)(((uint64_t)n * C * 4 + 15) & ~15ull);
+            mbar_expect_tx(&s_bar, bytes);
+            tma_load_1d(s_in, src, bytes, &s_bar);
+            s_deg = 0;
+        }
         for (int r = threadIdx.x; r < n; r += kStepThreads) s_cnt[r] = 0;
-        if (threadIdx.x == 0) s_deg = 0;
         __syncthreads();
 
-        // 2-3. probe and count
+        // 2-3. probe and count, start columns read from global memory
 #pragma unroll 1
-        for (int b = 0; b < kRowsPerGroup; b += kUnroll) {
-            uint64_t bstart[kUnroll], nbk[kUnroll], key[kUnroll], ptr[kUnroll];
-            bool valid[kUnroll];
+        for (int b = 0; b < kBatches; ++b) {
+            uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
+            bool valid[kUnroll], pending[kUnroll];
             int row[kUnroll];
+            uint32_t target[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
-                row[u] = gid + kGroups * (b + u);
+                row[u] = (b * kUnroll + u) * kGroups + grp;
                 valid[u] = row[u] < n;
-                const uint32_t cur = valid[u] ? s_in[row[u] * C + a.col_start] : kBlankId;
+                const uint32_t cur = valid[u] ? __ldg(src + (uint64_t)row[u] * C + a.col_start) : kBlankId;
+                target[u] = (OP == kOpK2K) ? (valid[u] ? __ldg(src + (uint64_t)row[u] * C + a.col_end) : 0)
+                                           : a.end_const;
                 const SegDesc* sg = &a.seg;
                 if (OP == kOpK2U && a.type_index) {
                     // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
@@ -299,24 +431,22 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
                     if (cur == 0) sg = &a.seg_index;   // vid 0 names the index segment
                 }
                 if (cur == kBlankId) valid[u] = false;
-                bstart[u] = sg->bucket_start;
-                nbk[u] = sg->num_buckets;
+                pending[u] = valid[u] && sg->num_buckets != 0 && key[u] != 0;
+                bucket[u] = pending[u] ? bucket_of(key[u], *sg) : 0;
             }
-            group_probe(a.store, bstart, nbk, key, valid, ptr, &a.ctl->err);
+            group_probe<L>(a.store, key, bucket, pending, ptr, &a.ctl->err);
             uint64_t off[kUnroll], deg[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u) {
                 off[u] = ptr_off(ptr[u]);
                 deg[u] = ptr_size(ptr[u]);
                 if (off[u] + deg[u] > a.store.n_edges) {
-                    if (gl == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
+                    if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
                     deg[u] = 0;
                 }
-                if (OP != kOpK2U && gl == 0 && valid[u] && deg[u])
-                    atomicAdd(&s_deg, (unsigned long long)deg[u]);
             }
             if (OP == kOpK2U) {
-                if (gl == 0) {
+                if (h == 0) {
 #pragma unroll
                     for (int u = 0; u < kUnroll; ++u)
                         if (valid[u]) {
@@ -325,44 +455,19 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
                         }
                 }
             } else {
-                // membership of the target in the neighbour list, 8 elements per round
-                uint32_t target[kUnroll];
-                bool active[kUnroll], found[kUnroll];
+                bool has[kUnroll], found[kUnroll];
 #pragma unroll
-                for (int u = 0; u < kUnroll; ++u) {
-                    target[u] = (OP == kOpK2K) ? (valid[u] ? s_in[row[u] * C + a.col_end] : 0)
-                                               : a.end_const;
-                    active[u] = valid[u] && deg[u] > 0;
-                    found[u] = false;
-                }
-                for (uint64_t k = 0;; k += kGroup) {
-                    bool any = false;
-#pragma unroll
-                    for (int u = 0; u < kUnroll; ++u) any |= active[u];
-                    if (!__any_sync(kFull, any)) break;
-                    uint32_t v[kUnroll];
+                for (int u = 0; u < kUnroll; ++u) has[u] = valid[u] && deg[u] > 0;
+                group_member<L>(a.store.edges, off, deg, target, has, a.sorted_lists != 0, found);
+                if (h == 0) {
+                    unsigned long long d = 0;
 #pragma unroll
                     for (int u = 0; u < kUnroll; ++u)
-                        v[u] = (active[u] && k + gl < deg[u]) ? __ldg(a.store.edges + off[u] + k + gl)
-                                                              : 0;
-#pragma unroll
-                    for (int u = 0; u < kUnroll; ++u) {
-                        const bool hit = active[u] && k + gl < deg[u] && v[u] == target[u];
-                        const unsigned m = (__ballot_sync(kFull, hit) >> gbase) & 0xFFu;
-                        if (active[u]) {
-                            if (m) {
-                                found[u] = true;
-                                active[u] = false;
-                            } else if (k + kGroup >= deg[u]) {
-                                active[u] = false;
-                            }
+                        if (valid[u]) {
+                            s_cnt[row[u]] = found[u] ? 1u : 0u;
+                            d += deg[u];
                         }
-                    }
-                }
-                if (gl == 0) {
-#pragma unroll
-                    for (int u = 0; u < kUnroll; ++u)
-                        if (valid[u]) s_cnt[row[u]] = found[u] ? 1u : 0u;
+                    if (d) atomicAdd(&s_deg, d);
                 }
             }
         }
@@ -374,6 +479,8 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
             s_excl = lookback(a.status, a.ctl, tile, total, epoch);
             atomicAdd(&a.ctl->sum_deg, (unsigned long long)(OP == kOpK2U ? total : s_deg));
         }
+        mbar_wait(&s_bar, phase, &a.ctl->err);   // the tile's rows are in shared memory
+        phase ^= 1;
         __syncthreads();
         const uint64_t excl = s_excl;
         if (tile == ntiles - 1 && threadIdx.x == 0) *a.out_rows = excl + total;
@@ -427,12 +534,12 @@ __global__ void __launch_bounds__(kStepThreads) step_kernel(const StepArgs a, in
 __global__ void list_kernel(const ListArgs a) {
     __shared__ uint64_t s_ptr;
     if (threadIdx.x < 32) {
-        uint64_t bstart[kUnroll] = {a.seg.bucket_start, 0, 0, 0};
-        uint64_t nbk[kUnroll] = {a.seg.num_buckets, 0, 0, 0};
         uint64_t key[kUnroll] = {a.key, 0, 0, 0};
-        bool valid[kUnroll] = {threadIdx.x < kGroup, false, false, false};
+        bool pending[kUnroll] = {threadIdx.x < 8 && a.seg.num_buckets != 0 && a.key != 0, false, false,
+                                 false};
+        uint64_t bucket[kUnroll] = {pending[0] ? bucket_of(a.key, a.seg) : 0, 0, 0, 0};
         uint64_t ptr[kUnroll];
-        group_probe(a.store, bstart, nbk, key, valid, ptr, &a.ctl->err);
+        group_probe<8>(a.store, key, bucket, pending, ptr, &a.ctl->err);
         if (threadIdx.x == 0) s_ptr = ptr[0];
     }
     __syncthreads();
@@ -463,6 +570,54 @@ __global__ void list_kernel(const ListArgs a) {
         a.out[i] = __ldg(srcp + i);
 }
 
+// Checks that every key's list is strictly ascending (the loader's sort + dedup), which lets
+// the filters binary-search long lists.
+__global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const uint32_t* edges,
+                                    uint64_t n_edges, unsigned* unsorted) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_slots;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if ((i & (kAssoc - 1)) == kAssoc - 1) continue;   // chain link
+        const Slot s = slots[i];
+        if (s.key == 0) continue;
+        const uint64_t off = ptr_off(s.ptr), sz = ptr_size(s.ptr);
+        if (off + sz > n_edges) {
+            atomicOr(unsorted, 2u);
+            continue;
+        }
+        for (uint64_t k = 1; k < sz; ++k)
+            if (edges[off + k - 1] >= edges[off + k]) {
+                atomicOr(unsorted, 1u);
+                break;
+            }
+    }
+}
+
+template <int OP>
+cudaError_t launch_op(const StepArgs& a, int grid, int lanes, size_t smem, int chunk, cudaStream_t s) {
+    switch (lanes) {
+    case 2: step_kernel<OP, 2><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
+    case 4: step_kernel<OP, 4><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
+    case 8: step_kernel<OP, 8><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <int OP, int L>
+cudaError_t set_attr(int bytes) {
+    return cudaFuncSetAttribute(step_kernel<OP, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+template <int OP>
+int occupancy(int lanes, size_t smem) {
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (lanes == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<OP, 2>, kStepThreads, smem);
+    if (lanes == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<OP, 4>, kStepThreads, smem);
+    if (lanes == 8) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<OP, 8>, kStepThreads, smem);
+    return (e == cudaSuccess && nb > 0) ? nb : 1;
+}
+
 }  // namespace
 
 size_t step_smem_bytes(int cols, int op, int* out_chunk_rows) {
@@ -487,44 +642,45 @@ cudaError_t step_kernel_attrs(int max_cols) {
         size_t b = step_smem_bytes(max_cols, op, nullptr);
         if (b > mx) mx = b;
     }
+    const int bytes = (int)mx;
     cudaError_t e;
-    e = cudaFuncSetAttribute(step_kernel<kOpK2U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(step_kernel<kOpK2K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(step_kernel<kOpK2C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mx);
+#define WK_ATTR(OPV, LV) \
+    if ((e = set_attr<OPV, LV>(bytes)) != cudaSuccess) return e;
+    WK_ATTR(kOpK2U, 2) WK_ATTR(kOpK2U, 4) WK_ATTR(kOpK2U, 8)
+    WK_ATTR(kOpK2K, 2) WK_ATTR(kOpK2K, 4) WK_ATTR(kOpK2K, 8)
+    WK_ATTR(kOpK2C, 2) WK_ATTR(kOpK2C, 4) WK_ATTR(kOpK2C, 8)
+#undef WK_ATTR
+    return cudaSuccess;
 }
 
-int step_blocks_per_sm(int cols, int op) {
+int step_blocks_per_sm(int cols, int op, int lanes) {
     size_t smem = step_smem_bytes(cols, op, nullptr);
-    int nb = 0;
-    cudaError_t e;
-    if (op == kOpK2U)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<kOpK2U>, kStepThreads, smem);
-    else if (op == kOpK2K)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<kOpK2K>, kStepThreads, smem);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, step_kernel<kOpK2C>, kStepThreads, smem);
-    if (e != cudaSuccess || nb < 1) nb = 1;
-    return nb;
+    if (op == kOpK2U) return occupancy<kOpK2U>(lanes, smem);
+    if (op == kOpK2K) return occupancy<kOpK2K>(lanes, smem);
+    return occupancy<kOpK2C>(lanes, smem);
 }
 
 cudaError_t launch_step(const StepArgs& a, int grid, cudaStream_t s) {
     int chunk = 0;
     size_t smem = step_smem_bytes(a.cols, a.op, &chunk);
     if (grid < 1) grid = 1;
+    const int lanes = a.lanes ? a.lanes : 2;
     switch (a.op) {
-    case kOpK2U: step_kernel<kOpK2U><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
-    case kOpK2K: step_kernel<kOpK2K><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
-    case kOpK2C: step_kernel<kOpK2C><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
+    case kOpK2U: return launch_op<kOpK2U>(a, grid, lanes, smem, chunk, s);
+    case kOpK2K: return launch_op<kOpK2K>(a, grid, lanes, smem, chunk, s);
+    case kOpK2C: return launch_op<kOpK2C>(a, grid, lanes, smem, chunk, s);
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s) {
     if (grid < 1) grid = 1;
     list_kernel<<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s) {
+    sorted_check_kernel<<<1024, 256, 0, s>>>(st.slots, st.n_buckets * kAssoc, st.edges, st.n_edges, d_flag);
     return cudaGetLastError();
 }
 

@@ -59,6 +59,8 @@ struct StepArgs {
     uint32_t pid;
     int32_t dir;
     int32_t type_index;      // K2U with pid == TYPE_ID and dir == IN: key = [0|cur|IN]
+    int32_t sorted_lists;    // every list ascending + unique (checked at upload)
+    int32_t lanes;           // lanes per probe group: 2, 4 or 8 (slots read per request)
 };
 
 struct ListArgs {
@@ -76,10 +78,11 @@ struct ListArgs {
 constexpr int kStepThreads = 256;
 constexpr int kTileRows = 512;
 size_t step_smem_bytes(int cols, int op, int* out_chunk_rows);
-int step_blocks_per_sm(int cols, int op);
+int step_blocks_per_sm(int cols, int op, int lanes);
 
 cudaError_t launch_step(const StepArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);
 cudaError_t step_kernel_attrs(int max_cols);
 
 }  // namespace wk
