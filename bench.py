@@ -1,18 +1,21 @@
 """Benchmark of the B200 triple-pattern exploration step.
 
-Workload: the seeded LUBM-shaped synthetic graph (1,000 organisations by default) resident in
-HBM, and the heavy queries of the heavy-query configuration: (a) a 3-pattern star from the
-PersonA type index, (b) the memberOf / subOrgOf / degreeFrom triangle from the memberOf
-predicate index.  One step = both heavy queries, each from its index start to its final table.
+Graph: the seeded LUBM-shaped synthetic graph (default 1,000 organisations) resident in HBM.
 
-  value   heavy queries/s, device-resident: CUDA-graph replays timed with CUDA events on the
-          library's stream, L2 flushed between steps (outside the timed brackets)
-  e2e     the same through wk_query_execute_host: plan in, final table copied to pinned host
-          memory every step, timed on the host clock
-  plain   the one-launch-per-pattern path with a host sync per step (reference-shaped)
-
-`--impl reference` times the CPU restatement of the reference engine (oracle/) on the host
-cores with the reference's own intra-query split (mt_factor = cores) on the same config.
+Headline (`value`): light-query QPS of the batched path.  One step = one batch of 16,384 light
+queries (2-6 patterns from uniformly random constants of randomly drawn start classes),
+all executed to their final tables by the per-level persistent launches replayed from a CUDA
+graph; timed with CUDA events on the library's stream, L2 flushed between steps outside the
+timed brackets.  Every query of a batch completes when the batch does, so the batch time is
+each query's device latency; p50/p99 are over the timed batches.
+`e2e`: the same batch through wk_batch_execute from the host: plans in, every query's final
+table copied to pinned host memory, host clock.
+`plain_path`: one launch per pattern per query with a host sync per step (the reference's
+shape) on a sample of the same queries.
+`heavy`: the heavy-query configuration's two queries (PersonA star, memberOf / subOrgOf /
+degreeFrom triangle), device-resident graph replays.
+`--impl reference` times the CPU restatement of the reference engine (oracle/) on all host
+cores on the same light batch (one query per thread, as the CPU engines run light queries).
 """
 import argparse
 import json
@@ -28,6 +31,8 @@ sys.path.insert(0, os.path.join(ROOT, "wukong-cube_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 import numpy as np  # noqa: E402
+
+METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU path"
 
 
 def peaks():
@@ -52,10 +57,11 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            time.sleep(0.3)
         except OSError:
             self.proc = None
         return self
@@ -66,6 +72,7 @@ class Clocks:
 
     def __exit__(self, *a):
         if self.proc:
+            time.sleep(0.1)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -73,29 +80,25 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        good = [r for r in self.rows if len(r) >= 9]
+        if not good:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [num(r[1]) for r in good if num(r[1]) is not None]
+        mx = [num(r[2]) for r in good if num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in good:
             for i, n in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower().startswith("active"):
+                if r[5 + i].lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.rows)}
-
-
-def step_bytes(s):
-    """Algorithmic bytes of one step (4-byte ids, 16-byte slots)."""
-    k, R, C, Rp, D = s["kind"], s["rows_in"], s["cols_in"], s["rows_out"], s["sum_deg"]
-    if k in ("index_to_unknown", "const_to_unknown"):
-        return 16 + Rp * 4 + Rp * 4
-    if k == "known_to_unknown":
-        return R * C * 4 + R * 16 + D * 4 + Rp * (C + 1) * 4
-    return R * C * 4 + R * 16 + D * 4 + Rp * C * 4
+                "samples": len(good)}
 
 
 def build_graph(orgs, seed):
@@ -105,8 +108,17 @@ def build_graph(orgs, seed):
     t1 = time.time()
     g = wk.GStore(tr)
     t2 = time.time()
-    return tr, v, g, {"triples": int(tr.shape[0]), "gen_s": round(t1 - t0, 2),
-                      "build_s": round(t2 - t1, 2), **g.info()}
+    inst = {t: g.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+    return tr, v, g, inst, {"triples": int(tr.shape[0]), "gen_s": round(t1 - t0, 2),
+                            "build_s": round(t2 - t1, 2), **g.info()}
+
+
+def config(args, ginfo):
+    return {"workload": "batches of %d light queries (2-6 patterns from random constants) on the "
+                        "seeded LUBM-shaped graph of %d organisations; heavy star + triangle "
+                        "alongside" % (args.light, args.orgs),
+            "orgs": args.orgs, "seed": args.seed, "light_queries_per_step": args.light,
+            "graph": ginfo, "l2": "flushed between timed steps (256 MiB write)"}
 
 
 def run_reference(args, world, rank):
@@ -115,45 +127,49 @@ def run_reference(args, world, rank):
         return
     import oracle
     import workloads
-    import wukong_b200 as wk
     cores = os.cpu_count() or 1
-    tr, v, g, ginfo = build_graph(args.orgs, args.seed)
-    del g
+    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
     o = oracle.OracleStore(tr)
-    qs = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+    qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
+    flat = [q.flat() for q in qs]
+    nv = [q.nvars for q in qs]
     for _ in range(args.warmup):
-        for q in qs:
-            o.run(q.flat(), q.nvars, mt_factor=cores)
+        o.run_many(flat, nv, cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        for q in qs:
-            st, tab, _ = o.run(q.flat(), q.nvars, mt_factor=cores)
-            assert st == 0
+        _, st = o.run_many(flat, nv, cores)
         times.append(time.perf_counter() - t0)
-    ms = 1000 * sum(times) / len(times)
-    value = 2 * args.steps / sum(times)
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": config(args, ginfo),
-            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "port",
-                             "sample": "%d steps x (heavy star + heavy triangle), mt_factor=%d" %
-                                       (args.steps, cores)},
-            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+        assert (st == 0).all()
+    value = len(qs) * args.steps / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "light queries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": config(args, ginfo),
+            "cpu_baseline": {"value": value, "unit": "light queries/s", "cores": cores, "kind": "port",
+                             "sample": "%d steps x %d light queries, one query per thread" %
+                                       (args.steps, len(qs))},
+            "e2e": {"value": value, "unit": "light queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU path"
-
-
-def config(args, ginfo):
-    return {"workload": "heavy queries (star from PersonA type index + memberOf/subOrgOf/"
-                        "degreeFrom triangle from predicate index) on the seeded LUBM-shaped "
-                        "graph, %d organisations" % args.orgs,
-            "orgs": args.orgs, "seed": args.seed, "graph": ginfo,
-            "l2": "flushed between timed steps (256 MiB write)"}
+def timed(stream, flush, steps, fn):
+    """Per-step device ms with CUDA events on `stream`; L2 flushed outside the brackets."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize()
+    for i in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[i][0].record(stream)
+        fn()
+        with torch.cuda.stream(stream):
+            ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev]
 
 
 def run_ours(args, world, rank, local_rank):
@@ -164,48 +180,35 @@ def run_ours(args, world, rank, local_rank):
     import wukong_b200 as wk
 
     torch.cuda.set_device(local_rank)
-    tr, v, g, ginfo = build_graph(args.orgs, args.seed)
+    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
     ctx = wk.Context(local_rank)
     ctx.upload_gstore(g)
     ginfo["device_store_bytes"] = ctx.store_bytes()
-    qs = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
     stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+    cores = os.cpu_count() or 1
+    o = oracle.OracleStore(tr) if rank == 0 else None
 
-    # correctness gate on the bench config: each heavy query vs the oracle
-    rows = []
-    o = oracle.OracleStore(tr) if rank == 0 and not args.no_check else None
-    for q in qs:
-        got, _ = ctx.execute(q, wk.MODE_GRAPH)
-        rows.append(int(got.shape[0]))
-        if o is not None:
-            st, want, _ = o.run(q.flat(), q.nvars, mt_factor=os.cpu_count() or 1)
-            assert st == 0 and np.array_equal(oracle.sorted_rows(got), oracle.sorted_rows(want)), \
-                "GPU result differs from the oracle"
-
-    def one_step():
-        for q in qs:
-            ctx.enqueue(q, wk.MODE_GRAPH)
-
+    # ---- light batch: correctness gate, then timing
+    qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1 + rank)
+    res = ctx.batch(qs)
+    light_rows = np.array([r[0].shape[0] if r[0] is not None else 0 for r in res], np.int64)
+    if o is not None and not args.no_check:
+        orows, ost = o.run_many([q.flat() for q in qs], [q.nvars for q in qs], cores)
+        assert (ost == 0).all() and np.array_equal(orows.astype(np.int64), light_rows), \
+            "light batch row counts differ from the oracle"
+        for i in range(0, len(qs), max(1, len(qs) // 256)):
+            st, want, _ = o.run(qs[i].flat(), qs[i].nvars)
+            assert np.array_equal(oracle.sorted_rows(res[i][0]), oracle.sorted_rows(want)), i
+    ctx.batch_device(qs)   # capture for replay
     for _ in range(args.warmup):
-        one_step()
+        ctx.batch_replay()
     ctx.check()
     if world > 1:
         torch.distributed.barrier()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    torch.cuda.synchronize()
     with Clocks(local_rank) as clk:
-        for i in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                ev[i][0].record(stream)
-            one_step()
-            with torch.cuda.stream(stream):
-                ev[i][1].record(stream)
-        torch.cuda.synchronize()
+        step_ms = timed(stream, flush, args.steps, ctx.batch_replay)
     ctx.check()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
     tot_ms = sum(step_ms)
     if world > 1:
         t = torch.tensor([tot_ms], device="cuda")
@@ -213,66 +216,103 @@ def run_ours(args, world, rank, local_rank):
         tot_ms = float(t.item())
     value = len(qs) * args.steps * world / (tot_ms / 1000.0)
 
-    # e2e through the C ABI with pinned host buffers (result table copied to the host)
-    host = [torch.empty(max(r * 3 + 64, 64), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-            for r in rows]
-    for q, h in zip(qs, host):
-        ctx.execute_host(q, h, wk.MODE_GRAPH)
-    t0 = time.perf_counter()
-    d2h = 0
+    # ---- e2e through the C ABI from the host (plans in, tables out to pinned memory)
+    qs_c, keep = wk.queries_as_c(qs)
+    total_elems = int(sum((r[0].size if r[0] is not None else 0) for r in res))
+    host = torch.empty(total_elems + 1024, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    qres = (wk.QResult * len(qs))()
+    import ctypes as C
+    L = wk.lib()
+    rc = L.wk_batch_execute(ctx.h, qs_c, len(qs), C.c_void_p(host.ctypes.data), host.size, qres)
+    assert rc == 0
+    e2e_t = []
     for _ in range(args.steps):
-        for q, h in zip(qs, host):
-            r, c = ctx.execute_host(q, h, wk.MODE_GRAPH)
-            d2h += r * c * 4
-    e2e_s = time.perf_counter() - t0
-    e2e = len(qs) * args.steps / e2e_s
-    h2d = sum(len(q.patterns) * 20 for q in qs)
+        t0 = time.perf_counter()
+        rc = L.wk_batch_execute(ctx.h, qs_c, len(qs), C.c_void_p(host.ctypes.data), host.size, qres)
+        e2e_t.append(time.perf_counter() - t0)
+        assert rc == 0
+    e2e = len(qs) * args.steps / sum(e2e_t)
+    h2d = sum(len(q.patterns) * 64 for q in qs)
+    d2h = total_elems * 4 + len(qs) * 16
 
-    # plain path: one launch per pattern, host sync per step
-    for q in qs:
-        ctx.execute(q, wk.MODE_PLAIN)
+    # ---- plain path (one launch per pattern, host sync per step) and the single-query
+    # resident path on a sample of the same queries
+    sample = qs[:args.plain_sample]
+    buf = np.zeros(max(int(light_rows.max()) * 8, 64), np.uint32)
+    for q in sample[:8]:
+        ctx.execute_host(q, buf, wk.MODE_PLAIN)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for q, h in zip(qs, host):
-            ctx.execute_host(q, h, wk.MODE_PLAIN)
-    plain = len(qs) * args.steps / (time.perf_counter() - t0)
+    for q in sample:
+        ctx.execute_host(q, buf, wk.MODE_PLAIN)
+    plain = len(sample) / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for q in sample:
+        ctx.execute_host(q, buf, wk.MODE_RESIDENT)
+    single_resident = len(sample) / (time.perf_counter() - t0)
 
-    # roofline of the dominant kernel: per-step kernel times on the library stream
-    prof = [ctx.profile(q, iters=max(3, args.steps)) for q in qs]
-    steps = [s for p in prof for s in p]
-    dom = max(steps, key=lambda s: s["ms"])
+    # ---- heavy queries (device-resident graph replays)
+    hq = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+    heavy_rows = []
+    for q in hq:
+        got, _ = ctx.execute(q, wk.MODE_GRAPH)
+        heavy_rows.append(int(got.shape[0]))
+        if o is not None and not args.no_check:
+            st, want, _ = o.run(q.flat(), q.nvars, mt_factor=cores)
+            assert st == 0 and np.array_equal(oracle.sorted_rows(got), oracle.sorted_rows(want))
+    heavy = {}
+    for name, q in zip(("star", "triangle"), hq):
+        ms = timed(stream, flush, args.steps, lambda q=q: ctx.enqueue(q, wk.MODE_GRAPH))
+        ctx.check()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            ctx.execute(q, wk.MODE_PLAIN)
+        plain_ms = (time.perf_counter() - t0) / 3 * 1000
+        heavy[name] = {"ms": statistics.median(ms), "rows": heavy_rows[len(heavy)],
+                       "plain_ms": plain_ms, "profile": ctx.profile(q, iters=3)}
+
+    # ---- roofline: dominant kernel of the light batch (one level launch), CUDA events on the
+    # library stream; and of the heavy queries
     peak, src = peaks()
-    algo = step_bytes(dom)
-    achieved = algo / (dom["ms"] / 1000.0) / 1e9
-    line = {"metric": METRIC, "value": value, "unit": "heavy queries/s", "n_gpus": world,
+    levels = ctx.batch_profile(qs, iters=3)
+    dom = max(levels, key=lambda s: s["ms"])
+    achieved = dom["alg_bytes"] / (dom["ms"] / 1000.0) / 1e9
+    hsteps = [s for h in heavy.values() for s in h["profile"]]
+    hdom = max(hsteps, key=lambda s: s["ms"])
+    hach = hdom["alg_bytes"] / (hdom["ms"] / 1000.0) / 1e9
+
+    lat = sorted(step_ms)
+    line = {"metric": METRIC, "value": value, "unit": "light queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": config(args, ginfo),
-            "heavy_ms": {"star": None, "triangle": None},
-            "e2e": {"value": e2e, "unit": "heavy queries/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h // max(args.steps, 1)},
-            "plain_path": {"value": plain, "unit": "heavy queries/s"},
-            "rows": rows,
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                           "max": lat[-1], "note": "every query of a batch completes with the batch"},
+            "e2e": {"value": e2e, "unit": "light queries/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "plain_path": {"value": plain, "unit": "light queries/s", "sample": len(sample)},
+            "single_query_resident": {"value": single_resident, "unit": "light queries/s"},
+            "speedup_vs_plain": value / plain,
+            "light_rows": {"p50": int(np.percentile(light_rows, 50)),
+                           "p99": int(np.percentile(light_rows, 99)), "max": int(light_rows.max())},
+            "heavy": heavy,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": src,
-                         "kernel": dom["kind"], "algorithmic_bytes": algo, "kernel_ms": dom["ms"]},
-            "profile": prof,
-            "gpu_launches": sum(len(q.patterns) for q in qs) * args.steps,
+                         "kernel": "level_kernel (batch level %d)" % levels.index(dom),
+                         "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"]},
+            "roofline_heavy": {"bound": "hbm", "achieved": hach, "peak": peak, "unit": "GB/s",
+                               "frac": hach / peak, "kernel": "step_kernel " + hdom["kind"],
+                               "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"]},
+            "batch_levels": levels,
+            "gpu_launches": args.steps * (2 * len(levels) + 2),
             "clocks": clk.summary()}
-    for name, p in zip(("star", "triangle"), prof):
-        line["heavy_ms"][name] = sum(s["ms"] for s in p)
     if rank == 0:
         if not args.no_cpu:
-            import oracle as orc
-            cores = os.cpu_count() or 1
-            if o is None:
-                o = orc.OracleStore(tr)
             t0 = time.perf_counter()
-            for q in qs:
-                o.run(q.flat(), q.nvars, mt_factor=cores)
+            _, st = o.run_many([q.flat() for q in qs], [q.nvars for q in qs], cores)
             dt = time.perf_counter() - t0
-            line["cpu_baseline"] = {"value": len(qs) / dt, "unit": "heavy queries/s", "cores": cores,
-                                    "kind": "port", "sample": "one run of each heavy query, mt_factor=%d" % cores}
+            line["cpu_baseline"] = {"value": len(qs) / dt, "unit": "light queries/s", "cores": cores,
+                                    "kind": "port",
+                                    "sample": "one batch of %d light queries, one query per thread" % len(qs)}
         print(json.dumps(line))
     ctx.close()
 
@@ -284,6 +324,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--orgs", type=int, default=1000)
+    ap.add_argument("--light", type=int, default=16384)
+    ap.add_argument("--plain-sample", type=int, default=512)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

@@ -258,13 +258,15 @@ int wk_query_enqueue(wk_ctx* ctx, const wk_query* q, int32_t mode);
  * 3 known_to_known, 4 known_to_const.  sum_deg = total neighbour-list length the step's
  * probes found (the edges an exhaustive list scan reads). */
 typedef struct wk_step_prof {
-    int32_t kind;
+    int32_t kind;            /* 0..4 as above; 5 = one level of a batch */
     int32_t cols_in;
     int32_t cols_out;
     int32_t reserved;
     uint64_t rows_in;
     uint64_t rows_out;
     uint64_t sum_deg;
+    uint64_t alg_bytes;      /* rows in * cols * 4 + 16 per probe + 4 per list entry read
+                                + rows out * cols * 4 */
     double ms;               /* mean kernel time of the step */
 } wk_step_prof;
 int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof* out,
@@ -280,6 +282,13 @@ int wk_batch_execute(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t*
  * receives the sum of final rows. */
 int wk_batch_execute_device(wk_ctx* ctx, const wk_query* queries, uint32_t n,
                             uint64_t* total_rows);
+/* Replay the last batch of this context on its stream and return without waiting (for
+ * device-side timing of an identical batch; errors surface through wk_ctx_check). */
+int wk_batch_replay(wk_ctx* ctx);
+/* Per-level profile of a batch: each level launch between CUDA events on the context stream,
+ * averaged over `iters` runs after one warm-up; out[k].kind = 5. */
+int wk_batch_profile(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters,
+                     wk_step_prof* out, int32_t max_levels, int32_t* n_levels);
 
 /* ---------------------------------------------------------------- serving
  * Continuous batching over an open-loop arrival schedule (no reference counterpart; shaped

@@ -9,6 +9,7 @@
 #include <new>
 #include <string>
 
+#include "wk_batch.h"
 #include "wk_ctx.h"
 
 #define WK_CUDA(ctx, call)                                   \
@@ -297,6 +298,8 @@ extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     if (e != cudaSuccess) return bail(e, "stream");
     e = wk::step_kernel_attrs(ctx->cfg.max_cols);
     if (e != cudaSuccess) return bail(e, "kernel attributes");
+    e = wk::level_kernel_attrs();
+    if (e != cudaSuccess) return bail(e, "batch kernel attributes");
     e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
     e = cudaMallocHost(&ctx->h_ctl, sizeof(wk::StepCtl));
@@ -821,7 +824,7 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
         for (size_t i = 0; i < steps.size(); ++i) {
             const wk_table* in = i ? &ctx->rbuf[(i - 1) & 1] : nullptr;
             wk_table* o = &ctx->rbuf[i & 1];
-            WK_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 8, ctx->stream));
+            WK_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 16, ctx->stream));
             WK_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
             rc = wk::enqueue_step(ctx, steps[i], in, o, q->mt_tid, q->mt_factor, ctx->stream, 0);
             if (rc) return rc;
@@ -845,7 +848,7 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
                 rc = table_rows(ctx, o, &r);
                 if (rc) return rc;
                 p.rows_out = r;
-                WK_CUDA(ctx, cudaMemcpy(&p.sum_deg, &ctx->d_ctl->sum_deg, 8, cudaMemcpyDeviceToHost));
+                WK_CUDA(ctx, cudaMemcpy(&p.sum_deg, &ctx->d_ctl->sum_deg, 16, cudaMemcpyDeviceToHost));
             }
         }
     }

@@ -71,6 +71,7 @@ struct wk_ctx {
     bool has_store = false;
     int sorted_lists = 0;
     int default_lanes = 2;
+    int batch_lanes = 4;
     std::map<int, int> tuned_lanes;
 
     // scan control of the context stream

@@ -1,0 +1,351 @@
+// Device-side building blocks shared by the single-query and the batched step kernels:
+// bounded mbarrier waits and TMA bulk copies, the sector-granular group probe of the key table,
+// the block scan, the warp-parallel decoupled look-back, 16-byte stores from shared memory,
+// list membership and the self-resetting exit protocol of a launch.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "wk_kernels.h"
+
+namespace wk {
+namespace dev {
+namespace {   // internal linkage: every .cu that includes this gets its own copy
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kUnroll = 4;                                // rows per lane group in flight
+constexpr int kMaxProbeIters = 1 << 14;                   // chain walk limit
+constexpr unsigned long long kFlagAgg = 1, kFlagPrefix = 2;
+constexpr unsigned long long kValMask = (1ull << 46) - 1;
+constexpr unsigned long long kSpinLimit = 1ull << 24;     // look-back polls before giving up
+constexpr unsigned kTmaWaitLimit = 1u << 24;              // mbarrier polls before giving up
+constexpr int kChunkBytes = 32 * 1024;                    // staging of one output chunk
+constexpr int kLinear = 8;                                // list entries checked by ballot
+
+static_assert(kTileRows % kStepThreads == 0, "rows per thread");
+
+__device__ __forceinline__ unsigned long long pack_status(unsigned epoch, unsigned long long flag,
+                                                          unsigned long long v) {
+    return ((unsigned long long)epoch << 48) | (flag << 46) | (v & kValMask);
+}
+
+__device__ __forceinline__ ulonglong2 load_slot(const Slot* p) {
+    return __ldg(reinterpret_cast<const ulonglong2*>(p));
+}
+
+// ---------------------------------------------------------------- mbarrier + TMA bulk copy
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Global -> shared bulk copy; both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, unsigned bytes,
+                                            uint64_t* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Bounded wait for the current phase; a timeout sets kErrTimeout and waits once more (bounded)
+// so no copy is left in flight when the CTA moves on.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err) {
+    unsigned n = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++n > kTmaWaitLimit) {
+            if (threadIdx.x == 0) atomicOr(err, kErrTimeout);
+            for (unsigned m = 0; m < kTmaWaitLimit && !mbar_try_wait(bar, parity); ++m) __nanosleep(256);
+            return;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- probe
+__device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
+    return s.bucket_start + mod_barrett(hash_u64(key), s.num_buckets, s.magic);
+}
+
+// Probe kUnroll keys per group of L lanes.  Every lane of the warp must call this (ballots and
+// shuffles are warp-wide).  On entry bucket[u] is the key's home bucket and pending[u] says
+// whether to look; on return ptr[u] is the slot's pointer word in every lane of the group, or 0
+// when the key is absent.
+template <int L>
+__device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&key)[kUnroll],
+                                            uint64_t (&bucket)[kUnroll], bool (&pending)[kUnroll],
+                                            uint64_t (&ptr)[kUnroll], unsigned* err) {
+    const int lane = threadIdx.x & 31;
+    const int h = lane & (L - 1);
+    const int gbase = lane & ~(L - 1);
+    const unsigned gmask = (1u << L) - 1;
+    int round[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        ptr[u] = 0;
+        round[u] = 0;
+    }
+    for (int it = 0;; ++it) {
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) any |= pending[u];
+        if (!__any_sync(kFull, any)) break;
+        if (it >= kMaxProbeIters) {
+            if (any && h == 0) atomicOr(err, kErrCorrupt);
+            break;
+        }
+        ulonglong2 s[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            s[u] = make_ulonglong2(~0ull, 0);
+            if (pending[u]) {
+                if (bucket[u] >= st.n_buckets) {
+                    pending[u] = false;
+                    if (h == 0) atomicOr(err, kErrCorrupt);
+                } else {
+                    s[u] = load_slot(st.slots + bucket[u] * kAssoc + round[u] * L + h);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const bool data = round[u] * L + h < kAssoc - 1;
+            const bool hit = pending[u] && data && s[u].x == key[u];
+            const bool emp = pending[u] && data && s[u].x == 0;
+            const unsigned hm = (__ballot_sync(kFull, hit) >> gbase) & gmask;
+            const unsigned em = (__ballot_sync(kFull, emp) >> gbase) & gmask;
+            const int src = hm ? gbase + __ffs(hm) - 1 : gbase + L - 1;
+            const uint64_t kx = __shfl_sync(kFull, s[u].x, src);
+            const uint64_t py = __shfl_sync(kFull, s[u].y, src);
+            if (pending[u]) {
+                if (hm) {
+                    ptr[u] = py;
+                    pending[u] = false;
+                } else if (em) {
+                    pending[u] = false;           // first empty slot: the key is absent
+                } else if ((round[u] + 1) * L >= kAssoc) {
+                    if (kx == 0) {
+                        pending[u] = false;       // no extension bucket
+                    } else {
+                        bucket[u] = key_vid(kx);  // follow slot 7 (kvstore.hpp:303-310)
+                        round[u] = 0;
+                    }
+                } else {
+                    round[u]++;
+                }
+            }
+        }
+    }
+}
+
+// Exclusive block scan of s_cnt[0..n) into s_pre[0..n]; returns the tile total.
+__device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* s_pre, int n,
+                                               uint64_t* s_warp) {
+    constexpr int per = kTileRows / kStepThreads;
+    constexpr int nwarps = kStepThreads / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = threadIdx.x * per;
+    uint64_t v[per];
+    uint64_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < per; ++i) {
+        v[i] = (base + i < n) ? s_cnt[base + i] : 0;
+        sum += v[i];
+    }
+    uint64_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t w = lane < nwarps ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < nwarps; o <<= 1) {
+            uint64_t y = __shfl_up_sync(kFull, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nwarps) s_warp[lane] = w;
+    }
+    __syncthreads();
+    uint64_t run = (warp ? s_warp[warp - 1] : 0) + x - sum;
+#pragma unroll
+    for (int i = 0; i < per; ++i) {
+        if (base + i < n) s_pre[base + i] = run;
+        run += v[i];
+    }
+    const uint64_t total = s_warp[nwarps - 1];
+    if (threadIdx.x == 0) s_pre[n] = total;
+    __syncthreads();
+    return total;
+}
+
+// Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
+// Look-back", 2016) by one warp: each round reads the 32 nearest unvisited predecessors at once,
+// waits until all of them have published at least their aggregate, adds the aggregates up to
+// the nearest inclusive prefix and stops there.  Tiles are claimed in order from the tile
+// counter, so every predecessor is held by a running CTA and the wait ends; it is still bounded.
+// Called by all 32 lanes of one warp; returns the exclusive prefix in every lane.
+__device__ uint64_t lookback_warp(unsigned long long* status, StepCtl* ctl, uint64_t tile,
+                                  uint64_t agg, unsigned epoch) {
+    volatile unsigned long long* st = status;
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) st[0] = pack_status(epoch, kFlagPrefix, agg);
+        return 0;
+    }
+    if (lane == 0) st[tile] = pack_status(epoch, kFlagAgg, agg);
+    uint64_t excl = 0;
+    int64_t base = (int64_t)tile - 1;
+    unsigned long long spins = 0;
+    for (;;) {
+        const int64_t p = base - lane;
+        const unsigned long long s = p >= 0 ? st[p] : pack_status(epoch, kFlagPrefix, 0);
+        const unsigned long long flag = (s >> 46) & 3ull;
+        const bool ready = (unsigned)(s >> 48) == epoch && flag != 0;
+        if (!__all_sync(kFull, ready)) {
+            if (++spins > kSpinLimit) {
+                if (lane == 0) atomicOr(&ctl->err, kErrTimeout);
+                break;
+            }
+            if (spins > 32) __nanosleep(32);
+            continue;
+        }
+        const unsigned pm = __ballot_sync(kFull, flag == kFlagPrefix);
+        const int first = pm ? __ffs(pm) - 1 : 32;   // nearest predecessor holding a prefix
+        uint64_t v = lane <= first ? (s & kValMask) : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        excl += v;
+        if (pm) break;
+        base -= 32;
+    }
+    if (lane == 0) st[tile] = pack_status(epoch, kFlagPrefix, excl + agg);
+    return excl;
+}
+
+// Copy `count` words from shared memory to global memory with 16-byte stores where aligned.
+__device__ __forceinline__ void store_words(uint32_t* dst, const uint32_t* src, uint64_t count) {
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(dst);
+    uint64_t head = ((16 - (addr & 15)) & 15) >> 2;
+    if (head > count) head = count;
+    if (threadIdx.x < head) dst[threadIdx.x] = src[threadIdx.x];
+    const uint64_t nvec = (count - head) >> 2;
+    uint4* dv = reinterpret_cast<uint4*>(dst + head);
+    const uint32_t* sv = src + head;
+    for (uint64_t v = threadIdx.x; v < nvec; v += blockDim.x) {
+        uint4 x;
+        x.x = sv[4 * v];
+        x.y = sv[4 * v + 1];
+        x.z = sv[4 * v + 2];
+        x.w = sv[4 * v + 3];
+        dv[v] = x;
+    }
+    const uint64_t done = head + (nvec << 2);
+    if (threadIdx.x < count - done) dst[done + threadIdx.x] = src[done + threadIdx.x];
+}
+
+// The last CTA to leave resets the tile/exit counters and advances the epoch; when the 16-bit
+// epoch wraps it clears the status array first so no stale word can match the next epoch.
+__device__ void exit_protocol(StepCtl* ctl, unsigned long long* status, unsigned epoch) {
+    __shared__ int s_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->exit_counter, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    unsigned next = epoch + 1;
+    if (next > 0xFFFFu) {
+        for (unsigned long long i = threadIdx.x; i < ctl->status_cap; i += blockDim.x) status[i] = 0;
+        next = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->tile_counter = 0;
+        ctl->exit_counter = 0;
+        __threadfence();
+        *(volatile unsigned*)&ctl->epoch = next;
+        __threadfence();
+    }
+}
+
+// Membership of target[u] in the (ascending, unique when `sorted`) list edges[off, off+deg):
+// the first kLinear entries by a group ballot, the rest by binary search (sorted) or a scan.
+template <int L>
+__device__ __forceinline__ void group_member(const uint32_t* edges, const uint64_t (&off)[kUnroll],
+                                             const uint64_t (&deg)[kUnroll],
+                                             const uint32_t (&target)[kUnroll],
+                                             const bool (&valid)[kUnroll], bool sorted,
+                                             bool (&found)[kUnroll]) {
+    const int lane = threadIdx.x & 31;
+    const int h = lane & (L - 1);
+    const int gbase = lane & ~(L - 1);
+    const unsigned gmask = (1u << L) - 1;
+    constexpr int per = kLinear / L;
+    uint32_t v[kUnroll][per];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+#pragma unroll
+        for (int j = 0; j < per; ++j) {
+            const uint64_t k = (uint64_t)j * L + h;
+            v[u][j] = (valid[u] && k < deg[u]) ? __ldg(edges + off[u] + k) : ~target[u];
+        }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        bool hit = false;
+#pragma unroll
+        for (int j = 0; j < per; ++j) hit |= (v[u][j] == target[u]);
+        found[u] = ((__ballot_sync(kFull, hit && valid[u]) >> gbase) & gmask) != 0;
+    }
+    // long lists: one lane per group continues
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+        bool more = valid[u] && !found[u] && deg[u] > (uint64_t)kLinear;
+        bool f = false;
+        if (more && h == 0) {
+            const uint32_t* p = edges + off[u];
+            if (sorted) {
+                uint64_t lo = kLinear, hi = deg[u];
+                while (lo < hi) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (__ldg(p + mid) < target[u]) lo = mid + 1; else hi = mid;
+                }
+                f = lo < deg[u] && __ldg(p + lo) == target[u];
+            } else {
+                for (uint64_t k = kLinear; k < deg[u] && !f; ++k) f = __ldg(p + k) == target[u];
+            }
+        }
+        f = __shfl_sync(kFull, f, gbase);
+        found[u] = found[u] || f;
+    }
+}
+
+}  // namespace
+}  // namespace dev
+}  // namespace wk

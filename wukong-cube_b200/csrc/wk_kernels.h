@@ -27,6 +27,8 @@ struct StepCtl {
     unsigned long long need;     // largest output (elements) a launch asked for
     unsigned long long status_cap;   // entries in the status array that follows
     unsigned long long sum_deg;  // neighbour-list lengths the probes found (profiling)
+    unsigned long long alg_bytes;   // algorithmic bytes of the launches: rows in * cols * 4
+                                    // + 16 per probe + 4 per list entry read + rows out * cols * 4
 };
 
 // Where the store lives on the device.

@@ -22,7 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["wk_kernels.cu", "wk_batch.cu"]
 CPP_SOURCES = ["wk_ctx.cpp", "wk_gstore.cpp", "wk_synth.cpp"]
-HEADERS = ["wk_format.h", "wk_internal.h", "wk_kernels.h", "wk_ctx.h", "wk_batch.h"]
+HEADERS = ["wk_format.h", "wk_internal.h", "wk_kernels.h", "wk_ctx.h", "wk_batch.h",
+           "wk_device.cuh"]
 
 
 def _run(cmd):

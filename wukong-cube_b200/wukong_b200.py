@@ -79,11 +79,18 @@ class ServeConfig(C.Structure):
 class StepProf(C.Structure):
     _fields_ = [("kind", C.c_int32), ("cols_in", C.c_int32), ("cols_out", C.c_int32),
                 ("reserved", C.c_int32), ("rows_in", C.c_uint64), ("rows_out", C.c_uint64),
-                ("sum_deg", C.c_uint64), ("ms", C.c_double)]
+                ("sum_deg", C.c_uint64), ("alg_bytes", C.c_uint64), ("ms", C.c_double)]
 
 
 STEP_KINDS = ["index_to_unknown", "const_to_unknown", "known_to_unknown", "known_to_known",
-              "known_to_const"]
+              "known_to_const", "batch_level"]
+
+
+def _prof_list(arr, n):
+    return [{"kind": STEP_KINDS[arr[i].kind], "cols_in": arr[i].cols_in,
+             "cols_out": arr[i].cols_out, "rows_in": arr[i].rows_in, "rows_out": arr[i].rows_out,
+             "sum_deg": arr[i].sum_deg, "alg_bytes": arr[i].alg_bytes, "ms": arr[i].ms}
+            for i in range(n)]
 
 
 class QResult(C.Structure):
@@ -144,6 +151,9 @@ _SIGS = {
                                    C.POINTER(QResult)]),
     "wk_batch_execute_device": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32,
                                           C.POINTER(C.c_uint64)]),
+    "wk_batch_replay": (C.c_int, [_P]),
+    "wk_batch_profile": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32,
+                                   C.POINTER(StepProf), C.c_int32, C.POINTER(C.c_int32)]),
     "wk_serve_run_open_loop": (C.c_int, [_P, C.POINTER(ServeConfig), C.POINTER(QueryC),
                                          C.c_uint32, _P, _P, C.c_uint64, C.POINTER(QResult)]),
 }
@@ -430,10 +440,15 @@ class Context:
         arr = (StepProf * 16)()
         n = C.c_int32()
         _check(lib().wk_query_profile(self.h, C.byref(qc), iters, arr, 16, C.byref(n)), self.h)
-        return [{"kind": STEP_KINDS[arr[i].kind], "cols_in": arr[i].cols_in,
-                 "cols_out": arr[i].cols_out, "rows_in": arr[i].rows_in,
-                 "rows_out": arr[i].rows_out, "sum_deg": arr[i].sum_deg, "ms": arr[i].ms}
-                for i in range(n.value)]
+        return _prof_list(arr, n.value)
+
+    def batch_profile(self, queries, iters=3):
+        """Per-level kernel times and algorithmic bytes of a batch."""
+        qs, keep = queries_as_c(queries)
+        arr = (StepProf * 16)()
+        n = C.c_int32()
+        _check(lib().wk_batch_profile(self.h, qs, len(queries), iters, arr, 16, C.byref(n)), self.h)
+        return _prof_list(arr, n.value)
 
     def batch(self, queries, cap_elems=None):
         """Run queries together; returns list of (table, status)."""
@@ -462,3 +477,6 @@ class Context:
         tot = C.c_uint64()
         _check(lib().wk_batch_execute_device(self.h, qs, len(queries), C.byref(tot)), self.h)
         return tot.value
+
+    def batch_replay(self):
+        _check(lib().wk_batch_replay(self.h), self.h)
