@@ -65,9 +65,27 @@ int wk_ctx::blocks_per_sm(int op, int cols, int lanes) {
     long long k = ((long long)op * 1000 + cols) * 16 + lanes;
     auto it = bps_cache.find(k);
     if (it != bps_cache.end()) return it->second;
-    int nb = wk::step_blocks_per_sm(cols, op, lanes);
+    const int w_out = (op == wk::kXK2U || op == wk::kXStart) ? cols + 1 : cols;
+    int nb = wk::explore_blocks_per_sm(cols, w_out, lanes);
     bps_cache[k] = nb;
     return nb;
+}
+
+int wk_ctx::ensure_heavy(uint64_t out_rows_cap) {
+    const uint64_t need = out_rows_cap / wk::kHeavyRows + 64;
+    if (need <= heavy_cap) return WK_SUCCESS;
+    const uint64_t cap = need + need / 2;
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    if (d_heavy) cudaFree(d_heavy);
+    d_heavy = nullptr;
+    heavy_cap = 0;
+    if (cudaMalloc(&d_heavy, cap * sizeof(wk::HeavyItem)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WK_E_OOM, "long-list slice queue");
+    }
+    heavy_cap = cap;
+    drop_graphs();
+    return WK_SUCCESS;
 }
 
 int wk_ctx::ensure_status(uint64_t tiles) {
@@ -226,42 +244,89 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
         if (e != cudaSuccess) return ctx->cuda_fail(e, "list kernel launch");
         return WK_SUCCESS;
     }
-    if (!in) return WK_E_BADARG;
-    StepArgs a{};
+    if (!in || st.in_cols <= 0) return WK_E_BADARG;
+    ExploreArgs a{};
     a.store = ctx->dev_store();
-    a.seg = ctx->seg_of(1, st.pid, st.dir);   // any nonzero vid: the normal segment
-    a.seg_index = ctx->seg_of(0, 0, st.dir);
-    a.in = in->d;
+    a.seg_index[0] = ctx->seg_of(0, 0, kIn);
+    a.seg_index[1] = ctx->seg_of(0, 0, kOut);
+    a.one = make_step_desc(ctx, st);
+    a.desc = nullptr;
+    a.n_queries = 1;
+    a.virtual_rows = 0;
     a.in_rows = in->d_rows;
-    a.in_cap = in->cap;
+    a.owner_in = nullptr;
+    a.in = in->d;
+    a.w_in = st.in_cols;
+    a.in_cap_rows = in->cap / st.in_cols;
     a.out = out->d;
+    a.w_out = st.out_cols;
+    a.out_cap_rows = out->cap / st.out_cols;
+    a.owner_out = nullptr;
     a.out_rows = out->d_rows;
-    a.out_cap = out->cap;
+    a.qfirst = a.qcount = nullptr;
+    a.heavy = ctx->d_heavy;
+    a.heavy_cap = ctx->heavy_cap;
     a.ctl = ctx->d_ctl;
     a.status = ctx->d_status;
-    a.cols = st.in_cols;
-    a.col_start = st.cs;
-    a.col_end = st.ce;
-    a.end_const = st.end_const;
-    a.pid = st.pid;
-    a.dir = st.dir;
-    a.type_index = 0;
     a.sorted_lists = ctx->sorted_lists;
-    switch (st.kind) {
-    case PlanStep::kK2U:
-        a.op = kOpK2U;
-        a.type_index = (st.pid == kTypeId && st.dir == kIn) ? 1 : 0;
-        break;
-    case PlanStep::kK2K: a.op = kOpK2K; break;
-    default: a.op = kOpK2C; break;
-    }
-    if (st.in_cols <= 0) return WK_E_BADARG;
-    a.lanes = ctx->lanes_for(a.op, st.in_cols);
+    a.lanes = ctx->lanes_for(a.one.op, st.in_cols);
     int grid = grid_override > 0 ? grid_override
-                                 : ctx->blocks_per_sm(a.op, st.in_cols, a.lanes) * ctx->sm_count;
-    cudaError_t e = launch_step(a, grid, s);
-    if (e != cudaSuccess) return ctx->cuda_fail(e, "step kernel launch");
+                                 : ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
+    cudaError_t e = launch_explore(a, grid, s);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "exploration launch");
+    HeavyArgs hv{};
+    hv.store = a.store;
+    hv.one = a.one;
+    hv.desc = nullptr;
+    hv.in = a.in;
+    hv.w_in = a.w_in;
+    hv.out = a.out;
+    hv.w_out = a.w_out;
+    hv.owner_out = nullptr;
+    hv.heavy = ctx->d_heavy;
+    hv.heavy_cap = ctx->heavy_cap;
+    hv.ctl = ctx->d_ctl;
+    e = launch_heavy(hv, ctx->sm_count * 2, s);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "slice launch");
     return WK_SUCCESS;
+}
+
+StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s) {
+    StepDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.dir = (uint8_t)s.dir;
+    d.cin = (uint8_t)s.in_cols;
+    d.cout = (uint8_t)s.out_cols;
+    d.cs = (uint8_t)s.cs;
+    d.ce = (uint8_t)s.ce;
+    d.pid = s.pid;
+    d.end_const = s.end_const;
+    switch (s.kind) {
+    case PlanStep::kIndex:
+        d.op = kXStart;
+        d.start_key = make_key(0, s.start_const, s.dir);
+        d.seg = ctx->seg_of(0, s.start_const, s.dir);
+        break;
+    case PlanStep::kConst:
+        d.op = kXStart;
+        d.start_key = make_key(s.start_const, s.pid, s.dir);
+        d.seg = ctx->seg_of(s.start_const, s.pid, s.dir);
+        break;
+    case PlanStep::kK2U:
+        d.op = kXK2U;
+        d.type_index = (s.pid == kTypeId && s.dir == kIn) ? 1 : 0;
+        d.seg = ctx->seg_of(1, s.pid, s.dir);   // any nonzero vid: the normal segment
+        break;
+    case PlanStep::kK2K:
+        d.op = kXK2K;
+        d.seg = ctx->seg_of(1, s.pid, s.dir);
+        break;
+    default:
+        d.op = kXK2C;
+        d.seg = ctx->seg_of(1, s.pid, s.dir);
+        break;
+    }
+    return d;
 }
 
 }  // namespace wk
@@ -296,10 +361,8 @@ extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     if (e != cudaSuccess) return bail(e, "sm count");
     e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(e, "stream");
-    e = wk::step_kernel_attrs(ctx->cfg.max_cols);
+    e = wk::explore_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
-    e = wk::level_kernel_attrs();
-    if (e != cudaSuccess) return bail(e, "batch kernel attributes");
     e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
     e = cudaMallocHost(&ctx->h_ctl, sizeof(wk::StepCtl));
@@ -334,6 +397,7 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     if (ctx->d_slots) cudaFree(ctx->d_slots);
     if (ctx->d_edges) cudaFree(ctx->d_edges);
     if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_heavy) cudaFree(ctx->d_heavy);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_rows) cudaFreeHost(ctx->h_rows);
@@ -522,7 +586,9 @@ static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in
         if (rc) return rc;
     }
     for (int attempt = 0; attempt < 8; ++attempt) {
-        int rc = wk::enqueue_step(ctx, st, in, out, mt_tid, mt_factor, ctx->stream, 0);
+        int rc = ctx->ensure_heavy(out->cap);
+        if (rc) return rc;
+        rc = wk::enqueue_step(ctx, st, in, out, mt_tid, mt_factor, ctx->stream, 0);
         if (rc) return rc;
         uint32_t err = 0;
         uint64_t need = 0;
@@ -679,6 +745,8 @@ static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
             if (attempt >= 8) return ctx->fail(WK_E_CAPACITY, "results kept overflowing");
             uint64_t mx = std::max(ctx->rbuf[0].cap, ctx->rbuf[1].cap);
             rc = ctx->ensure_status(mx / wk::kTileRows + 2);
+            if (rc) return rc;
+            rc = ctx->ensure_heavy(mx);
             if (rc) return rc;
             if (mode == WK_MODE_GRAPH) {
                 std::string key = plan_key(steps, *q, ctx);

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "wk_internal.h"
+#include "wk_explore.h"
 #include "wk_kernels.h"
 
 // A device result table (the reference's rbuf + GPUResult, query.hpp:311-362).
@@ -76,6 +77,8 @@ struct wk_ctx {
 
     // scan control of the context stream
     wk::StepCtl* d_ctl = nullptr;
+    wk::HeavyItem* d_heavy = nullptr;    // long-list slices of the context stream
+    uint64_t heavy_cap = 0;
     unsigned long long* d_status = nullptr;
     uint64_t status_cap = 0;
     wk::StepCtl* h_ctl = nullptr;     // pinned
@@ -128,6 +131,7 @@ struct wk_ctx {
     }
     void drop_graphs();
     int ensure_status(uint64_t tiles);
+    int ensure_heavy(uint64_t out_rows_cap);
     int table_reserve(wk_table* t, uint64_t elems);
     int read_ctl(uint32_t* err, uint64_t* need);
     int clear_ctl_err();
@@ -137,4 +141,6 @@ namespace wk {
 // Enqueue one resolved step reading `in` (may be null for index/const starts) into `out`.
 int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* out,
                  int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override);
+// The device descriptor of a resolved step.
+StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s);
 }  // namespace wk

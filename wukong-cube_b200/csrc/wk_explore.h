@@ -1,0 +1,89 @@
+// The exploration launch shared by single queries and batches.
+//
+// One launch runs one pattern level: for a single query every input row runs the same step;
+// for a batch each input row belongs to one query (owner_in) whose step for this level is
+// desc[owner].  Output rows keep their query's rows contiguous and in input order.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "wk_kernels.h"
+
+namespace wk {
+
+enum ExploreOp : uint8_t { kXStart = 0, kXK2U = 1, kXK2K = 2, kXK2C = 3, kXDone = 4 };
+
+// One query's step at one level (64 bytes).
+struct StepDesc {
+    SegDesc seg;            // segment of the step's normal key, or of the start key
+    uint64_t start_key;     // kXStart: the constant / index key whose list starts the table
+    uint32_t pid;
+    uint32_t end_const;     // kXK2C
+    uint8_t op, dir, cin, cout;
+    uint8_t cs, ce, type_index, pad;
+    uint32_t pad2;
+};
+static_assert(sizeof(StepDesc) == 64, "StepDesc is 64 bytes");
+
+// A slice of a long neighbour list whose output rows another launch writes (rows whose
+// count exceeds kHeavyRows are split into kHeavyChunk-row slices and spread over all CTAs).
+struct HeavyItem {
+    uint64_t in_row;        // physical input row (virtual rows: unused)
+    uint64_t off;           // first edge of the slice
+    uint64_t out_pos;       // first output row of the slice
+    uint32_t count;         // output rows in the slice
+    uint32_t q;             // owner query
+};
+static_assert(sizeof(HeavyItem) == 32, "HeavyItem is 32 bytes");
+
+constexpr int kHeavyRows = 128;
+constexpr int kHeavyChunk = 2048;
+
+struct ExploreArgs {
+    DevStore store;
+    SegDesc seg_index[2];        // index segment of each direction
+    StepDesc one;                // the step of every row when desc is null
+    const StepDesc* desc;        // [n_queries] this level's step per query, or null
+    uint32_t n_queries;
+    int32_t virtual_rows;        // input row r is query r's start row (no input table)
+    const uint64_t* in_rows;     // device row count of the input (unused for virtual rows)
+    const uint32_t* owner_in;    // owner query of each input row, or null (query 0)
+    const uint32_t* in;          // input rows, stride w_in (tables carry >= 64 B of padding)
+    int32_t w_in;
+    uint64_t in_cap_rows;
+    uint32_t* out;               // output rows, stride w_out
+    int32_t w_out;
+    uint64_t out_cap_rows;
+    uint32_t* owner_out;         // owner query of each output row, or null
+    uint64_t* out_rows;          // rows written (set by the launch)
+    unsigned long long* qfirst;  // [n_queries] first output row per query (min), or null
+    unsigned long long* qcount;  // [n_queries] output rows per query (sum), or null
+    HeavyItem* heavy;
+    uint64_t heavy_cap;
+    StepCtl* ctl;
+    unsigned long long* status;
+    int32_t sorted_lists;
+    int32_t lanes;
+};
+
+struct HeavyArgs {
+    DevStore store;
+    StepDesc one;
+    const StepDesc* desc;
+    const uint32_t* in;
+    int32_t w_in;
+    uint32_t* out;
+    int32_t w_out;
+    uint32_t* owner_out;
+    const HeavyItem* heavy;
+    uint64_t heavy_cap;
+    StepCtl* ctl;
+};
+
+size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);
+cudaError_t explore_kernel_attrs();
+int explore_blocks_per_sm(int w_in, int w_out, int lanes);
+cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_heavy(const HeavyArgs& a, int grid, cudaStream_t s);
+
+}  // namespace wk

@@ -29,6 +29,9 @@ struct StepCtl {
     unsigned long long sum_deg;  // neighbour-list lengths the probes found (profiling)
     unsigned long long alg_bytes;   // algorithmic bytes of the launches: rows in * cols * 4
                                     // + 16 per probe + 4 per list entry read + rows out * cols * 4
+    unsigned long long heavy_n;     // long-list slices appended by an exploration launch
+    unsigned int heavy_exit;        // CTAs of the slice launch that have finished
+    unsigned int pad2;
 };
 
 // Where the store lives on the device.
@@ -37,32 +40,6 @@ struct DevStore {
     uint64_t n_buckets;   // slots / 8
     const uint32_t* edges;
     uint64_t n_edges;
-};
-
-enum StepOp : int32_t { kOpK2U = 0, kOpK2K = 1, kOpK2C = 2 };
-
-struct StepArgs {
-    DevStore store;
-    SegDesc seg;             // segment of [vid|pid|dir]
-    SegDesc seg_index;       // index segment of `dir` (rows whose value is 0 and TYPE_ID/IN)
-    const uint32_t* in;      // input table, row-major
-    const uint64_t* in_rows; // device row count of the input
-    uint64_t in_cap;         // elements the input buffer holds (reads never pass it)
-    uint32_t* out;
-    uint64_t* out_rows;      // written by the launch: rows of the output
-    uint64_t out_cap;        // elements the output buffer holds
-    StepCtl* ctl;
-    unsigned long long* status;
-    int32_t op;
-    int32_t cols;
-    int32_t col_start;
-    int32_t col_end;         // K2K
-    uint32_t end_const;      // K2C
-    uint32_t pid;
-    int32_t dir;
-    int32_t type_index;      // K2U with pid == TYPE_ID and dir == IN: key = [0|cur|IN]
-    int32_t sorted_lists;    // every list ascending + unique (checked at upload)
-    int32_t lanes;           // lanes per probe group: 2, 4 or 8 (slots read per request)
 };
 
 struct ListArgs {
@@ -76,15 +53,11 @@ struct ListArgs {
     StepCtl* ctl;
 };
 
-// Launch geometry helpers.
+// Launch geometry of the exploration launch.
 constexpr int kStepThreads = 256;
 constexpr int kTileRows = 512;
-size_t step_smem_bytes(int cols, int op, int* out_chunk_rows);
-int step_blocks_per_sm(int cols, int op, int lanes);
 
-cudaError_t launch_step(const StepArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);
-cudaError_t step_kernel_attrs(int max_cols);
 
 }  // namespace wk
