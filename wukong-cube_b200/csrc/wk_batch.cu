@@ -316,19 +316,6 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
         }
         cudaError_t e = wk::launch_explore(a, grid, s);
         if (e != cudaSuccess) return ctx->cuda_fail(e, "level launch");
-        wk::HeavyArgs hv{};
-        hv.store = a.store;
-        hv.desc = a.desc;
-        hv.in = a.in;
-        hv.w_in = a.w_in;
-        hv.out = a.out;
-        hv.w_out = a.w_out;
-        hv.owner_out = a.owner_out;
-        hv.heavy = ctx->d_heavy;
-        hv.heavy_cap = ctx->heavy_cap;
-        hv.ctl = ctx->d_ctl;
-        e = wk::launch_heavy(hv, ctx->sm_count * 2, s);
-        if (e != cudaSuccess) return ctx->cuda_fail(e, "slice launch");
         if (ph) {
             WKB_CUDA(ctx, cudaEventRecord(ph->ev[2 * k + 1], s));
             WKB_CUDA(ctx, cudaMemcpyAsync(ph->h_cnt + 2 * k, &ctx->d_ctl->sum_deg, 16,

@@ -274,20 +274,6 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
                                  : ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
     cudaError_t e = launch_explore(a, grid, s);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "exploration launch");
-    HeavyArgs hv{};
-    hv.store = a.store;
-    hv.one = a.one;
-    hv.desc = nullptr;
-    hv.in = a.in;
-    hv.w_in = a.w_in;
-    hv.out = a.out;
-    hv.w_out = a.w_out;
-    hv.owner_out = nullptr;
-    hv.heavy = ctx->d_heavy;
-    hv.heavy_cap = ctx->heavy_cap;
-    hv.ctl = ctx->d_ctl;
-    e = launch_heavy(hv, ctx->sm_count * 2, s);
-    if (e != cudaSuccess) return ctx->cuda_fail(e, "slice launch");
     return WK_SUCCESS;
 }
 
@@ -601,7 +587,9 @@ static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in
         if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "tile look-back timed out");
         if (err & wk::kErrStatus) return ctx->fail(WK_E_CAPACITY, "status array too small");
         if (err & wk::kErrOverflow) {
-            rc = ctx->table_reserve(out, need + need / 8 + 1024);
+            // `need` counts rows (the list copy of a start step has one column)
+            const uint64_t elems = need * (uint64_t)std::max(st.out_cols, 1);
+            rc = ctx->table_reserve(out, elems + elems / 8 + 1024);
             if (rc) return rc;
         }
     }
@@ -780,7 +768,10 @@ static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
             if (err & wk::kErrCorrupt) return ctx->fail(WK_E_CORRUPT, "key table chain out of range");
             if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "tile look-back timed out");
             if (err & (wk::kErrOverflow | wk::kErrStatus)) {
-                uint64_t want = std::max<uint64_t>(need + need / 4, mx * 2);
+                int wmax = 1;
+                for (auto& s : steps) wmax = std::max(wmax, s.out_cols);
+                const uint64_t elems = need * (uint64_t)wmax;   // `need` counts rows
+                uint64_t want = std::max<uint64_t>(elems + elems / 4, mx * 2);
                 for (auto& t : ctx->rbuf) {
                     rc = ctx->table_reserve(&t, want);
                     if (rc) return rc;

@@ -270,7 +270,10 @@ __device__ __forceinline__ void store_words(uint32_t* dst, const uint32_t* src, 
 
 // The last CTA to leave resets the tile/exit counters and advances the epoch; when the 16-bit
 // epoch wraps it clears the status array first so no stale word can match the next epoch.
-__device__ void exit_protocol(StepCtl* ctl, unsigned long long* status, unsigned epoch) {
+// `tags` / `tag_stride` / `n_tags`: epoch-tagged words of the long-list slice queue, cleared with
+// the status array when the epoch wraps.
+__device__ void exit_protocol(StepCtl* ctl, unsigned long long* status, unsigned epoch,
+                              unsigned* tags, unsigned tag_stride, unsigned long long n_tags) {
     __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -283,12 +286,16 @@ __device__ void exit_protocol(StepCtl* ctl, unsigned long long* status, unsigned
     unsigned next = epoch + 1;
     if (next > 0xFFFFu) {
         for (unsigned long long i = threadIdx.x; i < ctl->status_cap; i += blockDim.x) status[i] = 0;
+        for (unsigned long long i = threadIdx.x; i < n_tags; i += blockDim.x) tags[i * tag_stride] = 0;
         next = 1;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         ctl->tile_counter = 0;
         ctl->exit_counter = 0;
+        ctl->heavy_n = 0;
+        ctl->heavy_claim = 0;
+        ctl->tiles_done = 0;
         __threadfence();
         *(volatile unsigned*)&ctl->epoch = next;
         __threadfence();

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
                 if (i == n - 1 || s_q[i + 1] != q) atomicAdd(a.qcount + q, (unsigned long long)(excl + s_pre[i + 1]));
             }
         }
-        // long lists -> slices for the slice launch
+        // long lists -> slices on the queue (fields first, then the epoch tag)
         if (s_has_heavy && fits) {
             for (int i = threadIdx.x; i < n; i += kStepThreads) {
                 const uint32_t c = s_cnt[i];
@@ -218,13 +218,14 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
                         atomicOr(&a.ctl->err, kErrOverflow);
                         break;
                     }
-                    HeavyItem it;
-                    it.in_row = r0 + i;
-                    it.off = s_off[i] + (uint64_t)k * kHeavyChunk;
-                    it.out_pos = excl + s_pre[i] + (uint64_t)k * kHeavyChunk;
-                    it.count = min((uint32_t)kHeavyChunk, c - k * kHeavyChunk);
-                    it.q = s_q[i];
-                    a.heavy[at + k] = it;
+                    HeavyItem* it = a.heavy + at + k;
+                    it->in_row = r0 + i;
+                    it->off = s_off[i] + (uint64_t)k * kHeavyChunk;
+                    it->out_pos = excl + s_pre[i] + (uint64_t)k * kHeavyChunk;
+                    it->count = min((uint32_t)kHeavyChunk, c - k * kHeavyChunk);
+                    it->q = s_q[i];
+                    __threadfence();
+                    *(volatile uint32_t*)&it->tag = epoch;
                 }
             }
         }
@@ -269,49 +270,81 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0) {   // this tile's slices are all reserved
+            __threadfence();
+            atomicAdd(&a.ctl->tiles_done, 1ull);
+        }
     }
-    exit_protocol(a.ctl, a.status, epoch);
-}
 
-// Slice launch: every CTA writes whole kHeavyChunk-row slices of long lists.
-__global__ void __launch_bounds__(256) heavy_kernel(const HeavyArgs a) {
-    __shared__ uint32_t s_row[32];
-    __shared__ int s_last;
-    const uint64_t nitems = min((uint64_t)*(volatile unsigned long long*)&a.ctl->heavy_n, a.heavy_cap);
-    const int wo = a.w_out;
-    for (uint64_t i = blockIdx.x; i < nitems; i += gridDim.x) {
-        const HeavyItem it = a.heavy[i];
-        const StepDesc* d = a.desc ? a.desc + it.q : &a.one;
+    // Out of tiles: write queued long-list slices until every tile is done and the queue is
+    // drained.  A claimed index either gets reserved by a tile still running (wait for its
+    // tag) or lies past the final count (stop).  Every wait is bounded.
+    __syncthreads();   // every thread has read the last s_tile before it is reused
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long idx = atomicAdd(&a.ctl->heavy_claim, 1ull);
+            int state = 0;
+            unsigned long long spins = 0;
+            for (;;) {
+                unsigned long long hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
+                if (idx < hn) {
+                    if (idx >= a.heavy_cap) {
+                        state = 2;   // the queue overflowed; kErrOverflow is already set
+                        break;
+                    }
+                    if (*(volatile uint32_t*)&a.heavy[idx].tag == epoch) {
+                        __threadfence();
+                        state = 1;
+                        break;
+                    }
+                } else if (*(volatile unsigned long long*)&a.ctl->tiles_done >= ntiles) {
+                    __threadfence();
+                    hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
+                    if (idx >= hn) {
+                        state = 2;
+                        break;
+                    }
+                    continue;
+                }
+                if (++spins > kSpinLimit) {
+                    atomicOr(&a.ctl->err, kErrTimeout);
+                    state = 2;
+                    break;
+                }
+                if (spins > 32) __nanosleep(64);
+            }
+            s_tile = state == 1 ? idx : ~0ull;
+        }
+        __syncthreads();
+        const unsigned long long idx = s_tile;
+        if (idx == ~0ull) break;
+        const HeavyItem* it = a.heavy + idx;
+        const uint64_t in_row = __ldcg((const unsigned long long*)&it->in_row);
+        const uint64_t off = __ldcg((const unsigned long long*)&it->off);
+        const uint64_t out_pos = __ldcg((const unsigned long long*)&it->out_pos);
+        const uint32_t count = __ldcg((const unsigned int*)&it->count);
+        const uint32_t q = __ldcg((const unsigned int*)&it->q);
+        const StepDesc* d = a.desc ? a.desc + q : &a.one;
         const int opv = d->op, cin = d->cin;
+        if (opv != kXStart && threadIdx.x < cin) s_out[threadIdx.x] = __ldg(a.in + in_row * (uint64_t)a.w_in + threadIdx.x);
         __syncthreads();
-        if (opv != kXStart && threadIdx.x < cin && threadIdx.x < 32)
-            s_row[threadIdx.x] = a.in[it.in_row * (uint64_t)a.w_in + threadIdx.x];
-        __syncthreads();
-        const uint64_t ne = (uint64_t)it.count * wo;
-        uint32_t* dst = a.out + it.out_pos * wo;
-        for (uint64_t e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int ecol = opv == kXStart ? 0 : cin;
+        const uint64_t ne = (uint64_t)count * wo;
+        uint32_t* dst = a.out + out_pos * wo;
+        for (uint64_t e = threadIdx.x; e < ne; e += kStepThreads) {
             const uint64_t j = e / wo;
             const int c = (int)(e - j * wo);
             uint32_t v = 0;
-            if (opv != kXStart && c < cin) v = s_row[c];
-            else if (c == (opv == kXStart ? 0 : cin)) v = __ldg(a.store.edges + it.off + j);
+            if (c < ecol) v = s_out[c];
+            else if (c == ecol) v = __ldg(a.store.edges + off + j);
             dst[e] = v;
         }
         if (a.owner_out)
-            for (uint32_t j = threadIdx.x; j < it.count; j += blockDim.x) a.owner_out[it.out_pos + j] = it.q;
+            for (uint32_t j = threadIdx.x; j < count; j += kStepThreads) a.owner_out[out_pos + j] = q;
+        __syncthreads();
     }
-    // the last CTA to leave resets the slice count for the next level
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        s_last = atomicAdd(&a.ctl->heavy_exit, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        a.ctl->heavy_n = 0;
-        a.ctl->heavy_exit = 0;
-        __threadfence();
-    }
+    exit_protocol(a.ctl, a.status, epoch, a.heavy ? &a.heavy[0].tag : nullptr,
+                  sizeof(HeavyItem) / sizeof(uint32_t), a.heavy ? a.heavy_cap : 0);
 }
 
 template <int L>
@@ -360,12 +393,6 @@ cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s) {
     case 8: explore_kernel<8><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
     default: explore_kernel<4><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
     }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_heavy(const HeavyArgs& a, int grid, cudaStream_t s) {
-    if (grid < 1) grid = 1;
-    heavy_kernel<<<grid, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -25,16 +25,19 @@ struct StepDesc {
 };
 static_assert(sizeof(StepDesc) == 64, "StepDesc is 64 bytes");
 
-// A slice of a long neighbour list whose output rows another launch writes (rows whose
-// count exceeds kHeavyRows are split into kHeavyChunk-row slices and spread over all CTAs).
+// A slice of a long neighbour list.  Rows whose count exceeds kHeavyRows are not written by
+// the CTA that scanned them: it queues them as kHeavyChunk-row slices, and CTAs that run out of
+// tiles take slices from the queue, so a hub vertex is spread over every CTA.
 struct HeavyItem {
     uint64_t in_row;        // physical input row (virtual rows: unused)
     uint64_t off;           // first edge of the slice
     uint64_t out_pos;       // first output row of the slice
     uint32_t count;         // output rows in the slice
     uint32_t q;             // owner query
+    uint32_t tag;           // launch epoch, written last: the slice is ready
+    uint32_t pad;
 };
-static_assert(sizeof(HeavyItem) == 32, "HeavyItem is 32 bytes");
+static_assert(sizeof(HeavyItem) == 40, "HeavyItem is 40 bytes");
 
 constexpr int kHeavyRows = 128;
 constexpr int kHeavyChunk = 2048;
@@ -66,24 +69,9 @@ struct ExploreArgs {
     int32_t lanes;
 };
 
-struct HeavyArgs {
-    DevStore store;
-    StepDesc one;
-    const StepDesc* desc;
-    const uint32_t* in;
-    int32_t w_in;
-    uint32_t* out;
-    int32_t w_out;
-    uint32_t* owner_out;
-    const HeavyItem* heavy;
-    uint64_t heavy_cap;
-    StepCtl* ctl;
-};
-
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);
 cudaError_t explore_kernel_attrs();
 int explore_blocks_per_sm(int w_in, int w_out, int lanes);
 cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s);
-cudaError_t launch_heavy(const HeavyArgs& a, int grid, cudaStream_t s);
 
 }  // namespace wk

@@ -29,9 +29,9 @@ struct StepCtl {
     unsigned long long sum_deg;  // neighbour-list lengths the probes found (profiling)
     unsigned long long alg_bytes;   // algorithmic bytes of the launches: rows in * cols * 4
                                     // + 16 per probe + 4 per list entry read + rows out * cols * 4
-    unsigned long long heavy_n;     // long-list slices appended by an exploration launch
-    unsigned int heavy_exit;        // CTAs of the slice launch that have finished
-    unsigned int pad2;
+    unsigned long long heavy_n;     // long-list slices reserved by the running launch
+    unsigned long long heavy_claim; // slices claimed by CTAs that ran out of tiles
+    unsigned long long tiles_done;  // tiles whose slices are all reserved
 };
 
 // Where the store lives on the device.
