@@ -317,8 +317,29 @@ def run_ours(args, world, rank, local_rank):
     ctx.close()
 
 
+def run_profile_case(args):
+    """A small, self-contained case for ncu: the heavy triangle query (resident mode) and one
+    light batch, each run `--steps` times after `--warmup` runs, no oracle, no timing."""
+    import workloads
+    import wukong_b200 as wk
+    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
+    with wk.Context(0) as ctx:
+        ctx.upload_gstore(g)
+        q = workloads.heavy_triangle(v)
+        qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
+        for _ in range(args.warmup + args.steps):
+            ctx.execute(q, wk.MODE_RESIDENT)
+        ctx.batch_device(qs)
+        for _ in range(args.warmup + args.steps):
+            ctx.batch_replay()
+        ctx.check()
+    print(json.dumps({"profile_case": "ok", "graph": ginfo}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run the small ncu case instead of the benchmark")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
@@ -333,6 +354,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.profile_case:
+        run_profile_case(args)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         return
