@@ -166,7 +166,7 @@ void wk_free(void* p);
  * SegmentRDFGraph::init_gstore does (segment_rdf_dgraph.hpp:1182-1269) after the loader's
  * sort + dedup (base_loader.hpp:481-496).  pso and pos are the triples to insert in the OUT
  * and IN directions (normally the same array; n x 3 uint32 each).  load_factor is the mean
- * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.5). */
+ * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.2). */
 int wk_gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
                     double load_factor, wk_gstore** out);
 void wk_gstore_free(wk_gstore* g);
@@ -271,6 +271,20 @@ typedef struct wk_step_prof {
 } wk_step_prof;
 int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof* out,
                      int32_t max_steps, int32_t* n_steps);
+
+/* Diagnostics: clock64() cycles each phase of the exploration launch took, summed over CTAs
+ * (claim, stage, probe tail, scan, look-back, ranges, write, drain, probe setup, probe walk,
+ * membership), in a library built with -DWK_PHASE_TIMING; all zero otherwise.  n >= 12.
+ * No reference counterpart. */
+int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
+
+/* Tile-schedule knobs of the exploration launch (what the autotuner sets).  knob 0: lanes per
+ * probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte bucket slices per
+ * request); knob 1: the same for batches.  wk_ctx_tune_get reads a knob back. */
+#define WK_KNOB_LANES 0
+#define WK_KNOB_BATCH_LANES 1
+int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value);
+int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value);
 
 /* ---------------------------------------------------------------- batching
  * Run n planned queries together: all queries advance one pattern per level inside one

@@ -925,3 +925,28 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
     }
     return WK_SUCCESS;
 }
+
+extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
+    if (!ctx) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (value != 2 && value != 4 && value != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
+    if (knob == WK_KNOB_LANES) {
+        ctx->default_lanes = value;
+        ctx->tuned_lanes.clear();
+    } else if (knob == WK_KNOB_BATCH_LANES) {
+        ctx->batch_lanes = value;
+    } else {
+        return ctx->fail(WK_E_BADARG, "unknown knob");
+    }
+    ctx->drop_graphs();
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
+    if (!ctx || !value) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (knob == WK_KNOB_LANES) *value = ctx->default_lanes;
+    else if (knob == WK_KNOB_BATCH_LANES) *value = ctx->batch_lanes;
+    else return ctx->fail(WK_E_BADARG, "unknown knob");
+    return WK_SUCCESS;
+}

@@ -208,16 +208,20 @@ __device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* 
 // waits until all of them have published at least their aggregate, adds the aggregates up to
 // the nearest inclusive prefix and stops there.  Tiles are claimed in order from the tile
 // counter, so every predecessor is held by a running CTA and the wait ends; it is still bounded.
-// Called by all 32 lanes of one warp; returns the exclusive prefix in every lane.
-__device__ uint64_t lookback_warp(unsigned long long* status, StepCtl* ctl, uint64_t tile,
-                                  uint64_t agg, unsigned epoch) {
+// The tile's own entry is published first (publish_aggregate, by one thread, as soon as the
+// tile's total is known) and resolved later (resolve_prefix, by all 32 lanes of one warp, which
+// returns the exclusive prefix in every lane).
+__device__ __forceinline__ void publish_aggregate(unsigned long long* status, uint64_t tile,
+                                                  uint64_t agg, unsigned epoch) {
+    volatile unsigned long long* st = status;
+    st[tile] = pack_status(epoch, tile == 0 ? kFlagPrefix : kFlagAgg, agg);
+}
+
+__device__ uint64_t resolve_prefix(unsigned long long* status, StepCtl* ctl, uint64_t tile,
+                                   uint64_t agg, unsigned epoch) {
     volatile unsigned long long* st = status;
     const int lane = threadIdx.x & 31;
-    if (tile == 0) {
-        if (lane == 0) st[0] = pack_status(epoch, kFlagPrefix, agg);
-        return 0;
-    }
-    if (lane == 0) st[tile] = pack_status(epoch, kFlagAgg, agg);
+    if (tile == 0) return 0;   // tile 0 published its inclusive prefix already
     uint64_t excl = 0;
     int64_t base = (int64_t)tile - 1;
     unsigned long long spins = 0;

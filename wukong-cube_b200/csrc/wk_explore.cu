@@ -3,7 +3,8 @@
 //
 // The reference chains five kernels, a Thrust scan and two host syncs per pattern
 // (gpu_engine_cuda.hpp:169-177, gpu_hash.cu:96-836).  Here CTAs claim 512-row tiles from a
-// device counter and, per tile:
+// device counter, two at a time (the probes of the next tile run while the current one waits for
+// its position), and per tile:
 //   1. start a TMA bulk copy (cp.async.bulk + mbarrier) of the tile's rows into shared memory
 //      and, while it is in flight, read each row's start column straight from global memory;
 //   2. probe the key table with groups of L lanes, one 16-byte slot per lane, four rows per group
@@ -16,41 +17,345 @@
 //   4. scan the counts (block scan + warp-parallel decoupled look-back, 64-bit positions);
 //   5. write the rows whose lists are short through shared memory with coalesced stores, in
 //      row-major then edge order (what the CPU engine appends, sparql.hpp:328-370), and hand
-//      rows with long lists to the slice launch as kHeavyChunk-row slices so a hub vertex is
-//      spread over every CTA instead of holding one.
+//      rows with long lists to a device queue as kHeavyChunk-row slices that CTAs out of tiles
+//      drain, so a hub vertex is spread over every CTA instead of holding one.
 // Sizes are read from device memory, so levels chain without a host round trip; an output that
 // would not fit sets kErrOverflow and records the size needed instead of writing.
 #include <cuda_runtime.h>
 
+#include "../../include/wukong_b200.h"
 #include "wk_device.cuh"
 #include "wk_explore.h"
 
 namespace wk {
+
+// Optional per-phase cycle counters (build with -DWK_PHASE_TIMING): thread 0 of every CTA adds
+// the clock64() time spent in each phase of the launch; read with wk_debug_phase_cycles.
+__device__ unsigned long long g_phase_cycles[kPhaseSlots];
+
 namespace {
 using namespace dev;
+
+#ifdef WK_PHASE_TIMING
+__shared__ unsigned long long s_ph[kPhaseSlots];
+__shared__ long long s_ph_t;
+#define WK_PH_DECL                                              \
+    if (threadIdx.x < kPhaseSlots) s_ph[threadIdx.x] = 0;       \
+    if (threadIdx.x == 0) s_ph_t = clock64();
+#define WK_PH(k)                                                \
+    do {                                                        \
+        if (threadIdx.x == 0) {                                 \
+            const long long t_ = clock64();                     \
+            s_ph[k] += (unsigned long long)(t_ - s_ph_t);       \
+            s_ph_t = t_;                                        \
+        }                                                       \
+    } while (0)
+#define WK_PH_FLUSH                                                                              \
+    do {                                                                                         \
+        __syncthreads();                                                                         \
+        if (threadIdx.x < kPhaseSlots) atomicAdd(&g_phase_cycles[threadIdx.x], s_ph[threadIdx.x]); \
+    } while (0)
+#else
+#define WK_PH_DECL
+#define WK_PH(k) \
+    do {         \
+    } while (0)
+#define WK_PH_FLUSH \
+    do {            \
+    } while (0)
+#endif
+
+// Per-tile state kept in shared memory while the tile is between its front and back halves.
+struct TileState {
+    unsigned long long tile;
+    unsigned long long total;    // output rows of the tile
+    unsigned long long ltotal;   // output rows written by the tile itself (short lists)
+    unsigned long long alg, sd;  // byte accounting
+    int n;
+    int has_heavy;
+};
+
+// Shared-memory arrays of one tile buffer.
+struct TileBuf {
+    uint32_t* in;     // kTileRows * w_in words (TMA destination)
+    uint64_t* pre;    // kTileRows + 2: exclusive scan of cnt, pre[n] = total
+    uint64_t* lpre;   // kTileRows + 2: exclusive scan of lcnt
+    uint64_t* off;    // kTileRows: first edge of each row's list
+    uint32_t* cnt;    // kTileRows: output rows of each input row
+    uint32_t* lcnt;   // kTileRows: cnt for short lists, 0 for long ones
+    uint32_t* q;      // kTileRows: owner query
+    uint32_t* meta;   // kTileRows: op | cin << 8 | cout << 16
+};
+
+__device__ __forceinline__ TileBuf tile_buf(uint32_t* base, int wi) {
+    TileBuf b;
+    b.in = base;
+    b.pre = reinterpret_cast<uint64_t*>(base + (((size_t)kTileRows * wi + 3) & ~(size_t)3));
+    b.lpre = b.pre + kTileRows + 2;
+    b.off = b.lpre + kTileRows + 2;
+    b.cnt = reinterpret_cast<uint32_t*>(b.off + kTileRows);
+    b.lcnt = b.cnt + kTileRows;
+    b.q = b.lcnt + kTileRows;
+    b.meta = b.q + kTileRows;
+    return b;
+}
+
+// Front half of a tile: start the TMA copy of its rows, probe, count, scan, publish the tile's
+// aggregate.  Nothing here waits on another CTA.
+template <int L>
+__device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& B, TileState& S,
+                                           uint64_t* bar, uint64_t tile, uint64_t R, int wi,
+                                           unsigned epoch, uint64_t* s_warp) {
+    constexpr int kGroups = kStepThreads / L;
+    constexpr int kBatches = kTileRows / (kGroups * kUnroll);
+    static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
+    const int grp = threadIdx.x / L;
+    const int h = threadIdx.x & (L - 1);
+    const uint64_t r0 = tile * kTileRows;
+    const int n = (int)min((uint64_t)kTileRows, R - r0);
+    const uint32_t* src = a.in + r0 * (uint64_t)wi;
+    if (threadIdx.x == 0) {
+        if (wi) {
+            const unsigned bytes = (unsigned)(((uint64_t)n * wi * 4 + 15) & ~15ull);
+            mbar_expect_tx(bar, bytes);
+            tma_load_1d(B.in, src, bytes, bar);
+        }
+        S.tile = tile;
+        S.n = n;
+        S.alg = 0;
+        S.sd = 0;
+        S.has_heavy = 0;
+    }
+    for (int i = threadIdx.x; i < n; i += kStepThreads) {
+        B.q[i] = a.virtual_rows ? (uint32_t)(r0 + i) : (a.owner_in ? __ldg(a.owner_in + r0 + i) : 0u);
+        B.cnt[i] = 0;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int b = 0; b < kBatches; ++b) {
+        uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
+        bool valid[kUnroll], pending[kUnroll];
+        int row[kUnroll];
+        uint32_t target[kUnroll], op[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            row[u] = (b * kUnroll + u) * kGroups + grp;
+            valid[u] = row[u] < n;
+            const StepDesc* d = a.desc ? a.desc + (valid[u] ? B.q[row[u]] : 0) : &a.one;
+            op[u] = valid[u] ? d->op : kXDone;
+            if (op[u] == kXDone) valid[u] = false;
+            const SegDesc* sg = &d->seg;
+            target[u] = d->end_const;
+            if (op[u] == kXStart) {
+                key[u] = d->start_key;
+            } else {
+                const uint32_t* rin = src + (uint64_t)row[u] * wi;
+                const uint32_t cur = valid[u] ? __ldg(rin + d->cs) : kBlankId;
+                if (op[u] == kXK2K && valid[u]) target[u] = __ldg(rin + d->ce);
+                if (op[u] == kXK2U && d->type_index) {
+                    // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+                    key[u] = make_key(0, cur, kIn);
+                    sg = &a.seg_index[kIn];
+                    if (cur >= (1u << kNbitsIdx)) valid[u] = false;
+                } else {
+                    key[u] = make_key(cur, d->pid, d->dir);
+                    if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+                }
+                if (cur == kBlankId) valid[u] = false;
+            }
+            pending[u] = valid[u] && sg->num_buckets != 0 && key[u] != 0;
+            bucket[u] = pending[u] ? bucket_of(key[u], *sg) : 0;
+            if (h == 0 && row[u] < n)
+                B.meta[row[u]] = op[u] | ((uint32_t)d->cin << 8) | ((uint32_t)d->cout << 16);
+        }
+        WK_PH(8);
+        group_probe<L>(a.store, key, bucket, pending, ptr, &a.ctl->err);
+        WK_PH(9);
+        uint64_t off[kUnroll], deg[kUnroll];
+        bool has[kUnroll], found[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            off[u] = ptr_off(ptr[u]);
+            deg[u] = ptr_size(ptr[u]);
+            if (off[u] + deg[u] > a.store.n_edges) {
+                if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
+                deg[u] = 0;
+            }
+            has[u] = valid[u] && deg[u] > 0 && (op[u] == kXK2K || op[u] == kXK2C);
+        }
+        group_member<L>(a.store.edges, off, deg, target, has, a.sorted_lists != 0, found);
+        WK_PH(10);
+        unsigned long long alg = 0, sd = 0;
+        if (h == 0) {
+#pragma unroll
+            for (int u = 0; u < kUnroll; ++u)
+                if (valid[u]) {
+                    const bool filt = op[u] == kXK2K || op[u] == kXK2C;
+                    const uint32_t cnt = filt ? (found[u] ? 1u : 0u) : (uint32_t)deg[u];
+                    const uint32_t meta = B.meta[row[u]];
+                    B.off[row[u]] = off[u];
+                    B.cnt[row[u]] = cnt;
+                    sd += deg[u];
+                    alg += ((meta >> 8) & 0xFF) * 4ull + 16 + deg[u] * 4 +
+                           (unsigned long long)cnt * ((meta >> 16) & 0xFF) * 4;
+                }
+        }
+        // byte accounting: a warp reduction, then one shared atomic per warp
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            alg += __shfl_xor_sync(0xffffffffu, alg, o);
+            sd += __shfl_xor_sync(0xffffffffu, sd, o);
+        }
+        if ((threadIdx.x & 31) == 0 && alg) {
+            atomicAdd(&S.alg, alg);
+            atomicAdd(&S.sd, sd);
+        }
+    }
+    __syncthreads();
+    WK_PH(2);
+    for (int i = threadIdx.x; i < n; i += kStepThreads) {
+        const uint32_t c = B.cnt[i];
+        const bool heavy = c > (uint32_t)kHeavyRows;
+        B.lcnt[i] = heavy ? 0u : c;
+        if (heavy) S.has_heavy = 1;
+    }
+    __syncthreads();
+    const uint64_t total = block_scan(B.cnt, B.pre, n, s_warp);
+    const uint64_t ltotal = S.has_heavy ? block_scan(B.lcnt, B.lpre, n, s_warp) : total;
+    if (threadIdx.x == 0) {
+        S.total = total;
+        S.ltotal = ltotal;
+        publish_aggregate(a.status, tile, total, epoch);
+    }
+    __syncthreads();
+    WK_PH(3);
+}
+
+// Back half of a tile: resolve its position (look-back), wait for its rows, record per-query
+// ranges, queue long lists, write the short ones.
+template <int L>
+__device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B, TileState& S,
+                                          uint64_t* bar, unsigned phase, uint64_t ntiles, int wi,
+                                          int wo, int chunk_rows, unsigned epoch, uint64_t* s_pos,
+                                          uint32_t* s_out, unsigned long long* s_excl) {
+    const uint64_t tile = S.tile;
+    const int n = S.n;
+    const uint64_t total = S.total, ltotal = S.ltotal;
+    const uint64_t r0 = tile * kTileRows;
+    if (threadIdx.x < 32) {
+        const uint64_t ex = resolve_prefix(a.status, a.ctl, tile, total, epoch);
+        if (threadIdx.x == 0) {
+            *s_excl = ex;
+            atomicAdd(&a.ctl->alg_bytes, S.alg);
+            atomicAdd(&a.ctl->sum_deg, S.sd);
+        }
+    }
+    if (wi) mbar_wait(bar, phase, &a.ctl->err);   // the tile's rows are in shared memory
+    __syncthreads();
+    WK_PH(4);
+    const uint64_t excl = *s_excl;
+    if (tile == ntiles - 1 && threadIdx.x == 0) *a.out_rows = excl + total;
+    const bool fits = excl + total <= a.out_cap_rows;
+    if (!fits && threadIdx.x == 0) {
+        atomicOr(&a.ctl->err, kErrOverflow);
+        atomicMax(&a.ctl->need, (unsigned long long)(excl + total));
+    }
+    // per-query output ranges: each run of one query's rows adds (end - start)
+    if (a.qcount && fits) {
+        for (int i = threadIdx.x; i < n; i += kStepThreads) {
+            const uint32_t q = B.q[i];
+            if (i == 0 || B.q[i - 1] != q) {
+                atomicMin(a.qfirst + q, (unsigned long long)(excl + B.pre[i]));
+                atomicAdd(a.qcount + q, (unsigned long long)(0 - (excl + B.pre[i])));
+            }
+            if (i == n - 1 || B.q[i + 1] != q) atomicAdd(a.qcount + q, (unsigned long long)(excl + B.pre[i + 1]));
+        }
+    }
+    // long lists -> slices on the queue (fields first, then the epoch tag)
+    if (S.has_heavy && fits) {
+        for (int i = threadIdx.x; i < n; i += kStepThreads) {
+            const uint32_t c = B.cnt[i];
+            if (c <= (uint32_t)kHeavyRows) continue;
+            const uint32_t nch = (c + kHeavyChunk - 1) / kHeavyChunk;
+            const unsigned long long at = atomicAdd(&a.ctl->heavy_n, (unsigned long long)nch);
+            for (uint32_t k = 0; k < nch; ++k) {
+                if (at + k >= a.heavy_cap) {
+                    atomicOr(&a.ctl->err, kErrOverflow);
+                    break;
+                }
+                HeavyItem* it = a.heavy + at + k;
+                it->in_row = r0 + i;
+                it->off = B.off[i] + (uint64_t)k * kHeavyChunk;
+                it->out_pos = excl + B.pre[i] + (uint64_t)k * kHeavyChunk;
+                it->count = min((uint32_t)kHeavyChunk, c - k * kHeavyChunk);
+                it->q = B.q[i];
+                __threadfence();
+                *(volatile uint32_t*)&it->tag = epoch;
+            }
+        }
+    }
+    WK_PH(5);
+    // write the short-list rows: stride w_out, zero past the query's width
+    if (fits && ltotal) {
+        const bool contiguous = !S.has_heavy;
+        const uint64_t* lp = contiguous ? B.pre : B.lpre;
+        for (uint64_t c0 = 0; c0 < ltotal; c0 += chunk_rows) {
+            const int m = (int)min((uint64_t)chunk_rows, ltotal - c0);
+            for (int j = threadIdx.x; j < m; j += kStepThreads) {
+                const uint64_t o = c0 + j;
+                int lo = 0, hi = n;   // lp[lo] <= o < lp[hi]
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (lp[mid] <= o) lo = mid; else hi = mid;
+                }
+                const uint64_t k = o - lp[lo];
+                const uint32_t meta = B.meta[lo];
+                const int opv = meta & 0xFF, cin = (meta >> 8) & 0xFF;
+                uint32_t* dst = s_out + (size_t)j * wo;
+                const uint32_t* sr = B.in + lo * wi;
+                int c = 0;
+                if (opv != kXStart)
+                    for (; c < cin; ++c) dst[c] = sr[c];
+                if (opv == kXStart || opv == kXK2U) dst[c++] = __ldg(a.store.edges + B.off[lo] + k);
+                for (; c < wo; ++c) dst[c] = 0;
+                const uint64_t pos = excl + B.pre[lo] + k;
+                s_pos[j] = pos;
+                if (a.owner_out) a.owner_out[pos] = B.q[lo];
+            }
+            __syncthreads();
+            if (contiguous) {
+                store_words(a.out + (excl + c0) * wo, s_out, (uint64_t)m * wo);
+            } else {
+                for (int e = threadIdx.x; e < m * wo; e += kStepThreads) {
+                    const int j = e / wo, c = e - j * wo;
+                    a.out[s_pos[j] * wo + c] = s_out[e];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {   // this tile's slices are all reserved
+        __threadfence();
+        atomicAdd(&a.ctl->tiles_done, 1ull);
+    }
+    WK_PH(6);
+}
 
 template <int L>
 __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreArgs a, int chunk_rows) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ unsigned long long s_tile, s_excl, s_alg, s_sd;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ unsigned long long s_claim, s_excl;
     __shared__ uint64_t s_warp[kStepThreads / 32];
-    __shared__ int s_has_heavy;
-    constexpr int kGroups = kStepThreads / L;
-    constexpr int kBatches = kTileRows / (kGroups * kUnroll);
-    static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
+    __shared__ TileState s_ts[2];
 
     const int wi = a.virtual_rows ? 0 : a.w_in, wo = a.w_out;
-    uint32_t* s_in = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* s_pre = reinterpret_cast<uint64_t*>(s_in + ((kTileRows * wi + 3) & ~3));
-    uint64_t* s_lpre = s_pre + kTileRows + 2;
-    uint64_t* s_off = s_lpre + kTileRows + 2;
-    uint64_t* s_pos = s_off + kTileRows;
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_pos + chunk_rows);
-    uint32_t* s_lcnt = s_cnt + kTileRows;
-    uint32_t* s_q = s_lcnt + kTileRows;
-    uint32_t* s_meta = s_q + kTileRows;   // op | cin << 8 | cout << 16
-    uint32_t* s_out = s_meta + kTileRows;
+    const size_t buf_words = (((size_t)kTileRows * wi + 3) & ~(size_t)3) + 4 * (kTileRows + 2) +
+                             2 * kTileRows + 4 * kTileRows;
+    uint32_t* base = reinterpret_cast<uint32_t*>(smem);
+    uint64_t* s_pos = reinterpret_cast<uint64_t*>(base + 2 * buf_words);
+    uint32_t* s_out = reinterpret_cast<uint32_t*>(s_pos + chunk_rows);
 
     const unsigned epoch = *(volatile unsigned*)&a.ctl->epoch;
     uint64_t R = a.virtual_rows ? a.n_queries : *(volatile const uint64_t*)a.in_rows;
@@ -61,225 +366,40 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
         ntiles = 0;
     }
     if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = 0;
-    if (threadIdx.x == 0) mbar_init(&s_bar, 1);
+    WK_PH_DECL
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+    }
+    unsigned phases = 0;   // mbarrier phase bit of each tile buffer
+
+    // Two tiles in flight per CTA: the front half of the next tile runs before the back half
+    // of the current one, so the look-back and the row copy of one overlap the other's probes.
+    if (threadIdx.x == 0) s_claim = atomicAdd(&a.ctl->tile_counter, 1ull);
     __syncthreads();
-    const int grp = threadIdx.x / L;
-    const int h = threadIdx.x & (L - 1);
-    unsigned phase = 0;
-
-    for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(&a.ctl->tile_counter, 1ull);
+    uint64_t cur = s_claim;
+    int b = 0;
+    WK_PH(0);
+    if (cur < ntiles) tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], cur, R, wi, epoch, s_warp);
+    while (cur < ntiles) {
+        if (threadIdx.x == 0) s_claim = atomicAdd(&a.ctl->tile_counter, 1ull);
         __syncthreads();
-        const uint64_t tile = s_tile;
-        if (tile >= ntiles) break;
-        const uint64_t r0 = tile * kTileRows;
-        const int n = (int)min((uint64_t)kTileRows, R - r0);
-        const uint32_t* src = a.in + r0 * (uint64_t)wi;
-
-        // 1. rows -> shared memory, asynchronously; owners; zero counts
-        if (threadIdx.x == 0) {
-            if (wi) {
-                const unsigned bytes = (unsigned)(((uint64_t)n * wi * 4 + 15) & ~15ull);
-                mbar_expect_tx(&s_bar, bytes);
-                tma_load_1d(s_in, src, bytes, &s_bar);
-            }
-            s_alg = 0;
-            s_sd = 0;
-            s_has_heavy = 0;
-        }
-        for (int i = threadIdx.x; i < n; i += kStepThreads) {
-            s_q[i] = a.virtual_rows ? (uint32_t)(r0 + i) : (a.owner_in ? __ldg(a.owner_in + r0 + i) : 0u);
-            s_cnt[i] = 0;
-        }
-        __syncthreads();
-
-        // 2-3. probe and count; start columns straight from global memory
-#pragma unroll 1
-        for (int b = 0; b < kBatches; ++b) {
-            uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
-            bool valid[kUnroll], pending[kUnroll];
-            int row[kUnroll];
-            uint32_t target[kUnroll], op[kUnroll];
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                row[u] = (b * kUnroll + u) * kGroups + grp;
-                valid[u] = row[u] < n;
-                const StepDesc* d = a.desc ? a.desc + (valid[u] ? s_q[row[u]] : 0) : &a.one;
-                op[u] = valid[u] ? d->op : kXDone;
-                if (op[u] == kXDone) valid[u] = false;
-                const SegDesc* sg = &d->seg;
-                target[u] = d->end_const;
-                if (op[u] == kXStart) {
-                    key[u] = d->start_key;
-                } else {
-                    const uint32_t* rin = src + (uint64_t)row[u] * wi;
-                    const uint32_t cur = valid[u] ? __ldg(rin + d->cs) : kBlankId;
-                    if (op[u] == kXK2K && valid[u]) target[u] = __ldg(rin + d->ce);
-                    if (op[u] == kXK2U && d->type_index) {
-                        // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-                        key[u] = make_key(0, cur, kIn);
-                        sg = &a.seg_index[kIn];
-                        if (cur >= (1u << kNbitsIdx)) valid[u] = false;
-                    } else {
-                        key[u] = make_key(cur, d->pid, d->dir);
-                        if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
-                    }
-                    if (cur == kBlankId) valid[u] = false;
-                }
-                pending[u] = valid[u] && sg->num_buckets != 0 && key[u] != 0;
-                bucket[u] = pending[u] ? bucket_of(key[u], *sg) : 0;
-                if (h == 0 && row[u] < n)
-                    s_meta[row[u]] = op[u] | ((uint32_t)d->cin << 8) | ((uint32_t)d->cout << 16);
-            }
-            group_probe<L>(a.store, key, bucket, pending, ptr, &a.ctl->err);
-            uint64_t off[kUnroll], deg[kUnroll];
-            bool has[kUnroll], found[kUnroll];
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-                off[u] = ptr_off(ptr[u]);
-                deg[u] = ptr_size(ptr[u]);
-                if (off[u] + deg[u] > a.store.n_edges) {
-                    if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
-                    deg[u] = 0;
-                }
-                has[u] = valid[u] && deg[u] > 0 && (op[u] == kXK2K || op[u] == kXK2C);
-            }
-            group_member<L>(a.store.edges, off, deg, target, has, a.sorted_lists != 0, found);
-            if (h == 0) {
-                unsigned long long alg = 0, sd = 0;
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
-                    if (valid[u]) {
-                        const bool filt = op[u] == kXK2K || op[u] == kXK2C;
-                        const uint32_t cnt = filt ? (found[u] ? 1u : 0u) : (uint32_t)deg[u];
-                        const uint32_t meta = s_meta[row[u]];
-                        s_off[row[u]] = off[u];
-                        s_cnt[row[u]] = cnt;
-                        sd += deg[u];
-                        alg += ((meta >> 8) & 0xFF) * 4ull + 16 + deg[u] * 4 +
-                               (unsigned long long)cnt * ((meta >> 16) & 0xFF) * 4;
-                    }
-                if (alg) {
-                    atomicAdd(&s_alg, alg);
-                    atomicAdd(&s_sd, sd);
-                }
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kStepThreads) {
-            const uint32_t c = s_cnt[i];
-            const bool heavy = c > (uint32_t)kHeavyRows;
-            s_lcnt[i] = heavy ? 0u : c;
-            if (heavy) s_has_heavy = 1;
-        }
-        __syncthreads();
-
-        // 4. positions
-        const uint64_t total = block_scan(s_cnt, s_pre, n, s_warp);
-        const uint64_t ltotal = s_has_heavy ? block_scan(s_lcnt, s_lpre, n, s_warp) : total;
-        if (threadIdx.x < 32) {
-            const uint64_t ex = lookback_warp(a.status, a.ctl, tile, total, epoch);
-            if (threadIdx.x == 0) {
-                s_excl = ex;
-                atomicAdd(&a.ctl->alg_bytes, s_alg);
-                atomicAdd(&a.ctl->sum_deg, s_sd);
-            }
-        }
-        if (wi) mbar_wait(&s_bar, phase, &a.ctl->err);   // the tile's rows are in shared memory
-        phase ^= wi ? 1u : 0u;
-        __syncthreads();
-        const uint64_t excl = s_excl;
-        if (tile == ntiles - 1 && threadIdx.x == 0) *a.out_rows = excl + total;
-        const bool fits = excl + total <= a.out_cap_rows;
-        if (!fits && threadIdx.x == 0) {
-            atomicOr(&a.ctl->err, kErrOverflow);
-            atomicMax(&a.ctl->need, (unsigned long long)(excl + total));
-        }
-        // per-query output ranges: each run of one query's rows adds (end - start)
-        if (a.qcount && fits) {
-            for (int i = threadIdx.x; i < n; i += kStepThreads) {
-                const uint32_t q = s_q[i];
-                if (i == 0 || s_q[i - 1] != q) {
-                    atomicMin(a.qfirst + q, (unsigned long long)(excl + s_pre[i]));
-                    atomicAdd(a.qcount + q, (unsigned long long)(0 - (excl + s_pre[i])));
-                }
-                if (i == n - 1 || s_q[i + 1] != q) atomicAdd(a.qcount + q, (unsigned long long)(excl + s_pre[i + 1]));
-            }
-        }
-        // long lists -> slices on the queue (fields first, then the epoch tag)
-        if (s_has_heavy && fits) {
-            for (int i = threadIdx.x; i < n; i += kStepThreads) {
-                const uint32_t c = s_cnt[i];
-                if (c <= (uint32_t)kHeavyRows) continue;
-                const uint32_t nch = (c + kHeavyChunk - 1) / kHeavyChunk;
-                const unsigned long long at = atomicAdd(&a.ctl->heavy_n, (unsigned long long)nch);
-                for (uint32_t k = 0; k < nch; ++k) {
-                    if (at + k >= a.heavy_cap) {
-                        atomicOr(&a.ctl->err, kErrOverflow);
-                        break;
-                    }
-                    HeavyItem* it = a.heavy + at + k;
-                    it->in_row = r0 + i;
-                    it->off = s_off[i] + (uint64_t)k * kHeavyChunk;
-                    it->out_pos = excl + s_pre[i] + (uint64_t)k * kHeavyChunk;
-                    it->count = min((uint32_t)kHeavyChunk, c - k * kHeavyChunk);
-                    it->q = s_q[i];
-                    __threadfence();
-                    *(volatile uint32_t*)&it->tag = epoch;
-                }
-            }
-        }
-
-        // 5. write the short-list rows: stride w_out, zero past the query's width
-        if (fits && ltotal) {
-            const bool contiguous = !s_has_heavy;
-            const uint64_t* lp = contiguous ? s_pre : s_lpre;
-            for (uint64_t c0 = 0; c0 < ltotal; c0 += chunk_rows) {
-                const int m = (int)min((uint64_t)chunk_rows, ltotal - c0);
-                for (int j = threadIdx.x; j < m; j += kStepThreads) {
-                    const uint64_t o = c0 + j;
-                    int lo = 0, hi = n;   // lp[lo] <= o < lp[hi]
-                    while (hi - lo > 1) {
-                        const int mid = (lo + hi) >> 1;
-                        if (lp[mid] <= o) lo = mid; else hi = mid;
-                    }
-                    const uint64_t k = o - lp[lo];
-                    const uint32_t meta = s_meta[lo];
-                    const int opv = meta & 0xFF, cin = (meta >> 8) & 0xFF;
-                    uint32_t* dst = s_out + (size_t)j * wo;
-                    const uint32_t* sr = s_in + lo * wi;
-                    int c = 0;
-                    if (opv != kXStart)
-                        for (; c < cin; ++c) dst[c] = sr[c];
-                    if (opv == kXStart || opv == kXK2U) dst[c++] = __ldg(a.store.edges + s_off[lo] + k);
-                    for (; c < wo; ++c) dst[c] = 0;
-                    const uint64_t pos = excl + s_pre[lo] + k;
-                    s_pos[j] = pos;
-                    if (a.owner_out) a.owner_out[pos] = s_q[lo];
-                }
-                __syncthreads();
-                if (contiguous) {
-                    store_words(a.out + (excl + c0) * wo, s_out, (uint64_t)m * wo);
-                } else {
-                    for (int e = threadIdx.x; e < m * wo; e += kStepThreads) {
-                        const int j = e / wo, c = e - j * wo;
-                        a.out[s_pos[j] * wo + c] = s_out[e];
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {   // this tile's slices are all reserved
-            __threadfence();
-            atomicAdd(&a.ctl->tiles_done, 1ull);
-        }
+        const uint64_t next = s_claim;
+        WK_PH(0);
+        if (next < ntiles)
+            tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1], next, R,
+                          wi, epoch, s_warp);
+        tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
+                     wo, chunk_rows, epoch, s_pos, s_out, &s_excl);
+        if (wi) phases ^= 1u << b;
+        cur = next;
+        b ^= 1;
     }
 
     // Out of tiles: write queued long-list slices until every tile is done and the queue is
     // drained.  A claimed index either gets reserved by a tile still running (wait for its
     // tag) or lies past the final count (stop).  Every wait is bounded.
-    __syncthreads();   // every thread has read the last s_tile before it is reused
+    __syncthreads();
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned long long idx = atomicAdd(&a.ctl->heavy_claim, 1ull);
@@ -313,10 +433,10 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
                 }
                 if (spins > 32) __nanosleep(64);
             }
-            s_tile = state == 1 ? idx : ~0ull;
+            s_claim = state == 1 ? idx : ~0ull;
         }
         __syncthreads();
-        const unsigned long long idx = s_tile;
+        const unsigned long long idx = s_claim;
         if (idx == ~0ull) break;
         const HeavyItem* it = a.heavy + idx;
         const uint64_t in_row = __ldcg((const unsigned long long*)&it->in_row);
@@ -343,6 +463,8 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
             for (uint32_t j = threadIdx.x; j < count; j += kStepThreads) a.owner_out[out_pos + j] = q;
         __syncthreads();
     }
+    WK_PH(7);
+    WK_PH_FLUSH;
     exit_protocol(a.ctl, a.status, epoch, a.heavy ? &a.heavy[0].tag : nullptr,
                   sizeof(HeavyItem) / sizeof(uint32_t), a.heavy ? a.heavy_cap : 0);
 }
@@ -358,9 +480,10 @@ size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
     int chunk = 16 * 1024 / (w_out > 0 ? w_out * 4 : 4);
     if (chunk > 1024) chunk = 1024;
     if (chunk < 64) chunk = 64;
-    size_t in_words = ((size_t)kTileRows * w_in + 3) & ~(size_t)3;
-    size_t bytes = in_words * 4 + 2 * (kTileRows + 2) * 8 + kTileRows * 8 + (size_t)chunk * 8 +
-                   4 * kTileRows * 4 + (size_t)chunk * w_out * 4;
+    // two tile buffers (rows, two scans, list offsets, four per-row words) + the write staging
+    const size_t buf_words = (((size_t)kTileRows * w_in + 3) & ~(size_t)3) + 4 * (kTileRows + 2) +
+                             2 * kTileRows + 4 * kTileRows;
+    size_t bytes = 2 * buf_words * 4 + (size_t)chunk * 8 + (size_t)chunk * w_out * 4;
     if (chunk_rows) *chunk_rows = chunk;
     return bytes;
 }
@@ -397,3 +520,16 @@ cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s) {
 }
 
 }  // namespace wk
+
+// Phase cycle counters of an instrumented build (all zero otherwise); reset clears them.
+extern "C" int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset) {
+    if (!out || n < wk::kPhaseSlots) return WK_E_BADARG;
+    if (cudaMemcpyFromSymbol(out, wk::g_phase_cycles, sizeof(unsigned long long) * wk::kPhaseSlots) !=
+        cudaSuccess)
+        return WK_E_CUDA;
+    if (reset) {
+        unsigned long long z[wk::kPhaseSlots] = {0};
+        if (cudaMemcpyToSymbol(wk::g_phase_cycles, z, sizeof(z)) != cudaSuccess) return WK_E_CUDA;
+    }
+    return WK_SUCCESS;
+}

@@ -41,6 +41,7 @@ static_assert(sizeof(HeavyItem) == 40, "HeavyItem is 40 bytes");
 
 constexpr int kHeavyRows = 128;
 constexpr int kHeavyChunk = 2048;
+constexpr int kPhaseSlots = 12;  // phase cycle counters of an instrumented build
 
 struct ExploreArgs {
     DevStore store;

@@ -13,7 +13,7 @@
 //     overflowing through slot 7 into extension buckets (insert_key_to_seg :203-271).
 // How many buckets a segment gets is this builder's own choice (the reference derives it from
 // the configured memory size, :117-163): enough for a mean fill of load_factor of the 7 data
-// slots, so chains stay rare and most probes touch one 128-byte bucket.
+// slots, so chains stay rare and most probes touch only the bucket's first sector.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -136,7 +136,9 @@ uint64_t buckets_for(uint64_t keys, double load) {
 
 int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
                  double load, wk_gstore& g) {
-    if (load <= 0) load = 0.5;
+    // Default: about 1.4 keys per bucket, so nearly every key sits in the bucket's first
+    // 32-byte sector (slots 0-1) and a probe is one request; HBM is plentiful, latency is not.
+    if (load <= 0) load = 0.2;
     if (load > 1) return WK_E_BADARG;
     const size_t np = (size_t)1 << kNbitsIdx;
     DirLists outl, inl;

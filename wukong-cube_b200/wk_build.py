@@ -41,29 +41,35 @@ def _stale(target, deps):
     return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
 
 
-def build_lib(verbose=False, force=False):
-    os.makedirs(OBJ, exist_ok=True)
+def build_lib(verbose=False, force=False, variant=None, defines=()):
+    """Build the library; `variant` names an extra build (objects in _build/<variant>, library
+    libwukong_b200_<variant>.so) compiled with the given -D defines."""
+    obj = os.path.join(OBJ, variant) if variant else OBJ
+    lib = os.path.join(HERE, "libwukong_b200_%s.so" % variant) if variant else LIB
+    dflags = ["-D" + d for d in defines]
+    os.makedirs(obj, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "wukong_b200.h")]
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(obj, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            out = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                                        "-Xptxas", "-v", "-c", s, "-o", o])
+            out = _run([NVCC] + ARCH + dflags + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                                 "-Xptxas", "-v", "-c", s, "-o", o])
             if verbose:
                 print(out)
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(obj, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
-            _run([CXX, "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wno-unused-function",
-                  "-I" + os.path.join(CUDA_HOME, "include"), "-c", s, "-o", o])
-    if force or _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
-    return LIB
+            _run([CXX] + dflags + ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall",
+                                   "-Wno-unused-function", "-I" + os.path.join(CUDA_HOME, "include"),
+                                   "-c", s, "-o", o])
+    if force or _stale(lib, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"])
+    return lib
 
 
 def build_oracle():

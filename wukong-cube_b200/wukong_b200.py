@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libwukong_b200.so")
+# WK_LIB_PATH selects another build of the library (e.g. an instrumented variant)
+LIB_PATH = os.environ.get("WK_LIB_PATH") or os.path.join(HERE, "libwukong_b200.so")
 
 IN, OUT = 0, 1
 PREDICATE_ID, TYPE_ID = 0, 1
@@ -152,6 +153,9 @@ _SIGS = {
     "wk_batch_execute_device": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32,
                                           C.POINTER(C.c_uint64)]),
     "wk_batch_replay": (C.c_int, [_P]),
+    "wk_debug_phase_cycles": (C.c_int, [C.POINTER(C.c_ulonglong), C.c_int32, C.c_int32]),
+    "wk_ctx_tune_set": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "wk_ctx_tune_get": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32)]),
     "wk_batch_profile": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32,
                                    C.POINTER(StepProf), C.c_int32, C.POINTER(C.c_int32)]),
     "wk_serve_run_open_loop": (C.c_int, [_P, C.POINTER(ServeConfig), C.POINTER(QueryC),
@@ -287,6 +291,17 @@ class Query:
         return q
 
 
+PHASES = ["claim", "stage", "probe_tail", "scan", "lookback", "ranges", "write", "drain",
+          "probe_setup", "probe_walk", "membership", "spare"]
+
+
+def phase_cycles(reset=True):
+    """Per-phase cycle totals of the exploration launch (instrumented builds only)."""
+    arr = (C.c_ulonglong * len(PHASES))()
+    _check(lib().wk_debug_phase_cycles(arr, len(PHASES), 1 if reset else 0))
+    return dict(zip(PHASES, list(arr)))
+
+
 def validate(q, max_cols=32):
     """Plan check without a device: (status, v2c_map, col_num)."""
     qc = q.as_c()
@@ -368,6 +383,14 @@ class Context:
 
     def check(self):
         _check(lib().wk_ctx_check(self.h), self.h)
+
+    def tune_set(self, knob, value):
+        _check(lib().wk_ctx_tune_set(self.h, knob, value), self.h)
+
+    def tune_get(self, knob):
+        v = C.c_int32()
+        _check(lib().wk_ctx_tune_get(self.h, knob, C.byref(v)), self.h)
+        return v.value
 
     def upload_gstore(self, g):
         _check(lib().wk_store_upload_gstore(self.h, g.h), self.h)
