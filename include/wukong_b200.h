@@ -130,13 +130,18 @@ typedef struct wk_synth_vocab {
     uint32_t next_vid;      /* one past the last vertex id */
 } wk_synth_vocab;
 
-/* Serving configuration (wk_serve_run_open_loop). */
+/* Serving configuration (wk_serve_run_open_loop).  Zero fields take defaults. */
 typedef struct wk_serve_config {
     uint64_t working_set_cap_bytes;   /* admission cap on projected table bytes (40 GiB) */
-    uint64_t light_arena_bytes;       /* bytes of each light ping-pong arena (default 1 GiB) */
-    uint32_t max_inflight;            /* light queries resident at once (default 65536) */
-    uint32_t heavy_rows_per_iter;     /* heavy-step input rows per iteration (default 1<<20) */
-    int32_t reserved[6];
+    uint64_t arena_bytes;             /* initial bytes of each of the two table arenas (1 GiB);
+                                         they grow up to the cap when a step needs more */
+    uint64_t light_proj_bytes;        /* projected bytes of a query that starts from a
+                                         constant (256 KiB) */
+    uint64_t heavy_proj_bytes;        /* projected bytes of one that starts from an index
+                                         (256 MiB) */
+    uint32_t max_inflight;            /* queries resident at once (default 65536) */
+    uint32_t max_heavy_inflight;      /* index-start queries resident at once (default 4) */
+    int32_t reserved[4];
 } wk_serve_config;
 
 /* Per-query outcome of a batch or a serving run. */
@@ -300,7 +305,8 @@ int wk_batch_execute_device(wk_ctx* ctx, const wk_query* queries, uint32_t n,
  * device-side timing of an identical batch; errors surface through wk_ctx_check). */
 int wk_batch_replay(wk_ctx* ctx);
 /* Per-level profile of a batch: each level launch between CUDA events on the context stream,
- * averaged over `iters` runs after one warm-up; out[k].kind = 5. */
+ * averaged over `iters` runs after one warm-up; out[k].kind = 5, followed by three entries
+ * timing the setup memsets (kind 6), the result scan (7) and the gather (8). */
 int wk_batch_profile(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters,
                      wk_step_prof* out, int32_t max_levels, int32_t* n_levels);
 

@@ -270,6 +270,7 @@ int upload_plan(wk_ctx* ctx, BatchState* b, const Plan& P) {
 // Events and counter read-backs around each level launch (profiling runs only).
 struct ProfHooks {
     cudaEvent_t ev[2 * kMaxBatchLevels];
+    cudaEvent_t extra[6];        // around the setup memsets, the result scan, the gather
     unsigned long long* h_cnt;   // pinned [kMaxBatchLevels][2]: sum_deg, alg_bytes
 };
 
@@ -280,8 +281,10 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
     cudaStream_t s = ctx->stream;
     uint64_t region_off[kMaxBatchLevels + 1] = {0};
     for (int k = 0; k < L; ++k) region_off[k + 1] = region_off[k] + b->rows_cap * (uint64_t)P.width[k];
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[0], s));
     WKB_CUDA(ctx, cudaMemsetAsync(b->d_qfirst, 0xFF, 8ull * L * n, s));
     WKB_CUDA(ctx, cudaMemsetAsync(b->d_qcount, 0, 8ull * L * n, s));
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[1], s));
     const int lanes = ctx->batch_lanes;
     for (int k = 0; k < L; ++k) {
         wk::ExploreArgs a{};
@@ -332,8 +335,10 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
     ra.final_base = b->d_final_base;
     ra.final_rows = b->d_final_rows;
     ra.res_off = b->d_res_off;
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[2], s));
     cudaError_t e = wk::launch_result_scan(ra, s);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "result scan launch");
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[3], s));
     wk::GatherArgs ga{};
     ga.n = n;
     ga.final_level = b->d_final_level;
@@ -348,8 +353,10 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
     ga.out = b->d_result;
     ga.out_cap = b->result_cap;
     ga.ctl = ctx->d_ctl;
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[4], s));
     e = wk::launch_gather(ga, std::min<uint32_t>((n + 7) / 8, 4096), s);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "gather launch");
+    if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[5], s));
     return WK_SUCCESS;
 }
 
@@ -508,18 +515,23 @@ extern "C" int wk_batch_profile(wk_ctx* ctx, const wk_query* queries, uint32_t n
     Plan P;
     int rc = run_batch(ctx, b, queries, n, P);   // sizes the buffers
     if (rc) return rc;
-    if (P.levels > max_levels) return ctx->fail(WK_E_CAPACITY, "profile array too small");
+    if (P.levels + 3 > max_levels) return ctx->fail(WK_E_CAPACITY, "profile array too small");
     ProfHooks ph;
     for (auto& e : ph.ev) WKB_CUDA(ctx, cudaEventCreate(&e));
+    for (auto& e : ph.extra) WKB_CUDA(ctx, cudaEventCreate(&e));
     WKB_CUDA(ctx, cudaMallocHost(&ph.h_cnt, sizeof(unsigned long long) * 2 * kMaxBatchLevels));
-    std::vector<double> acc(P.levels, 0.0);
+    std::vector<double> acc(P.levels + 3, 0.0);
     for (int it = 0; it <= iters && rc == WK_SUCCESS; ++it) {
         rc = enqueue_batch(ctx, b, P, &ph);
         if (rc) break;
         WKB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        for (int k = 0; k < P.levels; ++k) {
+        for (int k = 0; k < P.levels + 3; ++k) {
             float ms = 0;
-            WKB_CUDA(ctx, cudaEventElapsedTime(&ms, ph.ev[2 * k], ph.ev[2 * k + 1]));
+            if (k < P.levels)
+                WKB_CUDA(ctx, cudaEventElapsedTime(&ms, ph.ev[2 * k], ph.ev[2 * k + 1]));
+            else
+                WKB_CUDA(ctx, cudaEventElapsedTime(&ms, ph.extra[2 * (k - P.levels)],
+                                                   ph.extra[2 * (k - P.levels) + 1]));
             if (it > 0) acc[k] += ms;
         }
     }
@@ -538,17 +550,17 @@ extern "C" int wk_batch_profile(wk_ctx* ctx, const wk_query* queries, uint32_t n
             p.alg_bytes = ph.h_cnt[2 * k + 1];
             p.ms = acc[k] / iters;
         }
-        if (n_levels) *n_levels = P.levels;
+        for (int k = 0; k < 3; ++k) {   // setup memsets, result scan, gather
+            wk_step_prof& p = out[P.levels + k];
+            std::memset(&p, 0, sizeof(p));
+            p.kind = 6 + k;
+            p.ms = acc[P.levels + k] / iters;
+        }
+        if (n_levels) *n_levels = P.levels + 3;
     }
+    for (auto& e : ph.extra) cudaEventDestroy(e);
     for (auto& e : ph.ev) cudaEventDestroy(e);
     cudaFreeHost(ph.h_cnt);
     return rc;
 }
 
-extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg, const wk_query* queries,
-                                      uint32_t n, const double* arrival_us, uint32_t* host_out,
-                                      uint64_t cap_elems, wk_qresult* results) {
-    (void)ctx; (void)cfg; (void)queries; (void)n; (void)arrival_us; (void)host_out; (void)cap_elems;
-    (void)results;
-    return WK_E_UNSUPPORTED;
-}

@@ -65,6 +65,17 @@ __shared__ long long s_ph_t;
     } while (0)
 #endif
 
+// The step every row of a finished query runs: nothing.
+__constant__ StepDesc c_done = {{0, 0, 0, 0}, 0, 0, 0, kXDone, 0, 0, 0, 0, 0, 0, 0, 0};
+
+// Step of query q at this launch.
+__device__ __forceinline__ const StepDesc* step_desc(const ExploreArgs& a, uint32_t q) {
+    if (!a.desc) return &a.one;
+    if (!a.desc_stride) return a.desc + q;
+    const uint32_t st = a.iter - __ldg(a.q_admit + q);
+    return st < a.desc_stride ? a.desc + (size_t)q * a.desc_stride + st : &c_done;
+}
+
 // Per-tile state kept in shared memory while the tile is between its front and back halves.
 struct TileState {
     unsigned long long tile;
@@ -127,7 +138,8 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         S.has_heavy = 0;
     }
     for (int i = threadIdx.x; i < n; i += kStepThreads) {
-        B.q[i] = a.virtual_rows ? (uint32_t)(r0 + i) : (a.owner_in ? __ldg(a.owner_in + r0 + i) : 0u);
+        B.q[i] = a.virtual_rows ? (a.virt_owner ? __ldg(a.virt_owner + r0 + i) : (uint32_t)(r0 + i))
+                                : (a.owner_in ? __ldg(a.owner_in + r0 + i) : 0u);
         B.cnt[i] = 0;
     }
     __syncthreads();
@@ -141,7 +153,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         for (int u = 0; u < kUnroll; ++u) {
             row[u] = (b * kUnroll + u) * kGroups + grp;
             valid[u] = row[u] < n;
-            const StepDesc* d = a.desc ? a.desc + (valid[u] ? B.q[row[u]] : 0) : &a.one;
+            const StepDesc* d = step_desc(a, valid[u] ? B.q[row[u]] : 0);
             op[u] = valid[u] ? d->op : kXDone;
             if (op[u] == kXDone) valid[u] = false;
             const SegDesc* sg = &d->seg;
@@ -237,7 +249,7 @@ template <int L>
 __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B, TileState& S,
                                           uint64_t* bar, unsigned phase, uint64_t ntiles, int wi,
                                           int wo, int chunk_rows, unsigned epoch, uint64_t* s_pos,
-                                          uint32_t* s_out, unsigned long long* s_excl) {
+                                          uint32_t* s_out, unsigned long long* s_excl, uint64_t obase) {
     const uint64_t tile = S.tile;
     const int n = S.n;
     const uint64_t total = S.total, ltotal = S.ltotal;
@@ -253,7 +265,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     if (wi) mbar_wait(bar, phase, &a.ctl->err);   // the tile's rows are in shared memory
     __syncthreads();
     WK_PH(4);
-    const uint64_t excl = *s_excl;
+    const uint64_t excl = *s_excl + obase;   // output positions start at the launch's base row
     if (tile == ntiles - 1 && threadIdx.x == 0) *a.out_rows = excl + total;
     const bool fits = excl + total <= a.out_cap_rows;
     if (!fits && threadIdx.x == 0) {
@@ -343,7 +355,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
 }
 
 template <int L>
-__global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreArgs a, int chunk_rows) {
+__global__ void __launch_bounds__(kStepThreads, 6) explore_kernel(const ExploreArgs a, int chunk_rows) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ unsigned long long s_claim, s_excl;
@@ -365,7 +377,8 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
         if (threadIdx.x == 0) atomicOr(&a.ctl->err, kErrStatus);
         ntiles = 0;
     }
-    if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = 0;
+    const uint64_t obase = a.out_base_rows ? *(volatile const uint64_t*)a.out_base_rows : 0;
+    if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = obase;
     WK_PH_DECL
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
@@ -390,7 +403,7 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
             tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1], next, R,
                           wi, epoch, s_warp);
         tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
-                     wo, chunk_rows, epoch, s_pos, s_out, &s_excl);
+                     wo, chunk_rows, epoch, s_pos, s_out, &s_excl, obase);
         if (wi) phases ^= 1u << b;
         cur = next;
         b ^= 1;
@@ -444,7 +457,7 @@ __global__ void __launch_bounds__(kStepThreads, 3) explore_kernel(const ExploreA
         const uint64_t out_pos = __ldcg((const unsigned long long*)&it->out_pos);
         const uint32_t count = __ldcg((const unsigned int*)&it->count);
         const uint32_t q = __ldcg((const unsigned int*)&it->q);
-        const StepDesc* d = a.desc ? a.desc + q : &a.one;
+        const StepDesc* d = step_desc(a, q);
         const int opv = d->op, cin = d->cin;
         if (opv != kXStart && threadIdx.x < cin) s_out[threadIdx.x] = __ldg(a.in + in_row * (uint64_t)a.w_in + threadIdx.x);
         __syncthreads();
@@ -477,8 +490,8 @@ cudaError_t set_attr(int bytes) {
 }  // namespace
 
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
-    int chunk = 16 * 1024 / (w_out > 0 ? w_out * 4 : 4);
-    if (chunk > 1024) chunk = 1024;
+    int chunk = 8 * 1024 / (w_out > 0 ? w_out * 4 : 4);
+    if (chunk > 512) chunk = 512;
     if (chunk < 64) chunk = 64;
     // two tile buffers (rows, two scans, list offsets, four per-row words) + the write staging
     const size_t buf_words = (((size_t)kTileRows * w_in + 3) & ~(size_t)3) + 4 * (kTileRows + 2) +

@@ -48,8 +48,15 @@ struct ExploreArgs {
     SegDesc seg_index[2];        // index segment of each direction
     StepDesc one;                // the step of every row when desc is null
     const StepDesc* desc;        // [n_queries] this level's step per query, or null
+    // Continuous batching: when desc_stride > 0, query q's step is
+    // desc[q * desc_stride + (iter - q_admit[q])] (kXDone past the plan).
+    uint32_t desc_stride;
+    uint32_t iter;
+    const uint32_t* q_admit;
     uint32_t n_queries;
-    int32_t virtual_rows;        // input row r is query r's start row (no input table)
+    int32_t virtual_rows;        // input row r is a start row (no input table)
+    const uint32_t* virt_owner;  // owner query of virtual row r, or null (query r)
+    const uint64_t* out_base_rows;   // first output row, read at launch (null: 0)
     const uint64_t* in_rows;     // device row count of the input (unused for virtual rows)
     const uint32_t* owner_in;    // owner query of each input row, or null (query 0)
     const uint32_t* in;          // input rows, stride w_in (tables carry >= 64 B of padding)

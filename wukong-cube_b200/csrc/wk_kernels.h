@@ -13,6 +13,7 @@ enum : uint32_t {
     kErrTimeout = 2u,    // a bounded wait (tile look-back) gave up
     kErrCorrupt = 4u,    // a key-table chain left the slot array or exceeded the hop limit
     kErrStatus = 8u,     // more tiles than the status array holds (host grows it and reruns)
+    kErrResult = 16u,    // a result gather did not fit its buffer (host grows it and reruns)
 };
 
 // Per-stream control block of the single-pass scan.  Kernels that use it reset the tile and
@@ -54,8 +55,8 @@ struct ListArgs {
 };
 
 // Launch geometry of the exploration launch.
-constexpr int kStepThreads = 256;
-constexpr int kTileRows = 512;
+constexpr int kStepThreads = 128;
+constexpr int kTileRows = 256;
 
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);

@@ -1,0 +1,499 @@
+// Serving: continuous batching of an open-loop arrival stream.
+//
+// No counterpart in the reference beyond the emulator's in-flight window
+// (ConsoleProxy::run_query_emu, console_proxy.hpp:287-439) and its latency CDF
+// (monitor.hpp:141-220).  Every iteration advances each resident query by one pattern:
+//   * queries that arrived since the last iteration are admitted while their projected table
+//     bytes fit under the working-set cap (and a cap on index-start queries in flight), get a
+//     slot, and have their planned steps installed on the device;
+//   * one exploration launch runs every continuing query's current step over its rows (taken
+//     from the previous iteration's arena, tagged with their slot), and a second one starts the
+//     newly admitted queries from their start keys, appending to the same arena;
+//   * queries whose last step ran have their tables gathered and copied to the host.
+// A query's step is iteration - admission iteration, so no per-step host upload is needed;
+// tables stay on the device between steps, light and index-start queries share iterations, and
+// their work overlaps on the device.  The integer work is the same exploration launch as the
+// single-query and batch paths, so a query's result does not depend on what it was mixed with.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <vector>
+
+#include "wk_batch.h"
+#include "wk_ctx.h"
+
+namespace wk {
+namespace {
+
+constexpr int kMaxSteps = kMaxBatchLevels;
+
+// Copy newly admitted queries' plans into their slots and stamp the admission iteration.
+__global__ void install_kernel(StepDesc* plans, uint32_t* admit, const StepDesc* stage,
+                               const uint32_t* slots, uint32_t n_new, uint32_t iter) {
+    for (uint32_t i = blockIdx.x; i < n_new; i += gridDim.x) {
+        const uint32_t s = slots[i];
+        for (int k = threadIdx.x; k < kMaxSteps; k += blockDim.x)
+            plans[(size_t)s * kMaxSteps + k] = stage[(size_t)i * kMaxSteps + k];
+        if (threadIdx.x == 0) admit[s] = iter;
+    }
+}
+
+// Rows and result offsets of the queries finishing this iteration (one CTA).
+__global__ void finish_scan_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
+                                   const unsigned long long* qcount, uint64_t* fin_rows,
+                                   uint64_t* fin_off) {
+    __shared__ uint64_t s_warp[32];
+    const uint32_t per = (n_fin + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = min(n_fin, threadIdx.x * per), i1 = min(n_fin, i0 + per);
+    uint64_t sum = 0;
+    for (uint32_t i = i0; i < i1; ++i) {
+        const uint64_t r = qcount[fin_slots[i]];
+        fin_rows[i] = r;
+        sum += r * fin_cols[i];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t w = lane < (int)(blockDim.x / 32) ? s_warp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        s_warp[lane] = w;
+    }
+    __syncthreads();
+    uint64_t run = (warp ? s_warp[warp - 1] : 0) + x - sum;
+    for (uint32_t i = i0; i < i1; ++i) {
+        fin_off[i] = run;
+        run += fin_rows[i] * fin_cols[i];
+    }
+    if (threadIdx.x == blockDim.x - 1) fin_off[n_fin] = run;
+}
+
+// Copy the finishing queries' tables (stride w in the arena) to the result buffer.
+__global__ void finish_gather_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
+                                     const unsigned long long* qfirst, const uint64_t* fin_rows,
+                                     const uint64_t* fin_off, const uint32_t* arena, int w,
+                                     uint32_t* out, uint64_t out_cap, StepCtl* ctl) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x / 32;
+    for (uint32_t i = blockIdx.x * wpb + threadIdx.x / 32; i < n_fin; i += gridDim.x * wpb) {
+        const uint64_t rows = fin_rows[i];
+        const uint32_t cols = fin_cols[i];
+        if (!rows || !cols) continue;
+        const uint64_t off = fin_off[i];
+        if (off + rows * cols > out_cap) {
+            if (lane == 0) atomicOr(&ctl->err, kErrResult);
+            continue;
+        }
+        const uint32_t* src = arena + qfirst[fin_slots[i]] * (uint64_t)w;
+        for (uint64_t r = 0; r < rows; ++r)
+            for (uint32_t c = lane; c < cols; c += 32) out[off + r * cols + c] = src[r * w + c];
+    }
+}
+
+struct QSlot {
+    uint32_t query;       // index into the caller's query array
+    uint32_t admit_iter;
+    uint32_t nsteps;
+    uint32_t cols;        // final column count
+    bool heavy;
+};
+
+#define WKS_CUDA(ctx, call)                                        \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return (ctx)->cuda_fail(e_, #call); \
+    } while (0)
+
+struct Serve {
+    wk_ctx* ctx;
+    wk_serve_config cfg;
+    uint32_t slots_n = 0;
+    int w = 1;
+    uint64_t rows_cap[2] = {0, 0};
+    StepDesc* d_plans = nullptr;
+    uint32_t* d_admit = nullptr;
+    uint32_t* d_arena[2] = {nullptr, nullptr};
+    uint32_t* d_owner[2] = {nullptr, nullptr};
+    uint64_t* d_total = nullptr;              // [2]
+    unsigned long long* d_qfirst = nullptr;   // [slots]
+    unsigned long long* d_qcount = nullptr;   // [slots]
+    uint32_t* d_new = nullptr;                // [slots]
+    StepDesc* d_stage = nullptr;              // [slots][kMaxSteps]
+    uint32_t* d_fin_slots = nullptr;          // [slots]
+    uint32_t* d_fin_cols = nullptr;           // [slots]
+    uint64_t* d_fin_rows = nullptr;           // [slots]
+    uint64_t* d_fin_off = nullptr;            // [slots + 1]
+    uint32_t* d_result = nullptr;
+    uint64_t result_cap = 0;
+    // pinned host staging
+    StepDesc* h_stage = nullptr;
+    uint32_t* h_new = nullptr;
+    uint32_t* h_fin_slots = nullptr;
+    uint32_t* h_fin_cols = nullptr;
+    uint64_t* h_fin_rows = nullptr;
+    uint64_t* h_fin_off = nullptr;
+    uint64_t* h_total = nullptr;
+    uint32_t* h_result = nullptr;
+
+    ~Serve() {
+        auto f = [](void* p) { if (p) cudaFree(p); };
+        auto fh = [](void* p) { if (p) cudaFreeHost(p); };
+        f(d_plans); f(d_admit); f(d_arena[0]); f(d_arena[1]); f(d_owner[0]); f(d_owner[1]);
+        f(d_total); f(d_qfirst); f(d_qcount); f(d_new); f(d_stage); f(d_fin_slots); f(d_fin_cols);
+        f(d_fin_rows); f(d_fin_off); f(d_result);
+        fh(h_stage); fh(h_new); fh(h_fin_slots); fh(h_fin_cols); fh(h_fin_rows); fh(h_fin_off);
+        fh(h_total); fh(h_result);
+    }
+
+    int alloc_arena(int k, uint64_t rows) {
+        if (d_arena[k]) cudaFree(d_arena[k]);
+        if (d_owner[k]) cudaFree(d_owner[k]);
+        d_arena[k] = nullptr;
+        d_owner[k] = nullptr;
+        rows = (rows + 15) & ~15ull;
+        if (cudaMalloc(&d_arena[k], rows * w * 4 + 256) != cudaSuccess ||
+            cudaMalloc(&d_owner[k], rows * 4 + 64) != cudaSuccess) {
+            cudaGetLastError();
+            return ctx->fail(WK_E_OOM, "serving arena");
+        }
+        rows_cap[k] = rows;
+        return WK_SUCCESS;
+    }
+
+    int alloc_result(uint64_t elems) {
+        if (d_result) cudaFree(d_result);
+        if (h_result) cudaFreeHost(h_result);
+        d_result = nullptr;
+        h_result = nullptr;
+        if (cudaMalloc(&d_result, elems * 4 + 64) != cudaSuccess ||
+            cudaMallocHost(&h_result, elems * 4 + 64) != cudaSuccess) {
+            cudaGetLastError();
+            return ctx->fail(WK_E_OOM, "serving result buffer");
+        }
+        result_cap = elems;
+        return WK_SUCCESS;
+    }
+
+    int init(uint32_t slots, int width) {
+        slots_n = slots;
+        w = std::max(width, 1);
+        auto dm = [&](void** p, size_t bytes) {
+            if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            return true;
+        };
+        auto hm = [&](void** p, size_t bytes) { return cudaMallocHost(p, std::max<size_t>(bytes, 16)) == cudaSuccess; };
+        bool ok = dm((void**)&d_plans, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
+                  dm((void**)&d_admit, 4ull * slots) && dm((void**)&d_total, 16) &&
+                  dm((void**)&d_qfirst, 8ull * slots) && dm((void**)&d_qcount, 8ull * slots) &&
+                  dm((void**)&d_new, 4ull * slots) &&
+                  dm((void**)&d_stage, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
+                  dm((void**)&d_fin_slots, 4ull * slots) && dm((void**)&d_fin_cols, 4ull * slots) &&
+                  dm((void**)&d_fin_rows, 8ull * slots) && dm((void**)&d_fin_off, 8ull * (slots + 1)) &&
+                  hm((void**)&h_stage, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
+                  hm((void**)&h_new, 4ull * slots) && hm((void**)&h_fin_slots, 4ull * slots) &&
+                  hm((void**)&h_fin_cols, 4ull * slots) && hm((void**)&h_fin_rows, 8ull * slots) &&
+                  hm((void**)&h_fin_off, 8ull * (slots + 1)) && hm((void**)&h_total, 16);
+        if (!ok) return ctx->fail(WK_E_OOM, "serving buffers");
+        const uint64_t rows = std::max<uint64_t>(cfg.arena_bytes / (4ull * w), 1 << 16);
+        int rc = alloc_arena(0, rows);
+        if (!rc) rc = alloc_arena(1, rows);
+        if (!rc) rc = alloc_result(1 << 22);
+        if (rc) return rc;
+        WKS_CUDA(ctx, cudaMemset(d_total, 0, 16));
+        return WK_SUCCESS;
+    }
+
+    ExploreArgs explore_args(uint32_t iter, int cur) const {
+        ExploreArgs a{};
+        a.store = ctx->dev_store();
+        a.seg_index[0] = ctx->seg_of(0, 0, kIn);
+        a.seg_index[1] = ctx->seg_of(0, 0, kOut);
+        a.desc = d_plans;
+        a.desc_stride = kMaxSteps;
+        a.iter = iter;
+        a.q_admit = d_admit;
+        a.out = d_arena[cur];
+        a.w_out = w;
+        a.out_cap_rows = rows_cap[cur];
+        a.owner_out = d_owner[cur];
+        a.out_rows = d_total + cur;
+        a.qfirst = d_qfirst;
+        a.qcount = d_qcount;
+        a.heavy = ctx->d_heavy;
+        a.heavy_cap = ctx->heavy_cap;
+        a.ctl = ctx->d_ctl;
+        a.status = ctx->d_status;
+        a.sorted_lists = ctx->sorted_lists;
+        a.lanes = ctx->batch_lanes;
+        return a;
+    }
+
+    // Enqueue one iteration (no host sync).
+    int enqueue_iteration(uint32_t iter, uint32_t n_new, bool has_cont, uint32_t n_fin) {
+        const int cur = iter & 1, prev = cur ^ 1;
+        cudaStream_t s = ctx->stream;
+        if (n_new) {
+            WKS_CUDA(ctx, cudaMemcpyAsync(d_stage, h_stage, sizeof(StepDesc) * kMaxSteps * (size_t)n_new,
+                                          cudaMemcpyHostToDevice, s));
+            WKS_CUDA(ctx, cudaMemcpyAsync(d_new, h_new, 4ull * n_new, cudaMemcpyHostToDevice, s));
+            install_kernel<<<std::min<uint32_t>(n_new, 1024), 32, 0, s>>>(d_plans, d_admit, d_stage, d_new, n_new, iter);
+            WKS_CUDA(ctx, cudaGetLastError());
+        }
+        WKS_CUDA(ctx, cudaMemsetAsync(d_qfirst, 0xFF, 8ull * slots_n, s));
+        WKS_CUDA(ctx, cudaMemsetAsync(d_qcount, 0, 8ull * slots_n, s));
+        WKS_CUDA(ctx, cudaMemsetAsync(d_total + cur, 0, 8, s));
+        const int grid = explore_blocks_per_sm(w, w, ctx->batch_lanes) * ctx->sm_count;
+        if (has_cont) {
+            ExploreArgs a = explore_args(iter, cur);
+            a.n_queries = slots_n;
+            a.virtual_rows = 0;
+            a.in_rows = d_total + prev;
+            a.owner_in = d_owner[prev];
+            a.in = d_arena[prev];
+            a.w_in = w;
+            a.in_cap_rows = rows_cap[prev];
+            cudaError_t e = launch_explore(a, grid, s);
+            if (e != cudaSuccess) return ctx->cuda_fail(e, "serving launch");
+        }
+        if (n_new) {
+            ExploreArgs a = explore_args(iter, cur);
+            a.n_queries = n_new;
+            a.virtual_rows = 1;
+            a.virt_owner = d_new;
+            a.out_base_rows = d_total + cur;
+            const int g0 = explore_blocks_per_sm(0, w, ctx->batch_lanes) * ctx->sm_count;
+            cudaError_t e = launch_explore(a, g0, s);
+            if (e != cudaSuccess) return ctx->cuda_fail(e, "serving start launch");
+        }
+        if (n_fin) {
+            WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_slots, h_fin_slots, 4ull * n_fin, cudaMemcpyHostToDevice, s));
+            WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_cols, h_fin_cols, 4ull * n_fin, cudaMemcpyHostToDevice, s));
+            finish_scan_kernel<<<1, 1024, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount, d_fin_rows, d_fin_off);
+            finish_gather_kernel<<<std::min<uint32_t>((n_fin + 7) / 8, 2048), 256, 0, s>>>(
+                d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_rows, d_fin_off, d_arena[cur], w, d_result,
+                result_cap, ctx->d_ctl);
+            WKS_CUDA(ctx, cudaGetLastError());
+            WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_rows, d_fin_rows, 8ull * n_fin, cudaMemcpyDeviceToHost, s));
+            WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_off, d_fin_off, 8ull * (n_fin + 1), cudaMemcpyDeviceToHost, s));
+        }
+        WKS_CUDA(ctx, cudaMemcpyAsync(h_total, d_total, 16, cudaMemcpyDeviceToHost, s));
+        return WK_SUCCESS;
+    }
+};
+
+}  // namespace
+}  // namespace wk
+
+using Clock = std::chrono::steady_clock;
+
+extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in, const wk_query* queries,
+                                      uint32_t n, const double* arrival_us, uint32_t* host_out,
+                                      uint64_t cap_elems, wk_qresult* results) {
+    if (!ctx || (!queries && n) || (!arrival_us && n) || (!results && n) || (!host_out && cap_elems))
+        return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    if (n == 0) return WK_SUCCESS;
+    wk::Serve S;
+    S.ctx = ctx;
+    S.cfg = cfg_in ? *cfg_in : wk_serve_config{};
+    if (!S.cfg.working_set_cap_bytes) S.cfg.working_set_cap_bytes = 40ull << 30;
+    if (!S.cfg.arena_bytes) S.cfg.arena_bytes = 1ull << 30;
+    if (!S.cfg.light_proj_bytes) S.cfg.light_proj_bytes = 256ull << 10;
+    if (!S.cfg.heavy_proj_bytes) S.cfg.heavy_proj_bytes = 256ull << 20;
+    if (!S.cfg.max_inflight) S.cfg.max_inflight = 65536;
+    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 4;
+
+    // Resolve every plan once (the same dispatch as a single query).
+    std::vector<std::vector<wk::PlanStep>> plans(n);
+    std::vector<int32_t> status(n, 0);
+    int width = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+        wk::ColMap cm(queries[i].nvars);
+        int rc = wk::resolve_plan(queries[i], ctx->cfg.max_cols, plans[i], cm);
+        if (rc == WK_SUCCESS && (int)plans[i].size() > wk::kMaxSteps) rc = WK_E_CAPACITY;
+        if (rc == WK_SUCCESS && queries[i].mt_factor != 1) rc = WK_E_UNSUPPORTED;
+        if (rc) {
+            status[i] = rc;
+            plans[i].clear();
+        }
+        for (auto& s : plans[i]) width = std::max(width, s.out_cols);
+    }
+    const uint32_t slots = std::min<uint32_t>(S.cfg.max_inflight, std::max<uint32_t>(n, 1));
+    int rc = S.init(slots, width);
+    if (rc) return rc;
+    rc = ctx->ensure_status(std::max(S.rows_cap[0], S.rows_cap[1]) / wk::kTileRows + 2);
+    if (!rc) rc = ctx->ensure_heavy(std::max(S.rows_cap[0], S.rows_cap[1]));
+    if (rc) return rc;
+
+    std::vector<wk::QSlot> slot(slots);
+    std::vector<uint32_t> free_slots;
+    for (uint32_t s = slots; s-- > 0;) free_slots.push_back(s);
+    std::vector<uint32_t> active;   // slots in use
+    std::vector<uint32_t> finished, cooling;
+    uint32_t heavy_inflight = 0;
+    uint64_t proj_bytes = 0;
+    uint64_t out_used = 0;
+    uint32_t next = 0, done = 0;
+    const auto t0 = Clock::now();
+    auto now_us = [&] { return std::chrono::duration<double, std::micro>(Clock::now() - t0).count(); };
+    for (uint32_t i = 0; i < n; ++i) {
+        std::memset(&results[i], 0, sizeof(results[i]));
+        results[i].t_arrive_us = arrival_us[i];
+    }
+    uint32_t iter = 1;   // admission iterations start at 1 so a zeroed admit[] never matches
+    std::deque<uint32_t> wait_heavy, wait_light;   // arrived, not yet admitted
+    // Give query q a slot and stage its plan (Done-padded) for installation this iteration.
+    auto admit = [&](uint32_t q, bool heavy, uint64_t pb, uint32_t& n_new) {
+        const uint32_t s = free_slots.back();
+        free_slots.pop_back();
+        slot[s] = {q, iter, (uint32_t)plans[q].size(), (uint32_t)plans[q].back().out_cols, heavy};
+        for (int k = 0; k < wk::kMaxSteps; ++k) {
+            wk::StepDesc& d = S.h_stage[(size_t)n_new * wk::kMaxSteps + k];
+            if (k < (int)plans[q].size()) {
+                d = wk::make_step_desc(ctx, plans[q][k]);
+            } else {
+                std::memset(&d, 0, sizeof(d));
+                d.op = wk::kXDone;
+            }
+        }
+        S.h_new[n_new++] = s;
+        heavy_inflight += heavy;
+        proj_bytes += pb;
+    };
+    while (done < n) {
+        // 1. admit arrivals
+        const double t = now_us();
+        while (next < n && arrival_us[next] <= t) {   // arrivals join their class's queue
+            const uint32_t q = next++;
+            if (status[q] || plans[q].empty()) {   // fails at dispatch, or nothing to run
+                results[q].status = status[q];
+                results[q].cols = 0;
+                results[q].t_done_us = now_us();
+                ++done;
+                continue;
+            }
+            (plans[q][0].kind == wk::PlanStep::kIndex ? wait_heavy : wait_light).push_back(q);
+        }
+        uint32_t n_new = 0;
+        // index-start queries first (bounded in number), then constant-start ones, FIFO within
+        // each class; a class stops at the first query that does not fit
+        for (int cls = 0; cls < 2; ++cls) {
+            std::deque<uint32_t>& wq = cls == 0 ? wait_heavy : wait_light;
+            const bool heavy = cls == 0;
+            const uint64_t pb = heavy ? S.cfg.heavy_proj_bytes : S.cfg.light_proj_bytes;
+            while (!wq.empty()) {
+                if (free_slots.empty() || (heavy && heavy_inflight >= S.cfg.max_heavy_inflight) ||
+                    (proj_bytes + pb > S.cfg.working_set_cap_bytes && (!active.empty() || n_new)))
+                    break;   // stays queued until slots / memory free up
+                const uint32_t q = wq.front();
+                wq.pop_front();
+                admit(q, heavy, pb, n_new);
+            }
+        }
+        const bool has_cont = !active.empty();
+        if (!has_cont) {   // nothing continues, so no launch will read the cooling slots' rows
+            for (uint32_t s : cooling) free_slots.push_back(s);
+            cooling.clear();
+        }
+        for (uint32_t i = 0; i < n_new; ++i) active.push_back(S.h_new[i]);
+        if (active.empty()) {
+            if (next < n && wait_heavy.empty() && wait_light.empty()) {   // idle until the next arrival
+                const double wait = arrival_us[next] - now_us();
+                if (wait > 200) std::this_thread::sleep_for(std::chrono::microseconds((long)(wait - 100)));
+            }
+            continue;
+        }
+        // 2. which queries run their last step in this iteration
+        uint32_t n_fin = 0;
+        for (uint32_t s : active) {
+            const wk::QSlot& sl = slot[s];
+            if (iter - sl.admit_iter == sl.nsteps - 1) {
+                S.h_fin_slots[n_fin] = s;
+                S.h_fin_cols[n_fin] = sl.cols;
+                ++n_fin;
+            }
+        }
+        // 3. run it; grow the output arena and rerun if a table did not fit
+        for (int attempt = 0;; ++attempt) {
+            if (attempt >= 6) return ctx->fail(WK_E_CAPACITY, "serving arena kept overflowing");
+            rc = S.enqueue_iteration(iter, n_new, has_cont, n_fin);
+            if (rc) return rc;
+            uint32_t err = 0;
+            uint64_t need = 0;
+            rc = ctx->read_ctl(&err, &need);   // synchronises the stream
+            if (rc) return rc;
+            if (!err) break;
+            ctx->clear_ctl_err();
+            if (err & wk::kErrCorrupt) return ctx->fail(WK_E_CORRUPT, "key table chain out of range");
+            if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "serving launch timed out");
+            if (err & wk::kErrResult) {
+                rc = S.alloc_result(S.h_fin_off[n_fin] + S.h_fin_off[n_fin] / 2 + 1024);
+                if (rc) return rc;
+            }
+            if (err & (wk::kErrOverflow | wk::kErrStatus)) {
+                const int cur = iter & 1;
+                uint64_t rows = std::max<uint64_t>(S.rows_cap[cur] * 2, need + need / 4);
+                if (rows * 4ull * S.w > S.cfg.working_set_cap_bytes)
+                    return ctx->fail(WK_E_CAPACITY, "a step exceeds the working-set cap");
+                rc = S.alloc_arena(cur, rows);
+                if (!rc) rc = ctx->ensure_status(S.rows_cap[cur] / wk::kTileRows + 2);
+                if (!rc) rc = ctx->ensure_heavy(S.rows_cap[cur]);
+                if (rc) return rc;
+            }
+        }
+        // 4. completions
+        if (n_fin) {
+            const uint64_t total = S.h_fin_off[n_fin];
+            if (total)
+                WKS_CUDA(ctx, cudaMemcpy(S.h_result, S.d_result, total * 4, cudaMemcpyDeviceToHost));
+            const double td = now_us();
+            for (uint32_t i = 0; i < n_fin; ++i) {
+                const uint32_t s = S.h_fin_slots[i];
+                const uint32_t q = slot[s].query;
+                wk_qresult& r = results[q];
+                r.rows = S.h_fin_rows[i];
+                r.cols = (int32_t)slot[s].cols;
+                r.status = WK_SUCCESS;
+                r.t_done_us = td;
+                const uint64_t elems = r.rows * (uint64_t)r.cols;
+                if (out_used + elems <= cap_elems) {
+                    r.elem_offset = out_used;
+                    if (elems) std::memcpy(host_out + out_used, S.h_result + S.h_fin_off[i], elems * 4);
+                    out_used += elems;
+                } else {
+                    r.status = WK_E_CAPACITY;   // the caller's buffer is full
+                }
+                heavy_inflight -= slot[s].heavy;
+                proj_bytes -= slot[s].heavy ? S.cfg.heavy_proj_bytes : S.cfg.light_proj_bytes;
+                finished.push_back(s);
+                ++done;
+            }
+            active.erase(std::remove_if(active.begin(), active.end(),
+                                        [&](uint32_t s) { return iter - slot[s].admit_iter == slot[s].nsteps - 1; }),
+                         active.end());
+        }
+        // A finished query's rows are still in this iteration's arena and are dropped by the
+        // next iteration; its slot is reused only after that.
+        for (uint32_t s : cooling) free_slots.push_back(s);
+        cooling.swap(finished);
+        finished.clear();
+        ++iter;
+    }
+    return WK_SUCCESS;
+}

@@ -72,9 +72,10 @@ class SynthVocab(C.Structure):
 
 
 class ServeConfig(C.Structure):
-    _fields_ = [("working_set_cap_bytes", C.c_uint64), ("light_arena_bytes", C.c_uint64),
-                ("max_inflight", C.c_uint32), ("heavy_rows_per_iter", C.c_uint32),
-                ("reserved", C.c_int32 * 6)]
+    _fields_ = [("working_set_cap_bytes", C.c_uint64), ("arena_bytes", C.c_uint64),
+                ("light_proj_bytes", C.c_uint64), ("heavy_proj_bytes", C.c_uint64),
+                ("max_inflight", C.c_uint32), ("max_heavy_inflight", C.c_uint32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class StepProf(C.Structure):
@@ -84,7 +85,7 @@ class StepProf(C.Structure):
 
 
 STEP_KINDS = ["index_to_unknown", "const_to_unknown", "known_to_unknown", "known_to_known",
-              "known_to_const", "batch_level"]
+              "known_to_const", "batch_level", "batch_setup", "batch_result_scan", "batch_gather"]
 
 
 def _prof_list(arr, n):
@@ -503,3 +504,24 @@ class Context:
 
     def batch_replay(self):
         _check(lib().wk_batch_replay(self.h), self.h)
+
+    def serve(self, queries, arrival_us, cap_elems=1 << 24, **cfg):
+        """Continuous batching over an open-loop arrival schedule (microseconds from start).
+        Returns [(table or None, status, t_arrive_us, t_done_us)] in query order."""
+        qs, keep = queries_as_c(queries)
+        arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        c = ServeConfig()
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        res = (QResult * max(len(queries), 1))()
+        out = np.zeros(max(cap_elems, 1), dtype=np.uint32)
+        _check(lib().wk_serve_run_open_loop(self.h, C.byref(c), qs, len(queries), _ptr(arr), _ptr(out),
+                                            out.size, res), self.h)
+        ret = []
+        for i in range(len(queries)):
+            r = res[i]
+            t = None
+            if r.status == 0:
+                t = out[r.elem_offset:r.elem_offset + r.rows * r.cols].reshape(r.rows, r.cols)
+            ret.append((t, r.status, r.t_arrive_us, r.t_done_us))
+        return ret
