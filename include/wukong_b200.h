@@ -139,9 +139,17 @@ typedef struct wk_serve_config {
                                          constant (256 KiB) */
     uint64_t heavy_proj_bytes;        /* projected bytes of one that starts from an index
                                          (256 MiB) */
-    uint32_t max_inflight;            /* queries resident at once (default 65536) */
-    uint32_t max_heavy_inflight;      /* index-start queries resident at once (default 4) */
-    int32_t reserved[4];
+    uint32_t max_inflight;            /* constant-start queries resident at once (default 65536) */
+    uint32_t max_heavy_inflight;      /* index-start queries running at once (default 1); each
+                                         runs whole on its own lane: a stream of the lowest
+                                         priority with its own tables, beside the iterations */
+    int32_t light_ctas_per_sm;        /* exploration CTAs per SM of the iteration launches; the
+                                         lanes leave these slots free so iterations never wait
+                                         for an index-start step (default 2) */
+    int32_t blind;                    /* 1: tables stay on the device and only row counts come
+                                         back, as the reference's emulator runs its queries
+                                         (result.blind, console_proxy.hpp:395) */
+    int32_t reserved[2];
 } wk_serve_config;
 
 /* Per-query outcome of a batch or a serving run. */

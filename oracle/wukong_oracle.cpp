@@ -130,6 +130,33 @@ struct error_code : std::runtime_error {
     int code;
     explicit error_code(int c) : std::runtime_error("wukong error"), code(c) {}
 };
+
+// Sort with one thread per chunk, then merge chunk pairs; for a total order the result is the
+// same sequence std::sort gives (this only shortens the oracle's build on large graphs).
+template <class T, class Cmp>
+static void par_sort(std::vector<T>& v, Cmp cmp) {
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 64));
+    if (v.size() < (1u << 20) || nt == 1) {
+        std::sort(v.begin(), v.end(), cmp);
+        return;
+    }
+    std::vector<size_t> b(nt + 1);
+    for (size_t i = 0; i <= nt; ++i) b[i] = v.size() * i / nt;
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < nt; ++i)
+        th.emplace_back([&, i] { std::sort(v.begin() + b[i], v.begin() + b[i + 1], cmp); });
+    for (auto& t : th) t.join();
+    for (size_t step = 1; step < nt; step *= 2) {
+        th.clear();
+        for (size_t i = 0; i + step < nt; i += 2 * step) {
+            const size_t lo = b[i], mid = b[i + step], hi = b[std::min(nt, i + 2 * step)];
+            th.emplace_back([&, lo, mid, hi] {
+                std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi, cmp);
+            });
+        }
+        for (auto& t : th) t.join();
+    }
+}
 enum { SUCCESS = 0, UNKNOWN_PATTERN = 3, OBJ_ERROR = 7, VERTEX_INVALID = 8, UNKNOWN_SUB = 9,
        FIRST_PATTERN_ERROR = 11, STORE_ERROR = 106 };
 #define ORACLE_ASSERT(c, code) \
@@ -445,8 +472,9 @@ public:
             if (a.o != b.o) return a.o < b.o;
             return a.s < b.s;
         };
-        std::sort(pso.begin(), pso.end(), by_pso);
-        std::sort(pos.begin(), pos.end(), by_pos);
+        // the orders are total, so a parallel sort gives the loader's sequence exactly
+        par_sort(pso, by_pso);
+        par_sort(pos, by_pos);
         pso.erase(std::unique(pso.begin(), pso.end()), pso.end());
         pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
         // predicates known to the string server: every predicate id used, plus the type ids

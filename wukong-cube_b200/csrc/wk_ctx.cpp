@@ -66,7 +66,7 @@ int wk_ctx::blocks_per_sm(int op, int cols, int lanes) {
     auto it = bps_cache.find(k);
     if (it != bps_cache.end()) return it->second;
     const int w_out = (op == wk::kXK2U || op == wk::kXStart) ? cols + 1 : cols;
-    int nb = wk::explore_blocks_per_sm(cols, w_out, lanes);
+    int nb = std::max(1, wk::explore_blocks_per_sm(cols, w_out, lanes) - reserve_ctas_per_sm);
     bps_cache[k] = nb;
     return nb;
 }
@@ -318,6 +318,8 @@ StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s) {
 }  // namespace wk
 
 // ---------------------------------------------------------------- context
+static int ctx_init_device(wk_ctx* ctx, bool low_priority);
+
 extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     if (!out) return WK_E_BADARG;
     wk_ctx* ctx = nullptr;
@@ -335,17 +337,63 @@ extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     if (ctx->cfg.rbuf_bytes == 0) ctx->cfg.rbuf_bytes = 64ull << 20;
     if (ctx->cfg.working_set_cap_bytes == 0) ctx->cfg.working_set_cap_bytes = 40ull << 30;
     ctx->device = ctx->cfg.device;
+    int rc = ctx_init_device(ctx, false);
+    if (rc) {
+        wk_ctx_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return WK_SUCCESS;
+}
+
+int wk::ctx_make_child(wk_ctx* parent, int reserve_ctas_per_sm, wk_ctx** out) {
+    wk_ctx* ctx = nullptr;
+    try {
+        ctx = new wk_ctx();
+    } catch (const std::bad_alloc&) {
+        return parent->fail(WK_E_OOM, "serving lane");
+    }
+    ctx->cfg = parent->cfg;
+    ctx->device = parent->device;
+    ctx->reserve_ctas_per_sm = std::max(0, reserve_ctas_per_sm);
+    int rc = ctx_init_device(ctx, true);
+    if (rc) {
+        parent->last_error = "serving lane: " + ctx->last_error;
+        wk_ctx_destroy(ctx);
+        return rc;
+    }
+    ctx->d_slots = parent->d_slots;
+    ctx->n_slots = parent->n_slots;
+    ctx->d_edges = parent->d_edges;
+    ctx->n_edges = parent->n_edges;
+    ctx->segs = parent->segs;
+    ctx->index = parent->index;
+    ctx->has_store = parent->has_store;
+    ctx->borrowed_store = true;
+    ctx->sorted_lists = parent->sorted_lists;
+    ctx->default_lanes = parent->default_lanes;
+    ctx->batch_lanes = parent->batch_lanes;
+    ctx->tuned_lanes = parent->tuned_lanes;
+    *out = ctx;
+    return WK_SUCCESS;
+}
+
+// Stream, control block and status array of a new context on its device.  Lanes (children)
+// get the lowest stream priority so that pending CTAs of the parent's launches go first.
+static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     auto bail = [&](cudaError_t e, const char* what) {
-        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
-        delete ctx;
-        (void)m;
+        cudaGetLastError();
+        ctx->last_error = std::string(what) + ": " + cudaGetErrorString(e);
         return WK_E_CUDA;
     };
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return bail(e, "cudaSetDevice");
     e = cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
     if (e != cudaSuccess) return bail(e, "sm count");
-    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;
+    e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e != cudaSuccess) return bail(e, "stream priorities");
+    e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, low_priority ? least : greatest);
     if (e != cudaSuccess) return bail(e, "stream");
     e = wk::explore_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
@@ -359,13 +407,7 @@ extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     init.epoch = 1;
     e = cudaMemcpy(ctx->d_ctl, &init, sizeof(init), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return bail(e, "control init");
-    int rc = ctx->ensure_status(1 << 14);
-    if (rc) {
-        delete ctx;
-        return rc;
-    }
-    *out = ctx;
-    return WK_SUCCESS;
+    return ctx->ensure_status(1 << 14);
 }
 
 void wk_batch_release(wk_ctx* ctx);   // wk_batch.cu
@@ -380,8 +422,8 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
         if (t.d) cudaFree(t.d);
         if (t.d_rows) cudaFree(t.d_rows);
     }
-    if (ctx->d_slots) cudaFree(ctx->d_slots);
-    if (ctx->d_edges) cudaFree(ctx->d_edges);
+    if (ctx->d_slots && !ctx->borrowed_store) cudaFree(ctx->d_slots);
+    if (ctx->d_edges && !ctx->borrowed_store) cudaFree(ctx->d_edges);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_heavy) cudaFree(ctx->d_heavy);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
@@ -813,6 +855,23 @@ extern "C" int wk_query_execute_host(wk_ctx* ctx, const wk_query* q, int32_t mod
     int rc = query_run(ctx, q, mode, &t, v2c_map, col_num);
     if (rc) return rc;
     return table_download(ctx, t, host_out, cap_elems, rows);
+}
+
+int wk::query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows) {
+    int rc = query_run(ctx, q, WK_MODE_RESIDENT, t, nullptr, nullptr);
+    if (rc) return rc;
+    rc = table_rows(ctx, *t, rows);
+    if (rc) return rc;
+    if (*rows * (uint64_t)(*t)->cols > (*t)->cap)
+        return ctx->fail(WK_E_CORRUPT, "row count beyond table capacity");
+    return WK_SUCCESS;
+}
+
+int wk::table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host) {
+    if (elems > t->cap) return ctx->fail(WK_E_BADARG, "copy beyond table capacity");
+    if (elems) WK_CUDA(ctx, cudaMemcpyAsync(host, t->d, elems * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return WK_SUCCESS;
 }
 
 // Enqueue a query on the context stream without waiting (for device-side timing).  Buffers

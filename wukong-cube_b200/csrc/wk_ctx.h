@@ -70,6 +70,8 @@ struct wk_ctx {
     std::vector<wk_seg_meta> segs;
     wk::SegIndex index;
     bool has_store = false;
+    bool borrowed_store = false;   // a serving lane: the store belongs to its parent context
+    int reserve_ctas_per_sm = 0;   // exploration CTA slots per SM this context leaves free
     int sorted_lists = 0;
     int default_lanes = 2;
     int batch_lanes = 4;
@@ -143,4 +145,14 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
                  int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override);
 // The device descriptor of a resolved step.
 StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s);
+
+// A context on its own (lowest-priority) stream with its own control block, status array,
+// slice queue and tables, reading the parent's resident store; its exploration launches
+// leave `reserve_ctas_per_sm` CTA slots per SM free.  Released with wk_ctx_destroy, before
+// the parent.
+int ctx_make_child(wk_ctx* parent, int reserve_ctas_per_sm, wk_ctx** out);
+// Run a whole query in RESIDENT mode and report its final table and row count (host sync).
+int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows);
+// Copy `elems` elements of a device table to host memory (host sync).
+int table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host);
 }  // namespace wk

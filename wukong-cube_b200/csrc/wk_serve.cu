@@ -2,24 +2,31 @@
 //
 // No counterpart in the reference beyond the emulator's in-flight window
 // (ConsoleProxy::run_query_emu, console_proxy.hpp:287-439) and its latency CDF
-// (monitor.hpp:141-220).  Every iteration advances each resident query by one pattern:
-//   * queries that arrived since the last iteration are admitted while their projected table
-//     bytes fit under the working-set cap (and a cap on index-start queries in flight), get a
-//     slot, and have their planned steps installed on the device;
+// (monitor.hpp:141-220).  Queries are admitted while their projected table bytes fit under the
+// working-set cap.  Constant-start (light) queries advance in iterations, one pattern each:
+//   * arrivals since the last iteration get a slot and have their planned steps installed on
+//     the device;
 //   * one exploration launch runs every continuing query's current step over its rows (taken
 //     from the previous iteration's arena, tagged with their slot), and a second one starts the
 //     newly admitted queries from their start keys, appending to the same arena;
 //   * queries whose last step ran have their tables gathered and copied to the host.
-// A query's step is iteration - admission iteration, so no per-step host upload is needed;
-// tables stay on the device between steps, light and index-start queries share iterations, and
-// their work overlaps on the device.  The integer work is the same exploration launch as the
-// single-query and batch paths, so a query's result does not depend on what it was mixed with.
+// A query's step is iteration - admission iteration, so no per-step host upload is needed, and
+// its tables stay on the device between steps.  Index-start (heavy) queries run whole on lanes
+// (child contexts on low-priority streams, one host thread each) beside the iterations; the
+// iteration launches and the lanes split each SM's CTA slots, so both run on the device at
+// once and a light query never waits for a heavy step.  The integer work is the same
+// exploration launch as the single-query and batch paths, so a query's result does not depend
+// on what it was mixed with.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -107,7 +114,6 @@ struct QSlot {
     uint32_t admit_iter;
     uint32_t nsteps;
     uint32_t cols;        // final column count
-    bool heavy;
 };
 
 #define WKS_CUDA(ctx, call)                                        \
@@ -257,7 +263,8 @@ struct Serve {
         WKS_CUDA(ctx, cudaMemsetAsync(d_qfirst, 0xFF, 8ull * slots_n, s));
         WKS_CUDA(ctx, cudaMemsetAsync(d_qcount, 0, 8ull * slots_n, s));
         WKS_CUDA(ctx, cudaMemsetAsync(d_total + cur, 0, 8, s));
-        const int grid = explore_blocks_per_sm(w, w, ctx->batch_lanes) * ctx->sm_count;
+        const int light = std::max(1, cfg.light_ctas_per_sm);
+        const int grid = std::min(explore_blocks_per_sm(w, w, ctx->batch_lanes), light) * ctx->sm_count;
         if (has_cont) {
             ExploreArgs a = explore_args(iter, cur);
             a.n_queries = slots_n;
@@ -276,7 +283,7 @@ struct Serve {
             a.virtual_rows = 1;
             a.virt_owner = d_new;
             a.out_base_rows = d_total + cur;
-            const int g0 = explore_blocks_per_sm(0, w, ctx->batch_lanes) * ctx->sm_count;
+            const int g0 = std::min(explore_blocks_per_sm(0, w, ctx->batch_lanes), light) * ctx->sm_count;
             cudaError_t e = launch_explore(a, g0, s);
             if (e != cudaSuccess) return ctx->cuda_fail(e, "serving start launch");
         }
@@ -284,15 +291,84 @@ struct Serve {
             WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_slots, h_fin_slots, 4ull * n_fin, cudaMemcpyHostToDevice, s));
             WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_cols, h_fin_cols, 4ull * n_fin, cudaMemcpyHostToDevice, s));
             finish_scan_kernel<<<1, 1024, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount, d_fin_rows, d_fin_off);
-            finish_gather_kernel<<<std::min<uint32_t>((n_fin + 7) / 8, 2048), 256, 0, s>>>(
-                d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_rows, d_fin_off, d_arena[cur], w, d_result,
-                result_cap, ctx->d_ctl);
+            if (!cfg.blind)
+                finish_gather_kernel<<<std::min<uint32_t>((n_fin + 7) / 8, 2048), 256, 0, s>>>(
+                    d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_rows, d_fin_off, d_arena[cur], w, d_result,
+                    result_cap, ctx->d_ctl);
             WKS_CUDA(ctx, cudaGetLastError());
             WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_rows, d_fin_rows, 8ull * n_fin, cudaMemcpyDeviceToHost, s));
             WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_off, d_fin_off, 8ull * (n_fin + 1), cudaMemcpyDeviceToHost, s));
         }
         WKS_CUDA(ctx, cudaMemcpyAsync(h_total, d_total, 16, cudaMemcpyDeviceToHost, s));
         return WK_SUCCESS;
+    }
+};
+
+// Index-start queries run whole, one at a time per lane: a child context (its own stream of
+// the lowest priority, control block, tables) driven by its own host thread, so the iteration
+// loop never waits for one of their steps.
+struct HeavyLanes {
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint32_t> work;
+    std::vector<uint32_t> completed;   // finished since the iteration loop last looked
+    int fatal = 0;                     // a lane's CUDA / device error ends the run
+    std::string fatal_msg;
+    bool stop = false;
+    std::vector<wk_ctx*> lanes;
+    std::vector<std::thread> threads;
+
+    ~HeavyLanes() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv_work.notify_all();
+        for (auto& t : threads) t.join();
+        for (wk_ctx* c : lanes) wk_ctx_destroy(c);
+    }
+
+    template <class Body>
+    int start(wk_ctx* parent, int n, int reserve_ctas, Body body) {
+        for (int i = 0; i < n; ++i) {
+            wk_ctx* c = nullptr;
+            int rc = ctx_make_child(parent, reserve_ctas, &c);
+            if (rc) return rc;
+            lanes.push_back(c);
+        }
+        for (wk_ctx* c : lanes)
+            threads.emplace_back([this, c, body] {
+                cudaSetDevice(c->device);
+                for (;;) {
+                    uint32_t q;
+                    {
+                        std::unique_lock<std::mutex> lk(mu);
+                        cv_work.wait(lk, [&] { return stop || !work.empty(); });
+                        if (stop) return;
+                        q = work.front();
+                        work.pop_front();
+                    }
+                    const int rc = body(c, q);
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        completed.push_back(q);
+                        if ((rc == WK_E_CUDA || rc == WK_E_TIMEOUT || rc == WK_E_CORRUPT) && !fatal) {
+                            fatal = rc;
+                            fatal_msg = c->last_error;
+                        }
+                    }
+                    cv_done.notify_one();
+                }
+            });
+        return WK_SUCCESS;
+    }
+
+    void submit(uint32_t q) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            work.push_back(q);
+        }
+        cv_work.notify_one();
     }
 };
 
@@ -317,12 +393,14 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     if (!S.cfg.light_proj_bytes) S.cfg.light_proj_bytes = 256ull << 10;
     if (!S.cfg.heavy_proj_bytes) S.cfg.heavy_proj_bytes = 256ull << 20;
     if (!S.cfg.max_inflight) S.cfg.max_inflight = 65536;
-    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 4;
+    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 1;
+    if (S.cfg.light_ctas_per_sm <= 0) S.cfg.light_ctas_per_sm = 2;
 
     // Resolve every plan once (the same dispatch as a single query).
     std::vector<std::vector<wk::PlanStep>> plans(n);
     std::vector<int32_t> status(n, 0);
     int width = 1;
+    bool any_heavy = false;
     for (uint32_t i = 0; i < n; ++i) {
         wk::ColMap cm(queries[i].nvars);
         int rc = wk::resolve_plan(queries[i], ctx->cfg.max_cols, plans[i], cm);
@@ -331,6 +409,10 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         if (rc) {
             status[i] = rc;
             plans[i].clear();
+        }
+        if (!plans[i].empty() && plans[i][0].kind == wk::PlanStep::kIndex) {
+            any_heavy = true;   // runs on a lane, not in the iterations
+            continue;
         }
         for (auto& s : plans[i]) width = std::max(width, s.out_cols);
     }
@@ -348,21 +430,61 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     std::vector<uint32_t> finished, cooling;
     uint32_t heavy_inflight = 0;
     uint64_t proj_bytes = 0;
-    uint64_t out_used = 0;
+    std::atomic<uint64_t> out_used{0};
     uint32_t next = 0, done = 0;
-    const auto t0 = Clock::now();
-    auto now_us = [&] { return std::chrono::duration<double, std::micro>(Clock::now() - t0).count(); };
     for (uint32_t i = 0; i < n; ++i) {
         std::memset(&results[i], 0, sizeof(results[i]));
         results[i].t_arrive_us = arrival_us[i];
     }
+    // Claim `elems` elements of the caller's buffer (lanes and the iteration loop share it).
+    auto reserve_out = [&](uint64_t elems, uint64_t* off) {
+        uint64_t cur = out_used.load();
+        do {
+            if (cur + elems > cap_elems) return false;
+        } while (!out_used.compare_exchange_weak(cur, cur + elems));
+        *off = cur;
+        return true;
+    };
+    const auto t0 = Clock::now();
+    auto now_us = [&] { return std::chrono::duration<double, std::micro>(Clock::now() - t0).count(); };
+
+    wk::HeavyLanes H;
+    if (any_heavy) {
+        rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, S.cfg.light_ctas_per_sm,
+                     [&](wk_ctx* lane, uint32_t q) {
+                         const wk_table* t = nullptr;
+                         uint64_t rows = 0, off = 0;
+                         wk_qresult& r = results[q];
+                         int qrc = wk::query_run_rows(lane, &queries[q], &t, &rows);
+                         if (qrc == WK_SUCCESS && S.cfg.blind) {
+                             r.rows = rows;
+                             r.cols = t->cols;
+                         } else if (qrc == WK_SUCCESS) {
+                             const uint64_t elems = rows * (uint64_t)t->cols;
+                             if (reserve_out(elems, &off)) {
+                                 qrc = wk::table_copy_out(lane, t, elems, host_out + off);
+                                 r.elem_offset = off;
+                                 r.rows = rows;
+                                 r.cols = t->cols;
+                             } else {
+                                 qrc = WK_E_CAPACITY;   // the caller's buffer is full
+                             }
+                         }
+                         r.status = qrc;
+                         r.t_done_us = now_us();
+                         return qrc;
+                     });
+        if (rc) return rc;
+    }
+
     uint32_t iter = 1;   // admission iterations start at 1 so a zeroed admit[] never matches
     std::deque<uint32_t> wait_heavy, wait_light;   // arrived, not yet admitted
-    // Give query q a slot and stage its plan (Done-padded) for installation this iteration.
-    auto admit = [&](uint32_t q, bool heavy, uint64_t pb, uint32_t& n_new) {
+    // Give constant-start query q a slot and stage its plan (Done-padded) for installation
+    // this iteration.
+    auto admit = [&](uint32_t q, uint32_t& n_new) {
         const uint32_t s = free_slots.back();
         free_slots.pop_back();
-        slot[s] = {q, iter, (uint32_t)plans[q].size(), (uint32_t)plans[q].back().out_cols, heavy};
+        slot[s] = {q, iter, (uint32_t)plans[q].size(), (uint32_t)plans[q].back().out_cols};
         for (int k = 0; k < wk::kMaxSteps; ++k) {
             wk::StepDesc& d = S.h_stage[(size_t)n_new * wk::kMaxSteps + k];
             if (k < (int)plans[q].size()) {
@@ -373,13 +495,26 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             }
         }
         S.h_new[n_new++] = s;
-        heavy_inflight += heavy;
-        proj_bytes += pb;
+        proj_bytes += S.cfg.light_proj_bytes;
     };
+    std::vector<uint32_t> lane_done;
     while (done < n) {
-        // 1. admit arrivals
+        // 0. index-start queries the lanes finished
+        {
+            std::lock_guard<std::mutex> lk(H.mu);
+            lane_done.swap(H.completed);
+            if (H.fatal) return ctx->fail(H.fatal, "serving lane: " + H.fatal_msg);
+        }
+        for (uint32_t q : lane_done) {
+            (void)q;
+            --heavy_inflight;
+            proj_bytes -= S.cfg.heavy_proj_bytes;
+            ++done;
+        }
+        lane_done.clear();
+        // 1. arrivals join their class's queue
         const double t = now_us();
-        while (next < n && arrival_us[next] <= t) {   // arrivals join their class's queue
+        while (next < n && arrival_us[next] <= t) {
             const uint32_t q = next++;
             if (status[q] || plans[q].empty()) {   // fails at dispatch, or nothing to run
                 results[q].status = status[q];
@@ -390,21 +525,22 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             }
             (plans[q][0].kind == wk::PlanStep::kIndex ? wait_heavy : wait_light).push_back(q);
         }
+        // 2. admission, FIFO within each class; a class stops at the first query that does not
+        // fit under the working-set cap (unless nothing at all is resident)
+        while (!wait_heavy.empty() && heavy_inflight < S.cfg.max_heavy_inflight &&
+               (proj_bytes + S.cfg.heavy_proj_bytes <= S.cfg.working_set_cap_bytes ||
+                (active.empty() && !heavy_inflight))) {
+            H.submit(wait_heavy.front());
+            wait_heavy.pop_front();
+            ++heavy_inflight;
+            proj_bytes += S.cfg.heavy_proj_bytes;
+        }
         uint32_t n_new = 0;
-        // index-start queries first (bounded in number), then constant-start ones, FIFO within
-        // each class; a class stops at the first query that does not fit
-        for (int cls = 0; cls < 2; ++cls) {
-            std::deque<uint32_t>& wq = cls == 0 ? wait_heavy : wait_light;
-            const bool heavy = cls == 0;
-            const uint64_t pb = heavy ? S.cfg.heavy_proj_bytes : S.cfg.light_proj_bytes;
-            while (!wq.empty()) {
-                if (free_slots.empty() || (heavy && heavy_inflight >= S.cfg.max_heavy_inflight) ||
-                    (proj_bytes + pb > S.cfg.working_set_cap_bytes && (!active.empty() || n_new)))
-                    break;   // stays queued until slots / memory free up
-                const uint32_t q = wq.front();
-                wq.pop_front();
-                admit(q, heavy, pb, n_new);
-            }
+        while (!wait_light.empty() && !free_slots.empty() &&
+               (proj_bytes + S.cfg.light_proj_bytes <= S.cfg.working_set_cap_bytes ||
+                (active.empty() && !heavy_inflight && !n_new))) {
+            admit(wait_light.front(), n_new);
+            wait_light.pop_front();
         }
         const bool has_cont = !active.empty();
         if (!has_cont) {   // nothing continues, so no launch will read the cooling slots' rows
@@ -413,13 +549,17 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         }
         for (uint32_t i = 0; i < n_new; ++i) active.push_back(S.h_new[i]);
         if (active.empty()) {
-            if (next < n && wait_heavy.empty() && wait_light.empty()) {   // idle until the next arrival
-                const double wait = arrival_us[next] - now_us();
-                if (wait > 200) std::this_thread::sleep_for(std::chrono::microseconds((long)(wait - 100)));
+            // idle until the next arrival or a lane finishing, whichever comes first
+            double wait = next < n ? arrival_us[next] - now_us() : 1e6;
+            if (!wait_light.empty() && !free_slots.empty()) wait = 0;
+            if (wait > 50) {
+                std::unique_lock<std::mutex> lk(H.mu);
+                if (H.completed.empty() && !H.fatal)
+                    H.cv_done.wait_for(lk, std::chrono::microseconds((long)std::min(wait - 20, 1e6)));
             }
             continue;
         }
-        // 2. which queries run their last step in this iteration
+        // 3. which queries run their last step in this iteration
         uint32_t n_fin = 0;
         for (uint32_t s : active) {
             const wk::QSlot& sl = slot[s];
@@ -429,7 +569,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                 ++n_fin;
             }
         }
-        // 3. run it; grow the output arena and rerun if a table did not fit
+        // 4. run it; grow the output arena and rerun if a table did not fit
         for (int attempt = 0;; ++attempt) {
             if (attempt >= 6) return ctx->fail(WK_E_CAPACITY, "serving arena kept overflowing");
             rc = S.enqueue_iteration(iter, n_new, has_cont, n_fin);
@@ -457,9 +597,9 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                 if (rc) return rc;
             }
         }
-        // 4. completions
+        // 5. completions
         if (n_fin) {
-            const uint64_t total = S.h_fin_off[n_fin];
+            const uint64_t total = S.cfg.blind ? 0 : S.h_fin_off[n_fin];
             if (total)
                 WKS_CUDA(ctx, cudaMemcpy(S.h_result, S.d_result, total * 4, cudaMemcpyDeviceToHost));
             const double td = now_us();
@@ -472,15 +612,16 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                 r.status = WK_SUCCESS;
                 r.t_done_us = td;
                 const uint64_t elems = r.rows * (uint64_t)r.cols;
-                if (out_used + elems <= cap_elems) {
-                    r.elem_offset = out_used;
-                    if (elems) std::memcpy(host_out + out_used, S.h_result + S.h_fin_off[i], elems * 4);
-                    out_used += elems;
+                uint64_t off = 0;
+                if (S.cfg.blind) {
+                    // row count only
+                } else if (reserve_out(elems, &off)) {
+                    r.elem_offset = off;
+                    if (elems) std::memcpy(host_out + off, S.h_result + S.h_fin_off[i], elems * 4);
                 } else {
                     r.status = WK_E_CAPACITY;   // the caller's buffer is full
                 }
-                heavy_inflight -= slot[s].heavy;
-                proj_bytes -= slot[s].heavy ? S.cfg.heavy_proj_bytes : S.cfg.light_proj_bytes;
+                proj_bytes -= S.cfg.light_proj_bytes;
                 finished.push_back(s);
                 ++done;
             }

@@ -75,7 +75,7 @@ class ServeConfig(C.Structure):
     _fields_ = [("working_set_cap_bytes", C.c_uint64), ("arena_bytes", C.c_uint64),
                 ("light_proj_bytes", C.c_uint64), ("heavy_proj_bytes", C.c_uint64),
                 ("max_inflight", C.c_uint32), ("max_heavy_inflight", C.c_uint32),
-                ("reserved", C.c_int32 * 4)]
+                ("light_ctas_per_sm", C.c_int32), ("blind", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class StepProf(C.Structure):
@@ -507,7 +507,8 @@ class Context:
 
     def serve(self, queries, arrival_us, cap_elems=1 << 24, **cfg):
         """Continuous batching over an open-loop arrival schedule (microseconds from start).
-        Returns [(table or None, status, t_arrive_us, t_done_us)] in query order."""
+        Returns [(table or None, status, t_arrive_us, t_done_us, rows)] in query order; with
+        blind=1 the tables stay on the device (None here) and only the row counts come back."""
         qs, keep = queries_as_c(queries)
         arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
         c = ServeConfig()
@@ -521,7 +522,7 @@ class Context:
         for i in range(len(queries)):
             r = res[i]
             t = None
-            if r.status == 0:
+            if r.status == 0 and not c.blind:
                 t = out[r.elem_offset:r.elem_offset + r.rows * r.cols].reshape(r.rows, r.cols)
-            ret.append((t, r.status, r.t_arrive_us, r.t_done_us))
+            ret.append((t, r.status, r.t_arrive_us, r.t_done_us, r.rows))
         return ret
