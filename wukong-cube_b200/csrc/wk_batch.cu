@@ -19,79 +19,61 @@
 
 #include "wk_batch.h"
 #include "wk_ctx.h"
+#include "wk_device.cuh"
 
 namespace wk {
 namespace {
 
 constexpr int kScanThreads = 1024;
 
-// Final table of each query: its rows at its last level, laid out back to back.
+// Final table of each query: its rows at its last level, laid out back to back.  One CTA walks
+// the queries 1024 at a time (coalesced loads, one block scan per round, a running carry).
 __global__ void __launch_bounds__(kScanThreads) result_scan_kernel(const ResultScanArgs a) {
     __shared__ uint64_t s_warp[kScanThreads / 32];
+    __shared__ uint64_t s_carry;
     const uint32_t n = a.n;
-    const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
-    const uint32_t q0 = min(n, threadIdx.x * per), q1 = min(n, q0 + per);
-    uint64_t sum = 0;
-    for (uint32_t q = q0; q < q1; ++q) {
-        const int lev = (int)a.nsteps[q] - 1;
-        uint64_t rows = 0, base = 0;
-        if (lev >= 0) {
-            rows = a.qcount[(size_t)lev * n + q];
-            base = a.qfirst[(size_t)lev * n + q];
+    if (threadIdx.x == 0) s_carry = 0;
+    for (uint32_t r0 = 0; r0 < n; r0 += kScanThreads) {
+        const uint32_t q = r0 + threadIdx.x;
+        uint64_t sum = 0;
+        if (q < n) {
+            const int lev = (int)a.nsteps[q] - 1;
+            uint64_t rows = 0, base = 0;
+            if (lev >= 0) {
+                rows = a.qcount[(size_t)lev * n + q];
+                base = a.qfirst[(size_t)lev * n + q];
+            }
+            a.final_level[q] = rows ? lev : -1;
+            a.final_base[q] = rows ? base : 0;
+            a.final_rows[q] = rows;
+            sum = rows * a.final_cols[q];
         }
-        a.final_level[q] = rows ? lev : -1;
-        a.final_base[q] = rows ? base : 0;
-        a.final_rows[q] = rows;
-        sum += rows * a.final_cols[q];
+        const uint64_t ex = dev::block_exclusive_sum<kScanThreads>(sum, s_warp);   // syncs
+        const uint64_t carry = s_carry;
+        if (q < n) a.res_off[q] = carry + ex;
+        __syncthreads();   // everyone has read s_carry
+        if (threadIdx.x == kScanThreads - 1) s_carry = carry + ex + sum;
+        __syncthreads();
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t x = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint64_t w = s_warp[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        s_warp[lane] = w;
-    }
-    __syncthreads();
-    uint64_t run = (warp ? s_warp[warp - 1] : 0) + x - sum;
-    for (uint32_t q = q0; q < q1; ++q) {
-        a.res_off[q] = run;
-        run += a.final_rows[q] * a.final_cols[q];
-    }
-    if (threadIdx.x == kScanThreads - 1) a.res_off[n] = run;
+    if (threadIdx.x == 0) a.res_off[n] = s_carry;
 }
 
 // Copy each query's final table (stride of its level) into the compact result buffer.
-__global__ void gather_kernel(const GatherArgs a) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t wpb = blockDim.x / 32;
-    for (uint32_t q = blockIdx.x * wpb + threadIdx.x / 32; q < a.n; q += gridDim.x * wpb) {
-        const int lev = a.final_level[q];
-        const uint64_t rows = a.final_rows[q];
-        const uint32_t cols = a.final_cols[q];
-        if (lev < 0 || lev >= kMaxBatchLevels || rows == 0 || cols == 0) continue;
-        const uint64_t off = a.res_off[q];
-        if (off + rows * cols > a.out_cap) {
-            if (lane == 0) atomicOr(&a.ctl->err, kErrOverflow);
-            continue;
-        }
-        const int w = a.width[lev];
-        const uint32_t* src = a.region[lev] + a.final_base[q] * (uint64_t)w;
-        for (uint64_t e = lane; e < rows * cols; e += 32) {
-            const uint64_t r = e / cols, c = e - r * cols;
-            a.out[off + e] = src[r * w + c];
-        }
+__global__ void __launch_bounds__(256) gather_kernel(const GatherArgs a) {
+    if (a.n == 0) return;
+    if (a.res_off[a.n] > a.out_cap) {   // the host grows the buffer and reruns
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&a.ctl->err, kErrOverflow);
+        return;
     }
+    // a table with rows has a valid final level (result_scan_kernel), so only those are read
+    dev::segmented_gather(a.n, a.res_off,
+                          [&](uint32_t q, const uint32_t*& row0, uint32_t& stride, uint32_t& cols) {
+                              const int lev = a.final_level[q];
+                              stride = (uint32_t)a.width[lev];
+                              row0 = a.region[lev] + a.final_base[q] * (uint64_t)stride;
+                              cols = a.final_cols[q];
+                          },
+                          a.out);
 }
 
 }  // namespace
@@ -354,7 +336,7 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
     ga.out_cap = b->result_cap;
     ga.ctl = ctx->d_ctl;
     if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[4], s));
-    e = wk::launch_gather(ga, std::min<uint32_t>((n + 7) / 8, 4096), s);
+    e = wk::launch_gather(ga, ctx->sm_count * 8, s);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "gather launch");
     if (ph) WKB_CUDA(ctx, cudaEventRecord(ph->extra[5], s));
     return WK_SUCCESS;

@@ -66,7 +66,8 @@ int wk_ctx::blocks_per_sm(int op, int cols, int lanes) {
     auto it = bps_cache.find(k);
     if (it != bps_cache.end()) return it->second;
     const int w_out = (op == wk::kXK2U || op == wk::kXStart) ? cols + 1 : cols;
-    int nb = std::max(1, wk::explore_blocks_per_sm(cols, w_out, lanes) - reserve_ctas_per_sm);
+    int nb = beside_ctas > 0 ? wk::explore_blocks_beside(cols, w_out, lanes, beside_use, beside_ctas)
+                             : wk::explore_blocks_per_sm(cols, w_out, lanes);
     bps_cache[k] = nb;
     return nb;
 }
@@ -346,7 +347,7 @@ extern "C" int wk_ctx_create(const wk_config* cfg, wk_ctx** out) {
     return WK_SUCCESS;
 }
 
-int wk::ctx_make_child(wk_ctx* parent, int reserve_ctas_per_sm, wk_ctx** out) {
+int wk::ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas, wk_ctx** out) {
     wk_ctx* ctx = nullptr;
     try {
         ctx = new wk_ctx();
@@ -355,7 +356,8 @@ int wk::ctx_make_child(wk_ctx* parent, int reserve_ctas_per_sm, wk_ctx** out) {
     }
     ctx->cfg = parent->cfg;
     ctx->device = parent->device;
-    ctx->reserve_ctas_per_sm = std::max(0, reserve_ctas_per_sm);
+    ctx->beside_use = beside_use;
+    ctx->beside_ctas = std::max(0, beside_ctas);
     int rc = ctx_init_device(ctx, true);
     if (rc) {
         parent->last_error = "serving lane: " + ctx->last_error;

@@ -71,7 +71,8 @@ struct wk_ctx {
     wk::SegIndex index;
     bool has_store = false;
     bool borrowed_store = false;   // a serving lane: the store belongs to its parent context
-    int reserve_ctas_per_sm = 0;   // exploration CTA slots per SM this context leaves free
+    wk::CtaUse beside_use{0, 0, 0};   // a serving lane leaves room on every SM for this many
+    int beside_ctas = 0;              // resident CTAs of this size (the iteration launches)
     int sorted_lists = 0;
     int default_lanes = 2;
     int batch_lanes = 4;
@@ -148,9 +149,9 @@ StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s);
 
 // A context on its own (lowest-priority) stream with its own control block, status array,
 // slice queue and tables, reading the parent's resident store; its exploration launches
-// leave `reserve_ctas_per_sm` CTA slots per SM free.  Released with wk_ctx_destroy, before
-// the parent.
-int ctx_make_child(wk_ctx* parent, int reserve_ctas_per_sm, wk_ctx** out);
+// leave room on every SM for `beside_ctas` CTAs of size `beside_use`.  Released with
+// wk_ctx_destroy, before the parent.
+int ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas, wk_ctx** out);
 // Run a whole query in RESIDENT mode and report its final table and row count (host sync).
 int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows);
 // Copy `elems` elements of a device table to host memory (host sync).

@@ -357,6 +357,86 @@ __device__ __forceinline__ void group_member(const uint32_t* edges, const uint64
     }
 }
 
+// ---------------------------------------------------------------- block-wide exclusive sum
+// Every thread of a kThreads-thread block passes x and gets the sum of x over the threads
+// before it.  s_warp holds kThreads / 32 words; the call synchronises the block.
+template <int kThreads>
+__device__ __forceinline__ uint64_t block_exclusive_sum(uint64_t x, uint64_t* s_warp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t v = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) s_warp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint64_t w = lane < kThreads / 32 ? s_warp[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < kThreads / 32) s_warp[lane] = w;
+    }
+    __syncthreads();
+    const uint64_t before = warp ? s_warp[warp - 1] : 0;
+    __syncthreads();   // s_warp may be reused by the caller's next round
+    return before + v - x;
+}
+
+// ---------------------------------------------------------------- segmented gather
+// Copy n tables laid out back to back in `out` (table i fills out[off[i], off[i+1]), row-major,
+// cols(i) columns) from their rows in strided arenas (src(i): first row, stride(i) words).
+// The output is cut into fixed chunks spread over the grid, so one long table is copied by
+// many CTAs and the stores are coalesced; each element finds its table by a binary search of
+// `off` narrowed to the chunk's first and last table.
+constexpr int kGatherChunk = 4096;
+
+template <class Src>
+__device__ void segmented_gather(uint32_t n, const uint64_t* __restrict__ off, Src src,
+                                 uint32_t* __restrict__ out) {
+    __shared__ uint32_t s_q[2];
+    const uint64_t total = off[n];
+    for (uint64_t base = (uint64_t)blockIdx.x * kGatherChunk; base < total;
+         base += (uint64_t)gridDim.x * kGatherChunk) {
+        const uint64_t end = min(total, base + (uint64_t)kGatherChunk);
+        if (threadIdx.x < 2) {
+            const uint64_t p = threadIdx.x ? end - 1 : base;
+            uint32_t lo = 0, hi = n - 1;   // last table whose offset is <= p
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (off[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            s_q[threadIdx.x] = lo;
+        }
+        __syncthreads();
+        const uint32_t q0 = s_q[0], q1 = s_q[1];
+        for (uint64_t p = base + threadIdx.x; p < end; p += blockDim.x) {
+            uint32_t lo = q0, hi = q1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (off[mid] <= p) lo = mid; else hi = mid - 1;
+            }
+            const uint64_t e = p - off[lo];
+            const uint32_t* row0;
+            uint32_t stride, cols;
+            src(lo, row0, stride, cols);
+            uint64_t r, c;
+            if (e < (1ull << 32)) {
+                r = (uint32_t)e / cols;
+                c = (uint32_t)e - (uint32_t)r * cols;
+            } else {
+                r = e / cols;
+                c = e - r * cols;
+            }
+            out[p] = __ldg(row0 + r * stride + c);
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 }  // namespace dev
 }  // namespace wk

@@ -2,7 +2,7 @@
 // the tables of every query of a batch.
 //
 // The reference chains five kernels, a Thrust scan and two host syncs per pattern
-// (gpu_engine_cuda.hpp:169-177, gpu_hash.cu:96-836).  Here CTAs claim 512-row tiles from a
+// (gpu_engine_cuda.hpp:169-177, gpu_hash.cu:96-836).  Here CTAs claim 256-row tiles from a
 // device counter, two at a time (the probes of the next tile run while the current one waits for
 // its position), and per tile:
 //   1. start a TMA bulk copy (cp.async.bulk + mbarrier) of the tile's rows into shared memory
@@ -22,6 +22,8 @@
 // Sizes are read from device memory, so levels chain without a host round trip; an output that
 // would not fit sets kErrOverflow and records the size needed instead of writing.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "../../include/wukong_b200.h"
 #include "wk_device.cuh"
@@ -507,6 +509,46 @@ cudaError_t explore_kernel_attrs() {
     if ((e = set_attr<2>(bytes)) != cudaSuccess) return e;
     if ((e = set_attr<4>(bytes)) != cudaSuccess) return e;
     return set_attr<8>(bytes);
+}
+
+CtaUse explore_cta_use(int w_in, int w_out, int lanes) {
+    CtaUse u{0, 0, kStepThreads};
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaErrorInvalidValue;
+    if (lanes == 2) e = cudaFuncGetAttributes(&fa, explore_kernel<2>);
+    if (lanes == 4) e = cudaFuncGetAttributes(&fa, explore_kernel<4>);
+    if (lanes == 8) e = cudaFuncGetAttributes(&fa, explore_kernel<8>);
+    int dev = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (e != cudaSuccess) fa.numRegs = 255;   // unknown: assume the worst
+    u.smem = explore_smem_bytes(w_in, w_out, nullptr) + fa.sharedSizeBytes + (size_t)reserved;
+    // registers are allocated per warp in units of 256
+    u.regs = ((fa.numRegs * 32 + 255) / 256) * 256 * (kStepThreads / 32);
+    return u;
+}
+
+int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, int other_ctas) {
+    const int alone = explore_blocks_per_sm(w_in, w_out, lanes);
+    if (other_ctas <= 0) return alone;
+    const CtaUse me = explore_cta_use(w_in, w_out, lanes);
+    int dev = 0, smem_sm = 0, regs_sm = 0, thr_sm = 0, blk_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    cudaDeviceGetAttribute(&blk_sm, cudaDevAttrMaxBlocksPerMultiprocessor, dev);
+    long long n = alone;
+    auto fit = [&](long long limit, long long theirs, long long mine) {
+        if (mine <= 0) return;
+        const long long left = limit - (long long)other_ctas * theirs;
+        n = std::min(n, left > 0 ? left / mine : 0ll);
+    };
+    fit(smem_sm, (long long)other.smem, (long long)me.smem);
+    fit(regs_sm, other.regs, me.regs);
+    fit(thr_sm, other.threads, me.threads);
+    fit(blk_sm, 1, 1);
+    return (int)std::max(1ll, n);
 }
 
 int explore_blocks_per_sm(int w_in, int w_out, int lanes) {

@@ -80,6 +80,17 @@ struct ExploreArgs {
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);
 cudaError_t explore_kernel_attrs();
 int explore_blocks_per_sm(int w_in, int w_out, int lanes);
+
+// Resources one CTA of the exploration launch holds on its SM.
+struct CtaUse {
+    size_t smem;   // dynamic + static + the per-block reservation, bytes
+    int regs;      // registers, in the per-warp allocation granularity
+    int threads;
+};
+CtaUse explore_cta_use(int w_in, int w_out, int lanes);
+// CTAs per SM of this launch that fit beside `other_ctas` resident CTAs using `other` each
+// (at least 1), so two persistent launches can be resident on every SM at once.
+int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, int other_ctas);
 cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s);
 
 }  // namespace wk

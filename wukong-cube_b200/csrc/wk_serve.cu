@@ -32,6 +32,7 @@
 
 #include "wk_batch.h"
 #include "wk_ctx.h"
+#include "wk_device.cuh"
 
 namespace wk {
 namespace {
@@ -50,63 +51,60 @@ __global__ void install_kernel(StepDesc* plans, uint32_t* admit, const StepDesc*
 }
 
 // Rows and result offsets of the queries finishing this iteration (one CTA).
-__global__ void finish_scan_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
-                                   const unsigned long long* qcount, uint64_t* fin_rows,
-                                   uint64_t* fin_off) {
-    __shared__ uint64_t s_warp[32];
-    const uint32_t per = (n_fin + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = min(n_fin, threadIdx.x * per), i1 = min(n_fin, i0 + per);
-    uint64_t sum = 0;
-    for (uint32_t i = i0; i < i1; ++i) {
-        const uint64_t r = qcount[fin_slots[i]];
-        fin_rows[i] = r;
-        sum += r * fin_cols[i];
+// Small CTAs: every kernel of an iteration must fit in the room the lanes leave on an SM.
+constexpr int kFinishThreads = 256;
+
+// Per-iteration reset of the slots' output ranges and of this iteration's row total.
+__global__ void __launch_bounds__(256)
+reset_kernel(unsigned long long* qfirst, unsigned long long* qcount, uint32_t n, uint64_t* total) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        qfirst[i] = ~0ull;
+        qcount[i] = 0;
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t x = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-        uint64_t w = lane < (int)(blockDim.x / 32) ? s_warp[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1) {
-            uint64_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *total = 0;
+}
+
+__global__ void __launch_bounds__(kFinishThreads)
+finish_scan_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
+                   const unsigned long long* qcount, uint64_t* fin_rows, uint64_t* fin_off) {
+    __shared__ uint64_t s_warp[kFinishThreads / 32];
+    __shared__ uint64_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    for (uint32_t r0 = 0; r0 < n_fin; r0 += kFinishThreads) {
+        const uint32_t i = r0 + threadIdx.x;
+        uint64_t sum = 0;
+        if (i < n_fin) {
+            const uint64_t r = qcount[fin_slots[i]];
+            fin_rows[i] = r;
+            sum = r * fin_cols[i];
         }
-        s_warp[lane] = w;
+        const uint64_t ex = dev::block_exclusive_sum<kFinishThreads>(sum, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < n_fin) fin_off[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == kFinishThreads - 1) s_carry = carry + ex + sum;
+        __syncthreads();
     }
-    __syncthreads();
-    uint64_t run = (warp ? s_warp[warp - 1] : 0) + x - sum;
-    for (uint32_t i = i0; i < i1; ++i) {
-        fin_off[i] = run;
-        run += fin_rows[i] * fin_cols[i];
-    }
-    if (threadIdx.x == blockDim.x - 1) fin_off[n_fin] = run;
+    if (threadIdx.x == 0) fin_off[n_fin] = s_carry;
 }
 
 // Copy the finishing queries' tables (stride w in the arena) to the result buffer.
-__global__ void finish_gather_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
-                                     const unsigned long long* qfirst, const uint64_t* fin_rows,
-                                     const uint64_t* fin_off, const uint32_t* arena, int w,
-                                     uint32_t* out, uint64_t out_cap, StepCtl* ctl) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t wpb = blockDim.x / 32;
-    for (uint32_t i = blockIdx.x * wpb + threadIdx.x / 32; i < n_fin; i += gridDim.x * wpb) {
-        const uint64_t rows = fin_rows[i];
-        const uint32_t cols = fin_cols[i];
-        if (!rows || !cols) continue;
-        const uint64_t off = fin_off[i];
-        if (off + rows * cols > out_cap) {
-            if (lane == 0) atomicOr(&ctl->err, kErrResult);
-            continue;
-        }
-        const uint32_t* src = arena + qfirst[fin_slots[i]] * (uint64_t)w;
-        for (uint64_t r = 0; r < rows; ++r)
-            for (uint32_t c = lane; c < cols; c += 32) out[off + r * cols + c] = src[r * w + c];
+__global__ void __launch_bounds__(256)
+finish_gather_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
+                     const unsigned long long* qfirst, const uint64_t* fin_off,
+                     const uint32_t* arena, int w, uint32_t* out, uint64_t out_cap, StepCtl* ctl) {
+    if (n_fin == 0) return;
+    if (fin_off[n_fin] > out_cap) {   // the host grows the buffer and reruns the iteration
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&ctl->err, kErrResult);
+        return;
     }
+    dev::segmented_gather(n_fin, fin_off,
+                          [&](uint32_t i, const uint32_t*& row0, uint32_t& stride, uint32_t& cols) {
+                              stride = (uint32_t)w;
+                              row0 = arena + qfirst[fin_slots[i]] * (uint64_t)w;
+                              cols = fin_cols[i];
+                          },
+                          out);
 }
 
 struct QSlot {
@@ -224,6 +222,8 @@ struct Serve {
         return WK_SUCCESS;
     }
 
+    int light_ctas() const { return std::max(1, cfg.light_ctas_per_sm); }
+
     ExploreArgs explore_args(uint32_t iter, int cur) const {
         ExploreArgs a{};
         a.store = ctx->dev_store();
@@ -260,10 +260,10 @@ struct Serve {
             install_kernel<<<std::min<uint32_t>(n_new, 1024), 32, 0, s>>>(d_plans, d_admit, d_stage, d_new, n_new, iter);
             WKS_CUDA(ctx, cudaGetLastError());
         }
-        WKS_CUDA(ctx, cudaMemsetAsync(d_qfirst, 0xFF, 8ull * slots_n, s));
-        WKS_CUDA(ctx, cudaMemsetAsync(d_qcount, 0, 8ull * slots_n, s));
-        WKS_CUDA(ctx, cudaMemsetAsync(d_total + cur, 0, 8, s));
-        const int light = std::max(1, cfg.light_ctas_per_sm);
+        reset_kernel<<<std::min<uint32_t>((slots_n + 255) / 256, 1024), 256, 0, s>>>(d_qfirst, d_qcount,
+                                                                                    slots_n, d_total + cur);
+        WKS_CUDA(ctx, cudaGetLastError());
+        const int light = light_ctas();
         const int grid = std::min(explore_blocks_per_sm(w, w, ctx->batch_lanes), light) * ctx->sm_count;
         if (has_cont) {
             ExploreArgs a = explore_args(iter, cur);
@@ -290,10 +290,11 @@ struct Serve {
         if (n_fin) {
             WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_slots, h_fin_slots, 4ull * n_fin, cudaMemcpyHostToDevice, s));
             WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_cols, h_fin_cols, 4ull * n_fin, cudaMemcpyHostToDevice, s));
-            finish_scan_kernel<<<1, 1024, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount, d_fin_rows, d_fin_off);
+            finish_scan_kernel<<<1, kFinishThreads, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount,
+                                                            d_fin_rows, d_fin_off);
             if (!cfg.blind)
-                finish_gather_kernel<<<std::min<uint32_t>((n_fin + 7) / 8, 2048), 256, 0, s>>>(
-                    d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_rows, d_fin_off, d_arena[cur], w, d_result,
+                finish_gather_kernel<<<ctx->sm_count * 4, 256, 0, s>>>(
+                    d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_off, d_arena[cur], w, d_result,
                     result_cap, ctx->d_ctl);
             WKS_CUDA(ctx, cudaGetLastError());
             WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_rows, d_fin_rows, 8ull * n_fin, cudaMemcpyDeviceToHost, s));
@@ -329,10 +330,10 @@ struct HeavyLanes {
     }
 
     template <class Body>
-    int start(wk_ctx* parent, int n, int reserve_ctas, Body body) {
+    int start(wk_ctx* parent, int n, const CtaUse& beside_use, int beside_ctas, Body body) {
         for (int i = 0; i < n; ++i) {
             wk_ctx* c = nullptr;
-            int rc = ctx_make_child(parent, reserve_ctas, &c);
+            int rc = ctx_make_child(parent, beside_use, beside_ctas, &c);
             if (rc) return rc;
             lanes.push_back(c);
         }
@@ -450,7 +451,14 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
 
     wk::HeavyLanes H;
     if (any_heavy) {
-        rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, S.cfg.light_ctas_per_sm,
+        // Lanes leave room on every SM for the iteration launches' CTAs (the larger of the two
+        // launch shapes, one CTA of margin), so both persistent launches stay resident at once
+        // and neither waits for the other to finish.
+        const wk::CtaUse a = wk::explore_cta_use(S.w, S.w, ctx->batch_lanes);
+        const wk::CtaUse b = wk::explore_cta_use(0, S.w, ctx->batch_lanes);
+        const wk::CtaUse light{std::max(a.smem, b.smem), std::max(a.regs, b.regs),
+                               std::max(a.threads, b.threads)};
+        rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, light, S.light_ctas() + 1,
                      [&](wk_ctx* lane, uint32_t q) {
                          const wk_table* t = nullptr;
                          uint64_t rows = 0, off = 0;
