@@ -89,6 +89,11 @@ cudaError_t launch_gather(const GatherArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t batch_kernel_attrs() {
+    cudaError_t e = use_max_shared_carveout(result_scan_kernel);
+    return e != cudaSuccess ? e : use_max_shared_carveout(gather_kernel);
+}
+
 }  // namespace wk
 
 // ---------------------------------------------------------------- host side of the batch

@@ -398,6 +398,9 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, low_priority ? least : greatest);
     if (e != cudaSuccess) return bail(e, "stream");
     e = wk::explore_kernel_attrs();
+    if (e == cudaSuccess) e = wk::small_kernel_attrs();
+    if (e == cudaSuccess) e = wk::batch_kernel_attrs();
+    if (e == cudaSuccess) e = wk::serve_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
     e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
@@ -418,6 +421,8 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     if (!ctx) return WK_E_BADARG;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (wk_ctx* lane : ctx->lanes) wk_ctx_destroy(lane);   // they read this context's store
+    ctx->lanes.clear();
     wk_batch_release(ctx);
     ctx->drop_graphs();
     for (auto& t : ctx->rbuf) {

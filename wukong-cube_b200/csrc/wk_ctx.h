@@ -103,6 +103,10 @@ struct wk_ctx {
 
     // batch / serving state (wk_batch.cu)
     void* batch = nullptr;
+    // serving lanes, kept between serving runs so their tables stay grown (wk_serve.cu)
+    std::vector<wk_ctx*> lanes;
+    wk::CtaUse lanes_use{0, 0, 0};
+    int lanes_ctas = 0;
 
     wk::DevStore dev_store() const {
         wk::DevStore s;

@@ -486,7 +486,8 @@ __global__ void __launch_bounds__(kStepThreads, 6) explore_kernel(const ExploreA
 
 template <int L>
 cudaError_t set_attr(int bytes) {
-    return cudaFuncSetAttribute(explore_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(explore_kernel<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e != cudaSuccess ? e : use_max_shared_carveout(explore_kernel<L>);
 }
 
 }  // namespace

@@ -86,4 +86,9 @@ cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream
     return cudaGetLastError();
 }
 
+cudaError_t small_kernel_attrs() {
+    cudaError_t e = use_max_shared_carveout(list_kernel);
+    return e != cudaSuccess ? e : use_max_shared_carveout(sorted_check_kernel);
+}
+
 }  // namespace wk

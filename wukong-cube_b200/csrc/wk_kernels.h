@@ -61,4 +61,18 @@ constexpr int kTileRows = 256;
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);
 
+// Every kernel of the library asks for the same L1 / shared-memory split, the largest shared
+// carveout.  The split is an SM-wide setting, so CTAs of launches that ask for different
+// splits cannot share an SM; with one split everywhere, a serving lane's launches and the
+// iteration launches run side by side instead of one draining SMs for the other.
+template <class K>
+inline cudaError_t use_max_shared_carveout(K kernel) {
+    return cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
+}
+// Set that attribute on the kernels of each translation unit (called at context creation).
+cudaError_t small_kernel_attrs();    // wk_kernels.cu
+cudaError_t batch_kernel_attrs();    // wk_batch.cu
+cudaError_t serve_kernel_attrs();    // wk_serve.cu
+
 }  // namespace wk

@@ -316,7 +316,6 @@ struct HeavyLanes {
     int fatal = 0;                     // a lane's CUDA / device error ends the run
     std::string fatal_msg;
     bool stop = false;
-    std::vector<wk_ctx*> lanes;
     std::vector<std::thread> threads;
 
     ~HeavyLanes() {
@@ -326,18 +325,29 @@ struct HeavyLanes {
         }
         cv_work.notify_all();
         for (auto& t : threads) t.join();
-        for (wk_ctx* c : lanes) wk_ctx_destroy(c);
     }
 
+    // Lanes are child contexts cached in the parent (their tables keep their grown size from
+    // one serving run to the next); they are rebuilt when the room they must leave changes.
     template <class Body>
     int start(wk_ctx* parent, int n, const CtaUse& beside_use, int beside_ctas, Body body) {
-        for (int i = 0; i < n; ++i) {
+        const bool same = parent->lanes_ctas == beside_ctas && parent->lanes_use.smem == beside_use.smem &&
+                          parent->lanes_use.regs == beside_use.regs &&
+                          parent->lanes_use.threads == beside_use.threads;
+        if (!same) {
+            for (wk_ctx* c : parent->lanes) wk_ctx_destroy(c);
+            parent->lanes.clear();
+            parent->lanes_use = beside_use;
+            parent->lanes_ctas = beside_ctas;
+        }
+        while ((int)parent->lanes.size() < n) {
             wk_ctx* c = nullptr;
             int rc = ctx_make_child(parent, beside_use, beside_ctas, &c);
             if (rc) return rc;
-            lanes.push_back(c);
+            parent->lanes.push_back(c);
         }
-        for (wk_ctx* c : lanes)
+        for (int i = 0; i < n; ++i) {
+            wk_ctx* c = parent->lanes[i];
             threads.emplace_back([this, c, body] {
                 cudaSetDevice(c->device);
                 for (;;) {
@@ -361,6 +371,7 @@ struct HeavyLanes {
                     cv_done.notify_one();
                 }
             });
+        }
         return WK_SUCCESS;
     }
 
@@ -374,6 +385,15 @@ struct HeavyLanes {
 };
 
 }  // namespace
+
+cudaError_t serve_kernel_attrs() {
+    cudaError_t e;
+    if ((e = use_max_shared_carveout(install_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(reset_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(finish_scan_kernel)) != cudaSuccess) return e;
+    return use_max_shared_carveout(finish_gather_kernel);
+}
+
 }  // namespace wk
 
 using Clock = std::chrono::steady_clock;
