@@ -231,6 +231,7 @@ def run_ours(args, world, rank, local_rank):
     import torch
 
     import oracle
+    import replicas
     import workloads
     import wukong_b200 as wk
 
@@ -244,8 +245,11 @@ def run_ours(args, world, rank, local_rank):
     cores = os.cpu_count() or 1
     o = oracle.OracleStore(tr) if rank == 0 else None
 
-    # ---- light batch: correctness gate, then timing
-    qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1 + rank)
+    # ---- light batch: correctness gate, then timing.  With N GPUs (replicas) the query stream
+    # holds N batches and each rank answers its own share of it.
+    stream_qs = workloads.light_queries(v, inst, args.light * world, seed=args.seed + 1)
+    lo, hi = replicas.shard(len(stream_qs), rank, world)
+    qs = stream_qs[lo:hi]
     res = ctx.batch(qs)
     light_rows = np.array([r[0].shape[0] if r[0] is not None else 0 for r in res], np.int64)
     if o is not None and not args.no_check:
@@ -264,12 +268,8 @@ def run_ours(args, world, rank, local_rank):
     with Clocks(local_rank) as clk:
         step_ms = timed(stream, flush, args.steps, ctx.batch_replay)
     ctx.check()
-    tot_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([tot_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        tot_ms = float(t.item())
-    value = len(qs) * args.steps * world / (tot_ms / 1000.0)
+    tot_ms = replicas.max_over_ranks(sum(step_ms), device="cuda")   # whole-job device time
+    value = replicas.sum_over_ranks(len(qs), device="cuda") * args.steps / (tot_ms / 1000.0)
 
     # ---- e2e through the C ABI from the host (plans in, tables out to pinned memory)
     qs_c, keep = wk.queries_as_c(qs)
