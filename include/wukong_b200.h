@@ -245,6 +245,32 @@ int wk_step_known_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_start, i
 /* ?X P C — GPUEngineCuda::known_to_const (gpu_engine_cuda.hpp:284-363). */
 int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t end_vid,
                            uint32_t pid, int32_t dir, wk_table* out);
+/* known_to_unknown that allocates nothing.  No reference counterpart: the reference allocates
+ * its buffers up front (GPUMem) and aborts when they overflow.
+ *
+ * For callers that must not allocate device memory during a step. Examples: a loop that runs
+ * while other streams of the device must not be stalled (cudaFree waits for the whole device),
+ * and code that budgets every device byte up front.
+ *
+ * The scan scratch (control block, per-tile status words, long-list slice queue) is one fixed
+ * 448 KiB device array per device, inside the library. The output table must already be large
+ * enough, and nothing is grown.
+ *
+ * Limits:
+ * - inputs of at most 4,194,304 rows (16,384 tiles of 256 rows);
+ * - at most 8,192 long-list slices of 2,048 output rows.
+ * Beyond them, or when the output does not fit, the call returns WK_E_CAPACITY and
+ * wk_last_error says which limit was hit.
+ *
+ * The first call on a device sets the scratch up: it takes its address and clears it. Make
+ * that first call before any stream capture on the device.
+ *
+ * The scratch is shared by every context and stream of the device, so calls that overlap in
+ * time on one device race; serialise them.
+ *
+ * Same arguments and results as wk_step_known_to_unknown. */
+int wk_step_known_to_unknown_noalloc(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t pid,
+                                     int32_t dir, wk_table* out);
 
 /* ---------------------------------------------------------------- whole query
  * GPUAgent::execute_sparql_query's pattern loop (gpu_agent.hpp:173-246) driving

@@ -138,6 +138,7 @@ _SIGS = {
     "wk_step_known_to_unknown": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _P]),
     "wk_step_known_to_known": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, _P]),
     "wk_step_known_to_const": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, _P]),
+    "wk_step_known_to_unknown_noalloc": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _P]),
     "wk_query_execute": (C.c_int, [_P, C.POINTER(QueryC), C.c_int32, C.POINTER(_P),
                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_uint64)]),
