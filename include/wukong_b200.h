@@ -317,13 +317,36 @@ int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof
  * No reference counterpart. */
 int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
 
-/* Tile-schedule knobs of the exploration launch (what the autotuner sets).  knob 0: lanes per
- * probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte bucket slices per
- * request); knob 1: the same for batches.  wk_ctx_tune_get reads a knob back. */
+/* Tile-schedule knobs of the exploration launch (what the autotuner sets).
+ *   knob 0: lanes per probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte
+ *           bucket slices staged per request);
+ *   knob 1: the same for batches and serving;
+ *   knob 2: the list length above which a row's output is written as 2,048-row slices by every
+ *           CTA (block-per-row) instead of by the CTA that probed it (group-per-row); 128 to
+ *           2^24, default 128;
+ *   knob 3: the same for batches and serving.
+ * wk_ctx_tune_get reads a knob back.  No reference counterpart (its launch shape is fixed,
+ * gpu_hash.cu:96-326). */
 #define WK_KNOB_LANES 0
 #define WK_KNOB_BATCH_LANES 1
+#define WK_KNOB_SLICE_ROWS 2
+#define WK_KNOB_BATCH_SLICE_ROWS 3
 int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value);
 int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value);
+
+/* The autotuner: times every combination of the knobs above on the caller's own workload and
+ * keeps the fastest.  Queries that start from a constant are timed as one batch (knobs 1, 3; CUDA
+ * events over `iters` graph replays); index-start queries one at a time, step by step (knob 0
+ * per (step kind, input columns), knob 2).  `out` receives the choice and its timings. */
+typedef struct wk_tune_result {
+    int32_t batch_lanes, batch_slice_rows;   /* chosen for batches */
+    int32_t lanes, slice_rows;               /* chosen default for single queries */
+    double batch_ms_default, batch_ms_tuned; /* one batch replay, before and after */
+    double single_ms_default, single_ms_tuned;   /* sum over the index-start queries */
+    int32_t candidates;                      /* configurations timed */
+    int32_t reserved[3];
+} wk_tune_result;
+int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters, wk_tune_result* out);
 
 /* ---------------------------------------------------------------- batching
  * Run n planned queries together: all queries advance one pattern per level inside one

@@ -299,6 +299,7 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
         a.status = ctx->d_status;
         a.sorted_lists = ctx->sorted_lists;
         a.lanes = lanes;
+        a.slice_rows = ctx->batch_slice_rows;
         const int grid = wk::explore_blocks_per_sm(a.virtual_rows ? 0 : a.w_in, a.w_out, lanes) * ctx->sm_count;
         if (ph) {
             WKB_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 16, s));
@@ -362,6 +363,7 @@ int launch_batch(wk_ctx* ctx, BatchState* b, const Plan& P) {
     put(&ctx->d_heavy, sizeof(void*));
     put(&ctx->heavy_cap, 8);
     put(&ctx->batch_lanes, 4);
+    put(&ctx->batch_slice_rows, 4);
     put(&ctx->d_slots, sizeof(void*));
     if (shape != b->shape || !b->exec) {
         if (b->exec) cudaGraphExecDestroy(b->exec);

@@ -271,6 +271,7 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
     a.status = ctx->d_status;
     a.sorted_lists = ctx->sorted_lists;
     a.lanes = ctx->lanes_for(a.one.op, st.in_cols);
+    a.slice_rows = ctx->slice_rows;
     int grid = grid_override > 0 ? grid_override
                                  : ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
     cudaError_t e = launch_explore(a, grid, s);
@@ -995,15 +996,30 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
 extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
     if (!ctx) return WK_E_BADARG;
     std::lock_guard<std::mutex> lk(ctx->mu);
-    if (value != 2 && value != 4 && value != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
-    if (knob == WK_KNOB_LANES) {
-        ctx->default_lanes = value;
-        ctx->tuned_lanes.clear();
-    } else if (knob == WK_KNOB_BATCH_LANES) {
-        ctx->batch_lanes = value;
+    if (knob == WK_KNOB_LANES || knob == WK_KNOB_BATCH_LANES) {
+        if (value != 2 && value != 4 && value != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
+        if (knob == WK_KNOB_LANES) {
+            ctx->default_lanes = value;
+            ctx->tuned_lanes.clear();
+        } else {
+            ctx->batch_lanes = value;
+        }
+    } else if (knob == WK_KNOB_SLICE_ROWS || knob == WK_KNOB_BATCH_SLICE_ROWS) {
+        if (value < wk::kHeavyRows || value > (1 << 24))
+            return ctx->fail(WK_E_BADARG, "slice threshold must be in [128, 2^24]");
+        (knob == WK_KNOB_SLICE_ROWS ? ctx->slice_rows : ctx->batch_slice_rows) = (uint32_t)value;
     } else {
         return ctx->fail(WK_E_BADARG, "unknown knob");
     }
+    ctx->drop_graphs();
+    return WK_SUCCESS;
+}
+
+// Lanes of one (op, input columns) step of single queries (an autotuner's per-step choice).
+int wk::tune_step_lanes(wk_ctx* ctx, int op, int cols, int lanes) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (lanes != 2 && lanes != 4 && lanes != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
+    ctx->tuned_lanes[op * 1000 + cols] = lanes;
     ctx->drop_graphs();
     return WK_SUCCESS;
 }
@@ -1013,6 +1029,9 @@ extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (knob == WK_KNOB_LANES) *value = ctx->default_lanes;
     else if (knob == WK_KNOB_BATCH_LANES) *value = ctx->batch_lanes;
+    else if (knob == WK_KNOB_SLICE_ROWS) *value = (int32_t)std::max<uint32_t>(ctx->slice_rows, wk::kHeavyRows);
+    else if (knob == WK_KNOB_BATCH_SLICE_ROWS)
+        *value = (int32_t)std::max<uint32_t>(ctx->batch_slice_rows, wk::kHeavyRows);
     else return ctx->fail(WK_E_BADARG, "unknown knob");
     return WK_SUCCESS;
 }

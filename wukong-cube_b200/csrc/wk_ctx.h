@@ -77,6 +77,8 @@ struct wk_ctx {
     int default_lanes = 2;
     int batch_lanes = 4;
     std::map<int, int> tuned_lanes;
+    uint32_t slice_rows = 0;         // list length above which rows go to the slice queue
+    uint32_t batch_slice_rows = 0;   // (0: the kernel's default, kHeavyRows)
 
     // scan control of the context stream
     wk::StepCtl* d_ctl = nullptr;
@@ -160,4 +162,6 @@ int ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas, wk
 int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows);
 // Copy `elems` elements of a device table to host memory (host sync).
 int table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host);
+// Lanes for one (explore op, input columns) step of single queries (the autotuner's choice).
+int tune_step_lanes(wk_ctx* ctx, int op, int cols, int lanes);
 }  // namespace wk

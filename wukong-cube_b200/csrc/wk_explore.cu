@@ -229,7 +229,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     WK_PH(2);
     for (int i = threadIdx.x; i < n; i += kStepThreads) {
         const uint32_t c = B.cnt[i];
-        const bool heavy = c > (uint32_t)kHeavyRows;
+        const bool heavy = c > max(a.slice_rows, (uint32_t)kHeavyRows);
         B.lcnt[i] = heavy ? 0u : c;
         if (heavy) S.has_heavy = 1;
     }
@@ -289,7 +289,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     if (S.has_heavy && fits) {
         for (int i = threadIdx.x; i < n; i += kStepThreads) {
             const uint32_t c = B.cnt[i];
-            if (c <= (uint32_t)kHeavyRows) continue;
+            if (c <= max(a.slice_rows, (uint32_t)kHeavyRows)) continue;
             const uint32_t nch = (c + kHeavyChunk - 1) / kHeavyChunk;
             const unsigned long long at = atomicAdd(&a.ctl->heavy_n, (unsigned long long)nch);
             for (uint32_t k = 0; k < nch; ++k) {

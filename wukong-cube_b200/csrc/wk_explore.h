@@ -75,6 +75,10 @@ struct ExploreArgs {
     unsigned long long* status;
     int32_t sorted_lists;
     int32_t lanes;
+    // Rows with more output rows than this go to the slice queue (spread over every CTA);
+    // shorter ones are written by the CTA that scanned them.  0 means kHeavyRows; values below
+    // kHeavyRows are raised to it (the queue is sized for that).
+    uint32_t slice_rows;
 };
 
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);

@@ -53,23 +53,24 @@ __global__ void list_kernel(const ListArgs a) {
 
 // Checks that every key's list is strictly ascending (the loader's sort + dedup), which lets
 // the filters binary-search long lists.
+// One warp per slot; the lanes walk the slot's list together (coalesced), so a hub list costs
+// len/32 steps of one warp instead of len steps of one thread.
 __global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const uint32_t* edges,
                                     uint64_t n_edges, unsigned* unsorted) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_slots;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t i = blockIdx.x * (uint64_t)(blockDim.x / 32) + threadIdx.x / 32; i < n_slots; i += warps) {
         if ((i & (kAssoc - 1)) == kAssoc - 1) continue;   // chain link
         const Slot s = slots[i];
         if (s.key == 0) continue;
         const uint64_t off = ptr_off(s.ptr), sz = ptr_size(s.ptr);
         if (off + sz > n_edges) {
-            atomicOr(unsorted, 2u);
+            if (lane == 0) atomicOr(unsorted, 2u);
             continue;
         }
-        for (uint64_t k = 1; k < sz; ++k)
-            if (edges[off + k - 1] >= edges[off + k]) {
-                atomicOr(unsorted, 1u);
-                break;
-            }
+        bool bad = false;
+        for (uint64_t k = 1 + lane; k < sz && !bad; k += 32) bad = __ldg(edges + off + k - 1) >= __ldg(edges + off + k);
+        if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(unsorted, 1u);
     }
 }
 
@@ -82,7 +83,7 @@ cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s) {
 }
 
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s) {
-    sorted_check_kernel<<<1024, 256, 0, s>>>(st.slots, st.n_buckets * kAssoc, st.edges, st.n_edges, d_flag);
+    sorted_check_kernel<<<4096, 256, 0, s>>>(st.slots, st.n_buckets * kAssoc, st.edges, st.n_edges, d_flag);
     return cudaGetLastError();
 }
 

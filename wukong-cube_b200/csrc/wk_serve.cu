@@ -246,6 +246,7 @@ struct Serve {
         a.status = ctx->d_status;
         a.sorted_lists = ctx->sorted_lists;
         a.lanes = ctx->batch_lanes;
+        a.slice_rows = ctx->batch_slice_rows;
         return a;
     }
 

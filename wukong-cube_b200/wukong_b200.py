@@ -19,6 +19,7 @@ IN, OUT = 0, 1
 PREDICATE_ID, TYPE_ID = 0, 1
 NO_RESULT = 0xFFFF
 MODE_PLAIN, MODE_RESIDENT, MODE_GRAPH = 0, 1, 2
+KNOB_LANES, KNOB_BATCH_LANES, KNOB_SLICE_ROWS, KNOB_BATCH_SLICE_ROWS = 0, 1, 2, 3
 
 SUCCESS = 0
 UNKNOWN_PATTERN = 3
@@ -76,6 +77,14 @@ class ServeConfig(C.Structure):
                 ("light_proj_bytes", C.c_uint64), ("heavy_proj_bytes", C.c_uint64),
                 ("max_inflight", C.c_uint32), ("max_heavy_inflight", C.c_uint32),
                 ("light_ctas_per_sm", C.c_int32), ("blind", C.c_int32), ("reserved", C.c_int32 * 2)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("batch_lanes", C.c_int32), ("batch_slice_rows", C.c_int32), ("lanes", C.c_int32),
+                ("slice_rows", C.c_int32), ("batch_ms_default", C.c_double),
+                ("batch_ms_tuned", C.c_double), ("single_ms_default", C.c_double),
+                ("single_ms_tuned", C.c_double), ("candidates", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class StepProf(C.Structure):
@@ -158,6 +167,7 @@ _SIGS = {
     "wk_debug_phase_cycles": (C.c_int, [C.POINTER(C.c_ulonglong), C.c_int32, C.c_int32]),
     "wk_ctx_tune_set": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "wk_ctx_tune_get": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32)]),
+    "wk_ctx_autotune": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
     "wk_batch_profile": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32,
                                    C.POINTER(StepProf), C.c_int32, C.POINTER(C.c_int32)]),
     "wk_serve_run_open_loop": (C.c_int, [_P, C.POINTER(ServeConfig), C.POINTER(QueryC),
@@ -393,6 +403,13 @@ class Context:
         v = C.c_int32()
         _check(lib().wk_ctx_tune_get(self.h, knob, C.byref(v)), self.h)
         return v.value
+
+    def autotune(self, queries, iters=5):
+        """Time every knob setting on these queries and keep the fastest; returns the choice."""
+        qs, keep = queries_as_c(queries)
+        r = TuneResult()
+        _check(lib().wk_ctx_autotune(self.h, qs, len(queries), iters, C.byref(r)), self.h)
+        return {k: getattr(r, k) for k, _ in TuneResult._fields_ if k != "reserved"}
 
     def upload_gstore(self, g):
         _check(lib().wk_store_upload_gstore(self.h, g.h), self.h)
