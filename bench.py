@@ -212,19 +212,27 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
             assert np.array_equal(orows.astype(np.int64), rows[light]), "serving row counts differ"
             for j, i in enumerate(hidx):
                 assert rows[i] == heavy_rows[j % 2], "serving heavy row count differs"
-        span = (max(r[3] for r in res) - arrivals[0]) / 1e6
+        done = np.array([r[3] for r in res])
+        span = (done.max() - arrivals[0]) / 1e6
+        light_span = (done[~is_heavy].max() - arrivals[0]) / 1e6
         ll, hl = lat[~is_heavy], lat[is_heavy]
         sweep.append({"offered_qps": qps, "queries": n, "heavy": int(is_heavy.sum()),
                       "completed_qps": n / span,
+                      "light_completed_qps": int((~is_heavy).sum()) / light_span,
+                      "light_offered_qps": qps * float((~is_heavy).mean()),
                       "light_us": {"p50": _pct(ll, 50), "p99": _pct(ll, 99), "p99.9": _pct(ll, 99.9)},
                       "heavy_us": {"p50": _pct(hl, 50), "p99": _pct(hl, 99), "max": float(hl.max())}})
-    ok = [s for s in sweep if s["light_us"]["p99"] <= 1000.0 and s["completed_qps"] >= 0.9 * s["offered_qps"]]
+    # light queries: the highest offered rate whose light p99 stays within 1 ms while light
+    # completions keep up with light arrivals; the heavy lane's throughput is reported apart
+    ok = [s for s in sweep if s["light_us"]["p99"] <= 1000.0 and
+          s["light_completed_qps"] >= 0.95 * s["light_offered_qps"]]
     best = max(ok, key=lambda s: s["offered_qps"]) if ok else None
     return {"mix": "98% light (batch shapes) / 2% heavy (star, triangle); open-loop Poisson; "
                    "blind replies (row counts); heavy queries on a low-priority lane",
             "sweep": sweep,
-            "sustained_qps_light_p99_le_1ms": best["offered_qps"] if best else None,
-            "sustained_vs_plain": (best["offered_qps"] / plain_qps) if best else None}
+            "sustained_qps_light_p99_le_1ms": best["light_offered_qps"] if best else None,
+            "sustained_offered_qps_at_that_point": best["offered_qps"] if best else None,
+            "sustained_vs_plain": (best["light_offered_qps"] / plain_qps) if best else None}
 
 
 def run_ours(args, world, rank, local_rank):
@@ -259,6 +267,9 @@ def run_ours(args, world, rank, local_rank):
         for i in range(0, len(qs), max(1, len(qs) // 256)):
             st, want, _ = o.run(qs[i].flat(), qs[i].nvars)
             assert np.array_equal(oracle.sorted_rows(res[i][0]), oracle.sorted_rows(want)), i
+    # the autotuner picks the tile schedule (lanes, slice threshold) on this batch and on the
+    # heavy queries; the timed runs below use its choice
+    tune = ctx.autotune(qs + [workloads.heavy_star(v), workloads.heavy_triangle(v)], iters=3)
     ctx.batch_device(qs)   # capture for replay
     for _ in range(args.warmup):
         ctx.batch_replay()
@@ -366,6 +377,7 @@ def run_ours(args, world, rank, local_rank):
                                "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"]},
             "batch_levels": levels,
             "batch_other_ms": overheads,
+            "autotune": tune,
             "serving": serving,
             "gpu_launches": args.steps * (len(levels) + 2),
             "clocks": clk.summary()}

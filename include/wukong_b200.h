@@ -324,13 +324,17 @@ int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
  *   knob 2: the list length above which a row's output is written as 2,048-row slices by every
  *           CTA (block-per-row) instead of by the CTA that probed it (group-per-row); 128 to
  *           2^24, default 128;
- *   knob 3: the same for batches and serving.
+ *   knob 3: the same for batches and serving;
+ *   knob 4: single-query steps of index-start plans (and single steps) whose input has at
+ *           least this many rows run as the flat count / scan / expand pipeline instead of the
+ *           tile launch; 0 never does (default 65,536).
  * wk_ctx_tune_get reads a knob back.  No reference counterpart (its launch shape is fixed,
  * gpu_hash.cu:96-326). */
 #define WK_KNOB_LANES 0
 #define WK_KNOB_BATCH_LANES 1
 #define WK_KNOB_SLICE_ROWS 2
 #define WK_KNOB_BATCH_SLICE_ROWS 3
+#define WK_KNOB_FLAT_ROWS 4
 int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value);
 int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value);
 

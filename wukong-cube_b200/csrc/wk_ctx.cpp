@@ -89,6 +89,22 @@ int wk_ctx::ensure_heavy(uint64_t out_rows_cap) {
     return WK_SUCCESS;
 }
 
+int wk_ctx::ensure_flat(uint64_t in_rows_cap) {
+    if (in_rows_cap <= flat_cap_rows && d_flat) return WK_SUCCESS;
+    const uint64_t rows = std::max<uint64_t>(in_rows_cap + in_rows_cap / 4, 1 << 16);
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    if (d_flat) cudaFree(d_flat);
+    d_flat = nullptr;
+    flat_cap_rows = 0;
+    if (cudaMalloc(&d_flat, wk::flat_scratch_bytes(rows, wk::flat_grid(sm_count))) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WK_E_OOM, "flat pipeline scratch");
+    }
+    flat_cap_rows = rows;
+    drop_graphs();   // captured launches hold the old scratch pointers
+    return WK_SUCCESS;
+}
+
 int wk_ctx::ensure_status(uint64_t tiles) {
     if (tiles <= status_cap) return WK_SUCCESS;
     uint64_t cap = std::max<uint64_t>(tiles + tiles / 2, 1 << 14);
@@ -220,7 +236,7 @@ int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, 
 }
 
 int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* out,
-                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override) {
+                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override, int flat_mode) {
     out->cols = st.out_cols;
     if (st.kind == PlanStep::kIndex || st.kind == PlanStep::kConst) {
         ListArgs a{};
@@ -272,10 +288,43 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
     a.sorted_lists = ctx->sorted_lists;
     a.lanes = ctx->lanes_for(a.one.op, st.in_cols);
     a.slice_rows = ctx->slice_rows;
-    int grid = grid_override > 0 ? grid_override
-                                 : ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
-    cudaError_t e = launch_explore(a, grid, s);
-    if (e != cudaSuccess) return ctx->cuda_fail(e, "exploration launch");
+    // The flat pipeline needs its scratch sized for this input; without it the tile launch runs.
+    if (!ctx->flat_min_rows || !ctx->d_flat || a.in_cap_rows > ctx->flat_cap_rows ||
+        a.in_cap_rows < ctx->flat_min_rows || grid_override > 0)
+        flat_mode = kTileOnly;
+    if (flat_mode != kFlatOnly) {
+        if (flat_mode == kFlatAuto) a.max_rows = ctx->flat_min_rows;
+        int grid = grid_override > 0 ? grid_override
+                                     : ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
+        cudaError_t e = launch_explore(a, grid, s);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "exploration launch");
+    }
+    if (flat_mode != kTileOnly) {
+        FlatArgs f{};
+        f.store = a.store;
+        f.seg_index[0] = a.seg_index[0];
+        f.seg_index[1] = a.seg_index[1];
+        f.step = a.one;
+        f.in_rows = a.in_rows;
+        f.in = a.in;
+        f.w_in = a.w_in;
+        f.in_cap_rows = a.in_cap_rows;
+        f.out = a.out;
+        f.w_out = a.w_out;
+        f.out_cap_rows = a.out_cap_rows;
+        f.out_rows = a.out_rows;
+        f.min_rows = flat_mode == kFlatAuto ? ctx->flat_min_rows : 0;
+        // a serving lane takes half of each SM (4 of 8 CTAs of 256 threads, 32 registers each),
+        // which leaves room for the iteration launches' CTAs beside it
+        const int grid = ctx->beside_ctas > 0 ? ctx->sm_count * 4 : flat_grid(ctx->sm_count);
+        f.pos = reinterpret_cast<uint64_t*>(ctx->d_flat);
+        f.off = f.pos + ctx->flat_cap_rows + 1;
+        f.part = f.off + ctx->flat_cap_rows;
+        f.ctl = ctx->d_ctl;
+        f.sorted_lists = ctx->sorted_lists;
+        cudaError_t e = launch_flat(f, grid, s);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "flat pipeline launch");
+    }
     return WK_SUCCESS;
 }
 
@@ -402,6 +451,7 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     if (e == cudaSuccess) e = wk::small_kernel_attrs();
     if (e == cudaSuccess) e = wk::batch_kernel_attrs();
     if (e == cudaSuccess) e = wk::serve_kernel_attrs();
+    if (e == cudaSuccess) e = wk::flat_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
     e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
@@ -434,6 +484,7 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     if (ctx->d_edges && !ctx->borrowed_store) cudaFree(ctx->d_edges);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_heavy) cudaFree(ctx->d_heavy);
+    if (ctx->d_flat) cudaFree(ctx->d_flat);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_rows) cudaFreeHost(ctx->h_rows);
@@ -617,14 +668,24 @@ extern "C" int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dp
 static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in, wk_table* out,
                          int32_t mt_tid, int32_t mt_factor) {
     if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    int flat = wk::kTileOnly;
     if (in && in->cols > 0) {
         int rc = ctx->ensure_status(in->cap / in->cols / wk::kTileRows + 2);
         if (rc) return rc;
+        // the host syncs after every step here anyway, so it picks the launch by the row count
+        uint64_t rows = 0;
+        rc = table_rows(ctx, in, &rows);
+        if (rc) return rc;
+        if (ctx->flat_min_rows && rows >= ctx->flat_min_rows) {
+            rc = ctx->ensure_flat(in->cap / in->cols);
+            if (rc) return rc;
+            flat = wk::kFlatOnly;
+        }
     }
     for (int attempt = 0; attempt < 8; ++attempt) {
         int rc = ctx->ensure_heavy(out->cap);
         if (rc) return rc;
-        rc = wk::enqueue_step(ctx, st, in, out, mt_tid, mt_factor, ctx->stream, 0);
+        rc = wk::enqueue_step(ctx, st, in, out, mt_tid, mt_factor, ctx->stream, 0, flat);
         if (rc) return rc;
         uint32_t err = 0;
         uint64_t need = 0;
@@ -741,14 +802,33 @@ static std::string plan_key(const std::vector<wk::PlanStep>& steps, const wk_que
         put(&t.cap, sizeof(t.cap));
     }
     put(&ctx->d_status, sizeof(ctx->d_status));
+    put(&ctx->d_flat, sizeof(ctx->d_flat));
+    put(&ctx->flat_cap_rows, sizeof(ctx->flat_cap_rows));
+    put(&ctx->flat_min_rows, sizeof(ctx->flat_min_rows));
     return k;
 }
 
+// Plans that start from an index build large tables: their steps launch both the tile launch
+// and the flat pipeline, and the device picks by the row count.
+static int plan_flat_mode(const std::vector<wk::PlanStep>& steps) {
+    return (!steps.empty() && steps[0].kind == wk::PlanStep::kIndex) ? wk::kFlatAuto : wk::kTileOnly;
+}
+
+// Flat scratch for every step input of a plan (the rbuf capacities bound the row counts).
+static int plan_ensure_flat(wk_ctx* ctx, const std::vector<wk::PlanStep>& steps) {
+    if (plan_flat_mode(steps) == wk::kTileOnly || !ctx->flat_min_rows) return WK_SUCCESS;
+    uint64_t rows = 0;
+    for (size_t i = 1; i < steps.size(); ++i)
+        if (steps[i].in_cols > 0) rows = std::max<uint64_t>(rows, ctx->rbuf[(i - 1) & 1].cap / steps[i].in_cols);
+    return rows >= ctx->flat_min_rows ? ctx->ensure_flat(rows) : WK_SUCCESS;
+}
+
 static int enqueue_plan(wk_ctx* ctx, const std::vector<wk::PlanStep>& steps, const wk_query& q) {
+    const int fm = plan_flat_mode(steps);
     for (size_t i = 0; i < steps.size(); ++i) {
         const wk_table* in = i ? &ctx->rbuf[(i - 1) & 1] : nullptr;
         wk_table* out = &ctx->rbuf[i & 1];
-        int rc = wk::enqueue_step(ctx, steps[i], in, out, q.mt_tid, q.mt_factor, ctx->stream, 0);
+        int rc = wk::enqueue_step(ctx, steps[i], in, out, q.mt_tid, q.mt_factor, ctx->stream, 0, fm);
         if (rc) return rc;
     }
     return WK_SUCCESS;
@@ -785,6 +865,8 @@ static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
             rc = ctx->ensure_status(mx / wk::kTileRows + 2);
             if (rc) return rc;
             rc = ctx->ensure_heavy(mx);
+            if (rc) return rc;
+            rc = plan_ensure_flat(ctx, steps);
             if (rc) return rc;
             if (mode == WK_MODE_GRAPH) {
                 std::string key = plan_key(steps, *q, ctx);
@@ -942,6 +1024,9 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
     const wk_table* t = nullptr;
     rc = query_run(ctx, q, WK_MODE_PLAIN, &t, nullptr, nullptr);   // sizes the buffers
     if (rc) return rc;
+    rc = plan_ensure_flat(ctx, steps);
+    if (rc) return rc;
+    const int fm = plan_flat_mode(steps);
     cudaEvent_t e0, e1;
     WK_CUDA(ctx, cudaEventCreate(&e0));
     WK_CUDA(ctx, cudaEventCreate(&e1));
@@ -952,7 +1037,7 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
             wk_table* o = &ctx->rbuf[i & 1];
             WK_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 16, ctx->stream));
             WK_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
-            rc = wk::enqueue_step(ctx, steps[i], in, o, q->mt_tid, q->mt_factor, ctx->stream, 0);
+            rc = wk::enqueue_step(ctx, steps[i], in, o, q->mt_tid, q->mt_factor, ctx->stream, 0, fm);
             if (rc) return rc;
             WK_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
             WK_CUDA(ctx, cudaEventSynchronize(e1));
@@ -1008,6 +1093,9 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
         if (value < wk::kHeavyRows || value > (1 << 24))
             return ctx->fail(WK_E_BADARG, "slice threshold must be in [128, 2^24]");
         (knob == WK_KNOB_SLICE_ROWS ? ctx->slice_rows : ctx->batch_slice_rows) = (uint32_t)value;
+    } else if (knob == WK_KNOB_FLAT_ROWS) {
+        if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
+        ctx->flat_min_rows = (uint64_t)value;
     } else {
         return ctx->fail(WK_E_BADARG, "unknown knob");
     }
@@ -1032,6 +1120,7 @@ extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
     else if (knob == WK_KNOB_SLICE_ROWS) *value = (int32_t)std::max<uint32_t>(ctx->slice_rows, wk::kHeavyRows);
     else if (knob == WK_KNOB_BATCH_SLICE_ROWS)
         *value = (int32_t)std::max<uint32_t>(ctx->batch_slice_rows, wk::kHeavyRows);
+    else if (knob == WK_KNOB_FLAT_ROWS) *value = (int32_t)std::min<uint64_t>(ctx->flat_min_rows, INT32_MAX);
     else return ctx->fail(WK_E_BADARG, "unknown knob");
     return WK_SUCCESS;
 }

@@ -9,6 +9,7 @@
 
 #include "wk_internal.h"
 #include "wk_explore.h"
+#include "wk_flat.h"
 #include "wk_kernels.h"
 
 // A device result table (the reference's rbuf + GPUResult, query.hpp:311-362).
@@ -79,6 +80,10 @@ struct wk_ctx {
     std::map<int, int> tuned_lanes;
     uint32_t slice_rows = 0;         // list length above which rows go to the slice queue
     uint32_t batch_slice_rows = 0;   // (0: the kernel's default, kHeavyRows)
+    // single-query steps with at least this many input rows run the flat pipeline (0: never)
+    uint64_t flat_min_rows = 65536;
+    void* d_flat = nullptr;          // its scratch (wk_flat.h)
+    uint64_t flat_cap_rows = 0;
 
     // scan control of the context stream
     wk::StepCtl* d_ctl = nullptr;
@@ -141,15 +146,23 @@ struct wk_ctx {
     void drop_graphs();
     int ensure_status(uint64_t tiles);
     int ensure_heavy(uint64_t out_rows_cap);
+    int ensure_flat(uint64_t in_rows_cap);
     int table_reserve(wk_table* t, uint64_t elems);
     int read_ctl(uint32_t* err, uint64_t* need);
     int clear_ctl_err();
 };
 
 namespace wk {
+// How a known_to_* step of a single query is launched.
+enum FlatMode {
+    kTileOnly = 0,   // the tile launch (wk_explore.cu)
+    kFlatAuto = 1,   // both, each guarded on the device by flat_min_rows: one of them runs
+    kFlatOnly = 2,   // the flat pipeline (wk_flat.cu); needs ensure_flat for the input
+};
 // Enqueue one resolved step reading `in` (may be null for index/const starts) into `out`.
 int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* out,
-                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override);
+                 int32_t mt_tid, int32_t mt_factor, cudaStream_t s, int grid_override,
+                 int flat_mode = kTileOnly);
 // The device descriptor of a resolved step.
 StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s);
 

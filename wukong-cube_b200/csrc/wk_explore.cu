@@ -374,13 +374,14 @@ __global__ void __launch_bounds__(kStepThreads, 6) explore_kernel(const ExploreA
     const unsigned epoch = *(volatile unsigned*)&a.ctl->epoch;
     uint64_t R = a.virtual_rows ? a.n_queries : *(volatile const uint64_t*)a.in_rows;
     if (!a.virtual_rows && R > a.in_cap_rows) R = a.in_cap_rows;
-    uint64_t ntiles = (R + kTileRows - 1) / kTileRows;
+    const bool handed_off = !a.virtual_rows && a.max_rows && R >= a.max_rows;   // flat pipeline's
+    uint64_t ntiles = handed_off ? 0 : (R + kTileRows - 1) / kTileRows;
     if (ntiles > a.ctl->status_cap) {
         if (threadIdx.x == 0) atomicOr(&a.ctl->err, kErrStatus);
         ntiles = 0;
     }
     const uint64_t obase = a.out_base_rows ? *(volatile const uint64_t*)a.out_base_rows : 0;
-    if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = obase;
+    if (ntiles == 0 && !handed_off && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = obase;
     WK_PH_DECL
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);

@@ -79,6 +79,9 @@ struct ExploreArgs {
     // shorter ones are written by the CTA that scanned them.  0 means kHeavyRows; values below
     // kHeavyRows are raised to it (the queue is sized for that).
     uint32_t slice_rows;
+    // When nonzero and the input has at least this many rows, the launch does nothing (the
+    // flat pipeline of wk_flat.cu runs the step instead).
+    uint64_t max_rows;
 };
 
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);

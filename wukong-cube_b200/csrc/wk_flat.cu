@@ -1,0 +1,299 @@
+// Flat pipeline for large single-query steps: count -> scan -> scatter.
+//
+// The tile launch (wk_explore.cu) keeps a whole step in one persistent launch, which suits the
+// many small tables of a batch but pays per-tile barriers and look-back waits, and runs at
+// the occupancy its shared memory allows.  For one large table (index-start queries: 1e5 to
+// 1e8 rows) the same step runs here as four short launches at full occupancy, each a
+// streaming pass except for the probes themselves:
+//   1. count: one thread per input row probes the key table (two 16-byte slots per load, the
+//      chain followed through slot 7), records the row's output count (list size for
+//      known_to_unknown, 0/1 membership for known_to_known / known_to_const) and its list offset;
+//      each CTA owns a contiguous chunk of rows and publishes the chunk total;
+//   2. scan: one CTA scans the chunk totals, checks the output capacity (overflow sets
+//      kErrOverflow and the rows needed, as the tile launch does) and sets the row count;
+//   3. place: each CTA scans its chunk into per-row output positions; filters copy their
+//      surviving rows straight to the output here;
+//   4. expand (known_to_unknown only): the output rows are split evenly over the CTAs; each CTA
+//      finds its first input row by a 32-way search of the positions and writes its rows in
+//      row-major then edge order (sparql.hpp:328-370), consecutive threads on consecutive rows.
+// Row counts are read on the device, so the launches chain without a host round trip and can
+// be captured in a graph.  Every launch returns at once unless the input has at least
+// `min_rows` rows; the tile launch of the same step is given the complementary bound, so
+// exactly one of the two writes the output.
+#include <cuda_runtime.h>
+
+#include "../../include/wukong_b200.h"
+#include "wk_device.cuh"
+#include "wk_flat.h"
+
+namespace wk {
+namespace {
+using namespace dev;
+
+constexpr int kFlatThreads = 256;
+constexpr int kWindow = 256;   // input rows staged per expand round
+
+__device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
+    uint64_t R = *(volatile const uint64_t*)a.in_rows;
+    return R > a.in_cap_rows ? a.in_cap_rows : R;
+}
+
+// Probe one key by one thread: the home bucket's slots two at a time (one 32-byte sector),
+// then the chain through slot 7.  Returns the pointer word, 0 when absent.
+__device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t key, uint64_t bucket,
+                                                 unsigned* err) {
+    for (int hop = 0; hop < kMaxProbeIters; ++hop) {
+        if (bucket >= st.n_buckets) {
+            atomicOr(err, kErrCorrupt);
+            return 0;
+        }
+        const Slot* b = st.slots + bucket * kAssoc;
+#pragma unroll
+        for (int s = 0; s < kAssoc - 1; s += 2) {
+            const ulonglong2 s0 = load_slot(b + s);   // both slots: one 32-byte sector
+            const ulonglong2 s1 = load_slot(b + s + 1);
+            if (s0.x == key) return s0.y;
+            if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
+            if (s + 1 == kAssoc - 1) {   // slot 7: the chain link
+                if (s1.x == 0) return 0;
+                bucket = key_vid(s1.x);
+                break;
+            }
+            if (s1.x == key) return s1.y;
+            if (s1.x == 0) return 0;
+        }
+    }
+    atomicOr(err, kErrCorrupt);
+    return 0;
+}
+
+// Is `target` in the list edges[off, off + deg)?  Binary search when lists are sorted.
+__device__ __forceinline__ bool thread_member(const uint32_t* edges, uint64_t off, uint64_t deg,
+                                              uint32_t target, bool sorted) {
+    const uint32_t* p = edges + off;
+    if (sorted) {
+        uint64_t lo = 0, hi = deg;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (__ldg(p + mid) < target) lo = mid + 1; else hi = mid;
+        }
+        return lo < deg && __ldg(p + lo) == target;
+    }
+    for (uint64_t k = 0; k < deg; ++k)
+        if (__ldg(p + k) == target) return true;
+    return false;
+}
+
+__device__ __forceinline__ void chunk_of(uint64_t R, uint64_t* lo, uint64_t* hi) {
+    const uint64_t chunk = (R + gridDim.x - 1) / gridDim.x;
+    *lo = min(R, (uint64_t)blockIdx.x * chunk);
+    *hi = min(R, *lo + chunk);
+}
+
+__device__ __forceinline__ uint64_t block_sum(uint64_t x, uint64_t* s_warp) {
+    const uint64_t ex = block_exclusive_sum<kFlatThreads>(x, s_warp);
+    __shared__ uint64_t s_tot;
+    if (threadIdx.x == kFlatThreads - 1) s_tot = ex + x;
+    __syncthreads();
+    const uint64_t t = s_tot;
+    __syncthreads();
+    return t;
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs a) {
+    __shared__ uint64_t s_warp[kFlatThreads / 32];
+    const uint64_t R = flat_rows(a);
+    if (R < a.min_rows) return;
+    uint64_t lo, hi;
+    chunk_of(R, &lo, &hi);
+    const StepDesc& d = a.step;
+    const bool filt = d.op == kXK2K || d.op == kXK2C;
+    uint64_t sum = 0, sd = 0, nvalid = 0;
+    for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
+        const uint32_t* row = a.in + r * (uint64_t)a.w_in;
+        const uint32_t cur = __ldg(row + d.cs);
+        uint32_t target = d.end_const;
+        if (d.op == kXK2K) target = __ldg(row + d.ce);
+        uint64_t key;
+        const SegDesc* sg = &d.seg;
+        bool valid = cur != kBlankId;
+        if (d.op == kXK2U && d.type_index) {
+            // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+            key = make_key(0, cur, kIn);
+            sg = &a.seg_index[kIn];
+            if (cur >= (1u << kNbitsIdx)) valid = false;
+        } else {
+            key = make_key(cur, d.pid, d.dir);
+            if (cur == 0) sg = &a.seg_index[d.dir & 1];   // vid 0 names the index
+        }
+        uint64_t off = 0, deg = 0;
+        if (valid && sg->num_buckets != 0 && key != 0) {
+            const uint64_t p = thread_probe(a.store, key, bucket_of(key, *sg), &a.ctl->err);
+            off = ptr_off(p);
+            deg = ptr_size(p);
+            if (off + deg > a.store.n_edges) {
+                if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
+                deg = 0;
+            }
+        }
+        uint32_t c = (uint32_t)deg;
+        if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
+        if (!valid) c = 0;
+        a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
+        if (!filt) a.off[r] = off;
+        sum += c;
+        if (valid) {
+            sd += deg;
+            ++nvalid;
+        }
+    }
+    const uint64_t total = block_sum(sum, s_warp);
+    const uint64_t tsd = block_sum(sd, s_warp);
+    const uint64_t tvalid = block_sum(nvalid, s_warp);
+    if (threadIdx.x == 0) {
+        a.part[blockIdx.x] = total;
+        if (tvalid) {
+            atomicAdd(&a.ctl->sum_deg, (unsigned long long)tsd);
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(tvalid * (d.cin * 4ull + 16) + tsd * 4));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) flat_scan_kernel(const FlatArgs a, uint32_t nparts) {
+    __shared__ uint64_t s_warp[32];
+    __shared__ uint64_t s_carry;
+    const uint64_t R = flat_rows(a);
+    if (R < a.min_rows) return;
+    if (threadIdx.x == 0) s_carry = 0;
+    for (uint32_t r0 = 0; r0 < nparts; r0 += 1024) {
+        const uint32_t i = r0 + threadIdx.x;
+        const uint64_t x = i < nparts ? a.part[i] : 0;
+        const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < nparts) a.part[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry = carry + ex + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint64_t total = s_carry;
+        a.part[nparts] = total;
+        a.pos[R] = total;
+        if (total > a.out_cap_rows) {
+            atomicOr(&a.ctl->err, kErrOverflow);
+            atomicMax(&a.ctl->need, (unsigned long long)total);
+            *a.out_rows = 0;
+        } else {
+            *a.out_rows = total;
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(total * a.step.cout * 4ull));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs a, uint32_t nparts) {
+    __shared__ uint64_t s_warp[kFlatThreads / 32];
+    __shared__ uint64_t s_carry;
+    const uint64_t R = flat_rows(a);
+    if (R < a.min_rows || a.part[nparts] > a.out_cap_rows) return;
+    uint64_t lo, hi;
+    chunk_of(R, &lo, &hi);
+    const bool filt = a.step.op == kXK2K || a.step.op == kXK2C;
+    if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
+    __syncthreads();
+    for (uint64_t r0 = lo; r0 < hi; r0 += kFlatThreads) {
+        const uint64_t r = r0 + threadIdx.x;
+        const uint64_t c = r < hi ? a.pos[r] : 0;
+        const uint64_t ex = block_exclusive_sum<kFlatThreads>(c, s_warp);
+        const uint64_t p = s_carry + ex;
+        if (r < hi) {
+            if (!filt) {
+                a.pos[r] = p;
+            } else if (c) {   // a surviving row keeps its columns (w_out == w_in)
+                const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+                uint32_t* dst = a.out + p * (uint64_t)a.w_out;
+                for (int k = 0; k < a.w_in; ++k) dst[k] = __ldg(src + k);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == kFlatThreads - 1) s_carry = p + c;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArgs a) {
+    __shared__ uint64_t s_pos[kWindow + 1];
+    __shared__ uint64_t s_off[kWindow];
+    __shared__ uint64_t s_i0;
+    const uint64_t R = flat_rows(a);
+    if (R < a.min_rows) return;
+    const uint64_t total = a.pos[R];
+    if (total > a.out_cap_rows || total == 0) return;
+    const uint64_t per = (total + gridDim.x - 1) / gridDim.x;
+    const uint64_t j0 = min(total, (uint64_t)blockIdx.x * per), j1 = min(total, j0 + per);
+    if (j0 >= j1) return;
+    // first input row whose outputs reach j0: the last r with pos[r] <= j0 (pos[R] = total > j0)
+    if (threadIdx.x < 32) {
+        uint64_t lo = 0, hi = R;   // invariant: pos[lo] <= j0 < pos[hi]
+        while (hi - lo > 1) {
+            const uint64_t step = (hi - lo + 31) / 32;
+            const uint64_t probe = min(hi, lo + (uint64_t)(threadIdx.x + 1) * step);
+            const bool le = probe < hi && a.pos[probe] <= j0;
+            const unsigned m = __ballot_sync(0xffffffffu, le);
+            const int k = m ? 31 - __clz(m) : -1;   // last lane whose probe is still <= j0
+            const uint64_t nlo = k >= 0 ? min(hi, lo + (uint64_t)(k + 1) * step) : lo;
+            const uint64_t nhi = min(hi, nlo + step);
+            lo = nlo;
+            hi = max(nhi, lo + 1);
+        }
+        if (threadIdx.x == 0) s_i0 = lo;
+    }
+    __syncthreads();
+    const int wo = a.w_out, cin = a.w_in, ecol = a.step.cin;
+    uint64_t i = s_i0;
+    uint64_t j = j0;
+    while (j < j1 && i < R) {
+        const uint64_t n = min((uint64_t)kWindow, R - i);
+        for (int t = threadIdx.x; t <= (int)n; t += kFlatThreads) s_pos[t] = a.pos[i + t];
+        for (int t = threadIdx.x; t < (int)n; t += kFlatThreads) s_off[t] = a.off[i + t];
+        __syncthreads();
+        const uint64_t wend = min(j1, s_pos[n]);
+        for (uint64_t jj = j + threadIdx.x; jj < wend; jj += kFlatThreads) {
+            int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+            }
+            const uint64_t r = i + lo;
+            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+            uint32_t* dst = a.out + jj * (uint64_t)wo;
+            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
+            dst[ecol] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
+            (void)cin;
+        }
+        j = max(j, wend);
+        i += n;
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int flat_grid(int sm_count) { return sm_count * (2048 / kFlatThreads); }
+
+cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
+    flat_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);
+    flat_scan_kernel<<<1, 1024, 0, s>>>(a, (uint32_t)grid);
+    flat_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
+    if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t flat_kernel_attrs() {
+    cudaError_t e;
+    if ((e = use_max_shared_carveout(flat_count_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_scan_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_place_kernel)) != cudaSuccess) return e;
+    return use_max_shared_carveout(flat_expand_kernel);
+}
+
+}  // namespace wk

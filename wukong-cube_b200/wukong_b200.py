@@ -19,7 +19,7 @@ IN, OUT = 0, 1
 PREDICATE_ID, TYPE_ID = 0, 1
 NO_RESULT = 0xFFFF
 MODE_PLAIN, MODE_RESIDENT, MODE_GRAPH = 0, 1, 2
-KNOB_LANES, KNOB_BATCH_LANES, KNOB_SLICE_ROWS, KNOB_BATCH_SLICE_ROWS = 0, 1, 2, 3
+KNOB_LANES, KNOB_BATCH_LANES, KNOB_SLICE_ROWS, KNOB_BATCH_SLICE_ROWS, KNOB_FLAT_ROWS = 0, 1, 2, 3, 4
 
 SUCCESS = 0
 UNKNOWN_PATTERN = 3
