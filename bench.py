@@ -189,6 +189,10 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
     completions keep up with arrivals."""
     import workloads
     hq = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+    # warm-up run (untimed): loads every kernel of the serving path and builds the lanes
+    wq = workloads.light_queries(v, inst, 1000, seed=args.seed + 4999)
+    wq[::50] = [hq[j % 2] for j in range(len(wq[::50]))]
+    ctx.serve(wq, np.linspace(0, 50000, len(wq)), blind=1)
     sweep = []
     for k, qps in enumerate(args.serve_rates):
         rng = np.random.default_rng(args.seed + 7000 + k)

@@ -957,6 +957,19 @@ int wk::query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint6
     return WK_SUCCESS;
 }
 
+int wk::lane_prepare(wk_ctx* lane, uint64_t elems) {
+    elems = std::max<uint64_t>(elems, lane->cfg.rbuf_bytes / 4);
+    for (auto& t : lane->rbuf) {
+        int rc = lane->table_reserve(&t, std::max(t.cap, elems));
+        if (rc) return rc;
+    }
+    const uint64_t mx = std::max(lane->rbuf[0].cap, lane->rbuf[1].cap);
+    int rc = lane->ensure_status(mx / kTileRows + 2);
+    if (!rc) rc = lane->ensure_heavy(mx);
+    if (!rc && lane->flat_min_rows) rc = lane->ensure_flat(mx);
+    return rc;
+}
+
 int wk::table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host) {
     if (elems > t->cap) return ctx->fail(WK_E_BADARG, "copy beyond table capacity");
     if (elems) WK_CUDA(ctx, cudaMemcpyAsync(host, t->d, elems * 4, cudaMemcpyDeviceToHost, ctx->stream));

@@ -175,6 +175,8 @@ int ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas, wk
 int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows);
 // Copy `elems` elements of a device table to host memory (host sync).
 int table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host);
+// Size a serving lane's tables and scan scratch for `elems`-element tables up front.
+int lane_prepare(wk_ctx* lane, uint64_t elems);
 // Lanes for one (explore op, input columns) step of single queries (the autotuner's choice).
 int tune_step_lanes(wk_ctx* ctx, int op, int cols, int lanes);
 }  // namespace wk

@@ -331,7 +331,8 @@ struct HeavyLanes {
     // Lanes are child contexts cached in the parent (their tables keep their grown size from
     // one serving run to the next); they are rebuilt when the room they must leave changes.
     template <class Body>
-    int start(wk_ctx* parent, int n, const CtaUse& beside_use, int beside_ctas, Body body) {
+    int start(wk_ctx* parent, int n, const CtaUse& beside_use, int beside_ctas, uint64_t table_elems,
+              Body body) {
         const bool same = parent->lanes_ctas == beside_ctas && parent->lanes_use.smem == beside_use.smem &&
                           parent->lanes_use.regs == beside_use.regs &&
                           parent->lanes_use.threads == beside_use.threads;
@@ -346,6 +347,15 @@ struct HeavyLanes {
             int rc = ctx_make_child(parent, beside_use, beside_ctas, &c);
             if (rc) return rc;
             parent->lanes.push_back(c);
+        }
+        // Size each lane for a projected index-start query before the run starts: growing a
+        // table later means a cudaFree, which waits for the whole device.
+        for (int i = 0; i < n; ++i) {
+            int rc = lane_prepare(parent->lanes[i], table_elems);
+            if (rc) {
+                parent->last_error = "serving lane: " + parent->lanes[i]->last_error;
+                return rc;
+            }
         }
         for (int i = 0; i < n; ++i) {
             wk_ctx* c = parent->lanes[i];
@@ -467,7 +477,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         *off = cur;
         return true;
     };
-    const auto t0 = Clock::now();
+    auto t0 = Clock::now();   // restarted once the lanes are ready
     auto now_us = [&] { return std::chrono::duration<double, std::micro>(Clock::now() - t0).count(); };
 
     wk::HeavyLanes H;
@@ -480,7 +490,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         const wk::CtaUse light{std::max(a.smem, b.smem), std::max(a.regs, b.regs),
                                std::max(a.threads, b.threads)};
         rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, light, S.light_ctas() + 1,
-                     [&](wk_ctx* lane, uint32_t q) {
+                     S.cfg.heavy_proj_bytes / 4, [&](wk_ctx* lane, uint32_t q) {
                          const wk_table* t = nullptr;
                          uint64_t rows = 0, off = 0;
                          wk_qresult& r = results[q];
@@ -505,6 +515,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                      });
         if (rc) return rc;
     }
+    t0 = Clock::now();   // arrival times count from here
 
     uint32_t iter = 1;   // admission iterations start at 1 so a zeroed admit[] never matches
     std::deque<uint32_t> wait_heavy, wait_light;   // arrived, not yet admitted
