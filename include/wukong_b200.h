@@ -358,6 +358,13 @@ int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t it
  * counterpart in the reference (it runs one query per GPU agent at a time). */
 int wk_batch_execute(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t* host_out,
                      uint64_t cap_elems, wk_qresult* results);
+/* A stream of batches: queries[0..n) run as consecutive batches of `batch` queries (0: 16,384)
+ * with the same launches and results as wk_batch_execute per batch, but pipelined.  While the
+ * device runs one batch, the host resolves the next one's plans and the previous one's tables
+ * are copied to host_out on a second stream.  Tables are laid out back to back in query
+ * order.  No counterpart in the reference. */
+int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t batch,
+                            uint32_t* host_out, uint64_t cap_elems, wk_qresult* results);
 /* Device-only variant: results stay on the device (for throughput timing).  *total_rows
  * receives the sum of final rows. */
 int wk_batch_execute_device(wk_ctx* ctx, const wk_query* queries, uint32_t n,

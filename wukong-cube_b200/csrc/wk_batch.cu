@@ -126,6 +126,7 @@ struct BatchState {
     uint32_t* h_final_cols = nullptr;
     uint64_t* h_final_rows = nullptr;
     uint64_t* h_res_off = nullptr;
+    wk::StepCtl* h_ctl = nullptr;         // control block snapshot after this state's batch
     // graph of the launch sequence for one batch shape
     cudaGraphExec_t exec = nullptr;
     std::string shape;
@@ -138,6 +139,7 @@ void free_state(BatchState* b) {
     f(b->d_final_rows); f(b->d_res_off); f(b->d_arena); f(b->d_result);
     auto fh = [](void* p) { if (p) cudaFreeHost(p); };
     fh(b->h_desc); fh(b->h_nsteps); fh(b->h_final_cols); fh(b->h_final_rows); fh(b->h_res_off);
+    fh(b->h_ctl);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     *b = BatchState();
 }
@@ -182,7 +184,8 @@ int ensure_state(wk_ctx* ctx, BatchState* b, uint32_t n, int levels, uint64_t ro
               dm((void**)&b->d_result, 4ull * result_cap + 64) &&
               hm((void**)&b->h_desc, sizeof(wk::StepDesc) * levels * (size_t)n) &&
               hm((void**)&b->h_nsteps, 4ull * n) && hm((void**)&b->h_final_cols, 4ull * n) &&
-              hm((void**)&b->h_final_rows, 8ull * n) && hm((void**)&b->h_res_off, 8ull * (n + 1));
+              hm((void**)&b->h_final_rows, 8ull * n) && hm((void**)&b->h_res_off, 8ull * (n + 1)) &&
+              hm((void**)&b->h_ctl, sizeof(wk::StepCtl));
     if (!ok) {
         free_state(b);
         return ctx->fail(WK_E_OOM, "batch buffers");
@@ -200,39 +203,63 @@ struct Plan {
     int levels = 0;
     int width[kMaxBatchLevels] = {0};
     std::vector<int32_t> status;
+    std::vector<wk::PlanStep> steps;    // [n][kMaxBatchLevels]
+    std::vector<uint8_t> nsteps;        // [n]
 };
 
-// Resolve every query and fill the pinned descriptor staging.
+// Resolve every query (host threads, no allocation per query) and fill the pinned descriptor
+// staging.
 int build_plan(wk_ctx* ctx, BatchState* b, const wk_query* queries, uint32_t n, Plan& P) {
     P.n = n;
     P.levels = 0;
     std::fill(P.width, P.width + kMaxBatchLevels, 0);
     P.status.assign(n, 0);
-    std::vector<std::vector<wk::PlanStep>> all(n);
-    for (uint32_t q = 0; q < n; ++q) {
-        wk::ColMap cm(queries[q].nvars);
-        int rc = wk::resolve_plan(queries[q], ctx->cfg.max_cols, all[q], cm);
-        if (rc == WK_SUCCESS && (int)all[q].size() > kMaxBatchLevels) rc = WK_E_CAPACITY;
-        if (rc == WK_SUCCESS && queries[q].mt_factor != 1) rc = WK_E_UNSUPPORTED;
-        if (rc) {
-            P.status[q] = rc;
-            all[q].clear();
+    P.steps.resize((size_t)n * kMaxBatchLevels);
+    P.nsteps.assign(n, 0);
+    const int max_cols = ctx->cfg.max_cols;
+#pragma omp parallel if (n >= 2048)
+    {
+        std::vector<wk::PlanStep> st;
+        st.reserve(kMaxBatchLevels + 4);
+        int levels = 0, width[kMaxBatchLevels] = {0};
+#pragma omp for schedule(static) nowait
+        for (int64_t qi = 0; qi < (int64_t)n; ++qi) {
+            const uint32_t q = (uint32_t)qi;
+            wk::ColMap cm(queries[q].nvars);
+            int rc = wk::resolve_plan(queries[q], max_cols, st, cm);
+            if (rc == WK_SUCCESS && (int)st.size() > kMaxBatchLevels) rc = WK_E_CAPACITY;
+            if (rc == WK_SUCCESS && queries[q].mt_factor != 1) rc = WK_E_UNSUPPORTED;
+            if (rc) {
+                P.status[q] = rc;
+                st.clear();
+            }
+            P.nsteps[q] = (uint8_t)st.size();
+            std::copy(st.begin(), st.end(), P.steps.begin() + (size_t)q * kMaxBatchLevels);
+            levels = std::max<int>(levels, (int)st.size());
+            for (size_t k = 0; k < st.size(); ++k) width[k] = std::max(width[k], st[k].out_cols);
         }
-        P.levels = std::max<int>(P.levels, (int)all[q].size());
-        for (size_t k = 0; k < all[q].size(); ++k) P.width[k] = std::max(P.width[k], all[q][k].out_cols);
+#pragma omp critical
+        {
+            P.levels = std::max(P.levels, levels);
+            for (int k = 0; k < kMaxBatchLevels; ++k) P.width[k] = std::max(P.width[k], width[k]);
+        }
     }
     int w = 1;
     for (int k = 0; k < P.levels; ++k) w = std::max(w, P.width[k]);
     int rc = ensure_state(ctx, b, n, std::max(P.levels, 1), std::max<uint64_t>(b->rows_cap, 1 << 20),
                           std::max(b->w_cap, std::max(w, 8)), std::max<uint64_t>(b->result_cap, 1 << 22));
     if (rc) return rc;
-    for (uint32_t q = 0; q < n; ++q) {
-        const auto& st = all[q];
-        b->h_nsteps[q] = (uint32_t)st.size();
-        b->h_final_cols[q] = st.empty() ? 0 : (uint32_t)st.back().out_cols;
-        for (int k = 0; k < P.levels; ++k) {
+    const int L = P.levels;
+#pragma omp parallel for schedule(static) if (n >= 2048)
+    for (int64_t qi = 0; qi < (int64_t)n; ++qi) {
+        const uint32_t q = (uint32_t)qi;
+        const int ns = P.nsteps[q];
+        const wk::PlanStep* st = P.steps.data() + (size_t)q * kMaxBatchLevels;
+        b->h_nsteps[q] = (uint32_t)ns;
+        b->h_final_cols[q] = ns ? (uint32_t)st[ns - 1].out_cols : 0;
+        for (int k = 0; k < L; ++k) {
             wk::StepDesc& d = b->h_desc[(size_t)k * n + q];
-            if (k >= (int)st.size()) {
+            if (k >= ns) {
                 std::memset(&d, 0, sizeof(d));
                 d.op = wk::kXDone;
             } else {
@@ -430,14 +457,132 @@ BatchState* batch_state(wk_ctx* ctx) {
     return (BatchState*)ctx->batch;
 }
 
+// The second state of the pipelined path (wk_batch_execute_stream): two batches in flight.
+BatchState* batch_state2(wk_ctx* ctx) {
+    if (!ctx->batch2) ctx->batch2 = new BatchState();
+    return (BatchState*)ctx->batch2;
+}
+
 }  // namespace
 
 void wk_batch_release(wk_ctx* ctx) {
-    if (!ctx || !ctx->batch) return;
-    BatchState* b = (BatchState*)ctx->batch;
-    free_state(b);
-    delete b;
-    ctx->batch = nullptr;
+    if (!ctx) return;
+    for (void** p : {&ctx->batch, &ctx->batch2}) {
+        if (!*p) continue;
+        BatchState* b = (BatchState*)*p;
+        free_state(b);
+        delete b;
+        *p = nullptr;
+    }
+}
+
+// Pipelined batches.  Per batch, in stream order on the context stream: the descriptor upload,
+// the captured launch sequence, a snapshot of the control block (then its error word is
+// cleared), and the per-query row counts and offsets; an event marks the batch ready.  While
+// the device runs batch i, the host resolves batch i+1's plans into the other state and, once
+// batch i-1 is ready, copies its tables to the host on a second stream.  A batch whose snapshot
+// shows an overflow is rerun on its own (growing its buffers) before the pipeline goes on.
+extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t batch,
+                                       uint32_t* host_out, uint64_t cap_elems, wk_qresult* results) {
+    if (!ctx || (!queries && n) || (!host_out && cap_elems) || (!results && n)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    if (n == 0) return WK_SUCCESS;
+    if (batch == 0) batch = 16384;
+    BatchState* B[2] = {batch_state(ctx), batch_state2(ctx)};
+    Plan P[2];
+    uint32_t off[2] = {0, 0}, cnt[2] = {0, 0};
+    bool pend[2] = {false, false};
+    uint64_t out_used = 0;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ready[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    int rc = WK_SUCCESS;
+    auto cu = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && !rc) rc = ctx->cuda_fail(e, what);
+        return rc;
+    };
+    // Wait for the batch in state `k`, rerun it alone if it overflowed, then start its copy out.
+    auto finish = [&](int k) -> int {
+        if (cu(cudaEventSynchronize(ready[k]), "batch ready")) return rc;
+        pend[k] = false;
+        BatchState* b = B[k];
+        uint64_t total = b->h_res_off[cnt[k]];
+        if (b->h_ctl->err || total > b->result_cap) {
+            if (b->h_ctl->err & wk::kErrCorrupt) return rc = ctx->fail(WK_E_CORRUPT, "key table chain out of range");
+            if (b->h_ctl->err & wk::kErrTimeout) return rc = ctx->fail(WK_E_TIMEOUT, "batch look-back timed out");
+            if (cu(cudaStreamSynchronize(cs), "copy stream")) return rc;
+            if ((rc = run_batch(ctx, b, queries + off[k], cnt[k], P[k]))) return rc;
+            total = b->h_res_off[cnt[k]];
+        }
+        if (out_used + total > cap_elems) return rc = ctx->fail(WK_E_CAPACITY, "host buffer too small");
+        for (uint32_t i = 0; i < cnt[k]; ++i) {
+            wk_qresult& r = results[off[k] + i];
+            std::memset(&r, 0, sizeof(r));
+            r.status = P[k].status[i];
+            r.rows = r.status ? 0 : b->h_final_rows[i];
+            r.cols = (int32_t)b->h_final_cols[i];
+            r.elem_offset = out_used + b->h_res_off[i];
+        }
+        if (cu(cudaStreamWaitEvent(cs, ready[k], 0), "copy wait")) return rc;
+        if (total && cu(cudaMemcpyAsync(host_out + out_used, b->d_result, total * 4, cudaMemcpyDeviceToHost, cs),
+                        "result copy"))
+            return rc;
+        if (cu(cudaEventRecord(copied[k], cs), "copy event")) return rc;
+        out_used += total;
+        return rc;
+    };
+    cu(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "copy stream");
+    for (int k = 0; k < 2 && !rc; ++k) {
+        cu(cudaEventCreateWithFlags(&ready[k], cudaEventDisableTiming), "event");
+        cu(cudaEventCreateWithFlags(&copied[k], cudaEventDisableTiming), "event");
+        if (!rc) cu(cudaEventRecord(copied[k], cs), "event");
+    }
+    for (uint32_t i = 0, start = 0; !rc && start < n; ++i, start += batch) {
+        const int k = i & 1;
+        const uint32_t m = std::min(batch, n - start);
+        if (pend[k] && finish(k)) break;
+        // the copy of the batch two back has left this state's buffers
+        if (cu(cudaEventSynchronize(copied[k]), "copy done")) break;
+        if ((rc = build_plan(ctx, B[k], queries + start, m, P[k]))) break;
+        off[k] = start;
+        cnt[k] = m;
+        if (P[k].levels == 0) {   // nothing reaches the device: every plan failed or is empty
+            if (pend[k ^ 1] && finish(k ^ 1)) break;
+            for (uint32_t q = 0; q < m; ++q) {
+                wk_qresult& r = results[start + q];
+                std::memset(&r, 0, sizeof(r));
+                r.status = P[k].status[q];
+                r.elem_offset = out_used;
+            }
+            continue;
+        }
+        if ((rc = ctx->ensure_status(B[k]->rows_cap / wk::kTileRows + 2))) break;
+        if ((rc = ctx->ensure_heavy(B[k]->rows_cap))) break;
+        if (cu(cudaStreamWaitEvent(ctx->stream, copied[k], 0), "state free")) break;
+        if ((rc = upload_plan(ctx, B[k], P[k]))) break;
+        if ((rc = launch_batch(ctx, B[k], P[k]))) break;
+        cudaStream_t s = ctx->stream;
+        cu(cudaMemcpyAsync(B[k]->h_ctl, ctx->d_ctl, sizeof(wk::StepCtl), cudaMemcpyDeviceToHost, s), "ctl");
+        cu(cudaMemsetAsync(&ctx->d_ctl->err, 0, sizeof(unsigned), s), "ctl");
+        cu(cudaMemsetAsync(&ctx->d_ctl->need, 0, sizeof(unsigned long long), s), "ctl");
+        cu(cudaMemcpyAsync(B[k]->h_final_rows, B[k]->d_final_rows, 8ull * m, cudaMemcpyDeviceToHost, s), "rows");
+        cu(cudaMemcpyAsync(B[k]->h_res_off, B[k]->d_res_off, 8ull * (m + 1), cudaMemcpyDeviceToHost, s), "offsets");
+        cu(cudaEventRecord(ready[k], s), "ready");
+        if (rc) break;
+        pend[k] = true;
+        // the previous batch: its tables go to the host while this one runs
+        if (pend[k ^ 1] && finish(k ^ 1)) break;
+    }
+    for (int k = 0; k < 2 && !rc; ++k)   // the last batch is the only one still pending
+        if (pend[k]) finish(k);
+    if (cs) cudaStreamSynchronize(cs);
+    cudaStreamSynchronize(ctx->stream);
+    for (int k = 0; k < 2; ++k) {
+        if (ready[k]) cudaEventDestroy(ready[k]);
+        if (copied[k]) cudaEventDestroy(copied[k]);
+    }
+    if (cs) cudaStreamDestroy(cs);
+    return rc;
 }
 
 extern "C" int wk_batch_execute(wk_ctx* ctx, const wk_query* queries, uint32_t n, uint32_t* host_out,

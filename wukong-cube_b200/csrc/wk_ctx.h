@@ -108,8 +108,9 @@ struct wk_ctx {
     std::map<long long, int> bps_cache;   // (op, cols) -> blocks per SM
     std::string last_error;
 
-    // batch / serving state (wk_batch.cu)
+    // batch / serving state (wk_batch.cu); batch2 is the second state of the pipelined path
     void* batch = nullptr;
+    void* batch2 = nullptr;
     // serving lanes, kept between serving runs so their tables stay grown (wk_serve.cu)
     std::vector<wk_ctx*> lanes;
     wk::CtaUse lanes_use{0, 0, 0};

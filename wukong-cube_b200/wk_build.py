@@ -56,7 +56,7 @@ def build_lib(verbose=False, force=False, variant=None, defines=()):
         objs.append(o)
         if force or _stale(o, [s] + hdrs):
             out = _run([NVCC] + ARCH + dflags + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-                                                 "-Xptxas", "-v", "-c", s, "-o", o])
+                                                 "-Xcompiler", "-fopenmp", "-Xptxas", "-v", "-c", s, "-o", o])
             if verbose:
                 print(out)
     for src in CPP_SOURCES:

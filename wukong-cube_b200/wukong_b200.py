@@ -161,6 +161,8 @@ _SIGS = {
                                     C.POINTER(C.c_int32)]),
     "wk_batch_execute": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, _P, C.c_uint64,
                                    C.POINTER(QResult)]),
+    "wk_batch_execute_stream": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_uint32, _P,
+                                          C.c_uint64, C.POINTER(QResult)]),
     "wk_batch_execute_device": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32,
                                           C.POINTER(C.c_uint64)]),
     "wk_batch_replay": (C.c_int, [_P]),
@@ -492,15 +494,20 @@ class Context:
         _check(lib().wk_batch_profile(self.h, qs, len(queries), iters, arr, 16, C.byref(n)), self.h)
         return _prof_list(arr, n.value)
 
-    def batch(self, queries, cap_elems=None):
-        """Run queries together; returns list of (table, status)."""
+    def batch(self, queries, cap_elems=None, stream_batch=None):
+        """Run queries together; returns list of (table, status).  With stream_batch, the
+        queries run as a pipelined stream of batches of that size (wk_batch_execute_stream)."""
         qs, keep = queries_as_c(queries)
         res = (QResult * max(len(queries), 1))()
         if cap_elems is None:
             cap_elems = 1 << 22
         while True:
             out = np.zeros(max(cap_elems, 1), dtype=np.uint32)
-            rc = lib().wk_batch_execute(self.h, qs, len(queries), _ptr(out), out.size, res)
+            if stream_batch is None:
+                rc = lib().wk_batch_execute(self.h, qs, len(queries), _ptr(out), out.size, res)
+            else:
+                rc = lib().wk_batch_execute_stream(self.h, qs, len(queries), stream_batch, _ptr(out),
+                                                   out.size, res)
             if rc == E_CAPACITY and "host buffer" in lib().wk_last_error(self.h).decode():
                 cap_elems *= 4
                 continue
