@@ -271,9 +271,9 @@ int build_plan(wk_ctx* ctx, BatchState* b, const wk_query* queries, uint32_t n, 
 }
 
 // Copy the batch's descriptors from the pinned staging to the device.
-int upload_plan(wk_ctx* ctx, BatchState* b, const Plan& P) {
+int upload_plan(wk_ctx* ctx, BatchState* b, const Plan& P, cudaStream_t s = nullptr) {
     const uint32_t n = P.n;
-    cudaStream_t s = ctx->stream;
+    if (!s) s = ctx->stream;
     WKB_CUDA(ctx, cudaMemcpyAsync(b->d_desc, b->h_desc, sizeof(wk::StepDesc) * (size_t)P.levels * n,
                                   cudaMemcpyHostToDevice, s));
     WKB_CUDA(ctx, cudaMemcpyAsync(b->d_nsteps, b->h_nsteps, 4ull * n, cudaMemcpyHostToDevice, s));
@@ -494,8 +494,9 @@ extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uin
     uint32_t off[2] = {0, 0}, cnt[2] = {0, 0};
     bool pend[2] = {false, false};
     uint64_t out_used = 0;
-    cudaStream_t cs = nullptr;
+    cudaStream_t cs = nullptr, us = nullptr;   // copies to the host; descriptor uploads
     cudaEvent_t ready[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    cudaEvent_t uploaded[2] = {nullptr, nullptr};
     int rc = WK_SUCCESS;
     auto cu = [&](cudaError_t e, const char* what) {
         if (e != cudaSuccess && !rc) rc = ctx->cuda_fail(e, what);
@@ -532,9 +533,11 @@ extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uin
         return rc;
     };
     cu(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "copy stream");
+    cu(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking), "upload stream");
     for (int k = 0; k < 2 && !rc; ++k) {
         cu(cudaEventCreateWithFlags(&ready[k], cudaEventDisableTiming), "event");
         cu(cudaEventCreateWithFlags(&copied[k], cudaEventDisableTiming), "event");
+        cu(cudaEventCreateWithFlags(&uploaded[k], cudaEventDisableTiming), "event");
         if (!rc) cu(cudaEventRecord(copied[k], cs), "event");
     }
     for (uint32_t i = 0, start = 0; !rc && start < n; ++i, start += batch) {
@@ -558,8 +561,11 @@ extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uin
         }
         if ((rc = ctx->ensure_status(B[k]->rows_cap / wk::kTileRows + 2))) break;
         if ((rc = ctx->ensure_heavy(B[k]->rows_cap))) break;
+        // descriptors go up on their own stream while the previous batch still computes
+        if ((rc = upload_plan(ctx, B[k], P[k], us))) break;
+        if (cu(cudaEventRecord(uploaded[k], us), "upload event")) break;
+        if (cu(cudaStreamWaitEvent(ctx->stream, uploaded[k], 0), "upload wait")) break;
         if (cu(cudaStreamWaitEvent(ctx->stream, copied[k], 0), "state free")) break;
-        if ((rc = upload_plan(ctx, B[k], P[k]))) break;
         if ((rc = launch_batch(ctx, B[k], P[k]))) break;
         cudaStream_t s = ctx->stream;
         cu(cudaMemcpyAsync(B[k]->h_ctl, ctx->d_ctl, sizeof(wk::StepCtl), cudaMemcpyDeviceToHost, s), "ctl");
@@ -576,12 +582,15 @@ extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uin
     for (int k = 0; k < 2 && !rc; ++k)   // the last batch is the only one still pending
         if (pend[k]) finish(k);
     if (cs) cudaStreamSynchronize(cs);
+    if (us) cudaStreamSynchronize(us);
     cudaStreamSynchronize(ctx->stream);
     for (int k = 0; k < 2; ++k) {
         if (ready[k]) cudaEventDestroy(ready[k]);
         if (copied[k]) cudaEventDestroy(copied[k]);
+        if (uploaded[k]) cudaEventDestroy(uploaded[k]);
     }
     if (cs) cudaStreamDestroy(cs);
+    if (us) cudaStreamDestroy(us);
     return rc;
 }
 
