@@ -32,7 +32,6 @@ using namespace dev;
 
 constexpr int kFlatThreads = 256;
 constexpr int kWindow = 256;   // input rows staged per expand round
-constexpr int kRowsPerThread = 4;   // rows whose probes one thread keeps in flight
 
 __device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
     uint64_t R = *(volatile const uint64_t*)a.in_rows;
@@ -101,7 +100,7 @@ __device__ __forceinline__ uint64_t block_sum(uint64_t x, uint64_t* s_warp) {
     return t;
 }
 
-__global__ void __launch_bounds__(kFlatThreads, 4) flat_count_kernel(const FlatArgs a) {
+__global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
     const uint64_t R = flat_rows(a);
     if (R < a.min_rows) return;
@@ -110,85 +109,42 @@ __global__ void __launch_bounds__(kFlatThreads, 4) flat_count_kernel(const FlatA
     const StepDesc& d = a.step;
     const bool filt = d.op == kXK2K || d.op == kXK2C;
     uint64_t sum = 0, sd = 0, nvalid = 0;
-    // kRowsPerThread rows per thread at a time: their row loads, then their first bucket
-    // sectors, are all in flight together (the probes are latency-bound random reads)
-    for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += (uint64_t)kRowsPerThread * kFlatThreads) {
-        uint32_t cur[kRowsPerThread], target[kRowsPerThread];
-        bool valid[kRowsPerThread], look[kRowsPerThread];
-        uint64_t key[kRowsPerThread], bucket[kRowsPerThread], ptr[kRowsPerThread];
-#pragma unroll
-        for (int u = 0; u < kRowsPerThread; ++u) {
-            const uint64_t r = r0 + (uint64_t)u * kFlatThreads;
-            valid[u] = r < hi;
-            const uint32_t* row = a.in + r * (uint64_t)a.w_in;
-            cur[u] = valid[u] ? __ldg(row + d.cs) : kBlankId;
-            target[u] = d.end_const;
-            if (d.op == kXK2K && valid[u]) target[u] = __ldg(row + d.ce);
+    for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
+        const uint32_t* row = a.in + r * (uint64_t)a.w_in;
+        const uint32_t cur = __ldg(row + d.cs);
+        uint32_t target = d.end_const;
+        if (d.op == kXK2K) target = __ldg(row + d.ce);
+        uint64_t key;
+        const SegDesc* sg = &d.seg;
+        bool valid = cur != kBlankId;
+        if (d.op == kXK2U && d.type_index) {
+            // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+            key = make_key(0, cur, kIn);
+            sg = &a.seg_index[kIn];
+            if (cur >= (1u << kNbitsIdx)) valid = false;
+        } else {
+            key = make_key(cur, d.pid, d.dir);
+            if (cur == 0) sg = &a.seg_index[d.dir & 1];   // vid 0 names the index
         }
-#pragma unroll
-        for (int u = 0; u < kRowsPerThread; ++u) {
-            const SegDesc* sg = &d.seg;
-            if (cur[u] == kBlankId) valid[u] = false;
-            if (d.op == kXK2U && d.type_index) {
-                // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-                key[u] = make_key(0, cur[u], kIn);
-                sg = &a.seg_index[kIn];
-                if (cur[u] >= (1u << kNbitsIdx)) valid[u] = false;
-            } else {
-                key[u] = make_key(cur[u], d.pid, d.dir);
-                if (cur[u] == 0) sg = &a.seg_index[d.dir & 1];   // vid 0 names the index
-            }
-            look[u] = valid[u] && sg->num_buckets != 0 && key[u] != 0;
-            bucket[u] = look[u] ? bucket_of(key[u], *sg) : 0;
-            ptr[u] = 0;
-        }
-        // the keys of slots 0 and 1 of every home bucket at once (one 32-byte sector each); the
-        // matching pointer word is in the same sector, so its load hits L1; rows that sector
-        // does not settle walk on alone
-        uint64_t k0[kRowsPerThread], k1[kRowsPerThread];
-#pragma unroll
-        for (int u = 0; u < kRowsPerThread; ++u) {
-            k0[u] = ~0ull;
-            k1[u] = ~0ull;
-            if (look[u] && bucket[u] < a.store.n_buckets) {
-                const unsigned long long* s = reinterpret_cast<const unsigned long long*>(
-                    a.store.slots + bucket[u] * kAssoc);
-                k0[u] = __ldg(s);
-                k1[u] = __ldg(s + 2);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kRowsPerThread; ++u) {
-            if (!look[u]) continue;
-            const unsigned long long* s = reinterpret_cast<const unsigned long long*>(
-                a.store.slots + bucket[u] * kAssoc);
-            if (k0[u] == key[u]) ptr[u] = __ldg(s + 1);
-            else if (k0[u] == 0) ptr[u] = 0;
-            else if (k1[u] == key[u]) ptr[u] = __ldg(s + 3);
-            else if (k1[u] == 0) ptr[u] = 0;
-            else ptr[u] = thread_probe(a.store, key[u], bucket[u], &a.ctl->err);
-        }
-#pragma unroll
-        for (int u = 0; u < kRowsPerThread; ++u) {
-            const uint64_t r = r0 + (uint64_t)u * kFlatThreads;
-            if (r >= hi) continue;
-            uint64_t off = ptr_off(ptr[u]), deg = ptr_size(ptr[u]);
+        uint64_t off = 0, deg = 0;
+        if (valid && sg->num_buckets != 0 && key != 0) {
+            const uint64_t p = thread_probe(a.store, key, bucket_of(key, *sg), &a.ctl->err);
+            off = ptr_off(p);
+            deg = ptr_size(p);
             if (off + deg > a.store.n_edges) {
                 if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg = 0;
             }
-            uint32_t c = (uint32_t)deg;
-            if (filt)
-                c = (valid[u] && deg && thread_member(a.store.edges, off, deg, target[u], a.sorted_lists != 0)) ? 1u
-                                                                                                                  : 0u;
-            if (!valid[u]) c = 0;
-            a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
-            if (!filt) a.off[r] = off;
-            sum += c;
-            if (valid[u]) {
-                sd += deg;
-                ++nvalid;
-            }
+        }
+        uint32_t c = (uint32_t)deg;
+        if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
+        if (!valid) c = 0;
+        a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
+        if (!filt) a.off[r] = off;
+        sum += c;
+        if (valid) {
+            sd += deg;
+            ++nvalid;
         }
     }
     const uint64_t total = block_sum(sum, s_warp);
