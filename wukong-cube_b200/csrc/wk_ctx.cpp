@@ -73,7 +73,7 @@ int wk_ctx::blocks_per_sm(int op, int cols, int lanes) {
 }
 
 int wk_ctx::ensure_heavy(uint64_t out_rows_cap) {
-    const uint64_t need = out_rows_cap / wk::kHeavyRows + 64;
+    const uint64_t need = out_rows_cap / wk::kMinSliceRows + 64;
     if (need <= heavy_cap) return WK_SUCCESS;
     const uint64_t cap = need + need / 2;
     WK_CUDA(this, cudaStreamSynchronize(stream));
@@ -1103,8 +1103,8 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
             ctx->batch_lanes = value;
         }
     } else if (knob == WK_KNOB_SLICE_ROWS || knob == WK_KNOB_BATCH_SLICE_ROWS) {
-        if (value < wk::kHeavyRows || value > (1 << 24))
-            return ctx->fail(WK_E_BADARG, "slice threshold must be in [128, 2^24]");
+        if (value < wk::kMinSliceRows || value > (1 << 24))
+            return ctx->fail(WK_E_BADARG, "slice threshold must be in [32, 2^24]");
         (knob == WK_KNOB_SLICE_ROWS ? ctx->slice_rows : ctx->batch_slice_rows) = (uint32_t)value;
     } else if (knob == WK_KNOB_FLAT_ROWS) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
@@ -1130,9 +1130,9 @@ extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (knob == WK_KNOB_LANES) *value = ctx->default_lanes;
     else if (knob == WK_KNOB_BATCH_LANES) *value = ctx->batch_lanes;
-    else if (knob == WK_KNOB_SLICE_ROWS) *value = (int32_t)std::max<uint32_t>(ctx->slice_rows, wk::kHeavyRows);
+    else if (knob == WK_KNOB_SLICE_ROWS) *value = (int32_t)(ctx->slice_rows ? ctx->slice_rows : wk::kHeavyRows);
     else if (knob == WK_KNOB_BATCH_SLICE_ROWS)
-        *value = (int32_t)std::max<uint32_t>(ctx->batch_slice_rows, wk::kHeavyRows);
+        *value = (int32_t)(ctx->batch_slice_rows ? ctx->batch_slice_rows : wk::kHeavyRows);
     else if (knob == WK_KNOB_FLAT_ROWS) *value = (int32_t)std::min<uint64_t>(ctx->flat_min_rows, INT32_MAX);
     else return ctx->fail(WK_E_BADARG, "unknown knob");
     return WK_SUCCESS;

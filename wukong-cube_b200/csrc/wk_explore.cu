@@ -70,6 +70,11 @@ __shared__ long long s_ph_t;
 // The step every row of a finished query runs: nothing.
 __constant__ StepDesc c_done = {{0, 0, 0, 0}, 0, 0, 0, kXDone, 0, 0, 0, 0, 0, 0, 0, 0};
 
+// Rows with more output rows than this are written as slices from the queue.
+__device__ __forceinline__ uint32_t slice_threshold(const ExploreArgs& a) {
+    return a.slice_rows ? max(a.slice_rows, (uint32_t)kMinSliceRows) : (uint32_t)kHeavyRows;
+}
+
 // Step of query q at this launch.
 __device__ __forceinline__ const StepDesc* step_desc(const ExploreArgs& a, uint32_t q) {
     if (!a.desc) return &a.one;
@@ -229,7 +234,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     WK_PH(2);
     for (int i = threadIdx.x; i < n; i += kStepThreads) {
         const uint32_t c = B.cnt[i];
-        const bool heavy = c > max(a.slice_rows, (uint32_t)kHeavyRows);
+        const bool heavy = c > slice_threshold(a);
         B.lcnt[i] = heavy ? 0u : c;
         if (heavy) S.has_heavy = 1;
     }
@@ -289,7 +294,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     if (S.has_heavy && fits) {
         for (int i = threadIdx.x; i < n; i += kStepThreads) {
             const uint32_t c = B.cnt[i];
-            if (c <= max(a.slice_rows, (uint32_t)kHeavyRows)) continue;
+            if (c <= slice_threshold(a)) continue;
             const uint32_t nch = (c + kHeavyChunk - 1) / kHeavyChunk;
             const unsigned long long at = atomicAdd(&a.ctl->heavy_n, (unsigned long long)nch);
             for (uint32_t k = 0; k < nch; ++k) {
@@ -309,7 +314,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
         }
     }
     WK_PH(5);
-    // write the short-list rows: stride w_out, zero past the query's width
+    // write the short-list rows (stride w_out)
     if (fits && ltotal) {
         const bool contiguous = !S.has_heavy;
         const uint64_t* lp = contiguous ? B.pre : B.lpre;
@@ -331,7 +336,8 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
                 if (opv != kXStart)
                     for (; c < cin; ++c) dst[c] = sr[c];
                 if (opv == kXStart || opv == kXK2U) dst[c++] = __ldg(a.store.edges + B.off[lo] + k);
-                for (; c < wo; ++c) dst[c] = 0;
+                // columns past the query's own width are never read (later levels and the
+                // result gather use only the query's columns), so they are left as they are
                 const uint64_t pos = excl + B.pre[lo] + k;
                 s_pos[j] = pos;
                 if (a.owner_out) a.owner_out[pos] = B.q[lo];

@@ -39,7 +39,8 @@ struct HeavyItem {
 };
 static_assert(sizeof(HeavyItem) == 40, "HeavyItem is 40 bytes");
 
-constexpr int kHeavyRows = 128;
+constexpr int kHeavyRows = 128;     // slice threshold when a launch sets none
+constexpr int kMinSliceRows = 32;   // lowest threshold a launch may set (queues are sized for it)
 constexpr int kHeavyChunk = 2048;
 constexpr int kPhaseSlots = 12;  // phase cycle counters of an instrumented build
 
@@ -77,7 +78,7 @@ struct ExploreArgs {
     int32_t lanes;
     // Rows with more output rows than this go to the slice queue (spread over every CTA);
     // shorter ones are written by the CTA that scanned them.  0 means kHeavyRows; values below
-    // kHeavyRows are raised to it (the queue is sized for that).
+    // kMinSliceRows are raised to it (the queues of a context are sized for that).
     uint32_t slice_rows;
     // When nonzero and the input has at least this many rows, the launch does nothing (the
     // flat pipeline of wk_flat.cu runs the step instead).
