@@ -40,6 +40,13 @@ import numpy as np  # noqa: E402
 
 METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU path"
 
+# DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of the 16,384-query batch
+# on the 1,000-organisation graph: 42.21 MB + 0.16 MB for 2,617,493 input rows.  The same
+# capture on the full graph is not taken (its store is 11 GB); more of the store misses L2
+# there, so this scaled figure is a lower bound.
+LEVEL_TRAFFIC_PER_ROW = (42.21e6 + 0.164e6) / 2617493
+
 
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -408,11 +415,17 @@ def run_ours(args, world, rank, local_rank):
                            "p99": int(np.percentile(light_rows, 99)), "max": int(light_rows.max())},
             "heavy": heavy,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": src,
-                         "kernel": "level_kernel (batch level %d)" % levels.index(dom),
+                         "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                           "same level on the 1,000-organisation batch (16.19 B per "
+                                           "input row), scaled by this launch's input rows",
+                         "peak_source": src,
+                         "kernel": "explore_kernel (batch level %d)" % levels.index(dom),
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"]},
             "roofline_heavy": {"bound": "hbm", "achieved": hach, "peak": peak, "unit": "GB/s",
-                               "frac": hach / peak, "kernel": "step_kernel " + hdom["kind"],
+                               "frac": hach / peak, "traffic": None,
+                               "kernel": "single-query " + hdom["kind"] + " step (tile launch or "
+                                         "flat pipeline, whichever the device picked)",
                                "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"]},
             "batch_levels": levels,
             "batch_other_ms": overheads,
@@ -434,7 +447,11 @@ def run_ours(args, world, rank, local_rank):
 
 def run_profile_case(args):
     """A small, self-contained case for ncu: the heavy triangle query (resident mode) and one
-    light batch, each run `--steps` times after `--warmup` runs, no oracle, no timing."""
+    light batch, each run `--steps` times after `--warmup` runs, no oracle, no timing.  The
+    batch replays after the first sit in an NVTX range named "replay", so a capture can pick
+    a level of a replay (ncu --nvtx --nvtx-include replay/) whatever reruns came before."""
+    import torch
+
     import workloads
     import wukong_b200 as wk
     tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
@@ -445,8 +462,13 @@ def run_profile_case(args):
         for _ in range(args.warmup + args.steps):
             ctx.execute(q, wk.MODE_RESIDENT)
         ctx.batch_device(qs)
-        for _ in range(args.warmup + args.steps):
+        ctx.batch_replay()
+        ctx.sync()
+        torch.cuda.nvtx.range_push("replay")
+        for _ in range(args.warmup + args.steps - 1):
             ctx.batch_replay()
+        ctx.sync()
+        torch.cuda.nvtx.range_pop()
         ctx.check()
     print(json.dumps({"profile_case": "ok", "graph": ginfo}))
 

@@ -322,7 +322,7 @@ int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
  *           bucket slices staged per request);
  *   knob 1: the same for batches and serving;
  *   knob 2: the list length above which a row's output is written as 2,048-row slices by every
- *           CTA (block-per-row) instead of by the CTA that probed it (group-per-row); 32 to
+ *           CTA (block-per-row) instead of by the CTA that probed it (group-per-row); 8 to
  *           2^24, default 128;
  *   knob 3: the same for batches and serving;
  *   knob 4: single-query steps of index-start plans (and single steps) whose input has at

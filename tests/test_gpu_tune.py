@@ -11,14 +11,14 @@ pytestmark = pytest.mark.gpu
 
 
 def test_knob_values_are_checked(ctx):
-    for knob, bad in ((wk.KNOB_LANES, 3), (wk.KNOB_BATCH_LANES, 16), (wk.KNOB_SLICE_ROWS, 16),
+    for knob, bad in ((wk.KNOB_LANES, 3), (wk.KNOB_BATCH_LANES, 16), (wk.KNOB_SLICE_ROWS, 4),
                       (wk.KNOB_BATCH_SLICE_ROWS, 1 << 25), (9, 4)):
         with pytest.raises(wk.WukongError) as e:
             ctx.tune_set(knob, bad)
         assert e.value.code == wk.E_BADARG
 
 
-@pytest.mark.parametrize("lanes,slice_rows", [(2, 128), (8, 32), (4, 16384), (2, 64)])
+@pytest.mark.parametrize("lanes,slice_rows", [(2, 128), (8, 32), (4, 16384), (2, 8)])
 def test_every_setting_gives_the_oracle_results(ctx, graph20, lanes, slice_rows):
     v = graph20["vocab"]
     o = graph20["oracle"]
@@ -50,8 +50,8 @@ def test_autotune_picks_a_candidate_and_keeps_results(ctx, graph20):
     try:
         r = ctx.autotune(qs + heavy, iters=3)
         assert r["batch_lanes"] in (2, 4, 8) and r["lanes"] in (2, 4, 8)
-        assert r["batch_slice_rows"] in (32, 64, 128, 512, 2048)
-        assert r["slice_rows"] in (32, 64, 128, 512, 2048)
+        assert r["batch_slice_rows"] in (8, 16, 32, 128, 512)
+        assert r["slice_rows"] in (8, 16, 32, 128, 512)
         assert r["candidates"] == 3 * 5 + 3 + 5
         assert ctx.tune_get(wk.KNOB_BATCH_LANES) == r["batch_lanes"]
         assert ctx.tune_get(wk.KNOB_SLICE_ROWS) == r["slice_rows"]

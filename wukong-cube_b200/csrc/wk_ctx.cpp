@@ -1104,7 +1104,7 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
         }
     } else if (knob == WK_KNOB_SLICE_ROWS || knob == WK_KNOB_BATCH_SLICE_ROWS) {
         if (value < wk::kMinSliceRows || value > (1 << 24))
-            return ctx->fail(WK_E_BADARG, "slice threshold must be in [32, 2^24]");
+            return ctx->fail(WK_E_BADARG, "slice threshold must be in [8, 2^24]");
         (knob == WK_KNOB_SLICE_ROWS ? ctx->slice_rows : ctx->batch_slice_rows) = (uint32_t)value;
     } else if (knob == WK_KNOB_FLAT_ROWS) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");

@@ -40,7 +40,7 @@ struct HeavyItem {
 static_assert(sizeof(HeavyItem) == 40, "HeavyItem is 40 bytes");
 
 constexpr int kHeavyRows = 128;     // slice threshold when a launch sets none
-constexpr int kMinSliceRows = 32;   // lowest threshold a launch may set (queues are sized for it)
+constexpr int kMinSliceRows = 8;    // lowest threshold a launch may set (queues are sized for it)
 constexpr int kHeavyChunk = 2048;
 constexpr int kPhaseSlots = 12;  // phase cycle counters of an instrumented build
 

@@ -20,7 +20,7 @@
 namespace {
 
 constexpr int kLanes[] = {2, 4, 8};
-constexpr int kSlices[] = {32, 64, 128, 512, 2048};
+constexpr int kSlices[] = {8, 16, 32, 128, 512};
 
 struct Events {
     cudaEvent_t a = nullptr, b = nullptr;
