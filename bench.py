@@ -41,11 +41,10 @@ import numpy as np  # noqa: E402
 METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU path"
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of the 16,384-query batch
-# on the 1,000-organisation graph: 42.21 MB + 0.16 MB for 2,617,493 input rows.  The same
-# capture on the full graph is not taken (its store is 11 GB); more of the store misses L2
-# there, so this scaled figure is a lower bound.
-LEVEL_TRAFFIC_PER_ROW = (42.21e6 + 0.164e6) / 2617493
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
+# 16,384-query batch on the 10,000-organisation graph: 109.96 MB + 12.99 MB for 2,560,041 input
+# rows (the same level as the bench's dominant launch; the capture ran the default knobs).
+LEVEL_TRAFFIC_PER_ROW = (109.96e6 + 12.99e6) / 2560041
 
 
 def peaks():
@@ -416,9 +415,9 @@ def run_ours(args, world, rank, local_rank):
             "heavy": heavy,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
-                                           "same level on the 1,000-organisation batch (16.19 B per "
-                                           "input row), scaled by this launch's input rows",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                           "this level in a replay of the same batch (1 pass; "
+                                           "48.0 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": "explore_kernel (batch level %d)" % levels.index(dom),
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"]},

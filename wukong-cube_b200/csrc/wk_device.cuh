@@ -392,37 +392,45 @@ __device__ __forceinline__ uint64_t block_exclusive_sum(uint64_t x, uint64_t* s_
 // The output is cut into fixed chunks spread over the grid, so one long table is copied by
 // many CTAs and the stores are coalesced; each element finds its table by a binary search of
 // `off` narrowed to the chunk's first and last table.
-constexpr int kGatherChunk = 4096;
+constexpr int kGatherSpan = 1024;   // output elements per warp segment
 
+// Each warp copies contiguous segments of kGatherSpan elements, lane i taking elements i,
+// i + 32, ...: it finds the segment's first table once (binary search), then every lane walks
+// forward through the tables it crosses, so the per-element work is a compare, a division by
+// the table's width and the copy.  Stores are coalesced; one long table is spread over many
+// warps.
 template <class Src>
 __device__ void segmented_gather(uint32_t n, const uint64_t* __restrict__ off, Src src,
                                  uint32_t* __restrict__ out) {
-    __shared__ uint32_t s_q[2];
     const uint64_t total = off[n];
-    for (uint64_t base = (uint64_t)blockIdx.x * kGatherChunk; base < total;
-         base += (uint64_t)gridDim.x * kGatherChunk) {
-        const uint64_t end = min(total, base + (uint64_t)kGatherChunk);
-        if (threadIdx.x < 2) {
-            const uint64_t p = threadIdx.x ? end - 1 : base;
-            uint32_t lo = 0, hi = n - 1;   // last table whose offset is <= p
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (off[mid] <= p) lo = mid; else hi = mid - 1;
-            }
-            s_q[threadIdx.x] = lo;
+    const int lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+    for (uint64_t seg = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+         seg * kGatherSpan < total; seg += warps) {
+        const uint64_t base = seg * kGatherSpan;
+        const uint64_t end = min(total, base + (uint64_t)kGatherSpan);
+        uint32_t lo = 0, hi = n - 1;   // last table whose offset is <= base (same in every lane)
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(off + mid) <= base) lo = mid; else hi = mid - 1;
         }
-        __syncthreads();
-        const uint32_t q0 = s_q[0], q1 = s_q[1];
-        for (uint64_t p = base + threadIdx.x; p < end; p += blockDim.x) {
-            uint32_t lo = q0, hi = q1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (off[mid] <= p) lo = mid; else hi = mid - 1;
+        uint32_t q = lo;
+        uint64_t q_lo = __ldg(off + q), q_hi = __ldg(off + q + 1);
+        const uint32_t* row0 = nullptr;
+        uint32_t stride = 1, cols = 1;
+        bool have = false;
+        for (uint64_t p = base + lane; p < end; p += 32) {
+            while (p >= q_hi) {   // tables are back to back: step to the one holding p
+                ++q;
+                q_lo = q_hi;
+                q_hi = __ldg(off + q + 1);
+                have = false;
             }
-            const uint64_t e = p - off[lo];
-            const uint32_t* row0;
-            uint32_t stride, cols;
-            src(lo, row0, stride, cols);
+            if (!have) {
+                src(q, row0, stride, cols);
+                have = true;
+            }
+            const uint64_t e = p - q_lo;
             uint64_t r, c;
             if (e < (1ull << 32)) {
                 r = (uint32_t)e / cols;
@@ -433,7 +441,6 @@ __device__ void segmented_gather(uint32_t n, const uint64_t* __restrict__ off, S
             }
             out[p] = __ldg(row0 + r * stride + c);
         }
-        __syncthreads();
     }
 }
 
