@@ -316,6 +316,12 @@ int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, wk_step_prof
  * membership), in a library built with -DWK_PHASE_TIMING; all zero otherwise.  n >= 12.
  * No reference counterpart. */
 int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
+/* Fault injection on the host, for tests: the next time the context reads its device error
+ * word after a launch, it also sees `err_bits` (1 overflow, 2 bounded wait gave up, 4 corrupt
+ * chain).  The same handling runs as for a real device-side error: growth and rerun for an
+ * overflow, WK_E_TIMEOUT / WK_E_CORRUPT otherwise, with the context usable afterwards.  No GPU
+ * fault, trap or hang is involved.  No reference counterpart (the reference aborts). */
+int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
 
 /* Tile-schedule knobs of the exploration launch (what the autotuner sets).
  *   knob 0: lanes per probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte

@@ -26,9 +26,9 @@ namespace {
 
 constexpr int kScanThreads = 1024;
 
-// Final table of each query: its rows at its last level, laid out back to back.  One CTA; each
-// thread owns kScanPer consecutive queries per round (all their loads issued together, a
-// serial scan of its own queries), and one block scan per round joins the threads.
+// Final table of each query: its rows at its last level, laid out back to back.  One CTA walks
+// the queries kScanPer rounds of 1024 at a time: the loads of all those rounds are issued
+// together (coalesced), then one block scan per round with a running carry.
 constexpr int kScanPer = 8;
 
 __global__ void __launch_bounds__(kScanThreads) result_scan_kernel(const ResultScanArgs a) {
@@ -37,42 +37,40 @@ __global__ void __launch_bounds__(kScanThreads) result_scan_kernel(const ResultS
     const uint32_t n = a.n;
     if (threadIdx.x == 0) s_carry = 0;
     for (uint32_t r0 = 0; r0 < n; r0 += kScanThreads * kScanPer) {
-        const uint32_t q0 = r0 + threadIdx.x * kScanPer;
         int lev[kScanPer];
         uint64_t rows[kScanPer], base[kScanPer];
 #pragma unroll
-        for (int k = 0; k < kScanPer; ++k) lev[k] = q0 + k < n ? (int)a.nsteps[q0 + k] - 1 : -1;
+        for (int k = 0; k < kScanPer; ++k) {
+            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
+            lev[k] = q < n ? (int)a.nsteps[q] - 1 : -1;
+        }
 #pragma unroll
         for (int k = 0; k < kScanPer; ++k) {
+            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
             rows[k] = 0;
             base[k] = 0;
             if (lev[k] >= 0) {
-                rows[k] = a.qcount[(size_t)lev[k] * n + q0 + k];
-                base[k] = a.qfirst[(size_t)lev[k] * n + q0 + k];
+                rows[k] = a.qcount[(size_t)lev[k] * n + q];
+                base[k] = a.qfirst[(size_t)lev[k] * n + q];
             }
         }
-        uint64_t sum = 0;
 #pragma unroll
         for (int k = 0; k < kScanPer; ++k) {
-            const uint32_t q = q0 + k;
-            if (q >= n) break;
-            a.final_level[q] = rows[k] ? lev[k] : -1;
-            a.final_base[q] = rows[k] ? base[k] : 0;
-            a.final_rows[q] = rows[k];
-            rows[k] *= a.final_cols[q];   // elements from here on
-            sum += rows[k];
+            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
+            uint64_t elems = 0;
+            if (q < n) {
+                a.final_level[q] = rows[k] ? lev[k] : -1;
+                a.final_base[q] = rows[k] ? base[k] : 0;
+                a.final_rows[q] = rows[k];
+                elems = rows[k] * a.final_cols[q];
+            }
+            const uint64_t ex = dev::block_exclusive_sum<kScanThreads>(elems, s_warp);   // syncs
+            const uint64_t carry = s_carry;
+            if (q < n) a.res_off[q] = carry + ex;
+            __syncthreads();   // everyone has read s_carry
+            if (threadIdx.x == kScanThreads - 1) s_carry = carry + ex + elems;
+            __syncthreads();
         }
-        const uint64_t ex = dev::block_exclusive_sum<kScanThreads>(sum, s_warp);   // syncs
-        uint64_t run = s_carry + ex;
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            if (q0 + k >= n) break;
-            a.res_off[q0 + k] = run;
-            run += rows[k];
-        }
-        __syncthreads();   // everyone has read s_carry
-        if (threadIdx.x == kScanThreads - 1) s_carry = s_carry + ex + sum;
-        __syncthreads();
     }
     if (threadIdx.x == 0) a.res_off[n] = s_carry;
 }

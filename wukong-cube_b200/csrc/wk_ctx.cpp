@@ -156,8 +156,16 @@ int wk_ctx::table_reserve(wk_table* t, uint64_t elems) {
 int wk_ctx::read_ctl(uint32_t* err, uint64_t* need) {
     WK_CUDA(this, cudaMemcpyAsync(h_ctl, d_ctl, sizeof(wk::StepCtl), cudaMemcpyDeviceToHost, stream));
     WK_CUDA(this, cudaStreamSynchronize(stream));
-    *err = h_ctl->err;
+    *err = h_ctl->err | inject_err;   // a failure staged by wk_debug_fail_next counts once
     *need = h_ctl->need;
+    inject_err = 0;
+    return WK_SUCCESS;
+}
+
+extern "C" int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits) {
+    if (!ctx || (err_bits & ~(uint32_t)(wk::kErrOverflow | wk::kErrTimeout | wk::kErrCorrupt))) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->inject_err = err_bits;
     return WK_SUCCESS;
 }
 

@@ -93,6 +93,7 @@ struct wk_ctx {
     uint64_t status_cap = 0;
     wk::StepCtl* h_ctl = nullptr;     // pinned
     uint64_t* h_rows = nullptr;       // pinned
+    uint32_t inject_err = 0;          // error bits the next control-block read reports (tests)
 
     // ping-pong result buffers for whole queries (GPUMem rbuf pair, gpu_mem.hpp:53-60)
     wk_table rbuf[2];

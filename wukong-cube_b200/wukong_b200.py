@@ -167,6 +167,7 @@ _SIGS = {
                                           C.POINTER(C.c_uint64)]),
     "wk_batch_replay": (C.c_int, [_P]),
     "wk_debug_phase_cycles": (C.c_int, [C.POINTER(C.c_ulonglong), C.c_int32, C.c_int32]),
+    "wk_debug_fail_next": (C.c_int, [_P, C.c_uint32]),
     "wk_ctx_tune_set": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "wk_ctx_tune_get": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32)]),
     "wk_ctx_autotune": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
