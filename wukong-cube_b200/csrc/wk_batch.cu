@@ -26,53 +26,49 @@ namespace {
 
 constexpr int kScanThreads = 1024;
 
-// Final table of each query: its rows at its last level, laid out back to back.  One CTA walks
-// the queries kScanPer rounds of 1024 at a time: the loads of all those rounds are issued
-// together (coalesced), then one block scan per round with a running carry.
-constexpr int kScanPer = 8;
+// Final table of each query: its rows at its last level, laid out back to back.  CTA t owns
+// queries [t * 1024, (t + 1) * 1024): it first adds up the element counts of every query
+// before its own (a strided read of at most a few thousand words per thread block, from L2),
+// then scans its own queries.  No CTA waits for another.
+__device__ __forceinline__ uint64_t final_elems(const ResultScanArgs& a, uint32_t q, int* lev,
+                                                uint64_t* rows, uint64_t* base) {
+    *lev = (int)a.nsteps[q] - 1;
+    *rows = 0;
+    *base = 0;
+    if (*lev >= 0) {
+        *rows = a.qcount[(size_t)*lev * a.n + q];
+        *base = a.qfirst[(size_t)*lev * a.n + q];
+    }
+    return *rows * a.final_cols[q];
+}
 
 __global__ void __launch_bounds__(kScanThreads) result_scan_kernel(const ResultScanArgs a) {
     __shared__ uint64_t s_warp[kScanThreads / 32];
-    __shared__ uint64_t s_carry;
     const uint32_t n = a.n;
-    if (threadIdx.x == 0) s_carry = 0;
-    for (uint32_t r0 = 0; r0 < n; r0 += kScanThreads * kScanPer) {
-        int lev[kScanPer];
-        uint64_t rows[kScanPer], base[kScanPer];
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
-            lev[k] = q < n ? (int)a.nsteps[q] - 1 : -1;
-        }
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
-            rows[k] = 0;
-            base[k] = 0;
-            if (lev[k] >= 0) {
-                rows[k] = a.qcount[(size_t)lev[k] * n + q];
-                base[k] = a.qfirst[(size_t)lev[k] * n + q];
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kScanPer; ++k) {
-            const uint32_t q = r0 + k * kScanThreads + threadIdx.x;
-            uint64_t elems = 0;
-            if (q < n) {
-                a.final_level[q] = rows[k] ? lev[k] : -1;
-                a.final_base[q] = rows[k] ? base[k] : 0;
-                a.final_rows[q] = rows[k];
-                elems = rows[k] * a.final_cols[q];
-            }
-            const uint64_t ex = dev::block_exclusive_sum<kScanThreads>(elems, s_warp);   // syncs
-            const uint64_t carry = s_carry;
-            if (q < n) a.res_off[q] = carry + ex;
-            __syncthreads();   // everyone has read s_carry
-            if (threadIdx.x == kScanThreads - 1) s_carry = carry + ex + elems;
-            __syncthreads();
-        }
+    const uint32_t t0 = blockIdx.x * kScanThreads;
+    uint64_t before = 0;
+    for (uint32_t q = threadIdx.x; q < t0; q += kScanThreads) {
+        int lev;
+        uint64_t rows, base;
+        before += final_elems(a, q, &lev, &rows, &base);
     }
-    if (threadIdx.x == 0) a.res_off[n] = s_carry;
+    // block total of `before` (the inclusive sum of the last thread)
+    const uint64_t bex = dev::block_exclusive_sum<kScanThreads>(before, s_warp);
+    __shared__ uint64_t s_base;
+    if (threadIdx.x == kScanThreads - 1) s_base = bex + before;
+    __syncthreads();
+    const uint32_t q = t0 + threadIdx.x;
+    int lev = -1;
+    uint64_t rows = 0, base = 0, elems = 0;
+    if (q < n) {
+        elems = final_elems(a, q, &lev, &rows, &base);
+        a.final_level[q] = rows ? lev : -1;
+        a.final_base[q] = rows ? base : 0;
+        a.final_rows[q] = rows;
+    }
+    const uint64_t ex = dev::block_exclusive_sum<kScanThreads>(elems, s_warp);
+    if (q < n) a.res_off[q] = s_base + ex;
+    if (n > 0 ? q == n - 1 : q == 0) a.res_off[n] = s_base + ex + elems;
 }
 
 // Copy each query's final table (stride of its level) into the compact result buffer.
@@ -96,7 +92,7 @@ __global__ void __launch_bounds__(256) gather_kernel(const GatherArgs a) {
 }  // namespace
 
 cudaError_t launch_result_scan(const ResultScanArgs& a, cudaStream_t s) {
-    result_scan_kernel<<<1, kScanThreads, 0, s>>>(a);
+    result_scan_kernel<<<std::max<uint32_t>(1, (a.n + kScanThreads - 1) / kScanThreads), kScanThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 

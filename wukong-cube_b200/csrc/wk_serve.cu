@@ -39,45 +39,40 @@ namespace {
 
 constexpr int kMaxSteps = kMaxBatchLevels;
 
-// Copy newly admitted queries' plans into their slots and stamp the admission iteration.
-__global__ void install_kernel(StepDesc* plans, uint32_t* admit, const StepDesc* stage,
-                               const uint32_t* slots, uint32_t n_new, uint32_t iter) {
-    for (uint32_t i = blockIdx.x; i < n_new; i += gridDim.x) {
-        const uint32_t s = slots[i];
-        for (int k = threadIdx.x; k < kMaxSteps; k += blockDim.x)
-            plans[(size_t)s * kMaxSteps + k] = stage[(size_t)i * kMaxSteps + k];
-        if (threadIdx.x == 0) admit[s] = iter;
-    }
-}
-
-// Rows and result offsets of the queries finishing this iteration (one CTA).
 // Small CTAs: every kernel of an iteration must fit in the room the lanes leave on an SM.
 constexpr int kFinishThreads = 256;
 
-// Per-iteration reset of the slots' output ranges and of this iteration's row total.
+// Start of an iteration: reset the slots' output ranges and this iteration's row total, and
+// install the newly admitted queries' plans in their slots with the admission iteration.
 __global__ void __launch_bounds__(256)
-reset_kernel(unsigned long long* qfirst, unsigned long long* qcount, uint32_t n, uint64_t* total) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+prep_kernel(unsigned long long* qfirst, unsigned long long* qcount, uint32_t n_slots, uint64_t* total,
+            StepDesc* plans, uint32_t* admit, const StepDesc* stage, const uint32_t* new_slots,
+            uint32_t n_new, uint32_t iter) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nt = gridDim.x * blockDim.x;
+    for (uint32_t i = tid; i < n_slots; i += nt) {
         qfirst[i] = ~0ull;
         qcount[i] = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *total = 0;
+    for (uint32_t e = tid; e < n_new * (uint32_t)kMaxSteps; e += nt) {
+        const uint32_t i = e / kMaxSteps, k = e - i * kMaxSteps;
+        const uint32_t s = new_slots[i];
+        plans[(size_t)s * kMaxSteps + k] = stage[e];
+        if (k == 0) admit[s] = iter;
+    }
+    if (tid == 0) *total = 0;
 }
 
+// Result offsets of the queries finishing this iteration (one CTA).
 __global__ void __launch_bounds__(kFinishThreads)
 finish_scan_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32_t n_fin,
-                   const unsigned long long* qcount, uint64_t* fin_rows, uint64_t* fin_off) {
+                   const unsigned long long* qcount, uint64_t* fin_off) {
     __shared__ uint64_t s_warp[kFinishThreads / 32];
     __shared__ uint64_t s_carry;
     if (threadIdx.x == 0) s_carry = 0;
     for (uint32_t r0 = 0; r0 < n_fin; r0 += kFinishThreads) {
         const uint32_t i = r0 + threadIdx.x;
         uint64_t sum = 0;
-        if (i < n_fin) {
-            const uint64_t r = qcount[fin_slots[i]];
-            fin_rows[i] = r;
-            sum = r * fin_cols[i];
-        }
+        if (i < n_fin) sum = qcount[fin_slots[i]] * fin_cols[i];
         const uint64_t ex = dev::block_exclusive_sum<kFinishThreads>(sum, s_warp);
         const uint64_t carry = s_carry;
         if (i < n_fin) fin_off[i] = carry + ex;
@@ -107,6 +102,13 @@ finish_gather_kernel(const uint32_t* fin_slots, const uint32_t* fin_cols, uint32
                           out);
 }
 
+// End of an iteration: the error word and the size request go into the packet the host reads
+// back (after every other kernel of the iteration, so a result-buffer overflow is included).
+__global__ void pack_kernel(const StepCtl* ctl, uint64_t* pkt) {
+    pkt[0] = ctl->err;
+    pkt[1] = ctl->need;
+}
+
 struct QSlot {
     uint32_t query;       // index into the caller's query array
     uint32_t admit_iter;
@@ -133,32 +135,31 @@ struct Serve {
     uint64_t* d_total = nullptr;              // [2]
     unsigned long long* d_qfirst = nullptr;   // [slots]
     unsigned long long* d_qcount = nullptr;   // [slots]
-    uint32_t* d_new = nullptr;                // [slots]
-    StepDesc* d_stage = nullptr;              // [slots][kMaxSteps]
-    uint32_t* d_fin_slots = nullptr;          // [slots]
-    uint32_t* d_fin_cols = nullptr;           // [slots]
-    uint64_t* d_fin_rows = nullptr;           // [slots]
-    uint64_t* d_fin_off = nullptr;            // [slots + 1]
     uint32_t* d_result = nullptr;
     uint64_t result_cap = 0;
-    // pinned host staging
-    StepDesc* h_stage = nullptr;
-    uint32_t* h_new = nullptr;
-    uint32_t* h_fin_slots = nullptr;
-    uint32_t* h_fin_cols = nullptr;
-    uint64_t* h_fin_rows = nullptr;
-    uint64_t* h_fin_off = nullptr;
-    uint64_t* h_total = nullptr;
+    // What an iteration sends up, in one copy: the new queries' plans (n_new x kMaxSteps
+    // descriptors), then their slots, the finishing slots and their widths (u32 each).
+    unsigned char* d_in = nullptr;
+    unsigned char* h_in = nullptr;   // pinned
+    // What it reads back, in one copy: the error word, the size request, and the finishing
+    // queries' result offsets (n_fin + 1).
+    uint64_t* d_pkt = nullptr;
+    uint64_t* h_pkt = nullptr;       // pinned
     uint32_t* h_result = nullptr;
+    // this iteration's lists (host)
+    std::vector<uint32_t> new_slots, fin_slots, fin_cols;
+
+    StepDesc* h_stage() const { return reinterpret_cast<StepDesc*>(h_in); }
+    size_t in_bytes(uint32_t n_new, uint32_t n_fin) const {
+        return sizeof(StepDesc) * kMaxSteps * (size_t)n_new + 4ull * (n_new + 2ull * n_fin);
+    }
 
     ~Serve() {
         auto f = [](void* p) { if (p) cudaFree(p); };
         auto fh = [](void* p) { if (p) cudaFreeHost(p); };
         f(d_plans); f(d_admit); f(d_arena[0]); f(d_arena[1]); f(d_owner[0]); f(d_owner[1]);
-        f(d_total); f(d_qfirst); f(d_qcount); f(d_new); f(d_stage); f(d_fin_slots); f(d_fin_cols);
-        f(d_fin_rows); f(d_fin_off); f(d_result);
-        fh(h_stage); fh(h_new); fh(h_fin_slots); fh(h_fin_cols); fh(h_fin_rows); fh(h_fin_off);
-        fh(h_total); fh(h_result);
+        f(d_total); f(d_qfirst); f(d_qcount); f(d_in); f(d_pkt); f(d_result);
+        fh(h_in); fh(h_pkt); fh(h_result);
     }
 
     int alloc_arena(int k, uint64_t rows) {
@@ -201,18 +202,16 @@ struct Serve {
             return true;
         };
         auto hm = [&](void** p, size_t bytes) { return cudaMallocHost(p, std::max<size_t>(bytes, 16)) == cudaSuccess; };
+        const size_t in_cap = in_bytes(slots, slots) + 64;
         bool ok = dm((void**)&d_plans, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
                   dm((void**)&d_admit, 4ull * slots) && dm((void**)&d_total, 16) &&
                   dm((void**)&d_qfirst, 8ull * slots) && dm((void**)&d_qcount, 8ull * slots) &&
-                  dm((void**)&d_new, 4ull * slots) &&
-                  dm((void**)&d_stage, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
-                  dm((void**)&d_fin_slots, 4ull * slots) && dm((void**)&d_fin_cols, 4ull * slots) &&
-                  dm((void**)&d_fin_rows, 8ull * slots) && dm((void**)&d_fin_off, 8ull * (slots + 1)) &&
-                  hm((void**)&h_stage, sizeof(StepDesc) * kMaxSteps * (size_t)slots) &&
-                  hm((void**)&h_new, 4ull * slots) && hm((void**)&h_fin_slots, 4ull * slots) &&
-                  hm((void**)&h_fin_cols, 4ull * slots) && hm((void**)&h_fin_rows, 8ull * slots) &&
-                  hm((void**)&h_fin_off, 8ull * (slots + 1)) && hm((void**)&h_total, 16);
+                  dm((void**)&d_in, in_cap) && dm((void**)&d_pkt, 8ull * (slots + 3)) &&
+                  hm((void**)&h_in, in_cap) && hm((void**)&h_pkt, 8ull * (slots + 3));
         if (!ok) return ctx->fail(WK_E_OOM, "serving buffers");
+        new_slots.reserve(slots);
+        fin_slots.reserve(slots);
+        fin_cols.reserve(slots);
         const uint64_t rows = std::max<uint64_t>(cfg.arena_bytes / (4ull * w), 1 << 16);
         int rc = alloc_arena(0, rows);
         if (!rc) rc = alloc_arena(1, rows);
@@ -250,19 +249,27 @@ struct Serve {
         return a;
     }
 
-    // Enqueue one iteration (no host sync).
-    int enqueue_iteration(uint32_t iter, uint32_t n_new, bool has_cont, uint32_t n_fin) {
+    // Enqueue one iteration (no host sync): one copy up, the launches, one copy back.  The
+    // plans of the n_new admitted queries are already in h_stage(); new_slots, fin_slots and
+    // fin_cols hold this iteration's lists.
+    int enqueue_iteration(uint32_t iter, bool has_cont) {
         const int cur = iter & 1, prev = cur ^ 1;
+        const uint32_t n_new = (uint32_t)new_slots.size(), n_fin = (uint32_t)fin_slots.size();
         cudaStream_t s = ctx->stream;
-        if (n_new) {
-            WKS_CUDA(ctx, cudaMemcpyAsync(d_stage, h_stage, sizeof(StepDesc) * kMaxSteps * (size_t)n_new,
-                                          cudaMemcpyHostToDevice, s));
-            WKS_CUDA(ctx, cudaMemcpyAsync(d_new, h_new, 4ull * n_new, cudaMemcpyHostToDevice, s));
-            install_kernel<<<std::min<uint32_t>(n_new, 1024), 32, 0, s>>>(d_plans, d_admit, d_stage, d_new, n_new, iter);
-            WKS_CUDA(ctx, cudaGetLastError());
-        }
-        reset_kernel<<<std::min<uint32_t>((slots_n + 255) / 256, 1024), 256, 0, s>>>(d_qfirst, d_qcount,
-                                                                                    slots_n, d_total + cur);
+        const size_t stage_bytes = sizeof(StepDesc) * kMaxSteps * (size_t)n_new;
+        uint32_t* hl = reinterpret_cast<uint32_t*>(h_in + stage_bytes);
+        std::memcpy(hl, new_slots.data(), 4ull * n_new);
+        std::memcpy(hl + n_new, fin_slots.data(), 4ull * n_fin);
+        std::memcpy(hl + n_new + n_fin, fin_cols.data(), 4ull * n_fin);
+        const StepDesc* d_stage = reinterpret_cast<const StepDesc*>(d_in);
+        const uint32_t* d_new = reinterpret_cast<const uint32_t*>(d_in + stage_bytes);
+        const uint32_t* d_fin_slots = d_new + n_new;
+        const uint32_t* d_fin_cols = d_fin_slots + n_fin;
+        if (n_new || n_fin)
+            WKS_CUDA(ctx, cudaMemcpyAsync(d_in, h_in, in_bytes(n_new, n_fin), cudaMemcpyHostToDevice, s));
+        const uint32_t work = std::max<uint32_t>(slots_n, n_new * (uint32_t)kMaxSteps);
+        prep_kernel<<<std::min<uint32_t>((work + 255) / 256, 1024), 256, 0, s>>>(
+            d_qfirst, d_qcount, slots_n, d_total + cur, d_plans, d_admit, d_stage, d_new, n_new, iter);
         WKS_CUDA(ctx, cudaGetLastError());
         const int light = light_ctas();
         const int grid = std::min(explore_blocks_per_sm(w, w, ctx->batch_lanes), light) * ctx->sm_count;
@@ -288,22 +295,30 @@ struct Serve {
             cudaError_t e = launch_explore(a, g0, s);
             if (e != cudaSuccess) return ctx->cuda_fail(e, "serving start launch");
         }
+        uint64_t* d_fin_off = d_pkt + 2;
         if (n_fin) {
-            WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_slots, h_fin_slots, 4ull * n_fin, cudaMemcpyHostToDevice, s));
-            WKS_CUDA(ctx, cudaMemcpyAsync(d_fin_cols, h_fin_cols, 4ull * n_fin, cudaMemcpyHostToDevice, s));
-            finish_scan_kernel<<<1, kFinishThreads, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount,
-                                                            d_fin_rows, d_fin_off);
+            finish_scan_kernel<<<1, kFinishThreads, 0, s>>>(d_fin_slots, d_fin_cols, n_fin, d_qcount, d_fin_off);
             if (!cfg.blind)
                 finish_gather_kernel<<<ctx->sm_count * 4, 256, 0, s>>>(
                     d_fin_slots, d_fin_cols, n_fin, d_qfirst, d_fin_off, d_arena[cur], w, d_result,
                     result_cap, ctx->d_ctl);
-            WKS_CUDA(ctx, cudaGetLastError());
-            WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_rows, d_fin_rows, 8ull * n_fin, cudaMemcpyDeviceToHost, s));
-            WKS_CUDA(ctx, cudaMemcpyAsync(h_fin_off, d_fin_off, 8ull * (n_fin + 1), cudaMemcpyDeviceToHost, s));
         }
-        WKS_CUDA(ctx, cudaMemcpyAsync(h_total, d_total, 16, cudaMemcpyDeviceToHost, s));
+        pack_kernel<<<1, 1, 0, s>>>(ctx->d_ctl, d_pkt);
+        WKS_CUDA(ctx, cudaGetLastError());
+        WKS_CUDA(ctx, cudaMemcpyAsync(h_pkt, d_pkt, 8ull * (2 + (n_fin ? n_fin + 1 : 0)),
+                                      cudaMemcpyDeviceToHost, s));
         return WK_SUCCESS;
     }
+
+    // Wait for the iteration; the error word and the size request it ended with.
+    int finish_iteration(uint32_t* err, uint64_t* need) {
+        WKS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *err = (uint32_t)h_pkt[0] | ctx->inject_err;   // a staged test failure counts once
+        ctx->inject_err = 0;
+        *need = h_pkt[1];
+        return WK_SUCCESS;
+    }
+    const uint64_t* fin_off() const { return h_pkt + 2; }
 };
 
 // Index-start queries run whole, one at a time per lane: a child context (its own stream of
@@ -399,8 +414,8 @@ struct HeavyLanes {
 
 cudaError_t serve_kernel_attrs() {
     cudaError_t e;
-    if ((e = use_max_shared_carveout(install_kernel)) != cudaSuccess) return e;
-    if ((e = use_max_shared_carveout(reset_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(prep_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(pack_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(finish_scan_kernel)) != cudaSuccess) return e;
     return use_max_shared_carveout(finish_gather_kernel);
 }
@@ -521,12 +536,13 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     std::deque<uint32_t> wait_heavy, wait_light;   // arrived, not yet admitted
     // Give constant-start query q a slot and stage its plan (Done-padded) for installation
     // this iteration.
-    auto admit = [&](uint32_t q, uint32_t& n_new) {
+    auto admit = [&](uint32_t q) {
         const uint32_t s = free_slots.back();
         free_slots.pop_back();
         slot[s] = {q, iter, (uint32_t)plans[q].size(), (uint32_t)plans[q].back().out_cols};
+        const size_t j = S.new_slots.size();
         for (int k = 0; k < wk::kMaxSteps; ++k) {
-            wk::StepDesc& d = S.h_stage[(size_t)n_new * wk::kMaxSteps + k];
+            wk::StepDesc& d = S.h_stage()[j * wk::kMaxSteps + k];
             if (k < (int)plans[q].size()) {
                 d = wk::make_step_desc(ctx, plans[q][k]);
             } else {
@@ -534,7 +550,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                 d.op = wk::kXDone;
             }
         }
-        S.h_new[n_new++] = s;
+        S.new_slots.push_back(s);
         proj_bytes += S.cfg.light_proj_bytes;
     };
     std::vector<uint32_t> lane_done;
@@ -575,11 +591,11 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             ++heavy_inflight;
             proj_bytes += S.cfg.heavy_proj_bytes;
         }
-        uint32_t n_new = 0;
+        S.new_slots.clear();
         while (!wait_light.empty() && !free_slots.empty() &&
                (proj_bytes + S.cfg.light_proj_bytes <= S.cfg.working_set_cap_bytes ||
-                (active.empty() && !heavy_inflight && !n_new))) {
-            admit(wait_light.front(), n_new);
+                (active.empty() && !heavy_inflight && S.new_slots.empty()))) {
+            admit(wait_light.front());
             wait_light.pop_front();
         }
         const bool has_cont = !active.empty();
@@ -587,7 +603,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             for (uint32_t s : cooling) free_slots.push_back(s);
             cooling.clear();
         }
-        for (uint32_t i = 0; i < n_new; ++i) active.push_back(S.h_new[i]);
+        for (uint32_t s : S.new_slots) active.push_back(s);
         if (active.empty()) {
             // idle until the next arrival or a lane finishing, whichever comes first
             double wait = next < n ? arrival_us[next] - now_us() : 1e6;
@@ -600,30 +616,32 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             continue;
         }
         // 3. which queries run their last step in this iteration
-        uint32_t n_fin = 0;
+        S.fin_slots.clear();
+        S.fin_cols.clear();
         for (uint32_t s : active) {
             const wk::QSlot& sl = slot[s];
             if (iter - sl.admit_iter == sl.nsteps - 1) {
-                S.h_fin_slots[n_fin] = s;
-                S.h_fin_cols[n_fin] = sl.cols;
-                ++n_fin;
+                S.fin_slots.push_back(s);
+                S.fin_cols.push_back(sl.cols);
             }
         }
+        const uint32_t n_fin = (uint32_t)S.fin_slots.size();
         // 4. run it; grow the output arena and rerun if a table did not fit
         for (int attempt = 0;; ++attempt) {
             if (attempt >= 6) return ctx->fail(WK_E_CAPACITY, "serving arena kept overflowing");
-            rc = S.enqueue_iteration(iter, n_new, has_cont, n_fin);
+            rc = S.enqueue_iteration(iter, has_cont);
             if (rc) return rc;
             uint32_t err = 0;
             uint64_t need = 0;
-            rc = ctx->read_ctl(&err, &need);   // synchronises the stream
+            rc = S.finish_iteration(&err, &need);   // synchronises the stream
             if (rc) return rc;
             if (!err) break;
             ctx->clear_ctl_err();
             if (err & wk::kErrCorrupt) return ctx->fail(WK_E_CORRUPT, "key table chain out of range");
             if (err & wk::kErrTimeout) return ctx->fail(WK_E_TIMEOUT, "serving launch timed out");
             if (err & wk::kErrResult) {
-                rc = S.alloc_result(S.h_fin_off[n_fin] + S.h_fin_off[n_fin] / 2 + 1024);
+                const uint64_t total = S.fin_off()[n_fin];
+                rc = S.alloc_result(total + total / 2 + 1024);
                 if (rc) return rc;
             }
             if (err & (wk::kErrOverflow | wk::kErrStatus)) {
@@ -639,15 +657,18 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         }
         // 5. completions
         if (n_fin) {
-            const uint64_t total = S.cfg.blind ? 0 : S.h_fin_off[n_fin];
-            if (total)
-                WKS_CUDA(ctx, cudaMemcpy(S.h_result, S.d_result, total * 4, cudaMemcpyDeviceToHost));
+            const uint64_t* fo = S.fin_off();
+            const uint64_t total = S.cfg.blind ? 0 : fo[n_fin];
+            if (total) {
+                WKS_CUDA(ctx, cudaMemcpyAsync(S.h_result, S.d_result, total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+                WKS_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            }
             const double td = now_us();
             for (uint32_t i = 0; i < n_fin; ++i) {
-                const uint32_t s = S.h_fin_slots[i];
+                const uint32_t s = S.fin_slots[i];
                 const uint32_t q = slot[s].query;
                 wk_qresult& r = results[q];
-                r.rows = S.h_fin_rows[i];
+                r.rows = (fo[i + 1] - fo[i]) / slot[s].cols;   // every plan ends with >= 1 column
                 r.cols = (int32_t)slot[s].cols;
                 r.status = WK_SUCCESS;
                 r.t_done_us = td;
@@ -657,7 +678,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                     // row count only
                 } else if (reserve_out(elems, &off)) {
                     r.elem_offset = off;
-                    if (elems) std::memcpy(host_out + off, S.h_result + S.h_fin_off[i], elems * 4);
+                    if (elems) std::memcpy(host_out + off, S.h_result + fo[i], elems * 4);
                 } else {
                     r.status = WK_E_CAPACITY;   // the caller's buffer is full
                 }
