@@ -22,7 +22,7 @@ def test_knob_values_are_checked(ctx):
 def test_every_setting_gives_the_oracle_results(ctx, graph20, lanes, slice_rows):
     v = graph20["vocab"]
     o = graph20["oracle"]
-    old = [ctx.tune_get(k) for k in range(4)]
+    old = [ctx.tune_get(k) for k in range(6)]
     try:
         ctx.tune_set(wk.KNOB_LANES, lanes)
         ctx.tune_set(wk.KNOB_BATCH_LANES, lanes)
@@ -46,13 +46,14 @@ def test_autotune_picks_a_candidate_and_keeps_results(ctx, graph20):
     o = graph20["oracle"]
     qs = workloads.light_queries(v, graph20["instances"], 2000, seed=42)
     heavy = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
-    old = [ctx.tune_get(k) for k in range(4)]
+    old = [ctx.tune_get(k) for k in range(6)]
     try:
         r = ctx.autotune(qs + heavy, iters=3)
         assert r["batch_lanes"] in (2, 4, 8) and r["lanes"] in (2, 4, 8)
         assert r["batch_slice_rows"] in (8, 16, 32, 128, 512)
         assert r["slice_rows"] in (8, 16, 32, 128, 512)
-        assert r["candidates"] == 3 * 5 + 3 + 5
+        assert r["candidates"] == 1 + 3 * 5 + 3 + 5
+        assert r["batch_flat"] in (0, 1) and ctx.tune_get(wk.KNOB_BATCH_FLAT) == r["batch_flat"]
         assert ctx.tune_get(wk.KNOB_BATCH_LANES) == r["batch_lanes"]
         assert ctx.tune_get(wk.KNOB_SLICE_ROWS) == r["slice_rows"]
         assert 0 < r["batch_ms_tuned"] <= 1.25 * r["batch_ms_default"]

@@ -133,6 +133,8 @@ struct BatchState {
     uint32_t* d_arena = nullptr;          // [l_cap][rows_cap * w_cap] (+ padding)
     uint32_t* d_result = nullptr;         // compact results
     uint64_t result_cap = 0;
+    uint64_t* d_flat = nullptr;           // flat-level scratch: pos, off, part (wk_flat.h)
+    uint64_t flat_rows = 0;               // rows it is sized for: max(rows_cap, n_cap)
     // pinned host staging
     wk::StepDesc* h_desc = nullptr;
     uint32_t* h_nsteps = nullptr;
@@ -149,7 +151,7 @@ void free_state(BatchState* b) {
     auto f = [](void* p) { if (p) cudaFree(p); };
     f(b->d_desc); f(b->d_owner); f(b->d_total_out); f(b->d_qfirst); f(b->d_qcount);
     f(b->d_nsteps); f(b->d_final_cols); f(b->d_final_level); f(b->d_final_base);
-    f(b->d_final_rows); f(b->d_res_off); f(b->d_arena); f(b->d_result);
+    f(b->d_final_rows); f(b->d_res_off); f(b->d_arena); f(b->d_result); f(b->d_flat);
     auto fh = [](void* p) { if (p) cudaFreeHost(p); };
     fh(b->h_desc); fh(b->h_nsteps); fh(b->h_final_cols); fh(b->h_final_rows); fh(b->h_res_off);
     fh(b->h_ctl);
@@ -199,10 +201,13 @@ int ensure_state(wk_ctx* ctx, BatchState* b, uint32_t n, int levels, uint64_t ro
               hm((void**)&b->h_nsteps, 4ull * n) && hm((void**)&b->h_final_cols, 4ull * n) &&
               hm((void**)&b->h_final_rows, 8ull * n) && hm((void**)&b->h_res_off, 8ull * (n + 1)) &&
               hm((void**)&b->h_ctl, sizeof(wk::StepCtl));
+    const uint64_t frows = std::max<uint64_t>(rows_cap, n);
+    ok = ok && dm((void**)&b->d_flat, wk::flat_scratch_bytes(frows, wk::flat_grid(ctx->sm_count)));
     if (!ok) {
         free_state(b);
         return ctx->fail(WK_E_OOM, "batch buffers");
     }
+    b->flat_rows = frows;
     b->n_cap = n;
     b->l_cap = levels;
     b->rows_cap = rows_cap;
@@ -345,7 +350,36 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
             WKB_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 16, s));
             WKB_CUDA(ctx, cudaEventRecord(ph->ev[2 * k], s));
         }
-        cudaError_t e = wk::launch_explore(a, grid, s);
+        cudaError_t e;
+        if (ctx->batch_flat) {   // the four flat passes (wk_flat.cu) instead of the tile launch
+            wk::FlatLevelArgs f{};
+            f.store = a.store;
+            f.seg_index[0] = a.seg_index[0];
+            f.seg_index[1] = a.seg_index[1];
+            f.desc = a.desc;
+            f.n_queries = n;
+            f.virtual_rows = a.virtual_rows;
+            f.in_rows = a.in_rows;
+            f.owner_in = a.owner_in;
+            f.in = a.in;
+            f.w_in = a.w_in;
+            f.in_cap_rows = a.in_cap_rows;
+            f.out = a.out;
+            f.w_out = a.w_out;
+            f.out_cap_rows = a.out_cap_rows;
+            f.out_rows = a.out_rows;
+            f.owner_out = a.owner_out;
+            f.qfirst = a.qfirst;
+            f.qcount = a.qcount;
+            f.pos = b->d_flat;
+            f.off = b->d_flat + b->flat_rows + 1;
+            f.part = f.off + b->flat_rows;
+            f.ctl = a.ctl;
+            f.sorted_lists = a.sorted_lists;
+            e = wk::launch_flat_level(f, wk::flat_grid(ctx->sm_count), s);
+        } else {
+            e = wk::launch_explore(a, grid, s);
+        }
         if (e != cudaSuccess) return ctx->cuda_fail(e, "level launch");
         if (ph) {
             WKB_CUDA(ctx, cudaEventRecord(ph->ev[2 * k + 1], s));
@@ -404,6 +438,8 @@ int launch_batch(wk_ctx* ctx, BatchState* b, const Plan& P) {
     put(&ctx->heavy_cap, 8);
     put(&ctx->batch_lanes, 4);
     put(&ctx->batch_slice_rows, 4);
+    put(&ctx->batch_flat, 4);
+    put(&b->d_flat, sizeof(void*));
     put(&ctx->d_slots, sizeof(void*));
     if (shape != b->shape || !b->exec) {
         if (b->exec) cudaGraphExecDestroy(b->exec);

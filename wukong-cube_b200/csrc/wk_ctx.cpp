@@ -1117,6 +1117,9 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
     } else if (knob == WK_KNOB_FLAT_ROWS) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
         ctx->flat_min_rows = (uint64_t)value;
+    } else if (knob == WK_KNOB_BATCH_FLAT) {
+        if (value != 0 && value != 1) return ctx->fail(WK_E_BADARG, "batch level launch must be 0 or 1");
+        ctx->batch_flat = value;
     } else {
         return ctx->fail(WK_E_BADARG, "unknown knob");
     }
@@ -1142,6 +1145,7 @@ extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
     else if (knob == WK_KNOB_BATCH_SLICE_ROWS)
         *value = (int32_t)(ctx->batch_slice_rows ? ctx->batch_slice_rows : wk::kHeavyRows);
     else if (knob == WK_KNOB_FLAT_ROWS) *value = (int32_t)std::min<uint64_t>(ctx->flat_min_rows, INT32_MAX);
+    else if (knob == WK_KNOB_BATCH_FLAT) *value = ctx->batch_flat;
     else return ctx->fail(WK_E_BADARG, "unknown knob");
     return WK_SUCCESS;
 }

@@ -276,6 +276,215 @@ __global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArg
     }
 }
 
+// ---------------------------------------------------------------- batch levels
+// The same four passes over one level of a batch: every row carries its owner query, whose
+// step at this level (start, known_to_unknown, known_to_known, known_to_const or done) comes
+// from the level's descriptor array.  Rows keep their order, so each query's output rows stay
+// contiguous and its range is recorded from the runs of its rows.
+
+__device__ __forceinline__ uint64_t level_rows(const FlatLevelArgs& a) {
+    if (a.virtual_rows) return a.n_queries;
+    uint64_t R = *(volatile const uint64_t*)a.in_rows;
+    return R > a.in_cap_rows ? a.in_cap_rows : R;
+}
+
+__device__ __forceinline__ uint32_t level_owner(const FlatLevelArgs& a, uint64_t r) {
+    return a.virtual_rows ? (uint32_t)r : __ldg(a.owner_in + r);
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const FlatLevelArgs a) {
+    __shared__ uint64_t s_warp[kFlatThreads / 32];
+    const uint64_t R = level_rows(a);
+    uint64_t lo, hi;
+    chunk_of(R, &lo, &hi);
+    uint64_t sum = 0, sd = 0, alg = 0;
+    for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
+        const StepDesc* d = a.desc + level_owner(a, r);
+        const uint32_t op = d->op;
+        uint64_t key = 0;
+        const SegDesc* sg = &d->seg;
+        bool valid = op != kXDone;
+        uint32_t target = d->end_const, cin = 0;
+        if (valid && op == kXStart) {
+            key = d->start_key;
+        } else if (valid) {
+            cin = d->cin;
+            const uint32_t* row = a.in + r * (uint64_t)a.w_in;
+            const uint32_t cur = __ldg(row + d->cs);
+            if (op == kXK2K) target = __ldg(row + d->ce);
+            if (cur == kBlankId) valid = false;
+            if (op == kXK2U && d->type_index) {
+                // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+                key = make_key(0, cur, kIn);
+                sg = &a.seg_index[kIn];
+                if (cur >= (1u << kNbitsIdx)) valid = false;
+            } else {
+                key = make_key(cur, d->pid, d->dir);
+                if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+            }
+        }
+        uint64_t off = 0, deg = 0;
+        if (valid && sg->num_buckets != 0 && key != 0) {
+            const uint64_t p = thread_probe(a.store, key, bucket_of(key, *sg), &a.ctl->err);
+            off = ptr_off(p);
+            deg = ptr_size(p);
+            if (off + deg > a.store.n_edges) {
+                if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
+                deg = 0;
+            }
+        }
+        const bool filt = op == kXK2K || op == kXK2C;
+        uint32_t c = (uint32_t)deg;
+        if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
+        if (!valid) c = 0;
+        a.pos[r] = c;   // the count; flat_level_place_kernel turns it into the row's position
+        a.off[r] = off;
+        sum += c;
+        if (valid) {
+            sd += deg;
+            alg += cin * 4ull + 16 + deg * 4 + (uint64_t)c * d->cout * 4;
+        }
+    }
+    const uint64_t total = block_sum(sum, s_warp);
+    const uint64_t tsd = block_sum(sd, s_warp);
+    const uint64_t talg = block_sum(alg, s_warp);
+    if (threadIdx.x == 0) {
+        a.part[blockIdx.x] = total;
+        if (talg) {
+            atomicAdd(&a.ctl->sum_deg, (unsigned long long)tsd);
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)talg);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) flat_level_scan_kernel(const FlatLevelArgs a, uint32_t nparts) {
+    __shared__ uint64_t s_warp[32];
+    __shared__ uint64_t s_carry;
+    const uint64_t R = level_rows(a);
+    if (threadIdx.x == 0) s_carry = 0;
+    for (uint32_t r0 = 0; r0 < nparts; r0 += 1024) {
+        const uint32_t i = r0 + threadIdx.x;
+        const uint64_t x = i < nparts ? a.part[i] : 0;
+        const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < nparts) a.part[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry = carry + ex + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint64_t total = s_carry;
+        a.part[nparts] = total;
+        a.pos[R] = total;
+        if (total > a.out_cap_rows) {
+            atomicOr(&a.ctl->err, kErrOverflow);
+            atomicMax(&a.ctl->need, (unsigned long long)total);
+            *a.out_rows = 0;
+        } else {
+            *a.out_rows = total;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_level_place_kernel(const FlatLevelArgs a, uint32_t nparts) {
+    __shared__ uint64_t s_warp[kFlatThreads / 32];
+    __shared__ uint64_t s_carry;
+    const uint64_t R = level_rows(a);
+    if (a.part[nparts] > a.out_cap_rows) return;
+    uint64_t lo, hi;
+    chunk_of(R, &lo, &hi);
+    if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
+    __syncthreads();
+    for (uint64_t r0 = lo; r0 < hi; r0 += kFlatThreads) {
+        const uint64_t r = r0 + threadIdx.x;
+        const uint64_t c = r < hi ? a.pos[r] : 0;
+        const uint64_t ex = block_exclusive_sum<kFlatThreads>(c, s_warp);
+        const uint64_t p = s_carry + ex;
+        if (r < hi) {
+            a.pos[r] = p;
+            const uint32_t q = level_owner(a, r);
+            // the query's output range: (end - start) of every run of its rows
+            const bool first = r == lo || level_owner(a, r - 1) != q;
+            const bool last = r + 1 == hi || level_owner(a, r + 1) != q;
+            if (first) {
+                atomicMin(a.qfirst + q, (unsigned long long)p);
+                atomicAdd(a.qcount + q, (unsigned long long)(0 - p));
+            }
+            if (last) atomicAdd(a.qcount + q, (unsigned long long)(p + c));
+            const uint32_t op = a.desc[q].op;
+            if (c && (op == kXK2K || op == kXK2C)) {   // a surviving row keeps its columns
+                const int cin = a.desc[q].cin;
+                const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+                uint32_t* dst = a.out + p * (uint64_t)a.w_out;
+                for (int k = 0; k < cin; ++k) dst[k] = __ldg(src + k);
+                a.owner_out[p] = q;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == kFlatThreads - 1) s_carry = p + c;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const FlatLevelArgs a) {
+    __shared__ uint64_t s_pos[kWindow + 1];
+    __shared__ uint64_t s_off[kWindow];
+    __shared__ uint64_t s_i0;
+    const uint64_t R = level_rows(a);
+    const uint64_t total = a.pos[R];
+    if (total > a.out_cap_rows || total == 0) return;
+    const uint64_t per = (total + gridDim.x - 1) / gridDim.x;
+    const uint64_t j0 = min(total, (uint64_t)blockIdx.x * per), j1 = min(total, j0 + per);
+    if (j0 >= j1) return;
+    if (threadIdx.x < 32) {   // the last r with pos[r] <= j0 (pos[R] = total > j0)
+        uint64_t lo = 0, hi = R;
+        while (hi - lo > 1) {
+            const uint64_t step = (hi - lo + 31) / 32;
+            const uint64_t probe = min(hi, lo + (uint64_t)(threadIdx.x + 1) * step);
+            const bool le = probe < hi && a.pos[probe] <= j0;
+            const unsigned m = __ballot_sync(0xffffffffu, le);
+            const int k = m ? 31 - __clz(m) : -1;
+            const uint64_t nlo = k >= 0 ? min(hi, lo + (uint64_t)(k + 1) * step) : lo;
+            const uint64_t nhi = min(hi, nlo + step);
+            lo = nlo;
+            hi = max(nhi, lo + 1);
+        }
+        if (threadIdx.x == 0) s_i0 = lo;
+    }
+    __syncthreads();
+    const int wo = a.w_out;
+    uint64_t i = s_i0;
+    uint64_t j = j0;
+    while (j < j1 && i < R) {
+        const uint64_t n = min((uint64_t)kWindow, R - i);
+        for (int t = threadIdx.x; t <= (int)n; t += kFlatThreads) s_pos[t] = a.pos[i + t];
+        for (int t = threadIdx.x; t < (int)n; t += kFlatThreads) s_off[t] = a.off[i + t];
+        __syncthreads();
+        const uint64_t wend = min(j1, s_pos[n]);
+        for (uint64_t jj = j + threadIdx.x; jj < wend; jj += kFlatThreads) {
+            int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+            }
+            const uint64_t r = i + lo;
+            const uint32_t q = level_owner(a, r);
+            const StepDesc* d = a.desc + q;
+            const uint32_t op = d->op;
+            if (op != kXK2U && op != kXStart) continue;   // filters wrote their rows already
+            const int ecol = op == kXStart ? 0 : d->cin;
+            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+            uint32_t* dst = a.out + jj * (uint64_t)wo;
+            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
+            dst[ecol] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
+            a.owner_out[jj] = q;
+        }
+        j = max(j, wend);
+        i += n;
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 int flat_grid(int sm_count) { return sm_count * (2048 / kFlatThreads); }
@@ -288,12 +497,24 @@ cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+cudaError_t launch_flat_level(const FlatLevelArgs& a, int grid, cudaStream_t s) {
+    flat_level_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);
+    flat_level_scan_kernel<<<1, 1024, 0, s>>>(a, (uint32_t)grid);
+    flat_level_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
+    flat_level_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t flat_kernel_attrs() {
     cudaError_t e;
     if ((e = use_max_shared_carveout(flat_count_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_scan_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_place_kernel)) != cudaSuccess) return e;
-    return use_max_shared_carveout(flat_expand_kernel);
+    if ((e = use_max_shared_carveout(flat_expand_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_level_count_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_level_scan_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_level_place_kernel)) != cudaSuccess) return e;
+    return use_max_shared_carveout(flat_level_expand_kernel);
 }
 
 }  // namespace wk

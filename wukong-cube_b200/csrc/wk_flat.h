@@ -37,4 +37,33 @@ int flat_grid(int sm_count);
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s);
 cudaError_t flat_kernel_attrs();
 
+// One level of a batch through the flat passes: every row's step comes from its owner query's
+// descriptor.  Writes owner_out and each query's output range (qfirst / qcount, which the
+// caller has reset).  Level 0 has virtual rows: row r is query r's start.
+struct FlatLevelArgs {
+    DevStore store;
+    SegDesc seg_index[2];
+    const StepDesc* desc;        // [n_queries] this level's step per query
+    uint32_t n_queries;
+    int32_t virtual_rows;
+    const uint64_t* in_rows;
+    const uint32_t* owner_in;
+    const uint32_t* in;
+    int32_t w_in;
+    uint64_t in_cap_rows;
+    uint32_t* out;
+    int32_t w_out;
+    uint64_t out_cap_rows;
+    uint64_t* out_rows;
+    uint32_t* owner_out;
+    unsigned long long* qfirst;
+    unsigned long long* qcount;
+    uint64_t* pos;               // [max(in_cap_rows, n_queries) + 1]
+    uint64_t* off;               // [max(in_cap_rows, n_queries)]
+    uint64_t* part;              // [grid + 1]
+    StepCtl* ctl;
+    int32_t sorted_lists;
+};
+cudaError_t launch_flat_level(const FlatLevelArgs& a, int grid, cudaStream_t s);
+
 }  // namespace wk

@@ -102,7 +102,12 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
         double best = 0;
         if ((rc = time_batch(ctx, light, iters, s, ev, &best))) return rc;
         out->batch_ms_default = best;
-        int bl = out->batch_lanes, bs = out->batch_slice_rows;
+        int bl = out->batch_lanes, bs = out->batch_slice_rows, bf = 1;
+        // the flat passes first (lanes and slices do not apply to them), then every tile setting
+        if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, 1))) return rc;
+        if ((rc = time_batch(ctx, light, iters, s, ev, &best))) return rc;
+        ++out->candidates;
+        if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, 0))) return rc;
         for (int l : kLanes)
             for (int sl : kSlices) {
                 if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_LANES, l))) return rc;
@@ -114,12 +119,15 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
                     best = ms;
                     bl = l;
                     bs = sl;
+                    bf = 0;
                 }
             }
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_LANES, bl))) return rc;
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_SLICE_ROWS, bs))) return rc;
+        if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, bf))) return rc;
         out->batch_lanes = bl;
         out->batch_slice_rows = bs;
+        out->batch_flat = bf;
         out->batch_ms_tuned = best;
     }
 

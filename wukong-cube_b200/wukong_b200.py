@@ -4,7 +4,7 @@ A thin host-side mirror of the reference's GPU engine interface for Python calle
 bench): ``Context`` plays GPUEngine/GPUAgent (src/gpu/gpu_engine.hpp, gpu_agent.hpp), ``Query``
 is a planned SPARQLQuery pattern list (src/core/sparql/query.hpp:145-170) and every call raises
 ``WukongError`` carrying the status code of src/core/common/errors.hpp when the library fails.
-The library must be built (``python wukong-cube_b200/build.py``); there is no fallback path.
+The library must be built (``python wukong-cube_b200/wk_build.py``); there is no fallback path.
 """
 import ctypes as C
 import os
@@ -20,6 +20,7 @@ PREDICATE_ID, TYPE_ID = 0, 1
 NO_RESULT = 0xFFFF
 MODE_PLAIN, MODE_RESIDENT, MODE_GRAPH = 0, 1, 2
 KNOB_LANES, KNOB_BATCH_LANES, KNOB_SLICE_ROWS, KNOB_BATCH_SLICE_ROWS, KNOB_FLAT_ROWS = 0, 1, 2, 3, 4
+KNOB_BATCH_FLAT = 5
 
 SUCCESS = 0
 UNKNOWN_PATTERN = 3
@@ -84,7 +85,7 @@ class TuneResult(C.Structure):
                 ("slice_rows", C.c_int32), ("batch_ms_default", C.c_double),
                 ("batch_ms_tuned", C.c_double), ("single_ms_default", C.c_double),
                 ("single_ms_tuned", C.c_double), ("candidates", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("batch_flat", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class StepProf(C.Structure):
