@@ -430,7 +430,8 @@ def run_ours(args, world, rank, local_rank):
             "batch_other_ms": overheads,
             "autotune": tune,
             "serving": serving,
-            "gpu_launches": args.steps * (len(levels) + 2),
+            # per batch: one launch per level (four with the flat passes), result scan, gather
+            "gpu_launches": args.steps * (len(levels) * (4 if tune.get("batch_flat") else 1) + 2),
             "clocks": clk.summary()}
     if rank == 0:
         if not args.no_cpu:
