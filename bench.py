@@ -457,6 +457,7 @@ def run_profile_case(args):
     tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
     with wk.Context(0) as ctx:
         ctx.upload_gstore(g)
+        ctx.tune_set(wk.KNOB_BATCH_FLAT, 1 if args.batch_flat else 0)
         q = workloads.heavy_triangle(v)
         qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
         for _ in range(args.warmup + args.steps):
@@ -477,6 +478,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small ncu case instead of the benchmark")
+    ap.add_argument("--batch-flat", action="store_true",
+                    help="profile case: batch levels through the flat passes")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
