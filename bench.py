@@ -430,8 +430,10 @@ def run_ours(args, world, rank, local_rank):
             "batch_other_ms": overheads,
             "autotune": tune,
             "serving": serving,
-            # per batch: one launch per level (four with the flat passes), result scan, gather
-            "gpu_launches": args.steps * (len(levels) * (4 if tune.get("batch_flat") else 1) + 2),
+            # per batch: one launch per level (four where the level runs the flat passes),
+            # result scan, gather
+            "gpu_launches": args.steps * (sum(4 if (tune.get("batch_flat", 0) >> k) & 1 else 1
+                                              for k in range(len(levels))) + 2),
             "clocks": clk.summary()}
     if rank == 0:
         if not args.no_cpu:
@@ -457,7 +459,7 @@ def run_profile_case(args):
     tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
     with wk.Context(0) as ctx:
         ctx.upload_gstore(g)
-        ctx.tune_set(wk.KNOB_BATCH_FLAT, 1 if args.batch_flat else 0)
+        ctx.tune_set(wk.KNOB_BATCH_FLAT, args.batch_flat)
         q = workloads.heavy_triangle(v)
         qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
         for _ in range(args.warmup + args.steps):
@@ -478,8 +480,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--profile-case", action="store_true",
                     help="run the small ncu case instead of the benchmark")
-    ap.add_argument("--batch-flat", action="store_true",
-                    help="profile case: batch levels through the flat passes")
+    ap.add_argument("--batch-flat", type=lambda x: int(x, 0), default=0,
+                    help="profile case: mask of the batch levels run as the flat passes")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)

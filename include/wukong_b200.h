@@ -334,8 +334,9 @@ int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
  *   knob 4: single-query steps of index-start plans (and single steps) whose input has at
  *           least this many rows run as the flat count / scan / expand pipeline instead of the
  *           tile launch; 0 never does (default 65,536);
- *   knob 5: batch levels run as the tile launch (0, default) or as the flat passes (1): one
- *           thread per row, full occupancy, output rows split evenly over the grid.
+ *   knob 5: a mask over batch levels; level k runs as the flat passes when bit k is set (one
+ *           thread per row, full occupancy, output rows split evenly over the grid) and as
+ *           the tile launch otherwise (default 0: all tile launches).
  * wk_ctx_tune_get reads a knob back.  No reference counterpart (its launch shape is fixed,
  * gpu_hash.cu:96-326). */
 #define WK_KNOB_LANES 0
@@ -357,7 +358,7 @@ typedef struct wk_tune_result {
     double batch_ms_default, batch_ms_tuned; /* one batch replay, before and after */
     double single_ms_default, single_ms_tuned;   /* sum over the index-start queries */
     int32_t candidates;                      /* configurations timed */
-    int32_t batch_flat;                      /* chosen batch level launch (knob 5) */
+    int32_t batch_flat;                      /* chosen level mask of the flat passes (knob 5) */
     int32_t reserved[2];
 } wk_tune_result;
 int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters, wk_tune_result* out);

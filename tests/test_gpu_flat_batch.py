@@ -27,15 +27,19 @@ def _queries(graph, n, seed):
     return qs
 
 
-@pytest.mark.parametrize("n,seed", [(1, 91), (64, 92), (3000, 93)])
-def test_flat_levels_equal_tile_levels(flat_knob, graph20, n, seed):
+ALL_LEVELS = 0xFFFF   # knob 5 is a mask over batch levels; bit k sends level k to the flat passes
+
+
+@pytest.mark.parametrize("n,seed,mask", [(1, 91, ALL_LEVELS), (64, 92, ALL_LEVELS),
+                                         (3000, 93, ALL_LEVELS), (3000, 95, 0b101), (3000, 96, 0b10)])
+def test_flat_levels_equal_tile_levels(flat_knob, graph20, n, seed, mask):
     ctx = flat_knob
     o = graph20["oracle"]
     qs = _queries(graph20, max(n, 16), seed)[:n] if n > 16 else workloads.light_queries(
         graph20["vocab"], graph20["instances"], n, seed=seed)
     ctx.tune_set(wk.KNOB_BATCH_FLAT, 0)
     tile = ctx.batch(qs)
-    ctx.tune_set(wk.KNOB_BATCH_FLAT, 1)
+    ctx.tune_set(wk.KNOB_BATCH_FLAT, mask)
     flat = ctx.batch(qs)
     for q, (t0, s0), (t1, s1) in zip(qs, tile, flat):
         st, want, _ = o.run(q.flat(), q.nvars)
@@ -48,7 +52,7 @@ def test_flat_levels_equal_tile_levels(flat_knob, graph20, n, seed):
 def test_flat_levels_stream_and_device_replay(flat_knob, graph20):
     ctx = flat_knob
     o = graph20["oracle"]
-    ctx.tune_set(wk.KNOB_BATCH_FLAT, 1)
+    ctx.tune_set(wk.KNOB_BATCH_FLAT, ALL_LEVELS)
     qs = _queries(graph20, 900, 94)
     got = ctx.batch(qs, stream_batch=256, cap_elems=1024)
     for q, (t, st) in zip(qs, got):

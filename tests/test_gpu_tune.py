@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 
 def test_knob_values_are_checked(ctx):
     for knob, bad in ((wk.KNOB_LANES, 3), (wk.KNOB_BATCH_LANES, 16), (wk.KNOB_SLICE_ROWS, 4),
-                      (wk.KNOB_BATCH_SLICE_ROWS, 1 << 25), (9, 4)):
+                      (wk.KNOB_BATCH_SLICE_ROWS, 1 << 25), (wk.KNOB_BATCH_FLAT, 1 << 16),
+                      (wk.KNOB_BATCH_FLAT, -1), (9, 4)):
         with pytest.raises(wk.WukongError) as e:
             ctx.tune_set(knob, bad)
         assert e.value.code == wk.E_BADARG
@@ -52,8 +53,8 @@ def test_autotune_picks_a_candidate_and_keeps_results(ctx, graph20):
         assert r["batch_lanes"] in (2, 4, 8) and r["lanes"] in (2, 4, 8)
         assert r["batch_slice_rows"] in (8, 16, 32, 128, 512)
         assert r["slice_rows"] in (8, 16, 32, 128, 512)
-        assert r["candidates"] == 1 + 3 * 5 + 3 + 5
-        assert r["batch_flat"] in (0, 1) and ctx.tune_get(wk.KNOB_BATCH_FLAT) == r["batch_flat"]
+        assert r["candidates"] == 3 * 5 + max(len(q.patterns) for q in qs) + 3 + 5
+        assert 0 <= r["batch_flat"] < 64 and ctx.tune_get(wk.KNOB_BATCH_FLAT) == r["batch_flat"]
         assert ctx.tune_get(wk.KNOB_BATCH_LANES) == r["batch_lanes"]
         assert ctx.tune_get(wk.KNOB_SLICE_ROWS) == r["slice_rows"]
         assert 0 < r["batch_ms_tuned"] <= 1.25 * r["batch_ms_default"]

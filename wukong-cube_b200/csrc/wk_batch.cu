@@ -351,7 +351,7 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
             WKB_CUDA(ctx, cudaEventRecord(ph->ev[2 * k], s));
         }
         cudaError_t e;
-        if (ctx->batch_flat) {   // the four flat passes (wk_flat.cu) instead of the tile launch
+        if ((ctx->batch_flat >> k) & 1) {   // the four flat passes (wk_flat.cu), not the tile launch
             wk::FlatLevelArgs f{};
             f.store = a.store;
             f.seg_index[0] = a.seg_index[0];

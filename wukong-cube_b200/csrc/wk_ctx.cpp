@@ -1118,7 +1118,8 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
         ctx->flat_min_rows = (uint64_t)value;
     } else if (knob == WK_KNOB_BATCH_FLAT) {
-        if (value != 0 && value != 1) return ctx->fail(WK_E_BADARG, "batch level launch must be 0 or 1");
+        if (value < 0 || value >= (1 << wk::kMaxBatchLevels))
+            return ctx->fail(WK_E_BADARG, "batch level mask out of range");
         ctx->batch_flat = value;
     } else {
         return ctx->fail(WK_E_BADARG, "unknown knob");

@@ -80,7 +80,7 @@ struct wk_ctx {
     std::map<int, int> tuned_lanes;
     uint32_t slice_rows = 0;         // list length above which rows go to the slice queue
     uint32_t batch_slice_rows = 0;   // (0: the kernel's default, kHeavyRows)
-    int32_t batch_flat = 0;          // batch levels through the flat passes instead of the tiles
+    int32_t batch_flat = 0;          // bit k: batch level k runs as the flat passes, not tiles
     // single-query steps with at least this many input rows run the flat pipeline (0: never)
     uint64_t flat_min_rows = 65536;
     void* d_flat = nullptr;          // its scratch (wk_flat.h)

@@ -429,6 +429,8 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_place_kernel(const Fl
 __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const FlatLevelArgs a) {
     __shared__ uint64_t s_pos[kWindow + 1];
     __shared__ uint64_t s_off[kWindow];
+    __shared__ uint32_t s_q[kWindow];
+    __shared__ int32_t s_ecol[kWindow];   // column the edge goes to; -1: not an expanding row
     __shared__ uint64_t s_i0;
     const uint64_t R = level_rows(a);
     const uint64_t total = a.pos[R];
@@ -458,7 +460,15 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
     while (j < j1 && i < R) {
         const uint64_t n = min((uint64_t)kWindow, R - i);
         for (int t = threadIdx.x; t <= (int)n; t += kFlatThreads) s_pos[t] = a.pos[i + t];
-        for (int t = threadIdx.x; t < (int)n; t += kFlatThreads) s_off[t] = a.off[i + t];
+        for (int t = threadIdx.x; t < (int)n; t += kFlatThreads) {
+            // the window's rows once: list offset, owner, and where its step puts the edge
+            s_off[t] = a.off[i + t];
+            const uint32_t q = level_owner(a, i + t);
+            s_q[t] = q;
+            const StepDesc* d = a.desc + q;
+            const uint32_t op = d->op;
+            s_ecol[t] = op == kXStart ? 0 : op == kXK2U ? (int32_t)d->cin : -1;
+        }
         __syncthreads();
         const uint64_t wend = min(j1, s_pos[n]);
         for (uint64_t jj = j + threadIdx.x; jj < wend; jj += kFlatThreads) {
@@ -467,17 +477,14 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
                 const int mid = (lo + hi) >> 1;
                 if (s_pos[mid] <= jj) lo = mid; else hi = mid;
             }
+            const int ecol = s_ecol[lo];
+            if (ecol < 0) continue;   // filters wrote their rows already
             const uint64_t r = i + lo;
-            const uint32_t q = level_owner(a, r);
-            const StepDesc* d = a.desc + q;
-            const uint32_t op = d->op;
-            if (op != kXK2U && op != kXStart) continue;   // filters wrote their rows already
-            const int ecol = op == kXStart ? 0 : d->cin;
             const uint32_t* src = a.in + r * (uint64_t)a.w_in;
             uint32_t* dst = a.out + jj * (uint64_t)wo;
             for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
             dst[ecol] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
-            a.owner_out[jj] = q;
+            a.owner_out[jj] = s_q[lo];
         }
         j = max(j, wend);
         i += n;

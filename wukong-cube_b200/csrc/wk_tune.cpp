@@ -4,17 +4,21 @@
 //
 // Knobs (wk_ctx_tune_set): lanes per probe group (2 / 4 / 8 lanes, i.e. 32 / 64 / 128 bytes
 // of a bucket staged per request) and the slice threshold (lists longer than it are written
-// block-per-row as slices by every CTA, shorter ones group-per-row by the CTA that probed them).
+// block-per-row as slices by every CTA, shorter ones group-per-row by the CTA that probed them),
+// and for batches the mask of levels that run as the flat passes instead of the tile launch
+// (chosen greedily level by level after the tile settings).
 // Constant-start queries are timed as one batch replayed from its CUDA graph (CUDA events on
 // the context stream); index-start queries step by step through wk_query_profile, so lanes are
 // chosen per (step kind, input columns).  Everything goes through the public entry points, so
 // the tuner holds no lock of its own between them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <vector>
 
+#include "wk_batch.h"
 #include "wk_ctx.h"
 
 namespace {
@@ -75,11 +79,14 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
     if (!ctx || (!queries && n) || iters < 1 || !out) return WK_E_BADARG;
     std::memset(out, 0, sizeof(*out));
     std::vector<wk_query> light, heavy;
+    int light_levels = 0;   // levels of the light batch
     for (uint32_t i = 0; i < n; ++i) {
         std::vector<wk::PlanStep> steps;
         wk::ColMap cm(queries[i].nvars);
         if (wk::resolve_plan(queries[i], ctx->cfg.max_cols, steps, cm) || steps.empty()) continue;
-        (steps[0].kind == wk::PlanStep::kIndex ? heavy : light).push_back(queries[i]);
+        const bool is_heavy = steps[0].kind == wk::PlanStep::kIndex;
+        (is_heavy ? heavy : light).push_back(queries[i]);
+        if (!is_heavy) light_levels = std::max(light_levels, std::min((int)steps.size(), wk::kMaxBatchLevels));
     }
     void* sp = nullptr;
     int rc = wk_ctx_stream(ctx, &sp);
@@ -102,12 +109,10 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
         double best = 0;
         if ((rc = time_batch(ctx, light, iters, s, ev, &best))) return rc;
         out->batch_ms_default = best;
-        int bl = out->batch_lanes, bs = out->batch_slice_rows, bf = 1;
-        // the flat passes first (lanes and slices do not apply to them), then every tile setting
-        if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, 1))) return rc;
-        if ((rc = time_batch(ctx, light, iters, s, ev, &best))) return rc;
-        ++out->candidates;
+        int bl = out->batch_lanes, bs = out->batch_slice_rows, bf = 0;
+        // every tile setting (all levels on the tile launch) ...
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, 0))) return rc;
+        best = 1e30;
         for (int l : kLanes)
             for (int sl : kSlices) {
                 if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_LANES, l))) return rc;
@@ -119,11 +124,21 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
                     best = ms;
                     bl = l;
                     bs = sl;
-                    bf = 0;
                 }
             }
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_LANES, bl))) return rc;
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_SLICE_ROWS, bs))) return rc;
+        // ... then, level by level, the flat passes where they are faster (greedy)
+        for (int k = 0; k < light_levels; ++k) {
+            if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, bf | (1 << k)))) return rc;
+            double ms = 0;
+            if ((rc = time_batch(ctx, light, iters, s, ev, &ms))) return rc;
+            ++out->candidates;
+            if (ms < best) {
+                best = ms;
+                bf |= 1 << k;
+            }
+        }
         if ((rc = wk_ctx_tune_set(ctx, WK_KNOB_BATCH_FLAT, bf))) return rc;
         out->batch_lanes = bl;
         out->batch_slice_rows = bs;
