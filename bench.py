@@ -246,6 +246,19 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
             "sustained_vs_plain": (best["light_offered_qps"] / plain_qps) if best else None}
 
 
+def distinct_probe_keys(ctx, q, k):
+    """Distinct keys step k of query q probes: 1 for the start (one index or constant key),
+    else the distinct values of the step's known subject column in the table of the first k
+    patterns (run on the device; its tables match the oracle's)."""
+    import wukong_b200 as wk
+    if k == 0:
+        return 1
+    s = q.patterns[k][0]
+    prefix = wk.Query(q.patterns[:k], nvars=q.nvars)
+    table, v2c = ctx.execute(prefix, wk.MODE_RESIDENT)
+    return int(np.unique(table[:, v2c[-s - 1]]).size)
+
+
 def run_ours(args, world, rank, local_rank):
     import torch
 
@@ -393,6 +406,32 @@ def run_ours(args, world, rank, local_rank):
     hsteps = [s for h in heavy.values() for s in h["profile"]]
     hdom = max(hsteps, key=lambda s: s["ms"])
     hach = hdom["alg_bytes"] / (hdom["ms"] / 1000.0) / 1e9
+    # the random-read ceiling of this GPU, measured here: a probe is a random 16-byte read, and
+    # on this part each one moves a whole 128-byte line from DRAM, so the copy bandwidth
+    # overstates what probes can reach
+    rr_peak = ctx.measure_random_reads(8 << 30, iters=5)
+
+    def bound_s(s):
+        # a lower bound on a step's time: one random read per distinct probed key (its bucket
+        # must come from DRAM at least once; the store is far larger than L2) at the measured
+        # random-read rate, or its algorithmic bytes at the copy bandwidth, whichever is longer
+        return max(s["distinct_keys"] / rr_peak, s["alg_bytes"] / (peak * 1e9))
+
+    def random_roofline(s):
+        return {"bound": "one random read per distinct probed key at the measured random-read "
+                         "rate, or the algorithmic bytes at the copy bandwidth, whichever is longer",
+                "distinct_keys": s["distinct_keys"], "peak_reads_per_s": rr_peak,
+                "peak_bytes_per_s": peak * 1e9, "bound_ms": bound_s(s) * 1000.0,
+                "kernel_ms": s["ms"], "frac": bound_s(s) / (s["ms"] / 1000.0)}
+    for q, h in zip(hq, heavy.values()):
+        for k, s in enumerate(h["profile"]):
+            s["distinct_keys"] = distinct_probe_keys(ctx, q, k)
+        h["bound_ms"] = sum(bound_s(s) for s in h["profile"]) * 1000.0
+        h["frac_of_bound"] = h["bound_ms"] / sum(s["ms"] for s in h["profile"])
+    flat_mask = tune.get("batch_flat", 0)
+    dom_k = levels.index(dom)
+    dom_kernel = ("flat passes (batch level %d)" if (flat_mask >> dom_k) & 1
+                  else "explore_kernel (batch level %d)") % dom_k
 
     lat = sorted(step_ms)
     line = {"metric": METRIC, "value": value, "unit": "light queries/s", "n_gpus": world,
@@ -419,13 +458,21 @@ def run_ours(args, world, rank, local_rank):
                                            "this level in a replay of the same batch (1 pass; "
                                            "48.0 B per input row) x this launch's input rows",
                          "peak_source": src,
-                         "kernel": "explore_kernel (batch level %d)" % levels.index(dom),
-                         "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"]},
+                         "kernel": dom_kernel,
+                         "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
+                         "probe_rate": {"probes_per_s": dom["rows_in"] / (dom["ms"] / 1000.0),
+                                        "frac_of_random_read_peak":
+                                            dom["rows_in"] / (dom["ms"] / 1000.0) / rr_peak,
+                                        "note": "one probe per input row"}},
             "roofline_heavy": {"bound": "hbm", "achieved": hach, "peak": peak, "unit": "GB/s",
                                "frac": hach / peak, "traffic": None,
                                "kernel": "single-query " + hdom["kind"] + " step (tile launch or "
                                          "flat pipeline, whichever the device picked)",
-                               "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"]},
+                               "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"],
+                               "random_reads": random_roofline(hdom)},
+            "random_read_peak": {"value": rr_peak, "unit": "reads/s",
+                                 "how": "wk_measure_random_reads: independent random 16-byte "
+                                        "reads from an 8 GiB device buffer, CUDA events"},
             "batch_levels": levels,
             "batch_other_ms": overheads,
             "autotune": tune,
@@ -448,7 +495,7 @@ def run_ours(args, world, rank, local_rank):
 
 
 def run_profile_case(args):
-    """A small, self-contained case for ncu: the heavy triangle query (resident mode) and one
+    """A small, self-contained case for ncu: one heavy query (`--heavy`, resident mode) and one
     light batch, each run `--steps` times after `--warmup` runs, no oracle, no timing.  The
     batch replays after the first sit in an NVTX range named "replay", so a capture can pick
     a level of a replay (ncu --nvtx --nvtx-include replay/) whatever reruns came before."""
@@ -460,7 +507,7 @@ def run_profile_case(args):
     with wk.Context(0) as ctx:
         ctx.upload_gstore(g)
         ctx.tune_set(wk.KNOB_BATCH_FLAT, args.batch_flat)
-        q = workloads.heavy_triangle(v)
+        q = workloads.heavy_star(v) if args.heavy == "star" else workloads.heavy_triangle(v)
         qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
         for _ in range(args.warmup + args.steps):
             ctx.execute(q, wk.MODE_RESIDENT)
@@ -482,6 +529,8 @@ def main():
                     help="run the small ncu case instead of the benchmark")
     ap.add_argument("--batch-flat", type=lambda x: int(x, 0), default=0,
                     help="profile case: mask of the batch levels run as the flat passes")
+    ap.add_argument("--heavy", default="triangle", choices=["triangle", "star"],
+                    help="profile case: the heavy query it runs")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)

@@ -179,7 +179,7 @@ void wk_free(void* p);
  * SegmentRDFGraph::init_gstore does (segment_rdf_dgraph.hpp:1182-1269) after the loader's
  * sort + dedup (base_loader.hpp:481-496).  pso and pos are the triples to insert in the OUT
  * and IN directions (normally the same array; n x 3 uint32 each).  load_factor is the mean
- * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.2). */
+ * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.1). */
 int wk_gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
                     double load_factor, wk_gstore** out);
 void wk_gstore_free(wk_gstore* g);
@@ -362,6 +362,13 @@ typedef struct wk_tune_result {
     int32_t reserved[2];
 } wk_tune_result;
 int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters, wk_tune_result* out);
+
+/* Calibration: the rate of independent random 16-byte reads from a fresh `region_bytes` device
+ * buffer (each costs one 32-byte DRAM sector once the region is well above L2), timed with CUDA
+ * events over `iters` launches on the context stream; the buffer is freed before returning.
+ * The copy bandwidth overstates what random probes and short list reads can reach; this is
+ * their ceiling.  region_bytes >= 1 MiB.  No reference counterpart. */
+int wk_measure_random_reads(wk_ctx* ctx, uint64_t region_bytes, int32_t iters, double* reads_per_s);
 
 /* ---------------------------------------------------------------- batching
  * Run n planned queries together: all queries advance one pattern per level inside one

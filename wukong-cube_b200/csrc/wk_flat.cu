@@ -39,9 +39,10 @@ __device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
 }
 
 // Probe one key by one thread: the home bucket's slots two at a time (one 32-byte sector),
-// then the chain through slot 7.  Returns the pointer word, 0 when absent.
+// then the chain through slot 7.  Returns the pointer word, 0 when absent.  `first` skips the
+// home bucket's slots a caller has already compared (0 or an even slot).
 __device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t key, uint64_t bucket,
-                                                 unsigned* err) {
+                                                 unsigned* err, int first = 0) {
     for (int hop = 0; hop < kMaxProbeIters; ++hop) {
         if (bucket >= st.n_buckets) {
             atomicOr(err, kErrCorrupt);
@@ -50,6 +51,7 @@ __device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t ke
         const Slot* b = st.slots + bucket * kAssoc;
 #pragma unroll
         for (int s = 0; s < kAssoc - 1; s += 2) {
+            if (hop == 0 && s < first) continue;
             const ulonglong2 s0 = load_slot(b + s);   // both slots: one 32-byte sector
             const ulonglong2 s1 = load_slot(b + s + 1);
             if (s0.x == key) return s0.y;
@@ -115,20 +117,33 @@ __global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs
         uint32_t target = d.end_const;
         if (d.op == kXK2K) target = __ldg(row + d.ce);
         uint64_t key;
-        const SegDesc* sg = &d.seg;
+        SegDesc sg = d.seg;   // by value: registers, not a pointer into the parameter block
         bool valid = cur != kBlankId;
         if (d.op == kXK2U && d.type_index) {
             // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
             key = make_key(0, cur, kIn);
-            sg = &a.seg_index[kIn];
+            sg = a.seg_index[kIn];
             if (cur >= (1u << kNbitsIdx)) valid = false;
         } else {
             key = make_key(cur, d.pid, d.dir);
-            if (cur == 0) sg = &a.seg_index[d.dir & 1];   // vid 0 names the index
+            if (cur == 0) sg = a.seg_index[d.dir & 1];   // vid 0 names the index
         }
         uint64_t off = 0, deg = 0;
-        if (valid && sg->num_buckets != 0 && key != 0) {
-            const uint64_t p = thread_probe(a.store, key, bucket_of(key, *sg), &a.ctl->err);
+        if (valid && sg.num_buckets != 0 && key != 0) {
+            // the home bucket's first sector (slots 0 and 1, key and pointer) settles most keys;
+            // the rest walk on from slot 2
+            const uint64_t b = bucket_of(key, sg);
+            uint64_t p = 0;
+            if (b >= a.store.n_buckets) {
+                atomicOr(&a.ctl->err, kErrCorrupt);
+            } else {
+                const ulonglong2 s0 = load_slot(a.store.slots + b * kAssoc);
+                const ulonglong2 s1 = load_slot(a.store.slots + b * kAssoc + 1);
+                if (s0.x == key) p = s0.y;
+                else if (s0.x == 0) p = 0;
+                else if (s1.x == key) p = s1.y;
+                else if (s1.x != 0) p = thread_probe(a.store, key, b, &a.ctl->err, 2);
+            }
             off = ptr_off(p);
             deg = ptr_size(p);
             if (off + deg > a.store.n_edges) {
@@ -147,14 +162,14 @@ __global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs
             ++nvalid;
         }
     }
-    const uint64_t total = block_sum(sum, s_warp);
-    const uint64_t tsd = block_sum(sd, s_warp);
-    const uint64_t tvalid = block_sum(nvalid, s_warp);
+    sum = block_sum(sum, s_warp);
+    sd = block_sum(sd, s_warp);
+    nvalid = block_sum(nvalid, s_warp);
     if (threadIdx.x == 0) {
-        a.part[blockIdx.x] = total;
-        if (tvalid) {
-            atomicAdd(&a.ctl->sum_deg, (unsigned long long)tsd);
-            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(tvalid * (d.cin * 4ull + 16) + tsd * 4));
+        a.part[blockIdx.x] = sum;
+        if (nvalid) {
+            atomicAdd(&a.ctl->sum_deg, (unsigned long long)sd);
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(nvalid * (d.cin * 4ull + 16) + sd * 4));
         }
     }
 }
@@ -345,14 +360,14 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const Fl
             alg += cin * 4ull + 16 + deg * 4 + (uint64_t)c * d->cout * 4;
         }
     }
-    const uint64_t total = block_sum(sum, s_warp);
-    const uint64_t tsd = block_sum(sd, s_warp);
-    const uint64_t talg = block_sum(alg, s_warp);
+    sum = block_sum(sum, s_warp);
+    sd = block_sum(sd, s_warp);
+    alg = block_sum(alg, s_warp);
     if (threadIdx.x == 0) {
-        a.part[blockIdx.x] = total;
-        if (talg) {
-            atomicAdd(&a.ctl->sum_deg, (unsigned long long)tsd);
-            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)talg);
+        a.part[blockIdx.x] = sum;
+        if (alg) {
+            atomicAdd(&a.ctl->sum_deg, (unsigned long long)sd);
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)alg);
         }
     }
 }

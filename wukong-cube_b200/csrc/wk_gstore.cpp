@@ -136,9 +136,10 @@ uint64_t buckets_for(uint64_t keys, double load) {
 
 int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
                  double load, wk_gstore& g) {
-    // Default: about 1.4 keys per bucket, so nearly every key sits in the bucket's first
-    // 32-byte sector (slots 0-1) and a probe is one request; HBM is plentiful, latency is not.
-    if (load <= 0) load = 0.2;
+    // Default: about 0.7 keys per bucket.  A key's slot is its insertion rank in the bucket, so
+    // at this fill about 94% of keys sit in the first 32-byte sector (slots 0-1) and their probe
+    // is one request (at 1.4 keys per bucket it was 83%); HBM is plentiful, latency is not.
+    if (load <= 0) load = 0.1;
     if (load > 1) return WK_E_BADARG;
     const size_t np = (size_t)1 << kNbitsIdx;
     DirLists outl, inl;

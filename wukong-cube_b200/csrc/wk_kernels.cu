@@ -74,7 +74,35 @@ __global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const u
     }
 }
 
+// Random-read calibration: every thread makes `per` independent 16-byte reads at pseudo-random
+// 16-byte-aligned positions of buf (the splitmix64 finaliser of thread and read index), eight in
+// flight at a time.  With buf much larger than L2 each read costs one 32-byte DRAM sector, the
+// unit the probes and short list reads of the exploration step pay.  The words read are summed
+// and stored only if the sum is one the fill cannot produce, which keeps the reads live.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__global__ void __launch_bounds__(256) random_read_kernel(const uint4* __restrict__ buf, uint64_t n16,
+                                                          int per, uint64_t seed, uint32_t* sink) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint32_t acc = 0;
+#pragma unroll 8
+    for (int i = 0; i < per; ++i) {
+        const uint4 v = __ldg(buf + mix64(seed + t * 0x9e3779b97f4a7c15ull + (uint64_t)i) % n16);
+        acc += v.x + v.y + v.z + v.w;
+    }
+    if (acc == 1u) sink[0] = acc;
+}
+
 }  // namespace
+
+cudaError_t launch_random_reads(const void* buf, uint64_t bytes, int per, uint64_t seed,
+                                uint32_t* sink, int grid, cudaStream_t s) {
+    random_read_kernel<<<grid, 256, 0, s>>>((const uint4*)buf, bytes / 16, per, seed, sink);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s) {
     if (grid < 1) grid = 1;

@@ -74,6 +74,40 @@ int time_singles(wk_ctx* ctx, const std::vector<wk_query>& qs, int iters,
 
 }  // namespace
 
+extern "C" int wk_measure_random_reads(wk_ctx* ctx, uint64_t region_bytes, int32_t iters,
+                                       double* reads_per_s) {
+    if (!ctx || !reads_per_s || iters < 1 || region_bytes < (1ull << 20)) return WK_E_BADARG;
+    constexpr int kPer = 32;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int grid = ctx->sm_count * 8;
+    void* buf = nullptr;
+    uint32_t* sink = nullptr;
+    Events ev;
+    auto done = [&](int rc) {
+        if (buf) cudaFree(buf);
+        if (sink) cudaFree(sink);
+        return rc;
+    };
+    if (cudaMalloc(&buf, region_bytes) != cudaSuccess || cudaMalloc(&sink, 4) != cudaSuccess) {
+        cudaGetLastError();
+        return done(ctx->fail(WK_E_OOM, "random-read calibration buffer"));
+    }
+    cudaError_t e = cudaMemsetAsync(buf, 1, region_bytes, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev.a);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev.b);
+    if (e == cudaSuccess) e = wk::launch_random_reads(buf, region_bytes, kPer, 0, sink, grid, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev.a, ctx->stream);
+    for (int i = 0; i < iters && e == cudaSuccess; ++i)
+        e = wk::launch_random_reads(buf, region_bytes, kPer, 1 + (uint64_t)i, sink, grid, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev.b, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev.b);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev.a, ev.b);
+    if (e != cudaSuccess) return done(ctx->cuda_fail(e, "random-read calibration"));
+    *reads_per_s = (double)grid * 256 * kPer * iters / (ms * 1e-3);
+    return done(WK_SUCCESS);
+}
+
 extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n, int32_t iters,
                                wk_tune_result* out) {
     if (!ctx || (!queries && n) || iters < 1 || !out) return WK_E_BADARG;

@@ -172,6 +172,7 @@ _SIGS = {
     "wk_ctx_tune_set": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "wk_ctx_tune_get": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32)]),
     "wk_ctx_autotune": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
+    "wk_measure_random_reads": (C.c_int, [_P, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
     "wk_batch_profile": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32,
                                    C.POINTER(StepProf), C.c_int32, C.POINTER(C.c_int32)]),
     "wk_serve_run_open_loop": (C.c_int, [_P, C.POINTER(ServeConfig), C.POINTER(QueryC),
@@ -414,6 +415,13 @@ class Context:
         r = TuneResult()
         _check(lib().wk_ctx_autotune(self.h, qs, len(queries), iters, C.byref(r)), self.h)
         return {k: getattr(r, k) for k, _ in TuneResult._fields_ if k != "reserved"}
+
+    def measure_random_reads(self, region_bytes=8 << 30, iters=5):
+        """Independent random 16-byte reads per second from a fresh device buffer of this size
+        (the ceiling of probes and short list reads)."""
+        v = C.c_double()
+        _check(lib().wk_measure_random_reads(self.h, region_bytes, iters, C.byref(v)), self.h)
+        return v.value
 
     def upload_gstore(self, g):
         _check(lib().wk_store_upload_gstore(self.h, g.h), self.h)
