@@ -176,7 +176,8 @@ int ensure_state(wk_ctx* ctx, BatchState* b, uint32_t n, int levels, uint64_t ro
     rows_cap = std::max(rows_cap, b->rows_cap);
     w = std::max(w, b->w_cap);
     result_cap = std::max(result_cap, b->result_cap);
-    WKB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // every stream, the pipelined path's copy stream too, may still read the old buffers
+    WKB_CUDA(ctx, cudaDeviceSynchronize());
     free_state(b);
     auto dm = [&](void** p, size_t bytes) {
         if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
@@ -593,8 +594,11 @@ extern "C" int wk_batch_execute_stream(wk_ctx* ctx, const wk_query* queries, uin
         const int k = i & 1;
         const uint32_t m = std::min(batch, n - start);
         if (pend[k] && finish(k)) break;
-        // the copy of the batch two back has left this state's buffers
-        if (cu(cudaEventSynchronize(copied[k]), "copy done")) break;
+        // resolve this batch while the device runs the previous one and copies out the one
+        // before it: the host staging of this state was last read by that earlier batch's
+        // upload, which its launch waited for; its device buffers are guarded on the device
+        // (the launch below waits for the copy), and a buffer that has to grow waits for the
+        // whole device first (ensure_state)
         if ((rc = build_plan(ctx, B[k], queries + start, m, P[k]))) break;
         off[k] = start;
         cnt[k] = m;

@@ -264,7 +264,10 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
         a.out_rows = out->d_rows;
         a.out_cap = out->cap;
         a.ctl = ctx->d_ctl;
-        int grid = grid_override > 0 ? grid_override : std::min(ctx->sm_count * 2, 512);
+        // index lists are long (every instance of a type, every subject of a predicate): a
+        // full-occupancy grid; a constant's list is usually short
+        int grid = st.kind == PlanStep::kIndex ? ctx->sm_count * 8 : std::min(ctx->sm_count * 2, 512);
+        if (grid_override > 0) grid = grid_override;
         cudaError_t e = launch_list(a, grid, s);
         if (e != cudaSuccess) return ctx->cuda_fail(e, "list kernel launch");
         return WK_SUCCESS;

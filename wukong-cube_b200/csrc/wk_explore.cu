@@ -379,7 +379,9 @@ __global__ void __launch_bounds__(kStepThreads, 6) explore_kernel(const ExploreA
 
     const unsigned epoch = *(volatile unsigned*)&a.ctl->epoch;
     uint64_t R = a.virtual_rows ? a.n_queries : *(volatile const uint64_t*)a.in_rows;
-    if (!a.virtual_rows && R > a.in_cap_rows) R = a.in_cap_rows;
+    // an input count past its capacity means the step before overflowed (and said so): its rows
+    // were never written, so this step does no work and reports no size of its own
+    if (!a.virtual_rows && R > a.in_cap_rows) R = 0;
     const bool handed_off = !a.virtual_rows && a.max_rows && R >= a.max_rows;   // flat pipeline's
     uint64_t ntiles = handed_off ? 0 : (R + kTileRows - 1) / kTileRows;
     if (ntiles > a.ctl->status_cap) {

@@ -35,7 +35,7 @@ constexpr int kWindow = 256;   // input rows staged per expand round
 
 __device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
     uint64_t R = *(volatile const uint64_t*)a.in_rows;
-    return R > a.in_cap_rows ? a.in_cap_rows : R;
+    return R > a.in_cap_rows ? 0 : R;   // past capacity: the step before overflowed
 }
 
 // Probe one key by one thread: the home bucket's slots two at a time (one 32-byte sector),
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArg
 __device__ __forceinline__ uint64_t level_rows(const FlatLevelArgs& a) {
     if (a.virtual_rows) return a.n_queries;
     uint64_t R = *(volatile const uint64_t*)a.in_rows;
-    return R > a.in_cap_rows ? a.in_cap_rows : R;
+    return R > a.in_cap_rows ? 0 : R;   // past capacity: the step before overflowed
 }
 
 __device__ __forceinline__ uint32_t level_owner(const FlatLevelArgs& a, uint64_t r) {

@@ -45,10 +45,19 @@ __global__ void list_kernel(const ListArgs a) {
         }
     }
     if (n > a.out_cap) return;
+    // grid-stride copy, eight loads in flight per thread before their stores (the list starts
+    // at any word, so the words are moved one by one; each warp access is 128 contiguous bytes)
     const uint32_t* srcp = a.store.edges + off + b;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        a.out[i] = __ldg(srcp + i);
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (; i + 7 * stride < n; i += 8 * stride) {
+        uint32_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldg(srcp + i + k * stride);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a.out[i + k * stride] = v[k];
+    }
+    for (; i < n; i += stride) a.out[i] = __ldg(srcp + i);
 }
 
 // Checks that every key's list is strictly ascending (the loader's sort + dedup), which lets
