@@ -42,9 +42,10 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
-# 16,384-query batch on the 10,000-organisation graph: 109.96 MB + 12.99 MB for 2,560,041 input
-# rows (the same level as the bench's dominant launch; the capture ran the default knobs).
-LEVEL_TRAFFIC_PER_ROW = (109.96e6 + 12.99e6) / 2560041
+# 16,384-query batch on the 10,000-organisation graph: 110,006,272 B + 10,037,248 B for
+# 2,560,041 input rows, with the knobs the autotuner picks here (2 lanes, 32-row slices, flat
+# passes for levels 0 and 1).
+LEVEL_TRAFFIC_PER_ROW = (110006272 + 10037248) / 2560041
 
 
 def peaks():
@@ -456,7 +457,7 @@ def run_ours(args, world, rank, local_rank):
                          "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "this level in a replay of the same batch (1 pass; "
-                                           "48.0 B per input row) x this launch's input rows",
+                                           "46.9 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": dom_kernel,
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
@@ -507,6 +508,10 @@ def run_profile_case(args):
     with wk.Context(0) as ctx:
         ctx.upload_gstore(g)
         ctx.tune_set(wk.KNOB_BATCH_FLAT, args.batch_flat)
+        if args.batch_lanes:
+            ctx.tune_set(wk.KNOB_BATCH_LANES, args.batch_lanes)
+        if args.batch_slice_rows:
+            ctx.tune_set(wk.KNOB_BATCH_SLICE_ROWS, args.batch_slice_rows)
         q = workloads.heavy_star(v) if args.heavy == "star" else workloads.heavy_triangle(v)
         qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
         for _ in range(args.warmup + args.steps):
@@ -529,6 +534,10 @@ def main():
                     help="run the small ncu case instead of the benchmark")
     ap.add_argument("--batch-flat", type=lambda x: int(x, 0), default=0,
                     help="profile case: mask of the batch levels run as the flat passes")
+    ap.add_argument("--batch-lanes", type=int, default=0,
+                    help="profile case: lanes per probe group of the batch levels (0: default)")
+    ap.add_argument("--batch-slice-rows", type=int, default=0,
+                    help="profile case: slice threshold of the batch levels (0: default)")
     ap.add_argument("--heavy", default="triangle", choices=["triangle", "star"],
                     help="profile case: the heavy query it runs")
     ap.add_argument("--gpus", type=int, default=1)
