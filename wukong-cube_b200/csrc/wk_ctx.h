@@ -113,6 +113,7 @@ struct wk_ctx {
     // batch / serving state (wk_batch.cu); batch2 is the second state of the pipelined path
     void* batch = nullptr;
     void* batch2 = nullptr;
+    void* batch_host = nullptr;   // plans, streams and events reused by every batch call
     // serving lanes, kept between serving runs so their tables stay grown (wk_serve.cu)
     std::vector<wk_ctx*> lanes;
     wk::CtaUse lanes_use{0, 0, 0};
