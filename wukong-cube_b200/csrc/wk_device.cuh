@@ -396,9 +396,12 @@ constexpr int kGatherSpan = 1024;   // output elements per warp segment
 
 // Each warp copies contiguous segments of kGatherSpan elements, lane i taking elements i,
 // i + 32, ...: it finds the segment's first table once (binary search), then every lane walks
-// forward through the tables it crosses, so the per-element work is a compare, a division by
-// the table's width and the copy.  Stores are coalesced; one long table is spread over many
-// warps.
+// forward through the tables it crosses.  A lane keeps its element's (row, column) in its
+// table and steps it by 32 elements with a carry, so the only division is at a table change.
+// Eight elements' source addresses are worked out first, then their eight loads are issued
+// together, then the stores (coalesced).  One long table is spread over many warps.
+constexpr int kGatherUnroll = 8;
+
 template <class Src>
 __device__ void segmented_gather(uint32_t n, const uint64_t* __restrict__ off, Src src,
                                  uint32_t* __restrict__ out) {
@@ -417,29 +420,49 @@ __device__ void segmented_gather(uint32_t n, const uint64_t* __restrict__ off, S
         uint32_t q = lo;
         uint64_t q_lo = __ldg(off + q), q_hi = __ldg(off + q + 1);
         const uint32_t* row0 = nullptr;
-        uint32_t stride = 1, cols = 1;
-        bool have = false;
-        for (uint64_t p = base + lane; p < end; p += 32) {
-            while (p >= q_hi) {   // tables are back to back: step to the one holding p
-                ++q;
-                q_lo = q_hi;
-                q_hi = __ldg(off + q + 1);
-                have = false;
+        uint32_t stride = 1, cols = 1, step_r = 0, step_c = 0;
+        uint64_t r = 0;
+        uint32_t c = 0;
+        bool placed = false;   // (r, c) hold the position of the lane's current element
+        for (uint64_t p0 = base + lane; p0 < end; p0 += 32 * kGatherUnroll) {
+            const uint32_t* a[kGatherUnroll];
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u) {
+                const uint64_t p = p0 + 32ull * u;
+                a[u] = nullptr;
+                if (p >= end) continue;
+                if (p >= q_hi) {   // tables are back to back: step to the one holding p
+                    do {
+                        ++q;
+                        q_lo = q_hi;
+                        q_hi = __ldg(off + q + 1);
+                    } while (p >= q_hi);
+                    placed = false;
+                }
+                if (!placed) {
+                    src(q, row0, stride, cols);
+                    const uint64_t e = p - q_lo;
+                    r = e / cols;
+                    c = (uint32_t)(e - r * cols);
+                    step_r = 32 / cols;
+                    step_c = 32 % cols;
+                    placed = true;
+                } else {
+                    r += step_r;
+                    c += step_c;
+                    if (c >= cols) {
+                        c -= cols;
+                        ++r;
+                    }
+                }
+                a[u] = row0 + r * stride + c;
             }
-            if (!have) {
-                src(q, row0, stride, cols);
-                have = true;
-            }
-            const uint64_t e = p - q_lo;
-            uint64_t r, c;
-            if (e < (1ull << 32)) {
-                r = (uint32_t)e / cols;
-                c = (uint32_t)e - (uint32_t)r * cols;
-            } else {
-                r = e / cols;
-                c = e - r * cols;
-            }
-            out[p] = __ldg(row0 + r * stride + c);
+            uint32_t v[kGatherUnroll];
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u) v[u] = a[u] ? __ldg(a[u]) : 0u;
+#pragma unroll
+            for (int u = 0; u < kGatherUnroll; ++u)
+                if (a[u]) out[p0 + 32ull * u] = v[u];
         }
     }
 }
