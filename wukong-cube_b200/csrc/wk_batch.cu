@@ -46,11 +46,22 @@ __global__ void __launch_bounds__(kScanThreads) result_scan_kernel(const ResultS
     __shared__ uint64_t s_warp[kScanThreads / 32];
     const uint32_t n = a.n;
     const uint32_t t0 = blockIdx.x * kScanThreads;
+    // eight queries per thread at a time: their step counts, then their row counts and widths,
+    // are loaded together (one dependent round trip per eight queries, not per query)
     uint64_t before = 0;
-    for (uint32_t q = threadIdx.x; q < t0; q += kScanThreads) {
-        int lev;
-        uint64_t rows, base;
-        before += final_elems(a, q, &lev, &rows, &base);
+    constexpr int kU = 8;
+    for (uint32_t q0 = threadIdx.x; q0 < t0; q0 += kU * kScanThreads) {
+        int lev[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t q = q0 + u * kScanThreads;
+            lev[u] = q < t0 ? (int)a.nsteps[q] - 1 : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const uint32_t q = q0 + u * kScanThreads;
+            if (lev[u] >= 0) before += a.qcount[(size_t)lev[u] * a.n + q] * a.final_cols[q];
+        }
     }
     // block total of `before` (the inclusive sum of the last thread)
     const uint64_t bex = dev::block_exclusive_sum<kScanThreads>(before, s_warp);
