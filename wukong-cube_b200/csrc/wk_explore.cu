@@ -122,8 +122,8 @@ __device__ __forceinline__ TileBuf tile_buf(uint32_t* base, int wi) {
 // aggregate.  Nothing here waits on another CTA.
 template <int L>
 __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& B, TileState& S,
-                                           uint64_t* bar, uint64_t tile, uint64_t R, int wi,
-                                           unsigned epoch, uint64_t* s_warp) {
+                                           uint64_t* bar, unsigned phase, uint64_t tile, uint64_t R,
+                                           int wi, unsigned epoch, uint64_t* s_warp) {
     constexpr int kGroups = kStepThreads / L;
     constexpr int kBatches = kTileRows / (kGroups * kUnroll);
     static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
@@ -150,6 +150,8 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         B.cnt[i] = 0;
     }
     __syncthreads();
+    // the rows' copy ran alongside the owner loads; read the rows from shared memory
+    if (wi) mbar_wait(bar, phase, &a.ctl->err);
 #pragma unroll 1
     for (int b = 0; b < kBatches; ++b) {
         uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
@@ -168,9 +170,9 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
             if (op[u] == kXStart) {
                 key[u] = d->start_key;
             } else {
-                const uint32_t* rin = src + (uint64_t)row[u] * wi;
-                const uint32_t cur = valid[u] ? __ldg(rin + d->cs) : kBlankId;
-                if (op[u] == kXK2K && valid[u]) target[u] = __ldg(rin + d->ce);
+                const uint32_t* rin = B.in + row[u] * wi;   // shared memory: plain loads
+                const uint32_t cur = valid[u] ? rin[d->cs] : kBlankId;
+                if (op[u] == kXK2K && valid[u]) target[u] = rin[d->ce];
                 if (op[u] == kXK2U && d->type_index) {
                     // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
                     key[u] = make_key(0, cur, kIn);
@@ -408,15 +410,16 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     uint64_t cur = s_claim;
     int b = 0;
     WK_PH(0);
-    if (cur < ntiles) tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], cur, R, wi, epoch, s_warp);
+    if (cur < ntiles)
+        tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], phases & 1u, cur, R, wi, epoch, s_warp);
     while (cur < ntiles) {
         if (threadIdx.x == 0) s_claim = atomicAdd(&a.ctl->tile_counter, 1ull);
         __syncthreads();
         const uint64_t next = s_claim;
         WK_PH(0);
         if (next < ntiles)
-            tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1], next, R,
-                          wi, epoch, s_warp);
+            tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1],
+                          (phases >> (b ^ 1)) & 1u, next, R, wi, epoch, s_warp);
         tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
                      wo, chunk_rows, epoch, s_pos, s_out, &s_excl, obase);
         if (wi) phases ^= 1u << b;
