@@ -560,7 +560,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-rates", type=lambda s: [int(x) for x in s.split(",")],
-                    default=[1000, 10000, 50000, 100000, 200000, 500000])
+                    default=[1000, 10000, 50000, 100000, 125000, 150000, 175000, 200000, 500000])
     ap.add_argument("--serve-seconds", type=float, default=0.25,
                     help="arrival span of each serving rate")
     args = ap.parse_args()
