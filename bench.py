@@ -42,10 +42,10 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
-# 16,384-query batch on the 10,000-organisation graph: 110,006,272 B + 10,037,248 B for
+# 16,384-query batch on the 10,000-organisation graph: 110,025,216 B + 9,299,456 B for
 # 2,560,041 input rows, with the knobs the autotuner picks here (2 lanes, 32-row slices, flat
 # passes for levels 0 and 1).
-LEVEL_TRAFFIC_PER_ROW = (110006272 + 10037248) / 2560041
+LEVEL_TRAFFIC_PER_ROW = (110025216 + 9299456) / 2560041
 
 
 def peaks():
@@ -461,7 +461,7 @@ def run_ours(args, world, rank, local_rank):
                          "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "this level in a replay of the same batch (1 pass; "
-                                           "46.9 B per input row) x this launch's input rows",
+                                           "46.6 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": dom_kernel,
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
