@@ -32,6 +32,11 @@ using namespace dev;
 
 constexpr int kFlatThreads = 256;
 constexpr int kWindow = 256;   // input rows staged per expand round
+// part[] flag bit set by a count CTA whose rows do not each have exactly one output row; the
+// scan clears it from the totals and leaves part[nparts + 1] = 1 when every row has one
+// (known_to_unknown on a functional predicate: output row r is then input row r, and the
+// place pass and the expand search are skipped).  part has 256 spare bytes past nparts.
+constexpr uint64_t kNotOneToOne = 1ull << 63;
 
 __device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
     uint64_t R = *(volatile const uint64_t*)a.in_rows;
@@ -111,6 +116,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs
     const StepDesc& d = a.step;
     const bool filt = d.op == kXK2K || d.op == kXK2C;
     uint64_t sum = 0, sd = 0, nvalid = 0;
+    bool ones = true;   // every row of this thread has exactly one output row
     for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
         const uint32_t* row = a.in + r * (uint64_t)a.w_in;
         const uint32_t cur = __ldg(row + d.cs);
@@ -155,6 +161,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs
         if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
         if (!valid) c = 0;
         a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
+        if (c != 1) ones = false;
         if (!filt) a.off[r] = off;
         sum += c;
         if (valid) {
@@ -162,11 +169,12 @@ __global__ void __launch_bounds__(kFlatThreads) flat_count_kernel(const FlatArgs
             ++nvalid;
         }
     }
+    const bool all_ones = __syncthreads_and(ones);
     sum = block_sum(sum, s_warp);
     sd = block_sum(sd, s_warp);
     nvalid = block_sum(nvalid, s_warp);
     if (threadIdx.x == 0) {
-        a.part[blockIdx.x] = sum;
+        a.part[blockIdx.x] = sum | (all_ones ? 0 : kNotOneToOne);
         if (nvalid) {
             atomicAdd(&a.ctl->sum_deg, (unsigned long long)sd);
             atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(nvalid * (d.cin * 4ull + 16) + sd * 4));
@@ -180,9 +188,12 @@ __global__ void __launch_bounds__(1024) flat_scan_kernel(const FlatArgs a, uint3
     const uint64_t R = flat_rows(a);
     if (R < a.min_rows) return;
     if (threadIdx.x == 0) s_carry = 0;
+    bool not_ones = false;
     for (uint32_t r0 = 0; r0 < nparts; r0 += 1024) {
         const uint32_t i = r0 + threadIdx.x;
-        const uint64_t x = i < nparts ? a.part[i] : 0;
+        const uint64_t pv = i < nparts ? a.part[i] : 0;
+        not_ones |= (pv & kNotOneToOne) != 0;
+        const uint64_t x = pv & ~kNotOneToOne;
         const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
         const uint64_t carry = s_carry;
         if (i < nparts) a.part[i] = carry + ex;
@@ -190,9 +201,11 @@ __global__ void __launch_bounds__(1024) flat_scan_kernel(const FlatArgs a, uint3
         if (threadIdx.x == 1023) s_carry = carry + ex + x;
         __syncthreads();
     }
+    const bool one_to_one = !__syncthreads_or(not_ones);
     if (threadIdx.x == 0) {
         const uint64_t total = s_carry;
         a.part[nparts] = total;
+        a.part[nparts + 1] = one_to_one ? 1 : 0;
         a.pos[R] = total;
         if (total > a.out_cap_rows) {
             atomicOr(&a.ctl->err, kErrOverflow);
@@ -213,6 +226,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
     const bool filt = a.step.op == kXK2K || a.step.op == kXK2C;
+    if (!filt && a.part[nparts + 1] == 1) return;   // one output row per input row, in order
     if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
     __syncthreads();
     for (uint64_t r0 = lo; r0 < hi; r0 += kFlatThreads) {
@@ -235,7 +249,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs
     }
 }
 
-__global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArgs a) {
+__global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArgs a, uint32_t nparts) {
     __shared__ uint64_t s_pos[kWindow + 1];
     __shared__ uint64_t s_off[kWindow];
     __shared__ uint64_t s_i0;
@@ -243,6 +257,17 @@ __global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArg
     if (R < a.min_rows) return;
     const uint64_t total = a.pos[R];
     if (total > a.out_cap_rows || total == 0) return;
+    if (a.part[nparts + 1] == 1) {   // one output row per input row: row r is the output's row r
+        const int wo = a.w_out, ecol = a.step.cin;
+        for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < R;
+             r += (uint64_t)gridDim.x * blockDim.x) {
+            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+            uint32_t* dst = a.out + r * (uint64_t)wo;
+            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
+            dst[ecol] = __ldg(a.store.edges + a.off[r]);
+        }
+        return;
+    }
     const uint64_t per = (total + gridDim.x - 1) / gridDim.x;
     const uint64_t j0 = min(total, (uint64_t)blockIdx.x * per), j1 = min(total, j0 + per);
     if (j0 >= j1) return;
@@ -515,7 +540,7 @@ cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
     flat_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);
     flat_scan_kernel<<<1, 1024, 0, s>>>(a, (uint32_t)grid);
     flat_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
-    if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a);
+    if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     return cudaGetLastError();
 }
 
