@@ -12,10 +12,13 @@
 //   2. scan: one CTA scans the chunk totals, checks the output capacity (overflow sets
 //      kErrOverflow and the rows needed, as the tile launch does) and sets the row count;
 //   3. place: each CTA scans its chunk into per-row output positions; filters copy their
-//      surviving rows straight to the output here;
+//      surviving rows straight to the output here (a chunk without survivors returns at once);
 //   4. expand (known_to_unknown only): the output rows are split evenly over the CTAs; each CTA
 //      finds its first input row by a 32-way search of the positions and writes its rows in
 //      row-major then edge order (sparql.hpp:328-370), consecutive threads on consecutive rows.
+// When every input row of a known_to_unknown step has exactly one output row (a functional
+// predicate such as memberOf), output row r is input row r: place returns at once and expand
+// copies row by row without positions.
 // Row counts are read on the device, so the launches chain without a host round trip and can
 // be captured in a graph.  Every launch returns at once unless the input has at least
 // `min_rows` rows; the tile launch of the same step is given the complementary bound, so
@@ -227,6 +230,9 @@ __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs
     chunk_of(R, &lo, &hi);
     const bool filt = a.step.op == kXK2K || a.step.op == kXK2C;
     if (!filt && a.part[nparts + 1] == 1) return;   // one output row per input row, in order
+    // a filter's chunk without survivors has nothing to copy (part holds the exclusive scan of
+    // the chunk totals, part[nparts] the total)
+    if (filt && a.part[blockIdx.x + 1] == a.part[blockIdx.x]) return;
     if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
     __syncthreads();
     for (uint64_t r0 = lo; r0 < hi; r0 += kFlatThreads) {
