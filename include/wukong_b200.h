@@ -195,6 +195,28 @@ int wk_gstore_get_triples(const wk_gstore* g, uint32_t vid, uint32_t pid, int32_
 int wk_gstore_get_index(const wk_gstore* g, uint32_t tpid, int32_t dir, const uint32_t** edges,
                         uint64_t* sz);
 
+/* ---------------------------------------------------------------- datasets and plans */
+
+/* Read an ID-format dataset directory as the POSIX loader does (posix_loader.hpp:49-70,
+ * base_loader.hpp:235-280, 548): every entry whose name starts with "id_" (dot entries
+ * skipped), in sorted path order, each read as whitespace-separated decimal "s p o" triples up
+ * to the first token that is not a number in [0, 2^32).  *triples (n x 3 uint32) is allocated
+ * by the library and released with wk_free; pass it to wk_gstore_build, which sorts and
+ * dedups.  Attribute files ("attr_") are not read.  WK_E_BADARG if the directory or a file
+ * cannot be opened. */
+int wk_load_id_dir(const char* dir, uint32_t** triples, uint64_t* n_triples);
+
+/* Apply a user-defined plan (.fmt text) to a pattern group in written order, as
+ * Planner::set_plan and set_direction do (planner.hpp:667-699, 723-770): each line "k dir"
+ * takes pattern k (1-based) in that position; dir ">" keeps it (OUT), "<" swaps subject and
+ * object (IN), ">>" and "<<" turn it into a predicate-index pattern (OUT / IN).  A line
+ * without a direction keeps the previous one (initially ">"); "#" lines, blank lines and "{"
+ * are skipped, "}" ends the group.  WK_E_BADARG when fewer lines than patterns or a line names
+ * no pattern, WK_E_UNSUPPORTED for union / optional groups, WK_E_CAPACITY when out_cap is too
+ * small.  *n_out = the number of planned patterns. */
+int wk_plan_apply_fmt(const wk_pattern* patterns, int32_t n_patterns, const char* fmt_text,
+                      wk_pattern* out, int32_t out_cap, int32_t* n_out);
+
 /* ---------------------------------------------------------------- device context */
 int wk_ctx_create(const wk_config* cfg, wk_ctx** out);
 int wk_ctx_destroy(wk_ctx* ctx);

@@ -142,3 +142,77 @@ def sorted_rows(t):
         return np.zeros((0, 0 if t is None else t.shape[1]), np.uint32)
     idx = np.lexsort(t.T[::-1])
     return t[idx]
+
+
+# ---------------------------------------------------------------- dataset and plan readers
+# Plain-Python restatements of the reference's ID-format reader and .fmt plan reader, the
+# checkers of wk_load_id_dir and wk_plan_apply_fmt.
+
+def read_id_dir(path):
+    """Triples of a dataset directory as the reference's POSIX loader reads them: entries whose
+    name starts with "id_" (dot entries skipped; posix_loader.hpp:49-70, base_loader.hpp:548),
+    in sorted path order (base_loader.hpp:236), each file read as "s p o" triples until an
+    extraction fails (base_loader.hpp:242-247): a token that is not a number in [0, 2^32) ends
+    the file, and an incomplete last triple is dropped.  Returns an (n, 3) uint32 array."""
+    src = path if path.endswith("/") else path + "/"
+    names = sorted(src + e for e in os.listdir(src) if not e.startswith(".") and e.startswith("id_"))
+    out = []
+    for name in names:
+        with open(name, "rb") as f:
+            toks = f.read().split()
+        vals = []
+        for t in toks:
+            if not t.isdigit() or len(t) > 10 or int(t) > 0xFFFFFFFF:
+                break
+            vals.append(int(t))
+        out.extend(vals[:len(vals) - len(vals) % 3])
+    return np.array(out, dtype=np.uint32).reshape(-1, 3)
+
+
+def apply_fmt(written, text, predicate_id=0, in_dir=0, out_dir=1):
+    """Planned patterns [(s, p, d, o), ...] from written ones [(s, p, o), ...] and a .fmt text,
+    as Planner::set_plan (planner.hpp:723-770) reads it and set_direction
+    (planner.hpp:667-699) applies it.  Returns None where set_plan returns false (fewer lines
+    than patterns), raises ValueError where the reference would index out of range and
+    NotImplementedError for union / optional groups."""
+    orders, dirs = [], []
+    order, d = 0, ">"
+    for raw in text.split("\n"):
+        line = raw.strip()
+        if not line or line.startswith("#") or line == "{":
+            continue
+        if line == "}":
+            break
+        if line.lower().startswith("union") or line.lower().startswith("optional"):
+            raise NotImplementedError("nested group")
+        parts = line.split()
+        head = parts[0]
+        i = 1 if head[:1] in "+-" else 0
+        j = i
+        while j < len(head) and head[j].isdigit():
+            j += 1
+        if j == i:
+            order = 0                         # failed extraction stores 0; dir is untouched
+        else:
+            order = int(head[:j])
+            rest = head[j:] if j < len(head) else (parts[1] if len(parts) > 1 else "")
+            if rest:
+                d = rest
+        orders.append(order)
+        dirs.append(d)
+    if len(orders) < len(written):
+        return None
+    planned = []
+    for k, dd in zip(orders, dirs):
+        if k < 1 or k > len(written):
+            raise ValueError("line names no pattern")
+        s, p, o = written[k - 1]
+        direction = out_dir
+        if dd == "<":
+            direction, s, o = in_dir, o, s
+        elif dd == "<<":
+            direction, s, p, o = in_dir, p, predicate_id, s
+        elif dd == ">>":
+            direction, s, p = out_dir, p, predicate_id
+        planned.append((s, p, direction, o))
+    return planned

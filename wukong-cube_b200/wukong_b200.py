@@ -120,6 +120,9 @@ _SIGS = {
     "wk_synth_generate": (C.c_int, [C.POINTER(SynthParams), C.POINTER(C.POINTER(C.c_uint32)),
                                     C.POINTER(C.c_uint64), C.POINTER(SynthVocab)]),
     "wk_free": (None, [_P]),
+    "wk_load_id_dir": (C.c_int, [C.c_char_p, C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]),
+    "wk_plan_apply_fmt": (C.c_int, [C.POINTER(Pattern), C.c_int32, C.c_char_p, C.POINTER(Pattern),
+                                    C.c_int32, C.POINTER(C.c_int32)]),
     "wk_gstore_build": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.c_double, C.POINTER(_P)]),
     "wk_gstore_free": (None, [_P]),
     "wk_gstore_info": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
@@ -229,6 +232,35 @@ def synth_generate(n_orgs, seed=0, zipf=False, zipf_s=1.1):
         L.wk_free(buf)
     vocab = {f: getattr(v, f) for f, _ in SynthVocab._fields_}
     return arr, vocab
+
+
+def load_id_dir(path):
+    """The triples of an ID-format dataset directory (its id_* files) as an (n, 3) uint32
+    array, read as the reference's POSIX loader reads them (wk_load_id_dir)."""
+    L = lib()
+    buf = C.POINTER(C.c_uint32)()
+    n = C.c_uint64()
+    _check(L.wk_load_id_dir(os.fsencode(path), C.byref(buf), C.byref(n)))
+    try:
+        arr = np.ctypeslib.as_array(buf, shape=(max(n.value, 1) * 3,))[:n.value * 3].copy()
+    finally:
+        L.wk_free(buf)
+    return arr.reshape(-1, 3)
+
+
+def plan_fmt(written, fmt_text, nvars=None):
+    """A Query from a pattern group in written order [(subject, predicate, object), ...] and a
+    user-defined plan (.fmt text), ordered and oriented as the reference's planner applies
+    such a file (wk_plan_apply_fmt)."""
+    src = (Pattern * max(len(written), 1))()
+    for i, (s, p, o) in enumerate(written):
+        src[i] = Pattern(int(s), int(p), int(o), OUT, 0)
+    cap = max(len(fmt_text.splitlines()), 1)
+    out = (Pattern * cap)()
+    n = C.c_int32()
+    _check(lib().wk_plan_apply_fmt(src, len(written), fmt_text.encode(), out, cap, C.byref(n)))
+    return Query([(out[i].subject, out[i].predicate, out[i].direction, out[i].object)
+                  for i in range(n.value)], nvars=nvars)
 
 
 class GStore:
