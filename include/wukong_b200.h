@@ -245,6 +245,16 @@ int wk_table_upload(wk_ctx* ctx, wk_table* t, const uint32_t* host, uint64_t row
 /* The final thrust::copy D2H (gpu_engine_cuda.hpp:189-193); cap_elems bounds the copy. */
 int wk_table_download(wk_ctx* ctx, const wk_table* t, uint32_t* host, uint64_t cap_elems);
 int wk_table_shape(wk_ctx* ctx, const wk_table* t, uint64_t* rows, int32_t* cols);
+/* The post-pattern stage on the device, as SPARQLEngine::final_process applies it without
+ * ORDER BY (sparql.hpp:1419-1546): with `distinct`, the rows sorted by all their columns
+ * (signed 32-bit order) and, of each run of neighbours equal on the required columns, the first
+ * kept; then `offset` rows dropped and at most `limit` kept (limit < 0: all); then the
+ * projection onto keep_cols, the required variables' columns in their order.  The result goes
+ * to `out` (grown as needed; not `in`).  An empty input comes back empty with its columns
+ * unchanged, as the reference leaves it; WK_NO_REQUIRED_VAR if n_keep == 0.  ORDER BY compares
+ * the ids' strings in the reference and is not offered. */
+int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int32_t* keep_cols, int32_t n_keep,
+                           int32_t distinct, int64_t offset, int64_t limit, wk_table* out);
 /* Device address of the table's first element (for callers that keep data on the GPU). */
 int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dptr);
 

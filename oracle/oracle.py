@@ -216,3 +216,27 @@ def apply_fmt(written, text, predicate_id=0, in_dir=0, out_dir=1):
             direction, s, p = out_dir, p, predicate_id
         planned.append((s, p, direction, o))
     return planned
+
+
+def final_process(table, keep_cols, distinct=False, offset=0, limit=-1):
+    """SPARQLEngine::final_process without ORDER BY (sparql.hpp:1419-1546) on a row-major
+    uint32 table: an empty table is returned unchanged; with DISTINCT the rows are sorted by all
+    columns as signed 32-bit values (ReduceCmp, sparql.hpp:1403-1417) and of each run of
+    neighbours equal on the required columns the first is kept; then OFFSET and LIMIT; then the
+    projection onto the required columns in their order."""
+    t = np.asarray(table, dtype=np.uint32)
+    if t.shape[0] == 0:
+        return t
+    rows = [tuple(int(x) for x in r) for r in t.view(np.int32)]
+    if distinct:
+        rows.sort()
+        kept = [rows[0]]
+        for r in rows[1:]:
+            if any(r[c] != kept[-1][c] for c in keep_cols):
+                kept.append(r)
+        rows = kept
+    rows = rows[offset:]
+    if limit >= 0:
+        rows = rows[:limit]
+    out = np.array([[r[c] for c in keep_cols] for r in rows], dtype=np.int32).reshape(-1, len(keep_cols))
+    return out.view(np.uint32)

@@ -1,0 +1,65 @@
+"""The post-pattern stage on the device (wk_table_final_process) against the restatement of the
+reference's final_process in oracle/: DISTINCT (sort by every column as signed 32-bit values,
+first of each run equal on the required columns), OFFSET, LIMIT and projection, row for row."""
+import numpy as np
+import pytest
+
+import oracle
+import workloads
+import wukong_b200 as wk
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(ctx, table, keep, distinct, offset, limit):
+    t = wk.Table(ctx, max(table.size, 1))
+    t.upload(table)
+    out = t.final_process(keep, distinct=distinct, offset=offset, limit=limit)
+    got = out.download()
+    t.free()
+    out.free()
+    return got
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_tables(ctx, seed):
+    rng = np.random.default_rng(seed)
+    rows = int(rng.choice([1, 2, 37, 1000, 20000, 70000]))
+    cols = int(rng.integers(1, 6))
+    # few distinct values per column, some of them past 2^31 (negative as the reference's ints)
+    pool = np.array([0, 1, 2, 7, 300, 65536, 2**31 - 1, 2**31, 2**31 + 5, 2**32 - 1], dtype=np.uint64)
+    table = pool[rng.integers(0, len(pool), size=(rows, cols))].astype(np.uint32)
+    for _ in range(4):
+        keep = [int(c) for c in rng.permutation(cols)[:int(rng.integers(1, cols + 1))]]
+        distinct = bool(rng.integers(0, 2))
+        offset = int(rng.choice([0, 0, 1, 5, rows // 2, rows + 3]))
+        limit = int(rng.choice([-1, -1, 0, 1, 10, rows]))
+        got = _run(ctx, table, keep, distinct, offset, limit)
+        want = oracle.final_process(table, keep, distinct, offset, limit)
+        assert got.shape == want.shape, (keep, distinct, offset, limit)
+        assert np.array_equal(got, want), (keep, distinct, offset, limit)
+
+
+def test_query_results(ctx, graph20):
+    v = graph20["vocab"]
+    for q in (workloads.heavy_star(v), workloads.heavy_triangle(v)):
+        table, v2c = ctx.execute(q, wk.MODE_RESIDENT)
+        keep = [v2c[1], v2c[0]]   # ?x2 then ?x1, as a SELECT would list them
+        for distinct, offset, limit in ((True, 0, -1), (True, 3, 50), (False, 7, 100), (False, 0, -1)):
+            got = _run(ctx, table, keep, distinct, offset, limit)
+            assert np.array_equal(got, oracle.final_process(table, keep, distinct, offset, limit))
+
+
+def test_empty_and_refusals(ctx):
+    empty = np.zeros((0, 3), dtype=np.uint32)
+    t = wk.Table(ctx, 8)
+    t.upload(empty)
+    out = t.final_process([1], distinct=True)
+    assert out.shape() == (0, 3)   # left as it is, columns included
+    out.free()
+    t.upload(np.arange(12, dtype=np.uint32).reshape(4, 3))
+    for keep, code in (([], wk.NO_REQUIRED_VAR), ([3], wk.E_BADARG), ([-1], wk.E_BADARG)):
+        with pytest.raises(wk.WukongError) as e:
+            t.final_process(keep)
+        assert e.value.code == code
+    t.free()

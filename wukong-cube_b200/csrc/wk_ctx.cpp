@@ -463,6 +463,7 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     if (e == cudaSuccess) e = wk::batch_kernel_attrs();
     if (e == cudaSuccess) e = wk::serve_kernel_attrs();
     if (e == cudaSuccess) e = wk::flat_kernel_attrs();
+    if (e == cudaSuccess) e = wk::final_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
     e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");

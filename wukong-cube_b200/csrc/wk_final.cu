@@ -1,0 +1,294 @@
+// Post-pattern stage on the device: DISTINCT, OFFSET, LIMIT and the projection onto the
+// required variables, as SPARQLEngine::final_process applies them (sparql.hpp:1419-1546), so a
+// query's table can be finished without leaving the GPU.  ORDER BY is not here: the reference
+// orders by the strings of the ids (sparql.hpp:1378-1400), which needs the string server.
+//
+// DISTINCT follows the reference step for step: the rows are sorted by all their columns,
+// compared as signed 32-bit values (ReduceCmp over an int table, sparql.hpp:1403-1417), then
+// of each run of neighbours equal on the required columns the first is kept.  The sort is an
+// LSD radix sort of row indices, one stable 8-bit counting pass per byte of every column from
+// the last column to the first; rows equal in every column are interchangeable, so the result
+// does not depend on how the reference's std::sort orders them.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "wk_ctx.h"
+#include "wk_device.cuh"
+
+namespace wk {
+namespace {
+using namespace dev;
+
+#define WKF_CUDA(ctx, call)                                        \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return (ctx)->cuda_fail(e_, #call); \
+    } while (0)
+
+constexpr int kFinThreads = 256;
+constexpr int kDigits = 256;
+
+struct SortPass {
+    const uint32_t* table;   // row-major, `cols` words per row
+    int cols, col, shift;
+    const uint32_t* idx_in;
+    uint32_t* idx_out;
+    uint32_t n;
+    uint32_t* hist;          // [kDigits][grid]: digit-major, so one scan gives the offsets
+};
+
+__device__ __forceinline__ uint32_t digit_of(const SortPass& a, uint32_t row) {
+    // signed order: flipping the sign bit makes the unsigned order the signed one
+    const uint32_t v = a.table[(uint64_t)row * a.cols + a.col] ^ 0x80000000u;
+    return (v >> a.shift) & 0xFFu;
+}
+
+__device__ __forceinline__ void chunk(uint32_t n, uint32_t* lo, uint32_t* hi) {
+    const uint32_t c = (n + gridDim.x - 1) / gridDim.x;
+    *lo = min(n, blockIdx.x * c);
+    *hi = min(n, *lo + c);
+}
+
+__global__ void __launch_bounds__(kFinThreads) iota_kernel(uint32_t* idx, uint32_t n) {
+    for (uint32_t i = blockIdx.x * kFinThreads + threadIdx.x; i < n; i += gridDim.x * kFinThreads) idx[i] = i;
+}
+
+__global__ void __launch_bounds__(kFinThreads) hist_kernel(const SortPass a) {
+    __shared__ uint32_t s_h[kDigits];
+    s_h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads) atomicAdd(&s_h[digit_of(a, a.idx_in[i])], 1u);
+    __syncthreads();
+    a.hist[threadIdx.x * gridDim.x + blockIdx.x] = s_h[threadIdx.x];
+}
+
+// Exclusive scan of n words in place by one CTA of 1,024 threads.
+__global__ void __launch_bounds__(1024) scan_kernel(uint32_t* v, uint32_t n, uint32_t* total) {
+    __shared__ uint64_t s_warp[32];
+    __shared__ uint64_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t r0 = 0; r0 < n; r0 += 1024) {
+        const uint32_t i = r0 + threadIdx.x;
+        const uint64_t x = i < n ? v[i] : 0;
+        const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < n) v[i] = (uint32_t)(carry + ex);
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry = carry + ex + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = (uint32_t)s_carry;
+}
+
+// Stable scatter: the CTA walks its chunk 256 elements at a time in order; an element's place
+// is its digit's running offset, plus the count of its digit in the warps before it, plus its
+// rank among the lanes of its warp with that digit.
+__global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) {
+    __shared__ uint32_t s_run[kDigits];
+    __shared__ uint32_t s_cnt[kFinThreads / 32][kDigits];
+    __shared__ uint32_t s_tile[kDigits];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    s_run[threadIdx.x] = a.hist[threadIdx.x * gridDim.x + blockIdx.x];
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    for (uint32_t base = lo; base < hi; base += kFinThreads) {
+        for (int w = 0; w < kFinThreads / 32; ++w) s_cnt[w][threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t i = base + threadIdx.x;
+        const bool live = i < hi;
+        const uint32_t row = live ? a.idx_in[i] : 0;
+        const uint32_t dg = live ? digit_of(a, row) : kDigits + lane;   // lone sentinel
+        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+        const int rank = __popc(peers & ((1u << lane) - 1));
+        if (live && rank == 0) s_cnt[warp][dg] = __popc(peers);
+        __syncthreads();
+        {   // per digit: exclusive prefix over the warps, and the tile's count
+            uint32_t acc = 0;
+            for (int w = 0; w < kFinThreads / 32; ++w) {
+                const uint32_t c = s_cnt[w][threadIdx.x];
+                s_cnt[w][threadIdx.x] = acc;
+                acc += c;
+            }
+            s_tile[threadIdx.x] = acc;
+        }
+        __syncthreads();
+        if (live) a.idx_out[s_run[dg] + s_cnt[warp][dg] + rank] = row;
+        __syncthreads();
+        s_run[threadIdx.x] += s_tile[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+struct UniqueArgs {
+    const uint32_t* table;
+    int cols;
+    const int32_t* keep;   // required columns
+    int n_keep;
+    const uint32_t* idx;   // sorted row indices
+    uint32_t n;
+    uint32_t* part;        // [grid + 1] kept rows per CTA, then their exclusive scan
+    uint32_t* out;         // kept row indices
+};
+
+__device__ __forceinline__ bool starts_run(const UniqueArgs& a, uint32_t i) {
+    if (i == 0) return true;
+    const uint32_t* r = a.table + (uint64_t)a.idx[i] * a.cols;
+    const uint32_t* p = a.table + (uint64_t)a.idx[i - 1] * a.cols;
+    for (int k = 0; k < a.n_keep; ++k)
+        if (r[a.keep[k]] != p[a.keep[k]]) return true;
+    return false;
+}
+
+__global__ void __launch_bounds__(kFinThreads) unique_count_kernel(const UniqueArgs a) {
+    __shared__ uint64_t s_warp[kFinThreads / 32];
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    uint64_t c = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads) c += starts_run(a, i);
+    const uint64_t ex = block_exclusive_sum<kFinThreads>(c, s_warp);
+    if (threadIdx.x == kFinThreads - 1) a.part[blockIdx.x] = (uint32_t)(ex + c);
+}
+
+__global__ void __launch_bounds__(kFinThreads) unique_place_kernel(const UniqueArgs a) {
+    __shared__ uint64_t s_warp[kFinThreads / 32];
+    __shared__ uint64_t s_carry;
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
+    __syncthreads();
+    for (uint32_t base = lo; base < hi; base += kFinThreads) {
+        const uint32_t i = base + threadIdx.x;
+        const uint64_t m = i < hi ? starts_run(a, i) : 0;
+        const uint64_t ex = block_exclusive_sum<kFinThreads>(m, s_warp);
+        const uint64_t carry = s_carry;
+        if (m) a.out[carry + ex] = a.idx[i];
+        __syncthreads();
+        if (threadIdx.x == kFinThreads - 1) s_carry = carry + ex + m;
+        __syncthreads();
+    }
+}
+
+// out row j = the required columns of input row idx[start + j] (idx null: row start + j).
+__global__ void __launch_bounds__(kFinThreads) project_kernel(const uint32_t* table, int cols,
+                                                              const int32_t* keep, int n_keep,
+                                                              const uint32_t* idx, uint64_t start,
+                                                              uint64_t count, uint32_t* out,
+                                                              uint64_t* out_rows) {
+    const uint64_t total = count * n_keep;
+    for (uint64_t e = blockIdx.x * (uint64_t)kFinThreads + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * kFinThreads) {
+        const uint64_t j = e / n_keep;
+        const int k = (int)(e - j * n_keep);
+        const uint64_t row = idx ? idx[start + j] : start + j;
+        out[e] = table[row * cols + keep[k]];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *out_rows = count;
+}
+
+}  // namespace
+
+cudaError_t final_kernel_attrs() {
+    cudaError_t e = use_max_shared_carveout(iota_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(hist_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(scan_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(scatter_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(unique_count_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(unique_place_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(project_kernel);
+    return e;
+}
+
+}  // namespace wk
+
+extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int32_t* keep_cols,
+                                      int32_t n_keep, int32_t distinct, int64_t offset, int64_t limit,
+                                      wk_table* out) {
+    using namespace wk;
+    if (!ctx || !in || !out || in == out || (!keep_cols && n_keep) || n_keep < 0 || offset < 0)
+        return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const int cols = in->cols;
+    cudaStream_t s = ctx->stream;
+    uint64_t R = 0;
+    WKF_CUDA(ctx, cudaMemcpyAsync(ctx->h_rows, in->d_rows, 8, cudaMemcpyDeviceToHost, s));
+    WKF_CUDA(ctx, cudaStreamSynchronize(s));
+    R = ctx->h_rows[0];
+    if (R == 0) {   // an empty table is left as it is, columns included (sparql.hpp:1420-1421)
+        int rc = ctx->table_reserve(out, 1);
+        if (rc) return rc;
+        out->cols = cols;
+        WKF_CUDA(ctx, cudaMemsetAsync(out->d_rows, 0, 8, s));
+        WKF_CUDA(ctx, cudaStreamSynchronize(s));
+        return WK_SUCCESS;
+    }
+    if (n_keep == 0) return ctx->fail(WK_NO_REQUIRED_VAR, "no required variable");
+    for (int k = 0; k < n_keep; ++k)
+        if (keep_cols[k] < 0 || keep_cols[k] >= cols) return ctx->fail(WK_E_BADARG, "required column out of range");
+    if (R >= (1ull << 32)) return ctx->fail(WK_E_CAPACITY, "table too long for the post-pattern stage");
+    const uint32_t n = (uint32_t)R;
+    const int grid = std::max(1, std::min<int>(ctx->sm_count * 4, (int)((n + 2047) / 2048)));
+    // scratch: the required columns, two index arrays, the digit histogram, the CTA counts and
+    // the distinct total
+    const size_t keep_bytes = ((size_t)n_keep * 4 + 255) & ~(size_t)255;
+    const size_t bytes = keep_bytes + 2 * (size_t)n * 4 + (size_t)kDigits * grid * 4 +
+                         ((size_t)grid + 2) * 4 + 64;
+    char* scratch = nullptr;
+    if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return ctx->fail(WK_E_OOM, "post-pattern scratch");
+    }
+    auto done = [&](int rc) {
+        cudaStreamSynchronize(s);
+        cudaFree(scratch);
+        return rc;
+    };
+    int32_t* d_keep = reinterpret_cast<int32_t*>(scratch);
+    uint32_t* idx0 = reinterpret_cast<uint32_t*>(scratch + keep_bytes);
+    uint32_t* idx1 = idx0 + n;
+    uint32_t* hist = idx1 + n;
+    uint32_t* part = hist + (size_t)kDigits * grid;
+    uint32_t* d_total = part + grid + 1;
+    cudaError_t e = cudaMemcpyAsync(d_keep, keep_cols, (size_t)n_keep * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return done(ctx->cuda_fail(e, "post-pattern columns"));
+    const uint32_t* idx = nullptr;   // null: rows in table order
+    uint64_t m = n;
+    if (distinct && n > 1) {
+        iota_kernel<<<grid, kFinThreads, 0, s>>>(idx0, n);
+        uint32_t* a = idx0;
+        uint32_t* b = idx1;
+        for (int c = cols - 1; c >= 0; --c)
+            for (int shift = 0; shift < 32; shift += 8) {
+                SortPass p{in->d, cols, c, shift, a, b, n, hist};
+                hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
+                scan_kernel<<<1, 1024, 0, s>>>(hist, (uint32_t)(kDigits * grid), nullptr);
+                scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
+                std::swap(a, b);
+            }
+        UniqueArgs u{in->d, cols, d_keep, n_keep, a, n, part, b};
+        unique_count_kernel<<<grid, kFinThreads, 0, s>>>(u);
+        scan_kernel<<<1, 1024, 0, s>>>(part, (uint32_t)grid, d_total);
+        unique_place_kernel<<<grid, kFinThreads, 0, s>>>(u);
+        if ((e = cudaGetLastError()) != cudaSuccess) return done(ctx->cuda_fail(e, "distinct launches"));
+        uint32_t h_total = 0;
+        if ((e = cudaMemcpyAsync(&h_total, d_total, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return done(ctx->cuda_fail(e, "distinct count"));
+        m = h_total;
+        idx = b;
+    }
+    const uint64_t start = std::min<uint64_t>((uint64_t)offset, m);
+    const uint64_t count = limit < 0 ? m - start : std::min<uint64_t>((uint64_t)limit, m - start);
+    const int rc = ctx->table_reserve(out, std::max<uint64_t>(count * n_keep, 1));
+    if (rc) return done(rc);
+    out->cols = n_keep;
+    const int pgrid = std::max(1, std::min<int>(ctx->sm_count * 8, (int)((count * n_keep + 255) / 256)));
+    project_kernel<<<pgrid, kFinThreads, 0, s>>>(in->d, cols, d_keep, n_keep, idx, start, count, out->d,
+                                                 out->d_rows);
+    if ((e = cudaGetLastError()) != cudaSuccess) return done(ctx->cuda_fail(e, "projection launch"));
+    return done(WK_SUCCESS);
+}

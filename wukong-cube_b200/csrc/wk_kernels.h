@@ -77,5 +77,6 @@ inline cudaError_t use_max_shared_carveout(K kernel) {
 cudaError_t small_kernel_attrs();    // wk_kernels.cu
 cudaError_t batch_kernel_attrs();    // wk_batch.cu
 cudaError_t serve_kernel_attrs();    // wk_serve.cu
+cudaError_t final_kernel_attrs();    // wk_final.cu
 
 }  // namespace wk

@@ -25,6 +25,7 @@ KNOB_BATCH_FLAT = 5
 SUCCESS = 0
 UNKNOWN_PATTERN = 3
 ATTR_DISABLE = 4
+NO_REQUIRED_VAR = 5
 OBJ_ERROR = 7
 VERTEX_INVALID = 8
 UNKNOWN_SUB = 9
@@ -143,6 +144,8 @@ _SIGS = {
     "wk_table_alloc": (C.c_int, [_P, C.c_uint64, C.POINTER(_P)]),
     "wk_table_free": (C.c_int, [_P, _P]),
     "wk_table_upload": (C.c_int, [_P, _P, _P, C.c_uint64, C.c_int32]),
+    "wk_table_final_process": (C.c_int, [_P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_int32,
+                                         C.c_int64, C.c_int64, _P]),
     "wk_table_download": (C.c_int, [_P, _P, _P, C.c_uint64]),
     "wk_table_shape": (C.c_int, [_P, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
     "wk_table_device_ptr": (C.c_int, [_P, _P, C.POINTER(_P)]),
@@ -400,6 +403,14 @@ class Table:
         out = np.zeros(max(rows * cols, 1), dtype=np.uint32)
         _check(lib().wk_table_download(self.ctx.h, self.h, _ptr(out), out.size), self.ctx.h)
         return out[:rows * cols].reshape(rows, cols)
+
+    def final_process(self, keep_cols, distinct=False, offset=0, limit=-1):
+        """The post-pattern stage on the device (wk_table_final_process) into a new Table."""
+        out = Table(self.ctx)
+        keep = (C.c_int32 * max(len(keep_cols), 1))(*[int(c) for c in keep_cols])
+        _check(lib().wk_table_final_process(self.ctx.h, self.h, keep, len(keep_cols),
+                                            1 if distinct else 0, offset, limit, out.h), self.ctx.h)
+        return out
 
 
 class Context:
