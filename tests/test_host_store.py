@@ -124,3 +124,40 @@ def test_capi_exports_every_declared_symbol(built):
     missing = [n for n in sorted(names) if not hasattr(L, n)]
     assert not missing, missing
     assert set(wk.exported_symbols()) <= names
+
+
+def test_random_plans_dispatch_like_the_oracle(built):
+    """Seeded random pattern lists (constants, variables bound or not, index starts, both
+    directions, out-of-range variables, unknown predicates): the library's host-side dispatch
+    (wk_query_validate) gives the oracle's status and, on success, its column map."""
+    import oracle
+    import wukong_b200 as wk
+    V = 1 << 17
+    tr = np.array([(V + 1, 5, V + 2), (V + 2, 6, V + 3), (V + 1, 1, 7), (V + 3, 5, V + 1),
+                   (V + 2, 1, 7), (V + 3, 6, V + 2)], np.uint32)
+    o = oracle.OracleStore(tr)
+    rng = np.random.default_rng(11)
+    consts = [V + 1, V + 2, V + 3, 7]
+    seen = set()
+    for _ in range(600):
+        nvars = int(rng.integers(1, 4))
+        pats = []
+        for k in range(int(rng.integers(1, 5))):
+            def term():
+                if rng.random() < 0.5:
+                    return -int(rng.integers(1, nvars + 2))   # may be past nvars
+                return int(rng.choice(consts))
+            s = term()
+            p = int(rng.choice([5, 6, wk.TYPE_ID, wk.PREDICATE_ID, -1]))
+            d = int(rng.integers(0, 2))
+            pats.append((s, p, d, term()))
+        q = wk.Query(pats, nvars=nvars)
+        rc, v2c, cols = wk.validate(q)
+        st, tab, ov2c = o.run(q.flat(), q.nvars)
+        assert rc == st, (pats, nvars, rc, st)
+        if st == 0:
+            assert list(v2c) == list(ov2c), pats
+            assert cols == tab.shape[1], pats
+        seen.add(st)
+    assert len(seen) >= 4   # the sample reaches several outcomes, success among them
+    assert 0 in seen
