@@ -114,35 +114,51 @@ class Clocks:
                 "samples": len(good)}
 
 
-def build_graph(orgs, seed):
+def build_graph(args):
     import wukong_b200 as wk
     t0 = time.time()
-    tr, v = wk.synth_generate(orgs, seed=seed)
+    tr, v = wk.synth_generate(args.orgs, seed=args.seed, zipf=args.zipf, zipf_s=args.zipf_s)
     t1 = time.time()
-    g = wk.GStore(tr)
+    g = wk.GStore(tr, load_factor=args.load_factor)
     t2 = time.time()
     inst = {t: g.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
     return tr, v, g, inst, {"triples": int(tr.shape[0]), "gen_s": round(t1 - t0, 2),
                             "build_s": round(t2 - t1, 2), **g.info()}
 
 
-def config(args, ginfo):
+def graph_name(args):
+    skew = (", degreeFrom targets and course choices Zipf s=%g" % args.zipf_s) if args.zipf else ""
+    return "seeded LUBM-shaped graph of %d organisations%s" % (args.orgs, skew)
+
+
+def config(args):
+    """The workload, the same in both arms (graph sizes and build times go in "graph")."""
     return {"workload": "batches of %d light queries (2-6 patterns from random constants) on the "
-                        "seeded LUBM-shaped graph of %d organisations; heavy star + triangle "
-                        "alongside" % (args.light, args.orgs),
-            "orgs": args.orgs, "seed": args.seed, "light_queries_per_step": args.light,
-            "graph": ginfo, "l2": "flushed between timed steps (256 MiB write)"}
+                        "%s; heavy star + triangle alongside" % (args.light, graph_name(args)),
+            "orgs": args.orgs, "seed": args.seed, "zipf": args.zipf_s if args.zipf else None,
+            "light_queries_per_step": args.light,
+            "l2": "flushed between timed steps (256 MiB write)"}
 
 
 def run_reference(args, world, rank):
-    """CPU arm: the oracle (restated reference CPU engine) on all host cores."""
+    """CPU arm: the oracle (restated reference CPU engine) on all host cores.  The process loads
+    the generator's own library (libwk_synth.so) and the oracle, not the product library: the
+    graph comes from the generator, the type instances from the oracle's own store."""
     if rank != 0:
         return
     import oracle
     import workloads
+    import wukong_b200 as wk
     cores = os.cpu_count() or 1
-    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
+    t0 = time.time()
+    tr, v = wk.synth_generate(args.orgs, seed=args.seed, zipf=args.zipf, zipf_s=args.zipf_s,
+                              generator_only=True)
+    t1 = time.time()
     o = oracle.OracleStore(tr)
+    t2 = time.time()
+    inst = {t: o.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+    ginfo = {"triples": int(tr.shape[0]), "gen_s": round(t1 - t0, 2), "build_s": round(t2 - t1, 2),
+             "store": "oracle"}
     qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
     flat = [q.flat() for q in qs]
     nv = [q.nvars for q in qs]
@@ -159,7 +175,7 @@ def run_reference(args, world, rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": config(args, ginfo),
+            "config": config(args), "graph": ginfo,
             "cpu_baseline": {"value": value, "unit": "light queries/s", "cores": cores, "kind": "port",
                              "sample": "%d steps x %d light queries, one query per thread" %
                                        (args.steps, len(qs))},
@@ -269,7 +285,7 @@ def run_ours(args, world, rank, local_rank):
     import wukong_b200 as wk
 
     torch.cuda.set_device(local_rank)
-    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
+    tr, v, g, inst, ginfo = build_graph(args)
     ctx = wk.Context(local_rank)
     ctx.upload_gstore(g)
     ginfo["device_store_bytes"] = ctx.store_bytes()
@@ -378,12 +394,24 @@ def run_ours(args, world, rank, local_rank):
     # ---- heavy queries (device-resident graph replays)
     hq = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
     heavy_rows = []
-    for q in hq:
+    heavy_cpu = {}
+    for name, q in zip(("star", "triangle"), hq):
         got, _ = ctx.execute(q, wk.MODE_GRAPH)
         heavy_rows.append(int(got.shape[0]))
         if o is not None and not args.no_check:
             st, want, _ = o.run(q.flat(), q.nvars, mt_factor=cores)
             assert st == 0 and np.array_equal(oracle.sorted_rows(got), oracle.sorted_rows(want))
+        if o is not None and not args.no_cpu:
+            # the CPU engine on every host core, split as the reference splits an index start
+            # (mt_factor slices of the index list, one per thread; sparql.hpp:213-224); the
+            # correctness run above warmed it
+            cpu_t = []
+            for _ in range(args.heavy_cpu_reps):
+                t0 = time.perf_counter()
+                st, _, _ = o.run(q.flat(), q.nvars, mt_factor=cores)
+                cpu_t.append((time.perf_counter() - t0) * 1000)
+                assert st == 0
+            heavy_cpu[name] = statistics.median(cpu_t) if cpu_t else None
     heavy = {}
     for name, q in zip(("star", "triangle"), hq):
         ms = timed(stream, flush, args.steps, lambda q=q: ctx.enqueue(q, wk.MODE_GRAPH))
@@ -393,7 +421,12 @@ def run_ours(args, world, rank, local_rank):
             ctx.execute(q, wk.MODE_PLAIN)
         plain_ms = (time.perf_counter() - t0) / 3 * 1000
         heavy[name] = {"ms": statistics.median(ms), "rows": heavy_rows[len(heavy)],
-                       "plain_ms": plain_ms, "profile": ctx.profile(q, iters=3)}
+                       "plain_ms": plain_ms, "profile": ctx.profile(q, iters=3),
+                       "cpu_ms": heavy_cpu.get(name), "cpu_cores": cores,
+                       "cpu_how": "oracle (the reference CPU engine restated), mt_factor = cores, "
+                                  "median of %d runs after a warm run" % args.heavy_cpu_reps}
+        if heavy_cpu.get(name):
+            heavy[name]["speedup_vs_cpu"] = heavy_cpu[name] / heavy[name]["ms"]
 
     # ---- post-pattern stage on the device: DISTINCT ?x2 ?x1 over the heavy star's table
     star_table, star_v2c = ctx.execute(hq[0], wk.MODE_RESIDENT)
@@ -460,7 +493,7 @@ def run_ours(args, world, rank, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "light queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-            "data": "synthetic", "config": config(args, ginfo),
+            "data": "synthetic", "config": config(args), "graph": ginfo,
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                            "max": lat[-1], "note": "every query of a batch completes with the batch"},
             "e2e": {"value": e2e, "unit": "light queries/s", "h2d_bytes_per_step": h2d,
@@ -508,12 +541,20 @@ def run_ours(args, world, rank, local_rank):
             "clocks": clk.summary()}
     if rank == 0:
         if not args.no_cpu:
-            t0 = time.perf_counter()
-            _, st = o.run_many([q.flat() for q in qs], [q.nvars for q in qs], cores)
-            dt = time.perf_counter() - t0
-            line["cpu_baseline"] = {"value": len(qs) / dt, "unit": "light queries/s", "cores": cores,
-                                    "kind": "port",
-                                    "sample": "one batch of %d light queries, one query per thread" % len(qs)}
+            # the reference arm's method: warm-up runs, then --steps timed runs of the same batch
+            flat, nv = [q.flat() for q in qs], [q.nvars for q in qs]
+            for _ in range(args.warmup):
+                o.run_many(flat, nv, cores)
+            cpu_t = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                _, st = o.run_many(flat, nv, cores)
+                cpu_t.append(time.perf_counter() - t0)
+                assert (st == 0).all()
+            line["cpu_baseline"] = {"value": len(qs) * len(cpu_t) / sum(cpu_t), "unit": "light queries/s",
+                                    "cores": cores, "kind": "port",
+                                    "sample": "%d steps x %d light queries after %d warm-up steps, one "
+                                              "query per thread" % (args.steps, len(qs), args.warmup)}
         print(json.dumps(line))
     ctx.close()
 
@@ -527,7 +568,7 @@ def run_profile_case(args):
 
     import workloads
     import wukong_b200 as wk
-    tr, v, g, inst, ginfo = build_graph(args.orgs, args.seed)
+    tr, v, g, inst, ginfo = build_graph(args)
     with wk.Context(0) as ctx:
         ctx.upload_gstore(g)
         ctx.tune_set(wk.KNOB_BATCH_FLAT, args.batch_flat)
@@ -575,9 +616,18 @@ def main():
     ap.add_argument("--e2e-batches", type=int, default=8,
                     help="batches per end-to-end call (wk_batch_execute_stream)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--zipf", action="store_true",
+                    help="Zipf-skewed degreeFrom targets and course choices (the scale-and-skew "
+                         "configuration: hub organisations and popular courses)")
+    ap.add_argument("--zipf-s", type=float, default=1.1, help="Zipf exponent with --zipf")
+    ap.add_argument("--load-factor", type=float, default=0.0,
+                    help="store load factor (fraction of a bucket's 7 data slots in use; 0: the "
+                         "builder's default 0.1)")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--heavy-cpu-reps", type=int, default=3,
+                    help="timed CPU-engine runs of each heavy query (median reported)")
     ap.add_argument("--serve-rates", type=lambda s: [int(x) for x in s.split(",")],
                     default=[1000, 10000, 50000, 100000, 125000, 150000, 175000, 200000, 500000])
     ap.add_argument("--serve-seconds", type=float, default=0.25,

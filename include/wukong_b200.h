@@ -289,13 +289,19 @@ int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t col_start, u
  * enough, and nothing is grown.
  *
  * Limits:
- * - inputs of at most 4,194,304 rows (16,384 tiles of 256 rows);
- * - at most 8,192 long-list slices of 2,048 output rows.
+ * - inputs of at most 4,193,792 rows (16,382 tiles of 256 rows);
+ * - at most 8,192 long-list slices.  Every input row whose list is longer than the context's
+ *   slice threshold (knob 2: 128 rows unless tuned) takes ceil(length / 2,048) slices, so the
+ *   queue holds between 8,192 such rows (about 1 M output rows of 129-row lists) and 16.7 M
+ *   output rows of long lists.
  * Beyond them, or when the output does not fit, the call returns WK_E_CAPACITY and
- * wk_last_error says which limit was hit.
+ * wk_last_error says which limit was hit.  An input whose row count is past its capacity (a
+ * table left by a step that overflowed) is refused with WK_E_CORRUPT, as wk_table_download
+ * refuses it.
  *
- * The first call on a device sets the scratch up: it takes its address and clears it. Make
- * that first call before any stream capture on the device.
+ * The first call on a device sets the scratch up: it takes its address and clears it, and
+ * leaves the calling thread's current device as it found it. Make that first call before any
+ * stream capture on the device.
  *
  * The scratch is shared by every context and stream of the device, so calls that overlap in
  * time on one device race; serialise them.
@@ -355,6 +361,11 @@ int wk_debug_phase_cycles(unsigned long long* out, int32_t n, int32_t reset);
  * fault, trap or hang is involved.  No reference counterpart (the reference aborts). */
 int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
 
+/* Device allocations (cudaMalloc calls) the library has made in this process, over every
+ * context.  A caller that must not allocate during some call reads it before and after.  No
+ * reference counterpart. */
+int wk_debug_device_allocs(uint64_t* count);
+
 /* Tile-schedule knobs of the exploration launch (what the autotuner sets).
  *   knob 0: lanes per probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte
  *           bucket slices staged per request);
@@ -368,7 +379,11 @@ int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
  *           tile launch; 0 never does (default 65,536);
  *   knob 5: a mask over batch levels; level k runs as the flat passes when bit k is set (one
  *           thread per row, full occupancy, output rows split evenly over the grid) and as
- *           the tile launch otherwise (default 0: all tile launches).
+ *           the tile launch otherwise (default 0: all tile launches);
+ *   knob 6: polls a bounded device-side wait on another CTA (a tile's look-back, a CTA waiting
+ *           for the long-list slice queue) makes before it gives up and the call returns
+ *           WK_E_TIMEOUT; 0 restores the default (2^24).  A few polls make the waits run out,
+ *           which is how the timeout path is tested without hanging or faulting a GPU.
  * wk_ctx_tune_get reads a knob back.  No reference counterpart (its launch shape is fixed,
  * gpu_hash.cu:96-326). */
 #define WK_KNOB_LANES 0
@@ -377,6 +392,7 @@ int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
 #define WK_KNOB_BATCH_SLICE_ROWS 3
 #define WK_KNOB_FLAT_ROWS 4
 #define WK_KNOB_BATCH_FLAT 5
+#define WK_KNOB_SPIN_LIMIT 6
 int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value);
 int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value);
 

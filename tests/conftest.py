@@ -19,6 +19,7 @@ def built():
     """Build the product library and the oracle once per session."""
     import wk_build as wkbuild
     wkbuild.build_lib()
+    wkbuild.build_synth()
     wkbuild.build_oracle()
     return True
 

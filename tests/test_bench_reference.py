@@ -29,3 +29,18 @@ def test_reference_arm_json_line(built):
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_does_not_load_the_product(built):
+    """The reference arm generates its graph with the generator's own library and reads the
+    type instances from the oracle's store: the product library is never mapped."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--orgs', '5', "
+            "'--light', '64', '--steps', '1', '--warmup', '1']; "
+            "runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_MAPPED' if 'libwukong_b200' in maps else 'PRODUCT_NOT_MAPPED'); "
+            "print('ORACLE_MAPPED' if 'liboracle' in maps else 'ORACLE_NOT_MAPPED')")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "PRODUCT_NOT_MAPPED" in out.stdout and "ORACLE_MAPPED" in out.stdout

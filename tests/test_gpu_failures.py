@@ -61,3 +61,37 @@ def test_batch_and_serving_errors(ctx, graph20):
 
 def test_bad_injection_bits_are_refused(ctx):
     assert wk.lib().wk_debug_fail_next(ctx.h, 8) == wk.E_BADARG
+
+
+def test_device_waits_run_out_and_context_recovers(ctx, graph20):
+    """The real bounded waits, not a fake: with the spin limit at two polls (knob 6), a tile's
+    look-back on a predecessor that has not published yet, or a CTA left without tiles that
+    waits for the slice queue, gives up, sets the timeout bit and returns.  The call reports
+    WK_E_TIMEOUT; with the default limit back the same context answers correctly."""
+    v = graph20["vocab"]
+    o = graph20["oracle"]
+    persons = np.asarray(graph20["instances"][v["t_person_a"]], np.uint32).reshape(-1, 1)
+    assert persons.shape[0] > 8 * 256   # many tiles, far fewer than the launch's CTAs
+    want = o.step(0, persons, 0, v["p_takes"], wk.OUT)
+    tin = ctx.table(persons, capacity=persons.size)
+    out = ctx.table(capacity=want.size + 64)
+    ctx.tune_set(wk.KNOB_SPIN_LIMIT, 2)
+    try:
+        codes = []
+        for _ in range(5):
+            codes.append(wk.lib().wk_step_known_to_unknown(ctx.h, tin.h, 0, v["p_takes"], wk.OUT, out.h))
+            if codes[-1] == wk.E_TIMEOUT:
+                break
+        assert wk.E_TIMEOUT in codes, codes
+        assert set(codes) <= {wk.SUCCESS, wk.E_TIMEOUT}, codes
+    finally:
+        ctx.tune_set(wk.KNOB_SPIN_LIMIT, 0)
+    assert ctx.tune_get(wk.KNOB_SPIN_LIMIT) == 1 << 24
+    ctx.known_to_unknown(tin, 0, v["p_takes"], wk.OUT, out)
+    assert _same(out.download(), want)
+    q = workloads.heavy_star(v)
+    _, qwant, _ = o.run(q.flat(), q.nvars)
+    got, _ = ctx.execute(q, wk.MODE_GRAPH)
+    assert _same(got, qwant)
+    for t in (tin, out):
+        t.free()

@@ -161,3 +161,14 @@ def test_random_plans_dispatch_like_the_oracle(built):
         seen.add(st)
     assert len(seen) >= 4   # the sample reaches several outcomes, success among them
     assert 0 in seen
+
+
+def test_generator_library_matches_the_product(built):
+    import wukong_b200 as wk
+    """libwk_synth.so (the generator alone, used where the product must not be loaded) makes the
+    same triples and vocabulary as the product library, uniform and Zipf-skewed."""
+    for zipf in (False, True):
+        a, va = wk.synth_generate(7, seed=3, zipf=zipf)
+        b, vb = wk.synth_generate(7, seed=3, zipf=zipf, generator_only=True)
+        assert va == vb
+        assert np.array_equal(a, b)

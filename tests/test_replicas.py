@@ -89,3 +89,74 @@ def test_two_gloo_ranks_answer_the_stream(tmp_path, graph20):
         total, slowest = np.load(tmp_path / ("agg_%d.npy" % r))
         assert total == len(qs)
         assert slowest == 10.0 + world - 1
+
+
+def _elastic_rank(rank, world, port, result_dir, n_batches, per_batch):
+    """Rank 1 leaves between batches (announced) after its first batch; rank 2 takes a batch and
+    stops before answering it, without a word (its heartbeat goes stale).  Rank 0 stays."""
+    import datetime
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    for p in (os.path.join(root, "wukong-cube_b200"), os.path.join(root, "oracle")):
+        sys.path.insert(0, p)
+    import oracle
+    import workloads
+    import wukong_b200 as wk
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    store = dist.distributed_c10d._get_default_store()
+    tr, v = wk.synth_generate(5, seed=0, generator_only=True)
+    o = oracle.OracleStore(tr)
+    inst = {t: o.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+    qs = workloads.light_queries(v, inst, n_batches * per_batch, seed=9)
+    wq = replicas.WorkQueue(store, rank, world, n_batches, stale_s=1.0)
+    dist.barrier()   # every rank is in before any leaves
+    answered = 0
+    while True:
+        i = wq.claim()
+        if i is None:
+            break
+        if rank == 2 and answered == 1:
+            os._exit(0)   # took batch i and stopped: no answer, no goodbye
+        part = qs[i * per_batch:(i + 1) * per_batch]
+        rows, st = o.run_many([q.flat() for q in part], [q.nvars for q in part], 1)
+        assert (st == 0).all()
+        np.save(os.path.join(result_dir, "batch_%d.npy" % i), rows)
+        np.save(os.path.join(result_dir, "by_%d_%d.npy" % (i, rank)), np.array([rank]))
+        wq.done(i)
+        answered += 1
+        if rank == 1 and answered == 1:
+            wq.leave()   # between batches
+            break
+        if rank == 0 and answered == 1:
+            import time
+            time.sleep(0.5)   # let the others take their batches before rank 0 runs on
+    np.save(os.path.join(result_dir, "answered_%d.npy" % rank), np.array([answered]))
+    if rank == 0:
+        import time
+        time.sleep(0.2)
+    os._exit(0)   # a survivor leaves without a collective the departed ranks would never join
+
+
+def test_replicas_keep_answering_when_ranks_leave(tmp_path, graph20):
+    world, n_batches, per_batch = 3, 9, 20
+    mp.spawn(_elastic_rank, args=(world, _free_port(), str(tmp_path), n_batches, per_batch),
+             nprocs=world, join=True)
+    import oracle
+    import workloads
+    import wukong_b200 as wk
+    tr, v = wk.synth_generate(5, seed=0)
+    o = oracle.OracleStore(tr)
+    inst = {t: o.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+    qs = workloads.light_queries(v, inst, n_batches * per_batch, seed=9)
+    want, _ = o.run_many([q.flat() for q in qs], [q.nvars for q in qs], 1)
+    got = np.concatenate([np.load(tmp_path / ("batch_%d.npy" % i)) for i in range(n_batches)])
+    assert np.array_equal(got, want)   # every batch answered, once, whoever answered it
+    for i in range(n_batches):
+        assert len(list(tmp_path.glob("by_%d_*.npy" % i))) == 1
+    assert int(np.load(tmp_path / "answered_1.npy")[0]) == 1     # left after one batch
+    assert not (tmp_path / "answered_2.npy").exists()             # stopped mid-stream
+    assert len(list(tmp_path.glob("by_*_2.npy"))) == 1           # its one answered batch counts

@@ -191,7 +191,7 @@ int ensure_state(wk_ctx* ctx, BatchState* b, uint32_t n, int levels, uint64_t ro
     WKB_CUDA(ctx, cudaDeviceSynchronize());
     free_state(b);
     auto dm = [&](void** p, size_t bytes) {
-        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+        if (wk::dev_malloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
@@ -380,6 +380,7 @@ int enqueue_batch(wk_ctx* ctx, BatchState* b, const Plan& P, ProfHooks* ph = nul
         a.sorted_lists = ctx->sorted_lists;
         a.lanes = lanes;
         a.slice_rows = ctx->batch_slice_rows;
+        a.spin_limit = ctx->spin_limit;
         const int grid = wk::explore_blocks_per_sm(a.virtual_rows ? 0 : a.w_in, a.w_out, lanes) * ctx->sm_count;
         if (ph) {
             WKB_CUDA(ctx, cudaMemsetAsync(&ctx->d_ctl->sum_deg, 0, 16, s));

@@ -5,6 +5,7 @@
 // is uploaded once and stays resident, so there is no segment paging, no per-step mapping
 // upload and no per-step host sync unless the caller asks for the plain mode.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -39,7 +40,18 @@ const char* kMessages[] = {
 
 constexpr uint64_t kPadWords = 16;
 
+std::atomic<uint64_t> g_device_allocs{0};
+
 }  // namespace
+
+void wk::note_device_alloc() { g_device_allocs.fetch_add(1, std::memory_order_relaxed); }
+uint64_t wk::device_alloc_count() { return g_device_allocs.load(std::memory_order_relaxed); }
+
+extern "C" int wk_debug_device_allocs(uint64_t* count) {
+    if (!count) return WK_E_BADARG;
+    *count = wk::device_alloc_count();
+    return WK_SUCCESS;
+}
 
 extern "C" const char* wk_strerror(int code) {
     if (code >= 0 && code < (int)(sizeof(kMessages) / sizeof(kMessages[0]))) return kMessages[code];
@@ -80,7 +92,7 @@ int wk_ctx::ensure_heavy(uint64_t out_rows_cap) {
     if (d_heavy) cudaFree(d_heavy);
     d_heavy = nullptr;
     heavy_cap = 0;
-    if (cudaMalloc(&d_heavy, cap * sizeof(wk::HeavyItem)) != cudaSuccess) {
+    if (wk::dev_malloc(&d_heavy, cap * sizeof(wk::HeavyItem)) != cudaSuccess) {
         cudaGetLastError();
         return fail(WK_E_OOM, "long-list slice queue");
     }
@@ -96,7 +108,7 @@ int wk_ctx::ensure_flat(uint64_t in_rows_cap) {
     if (d_flat) cudaFree(d_flat);
     d_flat = nullptr;
     flat_cap_rows = 0;
-    if (cudaMalloc(&d_flat, wk::flat_scratch_bytes(rows, wk::flat_grid(sm_count))) != cudaSuccess) {
+    if (wk::dev_malloc(&d_flat, wk::flat_scratch_bytes(rows, wk::flat_grid(sm_count))) != cudaSuccess) {
         cudaGetLastError();
         return fail(WK_E_OOM, "flat pipeline scratch");
     }
@@ -111,7 +123,7 @@ int wk_ctx::ensure_status(uint64_t tiles) {
     WK_CUDA(this, cudaStreamSynchronize(stream));
     if (d_status) WK_CUDA(this, cudaFree(d_status));
     d_status = nullptr;
-    if (cudaMalloc(&d_status, cap * sizeof(unsigned long long)) != cudaSuccess) {
+    if (wk::dev_malloc(&d_status, cap * sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
         status_cap = 0;
         return fail(WK_E_OOM, "status array");
@@ -138,13 +150,13 @@ int wk_ctx::table_reserve(wk_table* t, uint64_t elems) {
     if (t->d) cudaFree(t->d);
     t->d = nullptr;
     t->cap = 0;
-    if (cudaMalloc(&t->d, (elems + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
+    if (wk::dev_malloc(&t->d, (elems + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
         cudaGetLastError();
         return fail(WK_E_OOM, "result table of " + std::to_string(elems) + " elements");
     }
     t->cap = elems;
     if (!t->d_rows) {
-        if (cudaMalloc(&t->d_rows, sizeof(uint64_t)) != cudaSuccess) {
+        if (wk::dev_malloc(&t->d_rows, sizeof(uint64_t)) != cudaSuccess) {
             cudaGetLastError();
             return fail(WK_E_OOM, "row counter");
         }
@@ -299,6 +311,7 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
     a.sorted_lists = ctx->sorted_lists;
     a.lanes = ctx->lanes_for(a.one.op, st.in_cols);
     a.slice_rows = ctx->slice_rows;
+    a.spin_limit = ctx->spin_limit;
     // The flat pipeline needs its scratch sized for this input; without it the tile launch runs.
     if (!ctx->flat_min_rows || !ctx->d_flat || a.in_cap_rows > ctx->flat_cap_rows ||
         a.in_cap_rows < ctx->flat_min_rows || grid_override > 0)
@@ -465,7 +478,7 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     if (e == cudaSuccess) e = wk::flat_kernel_attrs();
     if (e == cudaSuccess) e = wk::final_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
-    e = cudaMalloc(&ctx->d_ctl, sizeof(wk::StepCtl));
+    e = wk::dev_malloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
     e = cudaMallocHost(&ctx->h_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "pinned control block");
@@ -542,8 +555,8 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
     ctx->d_slots = nullptr;
     ctx->d_edges = nullptr;
     ctx->has_store = false;
-    if (cudaMalloc(&ctx->d_slots, std::max<uint64_t>(n_slots, wk::kAssoc) * sizeof(wk::Slot)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_edges, (n_edges + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
+    if (wk::dev_malloc(&ctx->d_slots, std::max<uint64_t>(n_slots, wk::kAssoc) * sizeof(wk::Slot)) != cudaSuccess ||
+        wk::dev_malloc(&ctx->d_edges, (n_edges + kPadWords) * sizeof(uint32_t)) != cudaSuccess) {
         cudaGetLastError();
         return ctx->fail(WK_E_OOM, "store upload");
     }
@@ -559,7 +572,7 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
     {
         // are all lists ascending + unique?  (lets the filters binary-search long lists)
         unsigned* d_flag = nullptr;
-        WK_CUDA(ctx, cudaMalloc(&d_flag, sizeof(unsigned)));
+        WK_CUDA(ctx, wk::dev_malloc(&d_flag, sizeof(unsigned)));
         WK_CUDA(ctx, cudaMemsetAsync(d_flag, 0, sizeof(unsigned), ctx->stream));
         cudaError_t e = wk::launch_sorted_check(ctx->dev_store(), d_flag, ctx->stream);
         unsigned flag = 0;
@@ -688,6 +701,9 @@ static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in
         uint64_t rows = 0;
         rc = table_rows(ctx, in, &rows);
         if (rc) return rc;
+        // a row count past the capacity marks a table whose writing step overflowed
+        if (rows * (uint64_t)in->cols > in->cap)
+            return ctx->fail(WK_E_CORRUPT, "input row count beyond table capacity");
         if (ctx->flat_min_rows && rows >= ctx->flat_min_rows) {
             rc = ctx->ensure_flat(in->cap / in->cols);
             if (rc) return rc;
@@ -1121,6 +1137,9 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
     } else if (knob == WK_KNOB_FLAT_ROWS) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
         ctx->flat_min_rows = (uint64_t)value;
+    } else if (knob == WK_KNOB_SPIN_LIMIT) {
+        if (value < 0) return ctx->fail(WK_E_BADARG, "spin limit must be >= 0");
+        ctx->spin_limit = (uint64_t)value;
     } else if (knob == WK_KNOB_BATCH_FLAT) {
         if (value < 0 || value >= (1 << wk::kMaxBatchLevels))
             return ctx->fail(WK_E_BADARG, "batch level mask out of range");
@@ -1151,6 +1170,8 @@ extern "C" int wk_ctx_tune_get(wk_ctx* ctx, int32_t knob, int32_t* value) {
         *value = (int32_t)(ctx->batch_slice_rows ? ctx->batch_slice_rows : wk::kHeavyRows);
     else if (knob == WK_KNOB_FLAT_ROWS) *value = (int32_t)std::min<uint64_t>(ctx->flat_min_rows, INT32_MAX);
     else if (knob == WK_KNOB_BATCH_FLAT) *value = ctx->batch_flat;
+    else if (knob == WK_KNOB_SPIN_LIMIT)
+        *value = (int32_t)std::min<uint64_t>(ctx->spin_limit ? ctx->spin_limit : wk::kDefaultSpinLimit, INT32_MAX);
     else return ctx->fail(WK_E_BADARG, "unknown knob");
     return WK_SUCCESS;
 }

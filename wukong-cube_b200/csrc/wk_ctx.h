@@ -78,6 +78,7 @@ struct wk_ctx {
     int default_lanes = 2;
     int batch_lanes = 4;
     std::map<int, int> tuned_lanes;
+    uint64_t spin_limit = 0;         // polls of a bounded wait on another CTA (0: the default)
     uint32_t slice_rows = 0;         // list length above which rows go to the slice queue
     uint32_t batch_slice_rows = 0;   // (0: the kernel's default, kHeavyRows)
     int32_t batch_flat = 0;          // bit k: batch level k runs as the flat passes, not tiles

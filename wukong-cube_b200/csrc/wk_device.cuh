@@ -15,7 +15,6 @@ constexpr int kUnroll = 4;                                // rows per lane group
 constexpr int kMaxProbeIters = 1 << 14;                   // chain walk limit
 constexpr unsigned long long kFlagAgg = 1, kFlagPrefix = 2;
 constexpr unsigned long long kValMask = (1ull << 46) - 1;
-constexpr unsigned long long kSpinLimit = 1ull << 24;     // look-back polls before giving up
 constexpr unsigned kTmaWaitLimit = 1u << 24;              // mbarrier polls before giving up
 constexpr int kChunkBytes = 32 * 1024;                    // staging of one output chunk
 constexpr int kLinear = 8;                                // list entries checked by ballot
@@ -218,7 +217,7 @@ __device__ __forceinline__ void publish_aggregate(unsigned long long* status, ui
 }
 
 __device__ uint64_t resolve_prefix(unsigned long long* status, StepCtl* ctl, uint64_t tile,
-                                   uint64_t agg, unsigned epoch) {
+                                   uint64_t agg, unsigned epoch, unsigned long long spin_limit) {
     volatile unsigned long long* st = status;
     const int lane = threadIdx.x & 31;
     if (tile == 0) return 0;   // tile 0 published its inclusive prefix already
@@ -231,7 +230,7 @@ __device__ uint64_t resolve_prefix(unsigned long long* status, StepCtl* ctl, uin
         const unsigned long long flag = (s >> 46) & 3ull;
         const bool ready = (unsigned)(s >> 48) == epoch && flag != 0;
         if (!__all_sync(kFull, ready)) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 if (lane == 0) atomicOr(&ctl->err, kErrTimeout);
                 break;
             }

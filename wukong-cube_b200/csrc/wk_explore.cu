@@ -75,6 +75,11 @@ __device__ __forceinline__ uint32_t slice_threshold(const ExploreArgs& a) {
     return a.slice_rows ? max(a.slice_rows, (uint32_t)kMinSliceRows) : (uint32_t)kHeavyRows;
 }
 
+// Polls of a bounded wait on another CTA (look-back, slice queue) before it gives up.
+__device__ __forceinline__ unsigned long long spin_limit(const ExploreArgs& a) {
+    return a.spin_limit ? a.spin_limit : kDefaultSpinLimit;
+}
+
 // Step of query q at this launch.
 __device__ __forceinline__ const StepDesc* step_desc(const ExploreArgs& a, uint32_t q) {
     if (!a.desc) return &a.one;
@@ -88,7 +93,6 @@ struct TileState {
     unsigned long long tile;
     unsigned long long total;    // output rows of the tile
     unsigned long long ltotal;   // output rows written by the tile itself (short lists)
-    unsigned long long alg, sd;  // byte accounting
     int n;
     int has_heavy;
 };
@@ -123,12 +127,14 @@ __device__ __forceinline__ TileBuf tile_buf(uint32_t* base, int wi) {
 template <int L>
 __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& B, TileState& S,
                                            uint64_t* bar, unsigned phase, uint64_t tile, uint64_t R,
-                                           int wi, unsigned epoch, uint64_t* s_warp) {
+                                           int wi, unsigned epoch, uint64_t* s_warp,
+                                           unsigned long long& acc_alg, unsigned long long& acc_sd) {
     constexpr int kGroups = kStepThreads / L;
     constexpr int kBatches = kTileRows / (kGroups * kUnroll);
     static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
     const int grp = threadIdx.x / L;
     const int h = threadIdx.x & (L - 1);
+    const int gbase = (threadIdx.x & 31) & ~(L - 1);
     const uint64_t r0 = tile * kTileRows;
     const int n = (int)min((uint64_t)kTileRows, R - r0);
     const uint32_t* src = a.in + r0 * (uint64_t)wi;
@@ -140,8 +146,6 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         }
         S.tile = tile;
         S.n = n;
-        S.alg = 0;
-        S.sd = 0;
         S.has_heavy = 0;
     }
     for (int i = threadIdx.x; i < n; i += kStepThreads) {
@@ -152,84 +156,107 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     __syncthreads();
     // the rows' copy ran alongside the owner loads; read the rows from shared memory
     if (wi) mbar_wait(bar, phase, &a.ctl->err);
+    constexpr int kOwn = (kUnroll + L - 1) / L;   // rows of a batch each lane works out
 #pragma unroll 1
     for (int b = 0; b < kBatches; ++b) {
+        // Row setup, split over the group's lanes: lane h works out the rows u = h, h + L, ...
+        // of the batch (descriptor, key, home bucket, filter target), then the group shares
+        // them by shuffles, so no row's hash or descriptor is worked out twice.
+        // flag: op | valid << 8 | pending << 9 | cin << 16 | cout << 24
+        uint64_t mkey[kOwn], mbkt[kOwn];
+        uint32_t mtgt[kOwn], mflag[kOwn];
+#pragma unroll
+        for (int j = 0; j < kOwn; ++j) {
+            const int u = j * L + h;
+            const int row = (b * kUnroll + u) * kGroups + grp;
+            mkey[j] = 0;
+            mbkt[j] = 0;
+            mtgt[j] = 0;
+            mflag[j] = kXDone;
+            if (u < kUnroll && row < n) {
+                const StepDesc* d = step_desc(a, B.q[row]);
+                const uint32_t op = d->op;
+                bool valid = op != kXDone;
+                const SegDesc* sg = &d->seg;
+                uint32_t target = d->end_const;
+                uint64_t key = 0;
+                if (op == kXStart) {
+                    key = d->start_key;
+                } else if (valid) {
+                    const uint32_t* rin = B.in + row * wi;   // shared memory: plain loads
+                    const uint32_t cur = rin[d->cs];
+                    if (op == kXK2K) target = rin[d->ce];
+                    if (op == kXK2U && d->type_index) {
+                        // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+                        key = make_key(0, cur, kIn);
+                        sg = &a.seg_index[kIn];
+                        if (cur >= (1u << kNbitsIdx)) valid = false;
+                    } else {
+                        key = make_key(cur, d->pid, d->dir);
+                        if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+                    }
+                    if (cur == kBlankId) valid = false;
+                }
+                const bool pending = valid && sg->num_buckets != 0 && key != 0;
+                const uint32_t cin = d->cin, cout = d->cout;
+                mkey[j] = key;
+                mbkt[j] = pending ? bucket_of(key, *sg) : 0;
+                mtgt[j] = target;
+                mflag[j] = op | (valid ? 0x100u : 0u) | (pending ? 0x200u : 0u) | (cin << 16) | (cout << 24);
+                B.meta[row] = op | (cin << 8) | (cout << 16);
+            }
+        }
         uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
         bool valid[kUnroll], pending[kUnroll];
         int row[kUnroll];
-        uint32_t target[kUnroll], op[kUnroll];
+        uint32_t target[kUnroll], flag[kUnroll];
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
+            const int src = gbase + u % L;
             row[u] = (b * kUnroll + u) * kGroups + grp;
-            valid[u] = row[u] < n;
-            const StepDesc* d = step_desc(a, valid[u] ? B.q[row[u]] : 0);
-            op[u] = valid[u] ? d->op : kXDone;
-            if (op[u] == kXDone) valid[u] = false;
-            const SegDesc* sg = &d->seg;
-            target[u] = d->end_const;
-            if (op[u] == kXStart) {
-                key[u] = d->start_key;
-            } else {
-                const uint32_t* rin = B.in + row[u] * wi;   // shared memory: plain loads
-                const uint32_t cur = valid[u] ? rin[d->cs] : kBlankId;
-                if (op[u] == kXK2K && valid[u]) target[u] = rin[d->ce];
-                if (op[u] == kXK2U && d->type_index) {
-                    // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-                    key[u] = make_key(0, cur, kIn);
-                    sg = &a.seg_index[kIn];
-                    if (cur >= (1u << kNbitsIdx)) valid[u] = false;
-                } else {
-                    key[u] = make_key(cur, d->pid, d->dir);
-                    if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
-                }
-                if (cur == kBlankId) valid[u] = false;
-            }
-            pending[u] = valid[u] && sg->num_buckets != 0 && key[u] != 0;
-            bucket[u] = pending[u] ? bucket_of(key[u], *sg) : 0;
-            if (h == 0 && row[u] < n)
-                B.meta[row[u]] = op[u] | ((uint32_t)d->cin << 8) | ((uint32_t)d->cout << 16);
+            key[u] = __shfl_sync(kFull, mkey[u / L], src);
+            bucket[u] = __shfl_sync(kFull, mbkt[u / L], src);
+            target[u] = __shfl_sync(kFull, mtgt[u / L], src);
+            flag[u] = __shfl_sync(kFull, mflag[u / L], src);
+            valid[u] = (flag[u] & 0x100u) != 0;
+            pending[u] = (flag[u] & 0x200u) != 0;
         }
         WK_PH(8);
         group_probe<L>(a.store, key, bucket, pending, ptr, &a.ctl->err);
         WK_PH(9);
         uint64_t off[kUnroll], deg[kUnroll];
-        bool has[kUnroll], found[kUnroll];
+        bool has[kUnroll], found[kUnroll], any_filter = false;
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
+            const uint32_t op = flag[u] & 0xFFu;
             off[u] = ptr_off(ptr[u]);
             deg[u] = ptr_size(ptr[u]);
             if (off[u] + deg[u] > a.store.n_edges) {
                 if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg[u] = 0;
             }
-            has[u] = valid[u] && deg[u] > 0 && (op[u] == kXK2K || op[u] == kXK2C);
+            has[u] = valid[u] && deg[u] > 0 && (op == kXK2K || op == kXK2C);
+            any_filter |= has[u];
+            found[u] = false;
         }
-        group_member<L>(a.store.edges, off, deg, target, has, a.sorted_lists != 0, found);
+        // membership only where a row of the warp filters (the test is warp-uniform)
+        if (__any_sync(kFull, any_filter))
+            group_member<L>(a.store.edges, off, deg, target, has, a.sorted_lists != 0, found);
         WK_PH(10);
-        unsigned long long alg = 0, sd = 0;
         if (h == 0) {
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
                 if (valid[u]) {
-                    const bool filt = op[u] == kXK2K || op[u] == kXK2C;
+                    const uint32_t op = flag[u] & 0xFFu;
+                    const bool filt = op == kXK2K || op == kXK2C;
                     const uint32_t cnt = filt ? (found[u] ? 1u : 0u) : (uint32_t)deg[u];
-                    const uint32_t meta = B.meta[row[u]];
                     B.off[row[u]] = off[u];
                     B.cnt[row[u]] = cnt;
-                    sd += deg[u];
-                    alg += ((meta >> 8) & 0xFF) * 4ull + 16 + deg[u] * 4 +
-                           (unsigned long long)cnt * ((meta >> 16) & 0xFF) * 4;
+                    // byte accounting, kept in registers until the CTA leaves
+                    acc_sd += deg[u];
+                    acc_alg += ((flag[u] >> 16) & 0xFF) * 4ull + 16 + deg[u] * 4 +
+                               (unsigned long long)cnt * (flag[u] >> 24) * 4;
                 }
-        }
-        // byte accounting: a warp reduction, then one shared atomic per warp
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            alg += __shfl_xor_sync(0xffffffffu, alg, o);
-            sd += __shfl_xor_sync(0xffffffffu, sd, o);
-        }
-        if ((threadIdx.x & 31) == 0 && alg) {
-            atomicAdd(&S.alg, alg);
-            atomicAdd(&S.sd, sd);
         }
     }
     __syncthreads();
@@ -264,12 +291,8 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     const uint64_t total = S.total, ltotal = S.ltotal;
     const uint64_t r0 = tile * kTileRows;
     if (threadIdx.x < 32) {
-        const uint64_t ex = resolve_prefix(a.status, a.ctl, tile, total, epoch);
-        if (threadIdx.x == 0) {
-            *s_excl = ex;
-            atomicAdd(&a.ctl->alg_bytes, S.alg);
-            atomicAdd(&a.ctl->sum_deg, S.sd);
-        }
+        const uint64_t ex = resolve_prefix(a.status, a.ctl, tile, total, epoch, spin_limit(a));
+        if (threadIdx.x == 0) *s_excl = ex;
     }
     if (wi) mbar_wait(bar, phase, &a.ctl->err);   // the tile's rows are in shared memory
     __syncthreads();
@@ -402,6 +425,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
         mbar_init(&s_bar[1], 1);
     }
     unsigned phases = 0;   // mbarrier phase bit of each tile buffer
+    unsigned long long acc_alg = 0, acc_sd = 0;   // this thread's share of the byte accounting
 
     // Two tiles in flight per CTA: the front half of the next tile runs before the back half
     // of the current one, so the look-back and the row copy of one overlap the other's probes.
@@ -411,7 +435,8 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     int b = 0;
     WK_PH(0);
     if (cur < ntiles)
-        tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], phases & 1u, cur, R, wi, epoch, s_warp);
+        tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], phases & 1u, cur, R, wi, epoch, s_warp,
+                      acc_alg, acc_sd);
     while (cur < ntiles) {
         if (threadIdx.x == 0) s_claim = atomicAdd(&a.ctl->tile_counter, 1ull);
         __syncthreads();
@@ -419,7 +444,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
         WK_PH(0);
         if (next < ntiles)
             tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1],
-                          (phases >> (b ^ 1)) & 1u, next, R, wi, epoch, s_warp);
+                          (phases >> (b ^ 1)) & 1u, next, R, wi, epoch, s_warp, acc_alg, acc_sd);
         tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
                      wo, chunk_rows, epoch, s_pos, s_out, &s_excl, obase);
         if (wi) phases ^= 1u << b;
@@ -457,7 +482,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
                     }
                     continue;
                 }
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit(a)) {
                     atomicOr(&a.ctl->err, kErrTimeout);
                     state = 2;
                     break;
@@ -496,6 +521,15 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     }
     WK_PH(7);
     WK_PH_FLUSH;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_alg += __shfl_xor_sync(0xffffffffu, acc_alg, o);
+        acc_sd += __shfl_xor_sync(0xffffffffu, acc_sd, o);
+    }
+    if ((threadIdx.x & 31) == 0 && acc_alg) {
+        atomicAdd(&a.ctl->alg_bytes, acc_alg);
+        atomicAdd(&a.ctl->sum_deg, acc_sd);
+    }
     exit_protocol(a.ctl, a.status, epoch, a.heavy ? &a.heavy[0].tag : nullptr,
                   sizeof(HeavyItem) / sizeof(uint32_t), a.heavy ? a.heavy_cap : 0);
 }

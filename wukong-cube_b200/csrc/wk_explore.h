@@ -83,7 +83,13 @@ struct ExploreArgs {
     // When nonzero and the input has at least this many rows, the launch does nothing (the
     // flat pipeline of wk_flat.cu runs the step instead).
     uint64_t max_rows;
+    // Polls a look-back on a predecessor tile or a wait for the slice queue makes before it
+    // gives up and sets kErrTimeout (0: kDefaultSpinLimit).  Tests lower it to make the waits
+    // run out; the wait for the launch's own bulk copies keeps its fixed limit.
+    uint64_t spin_limit;
 };
+
+constexpr uint64_t kDefaultSpinLimit = 1ull << 24;
 
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows);
 cudaError_t explore_kernel_attrs();

@@ -218,6 +218,10 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     WKF_CUDA(ctx, cudaMemcpyAsync(ctx->h_rows, in->d_rows, 8, cudaMemcpyDeviceToHost, s));
     WKF_CUDA(ctx, cudaStreamSynchronize(s));
     R = ctx->h_rows[0];
+    // a row count past the capacity marks a table whose writing step overflowed: refused before
+    // any launch (and before any scratch is sized from it), as wk_table_download refuses it
+    if (cols > 0 && R > in->cap / (uint64_t)cols)
+        return ctx->fail(WK_E_CORRUPT, "row count beyond table capacity");
     if (R == 0) {   // an empty table is left as it is, columns included (sparql.hpp:1420-1421)
         int rc = ctx->table_reserve(out, 1);
         if (rc) return rc;
@@ -238,7 +242,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     const size_t bytes = keep_bytes + 2 * (size_t)n * 4 + (size_t)kDigits * grid * 4 +
                          ((size_t)grid + 2) * 4 + 64;
     char* scratch = nullptr;
-    if (cudaMalloc(&scratch, bytes) != cudaSuccess) {
+    if (wk::dev_malloc(&scratch, bytes) != cudaSuccess) {
         cudaGetLastError();
         return ctx->fail(WK_E_OOM, "post-pattern scratch");
     }

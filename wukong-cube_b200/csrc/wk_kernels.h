@@ -64,6 +64,16 @@ cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream
 cudaError_t launch_random_reads(const void* buf, uint64_t bytes, int per, uint64_t seed,
                                 uint32_t* sink, int grid, cudaStream_t s);
 
+// Every device allocation of the library goes through dev_malloc, which counts it, so a caller
+// (and the tests) can see that a call allocated nothing (wk_debug_device_allocs).
+uint64_t device_alloc_count();
+void note_device_alloc();
+template <class T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+    note_device_alloc();
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
 // Every kernel of the library asks for the same L1 / shared-memory split, the largest shared
 // carveout.  The split is an SM-wide setting, so CTAs of launches that ask for different
 // splits cannot share an SM; with one split everywhere, a serving lane's launches and the

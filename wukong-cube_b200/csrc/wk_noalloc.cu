@@ -8,11 +8,14 @@
 // variant runs the same exploration launch with its scan scratch in one fixed device array of
 // this file, and fails with WK_E_CAPACITY where the other entry point would allocate.
 //
-// Limits: inputs up to kNoAllocTiles * kTileRows rows (16,384 tiles of 256 rows = 4,194,304
-// rows) and up to kNoAllocSlices long-list slices (8,192 slices of 2,048 output rows); the output
-// table must already hold the step's result.  The scratch is one array per device, shared by
-// every context and stream of that device, so calls that overlap in time on one device race and
-// the caller must serialise them.
+// Limits: inputs up to (kNoAllocTiles - 2) * kTileRows rows (16,382 tiles of 256 rows =
+// 4,193,792 rows; the status array keeps the two spare words the allocating path keeps) and up
+// to kNoAllocSlices long-list slices.  Every row whose list is longer than the context's slice
+// threshold (128 rows unless tuned) takes ceil(length / 2,048) slices, so 8,192 slices hold
+// between 8,192 such rows (about 1 M output rows at 129 rows each) and 16.7 M output rows of
+// long lists.  The output table must already hold the step's result.  The scratch is one array
+// per device, shared by every context and stream of that device, so calls that overlap in time
+// on one device race and the caller must serialise them.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -56,23 +59,39 @@ __global__ void noalloc_init_kernel(unsigned long long* base) {
     }
 }
 
-// Once per device, with that device current: the scratch's address, and its first clearing.
+// The set-up of one device, with that device current: the scratch's address and its first
+// clearing.
+int scratch_setup(wk_ctx* ctx, char** out) {
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaSetDevice");
+    void* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    e = wk::use_max_shared_carveout(noalloc_init_kernel);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "no-alloc kernel attribute");
+    noalloc_init_kernel<<<64, 256, 0, ctx->stream>>>((unsigned long long*)p);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return ctx->cuda_fail(e, "no-alloc scratch set-up");
+    *out = (char*)p;
+    return WK_SUCCESS;
+}
+
+// Once per device: the set-up above, after which the calling thread's current device is what
+// it was before the call, on success and on failure alike.
 int scratch_for(wk_ctx* ctx, char** out) {
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (ctx->device < 0 || ctx->device >= kMaxDevices) return ctx->fail(WK_E_BADARG, "device id");
     if (!g_scratch[ctx->device]) {
-        cudaError_t e = cudaSetDevice(ctx->device);
-        if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaSetDevice");
-        void* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        e = wk::use_max_shared_carveout(noalloc_init_kernel);
-        if (e != cudaSuccess) return ctx->cuda_fail(e, "no-alloc kernel attribute");
-        noalloc_init_kernel<<<64, 256, 0, ctx->stream>>>((unsigned long long*)p);
-        e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) return ctx->cuda_fail(e, "no-alloc scratch set-up");
-        g_scratch[ctx->device] = (char*)p;
+        int prev = 0;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaGetDevice");
+        char* p = nullptr;
+        const int rc = scratch_setup(ctx, &p);
+        e = cudaSetDevice(prev);
+        if (rc) return rc;
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "cudaSetDevice (restoring the caller's device)");
+        g_scratch[ctx->device] = p;
     }
     *out = g_scratch[ctx->device];
     return WK_SUCCESS;
@@ -100,6 +119,10 @@ extern "C" int wk_step_known_to_unknown_noalloc(wk_ctx* ctx, const wk_table* in,
     cudaError_t e = cudaMemcpyAsync(&rows, in->d_rows, sizeof(rows), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "input row count");
+    // a row count past the table's capacity marks a table whose writing step overflowed
+    if (rows * (uint64_t)in->cols > in->cap)
+        return ctx->fail(WK_E_CORRUPT, "input row count " + std::to_string(rows) +
+                                           " beyond the table's capacity (the step that wrote it overflowed)");
     if ((rows + wk::kTileRows - 1) / wk::kTileRows + 2 > kNoAllocTiles)
         return ctx->fail(WK_E_CAPACITY, "input has " + std::to_string(rows) + " rows; the no-alloc step takes at most " +
                                             std::to_string((kNoAllocTiles - 2) * wk::kTileRows));
@@ -131,8 +154,12 @@ extern "C" int wk_step_known_to_unknown_noalloc(wk_ctx* ctx, const wk_table* in,
     a.status = status;
     a.sorted_lists = ctx->sorted_lists;
     a.lanes = ctx->lanes_for(a.one.op, st.in_cols);
+    a.slice_rows = ctx->slice_rows;
+    a.spin_limit = ctx->spin_limit;
     out->cols = st.out_cols;
-    const int grid = wk::explore_blocks_per_sm(st.in_cols, st.out_cols, a.lanes) * ctx->sm_count;
+    // the same launch shape as wk_step_known_to_unknown's tile launch (a serving lane's context
+    // leaves room on every SM for the iteration launches)
+    const int grid = ctx->blocks_per_sm(a.one.op, st.in_cols, a.lanes) * ctx->sm_count;
     e = wk::launch_explore(a, grid, ctx->stream);
     if (e != cudaSuccess) return ctx->cuda_fail(e, "no-alloc exploration launch");
 

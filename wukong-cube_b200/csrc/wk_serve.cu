@@ -168,8 +168,8 @@ struct Serve {
         d_arena[k] = nullptr;
         d_owner[k] = nullptr;
         rows = (rows + 15) & ~15ull;
-        if (cudaMalloc(&d_arena[k], rows * w * 4 + 256) != cudaSuccess ||
-            cudaMalloc(&d_owner[k], rows * 4 + 64) != cudaSuccess) {
+        if (wk::dev_malloc(&d_arena[k], rows * w * 4 + 256) != cudaSuccess ||
+            wk::dev_malloc(&d_owner[k], rows * 4 + 64) != cudaSuccess) {
             cudaGetLastError();
             return ctx->fail(WK_E_OOM, "serving arena");
         }
@@ -182,7 +182,7 @@ struct Serve {
         if (h_result) cudaFreeHost(h_result);
         d_result = nullptr;
         h_result = nullptr;
-        if (cudaMalloc(&d_result, elems * 4 + 64) != cudaSuccess ||
+        if (wk::dev_malloc(&d_result, elems * 4 + 64) != cudaSuccess ||
             cudaMallocHost(&h_result, elems * 4 + 64) != cudaSuccess) {
             cudaGetLastError();
             return ctx->fail(WK_E_OOM, "serving result buffer");
@@ -195,7 +195,7 @@ struct Serve {
         slots_n = slots;
         w = std::max(width, 1);
         auto dm = [&](void** p, size_t bytes) {
-            if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+            if (wk::dev_malloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
                 cudaGetLastError();
                 return false;
             }
@@ -246,6 +246,7 @@ struct Serve {
         a.sorted_lists = ctx->sorted_lists;
         a.lanes = ctx->batch_lanes;
         a.slice_rows = ctx->batch_slice_rows;
+        a.spin_limit = ctx->spin_limit;
         return a;
     }
 

@@ -88,7 +88,7 @@ extern "C" int wk_measure_random_reads(wk_ctx* ctx, uint64_t region_bytes, int32
         if (sink) cudaFree(sink);
         return rc;
     };
-    if (cudaMalloc(&buf, region_bytes) != cudaSuccess || cudaMalloc(&sink, 4) != cudaSuccess) {
+    if (wk::dev_malloc(&buf, region_bytes) != cudaSuccess || wk::dev_malloc(&sink, 4) != cudaSuccess) {
         cudaGetLastError();
         return done(ctx->fail(WK_E_OOM, "random-read calibration buffer"));
     }

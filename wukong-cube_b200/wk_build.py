@@ -2,6 +2,9 @@
 
 Compiles in-tree so the shared objects travel with the repository snapshot:
   wukong-cube_b200/libwukong_b200.so   the product: kernels + C ABI (include/wukong_b200.h)
+  wukong-cube_b200/libwk_synth.so      the synthetic-graph generator alone (wk_synth.cpp), for
+                                       callers that need the workload without the product
+                                       (the bench's CPU reference arm)
   oracle/liboracle.so                  the CPU checker (test infrastructure only)
 """
 import os
@@ -72,6 +75,19 @@ def build_lib(verbose=False, force=False, variant=None, defines=()):
     return lib
 
 
+SYNTH_LIB = os.path.join(HERE, "libwk_synth.so")
+
+
+def build_synth(force=False):
+    """The generator on its own: the same wk_synth.cpp the product links, as a small library."""
+    src = os.path.join(CSRC, "wk_synth.cpp")
+    deps = [src] + [os.path.join(CSRC, h) for h in ("wk_format.h", "wk_internal.h")] + \
+        [os.path.join(ROOT, "include", "wukong_b200.h")]
+    if force or _stale(SYNTH_LIB, deps):
+        _run([CXX, "-O3", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", SYNTH_LIB, src])
+    return SYNTH_LIB
+
+
 def build_oracle():
     _run(["make", "-s", "-C", ORACLE_DIR])
     return os.path.join(ORACLE_DIR, "liboracle.so")
@@ -79,4 +95,5 @@ def build_oracle():
 
 if __name__ == "__main__":
     print(build_lib(verbose="-v" in sys.argv, force="-f" in sys.argv))
+    print(build_synth(force="-f" in sys.argv))
     print(build_oracle())

@@ -21,6 +21,7 @@ NO_RESULT = 0xFFFF
 MODE_PLAIN, MODE_RESIDENT, MODE_GRAPH = 0, 1, 2
 KNOB_LANES, KNOB_BATCH_LANES, KNOB_SLICE_ROWS, KNOB_BATCH_SLICE_ROWS, KNOB_FLAT_ROWS = 0, 1, 2, 3, 4
 KNOB_BATCH_FLAT = 5
+KNOB_SPIN_LIMIT = 6
 
 SUCCESS = 0
 UNKNOWN_PATTERN = 3
@@ -175,6 +176,7 @@ _SIGS = {
     "wk_batch_replay": (C.c_int, [_P]),
     "wk_debug_phase_cycles": (C.c_int, [C.POINTER(C.c_ulonglong), C.c_int32, C.c_int32]),
     "wk_debug_fail_next": (C.c_int, [_P, C.c_uint32]),
+    "wk_debug_device_allocs": (C.c_int, [C.POINTER(C.c_uint64)]),
     "wk_ctx_tune_set": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "wk_ctx_tune_get": (C.c_int, [_P, C.c_int32, C.POINTER(C.c_int32)]),
     "wk_ctx_autotune": (C.c_int, [_P, C.POINTER(QueryC), C.c_uint32, C.c_int32, C.POINTER(TuneResult)]),
@@ -221,9 +223,30 @@ def _ptr(a):
 
 
 # ---------------------------------------------------------------- synthetic graph + host store
-def synth_generate(n_orgs, seed=0, zipf=False, zipf_s=1.1):
-    """Seeded LUBM-shaped triples as an (n, 3) uint32 array and the id vocabulary."""
-    L = lib()
+SYNTH_LIB_PATH = os.path.join(HERE, "libwk_synth.so")
+_synth_lib = None
+
+
+def _synth_only_lib():
+    """The generator's own small library (libwk_synth.so: wk_synth.cpp alone)."""
+    global _synth_lib
+    if _synth_lib is None:
+        if not os.path.exists(SYNTH_LIB_PATH):
+            raise RuntimeError("libwk_synth.so is not built: run wukong-cube_b200/wk_build.py")
+        L = C.CDLL(SYNTH_LIB_PATH)
+        for name in ("wk_synth_generate", "wk_free"):
+            f = getattr(L, name)
+            f.restype, f.argtypes = _SIGS[name]
+        _synth_lib = L
+    return _synth_lib
+
+
+def synth_generate(n_orgs, seed=0, zipf=False, zipf_s=1.1, generator_only=False):
+    """Seeded LUBM-shaped triples as an (n, 3) uint32 array and the id vocabulary.
+
+    generator_only: use libwk_synth.so (the generator alone) instead of the product library,
+    so that a process that only needs the workload does not load the product."""
+    L = _synth_only_lib() if generator_only else lib()
     p = SynthParams(seed, n_orgs, 1 if zipf else 0, zipf_s)
     buf = C.POINTER(C.c_uint32)()
     n = C.c_uint64()
@@ -345,6 +368,13 @@ class Query:
 
 PHASES = ["claim", "stage", "probe_tail", "scan", "lookback", "ranges", "write", "drain",
           "probe_setup", "probe_walk", "membership", "spare"]
+
+
+def device_allocs():
+    """Device allocations the library has made in this process (wk_debug_device_allocs)."""
+    n = C.c_uint64()
+    _check(lib().wk_debug_device_allocs(C.byref(n)))
+    return n.value
 
 
 def phase_cycles(reset=True):
