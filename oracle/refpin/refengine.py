@@ -1,0 +1,115 @@
+"""CHECKER OF THE ORACLE — test infrastructure only: ctypes wrapper of oracle/_ref/libwkref.so,
+the reference's own CPU engine (src/core/engine/sparql.hpp and the headers it includes, compiled
+unmodified from the reference tree by oracle/Makefile against oracle/refpin/stubs).
+
+Only the golden-fixture script (tests/golden/make_ref_golden.py) and tests use it.  The library
+exists only where the reference tree was present when it was built.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "_ref", "libwkref.so")
+_lib = None
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.wkref_graph_new.restype = P
+        L.wkref_graph_free.argtypes = [P]
+        L.wkref_graph_put.argtypes = [P, C.c_uint32, C.c_uint32, C.c_int, P, C.c_uint64]
+        L.wkref_query.argtypes = [P, P, C.c_int, C.c_int, P, C.c_int, C.c_int, C.c_int, C.c_uint32,
+                                  C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_int), P]
+        L.wkref_free.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+class RefGraph:
+    """A graph the reference engine reads: every key's list as given (get_triples / get_index)."""
+
+    def __init__(self):
+        self.h = lib().wkref_graph_new()
+
+    def put(self, vid, pid, d, vals):
+        vals = np.ascontiguousarray(vals, dtype=np.uint32)
+        lib().wkref_graph_put(self.h, vid, pid, d, _p(vals), vals.size)
+
+    def close(self):
+        if self.h:
+            lib().wkref_graph_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def run(self, query_flat, nvars, required=None, distinct=False, limit=-1, offset=0):
+        """Run one planned query through SPARQLEngine::execute_sparql_query.
+        Returns (status, table, v2c)."""
+        q = np.ascontiguousarray(query_flat, dtype=np.int32)
+        req = np.array(required if required is not None else [-(i + 1) for i in range(nvars)], np.int32)
+        tab = C.POINTER(C.c_uint32)()
+        rows = C.c_uint64()
+        cols = C.c_int()
+        v2c = np.zeros(max(nvars, 1), np.int32)
+        rc = lib().wkref_query(self.h, _p(q), q.shape[0], nvars, _p(req), req.size, int(distinct),
+                               limit, offset, C.byref(tab), C.byref(rows), C.byref(cols), _p(v2c))
+        if rc:
+            return rc, None, None
+        n = rows.value * cols.value
+        try:
+            t = np.ctypeslib.as_array(tab, shape=(max(n, 1),))[:n].copy().reshape(rows.value, cols.value)
+        finally:
+            lib().wkref_free(tab)
+        return 0, t, list(v2c[:nvars])
+
+
+def graph_from_store(store, triples, vocab):
+    """A RefGraph holding every key of `triples` with the lists `store` (anything with
+    get_triples / get_index) answers: normal keys [s|p|OUT], [o|p|IN] (type triples only OUT),
+    the type index [0|t|IN] and the predicate indexes [0|p|IN], [0|p|OUT]."""
+    g = RefGraph()
+    seen = set()
+    for s, p, o in triples:
+        s, p, o = int(s), int(p), int(o)
+        for key in ((s, p, 1), (o, p, 0)):
+            if key[2] == 0 and p == 1:
+                continue
+            if key not in seen:
+                seen.add(key)
+                g.put(key[0], key[1], key[2], store.get_triples(*key))
+    preds = sorted(set(int(x) for x in np.unique(triples[:, 1])))
+    types = sorted(set(int(x) for x in np.unique(triples[triples[:, 1] == 1][:, 2])))
+    for t in types:
+        g.put(0, t, 0, store.get_index(t, 0))
+    for p in preds:
+        if p == 1:
+            continue
+        for d in (0, 1):
+            g.put(0, p, d, store.get_index(p, d))
+    return g
+
+
+def bound_vars(query_flat):
+    """The variables a planned pattern list binds, in the order their columns are added (the
+    object of an index or constant start, then the object of each known_to_unknown step).
+    Asking the final stage for exactly these keeps its projection (sparql.hpp:1500-1529) the
+    identity, so the reference's table is the pattern stage's table."""
+    bound = []
+    for s, p, o, d, t in np.asarray(query_flat).reshape(-1, 5):
+        if o < 0 and o not in bound:
+            bound.append(int(o))
+    return bound

@@ -1,0 +1,2 @@
+#pragma once
+#include "boost/serialization/wk_stub_serialization.hpp"

@@ -5,7 +5,7 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "wukong-cube_b200")
-for p in (PKG, os.path.join(ROOT, "oracle"), ROOT):
+for p in (PKG, os.path.join(ROOT, "oracle"), os.path.join(ROOT, "oracle", "refpin"), ROOT):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -88,8 +88,15 @@ def build_synth(force=False):
     return SYNTH_LIB
 
 
+REFERENCE_TREE = "/root/reference"
+
+
 def build_oracle():
+    """The oracle, and where the reference tree is present the reference's own engine
+    (oracle/_ref/libwkref.so, the oracle's checker); elsewhere a copy built before travels."""
     _run(["make", "-s", "-C", ORACLE_DIR])
+    if os.path.isdir(os.path.join(REFERENCE_TREE, "src")):
+        _run(["make", "-s", "-C", ORACLE_DIR, "ref", "REF=" + REFERENCE_TREE])
     return os.path.join(ORACLE_DIR, "liboracle.so")
 
 
