@@ -255,6 +255,15 @@ int wk_table_shape(wk_ctx* ctx, const wk_table* t, uint64_t* rows, int32_t* cols
  * the ids' strings in the reference and is not offered. */
 int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int32_t* keep_cols, int32_t n_keep,
                            int32_t distinct, int64_t offset, int64_t limit, wk_table* out);
+/* The BOUND filters of a query on the device: SPARQLEngine::bound_filter (sparql.hpp:1222-1234)
+ * for each column in bound_cols, ANDed as execute_filter applies a query's filters
+ * (sparql.hpp:1356-1376).  A row of `in` is kept when none of those columns holds BLANK_ID
+ * (0xFFFFFFFF, an unbound variable); kept rows keep their order and all their columns and go to
+ * `out` (grown as needed; not `in`).  n_bound == 0 copies the table.  At most 64 columns;
+ * WK_E_BADARG for a column out of range, WK_E_CORRUPT for an input whose row count is past its
+ * capacity. */
+int wk_table_filter_bound(wk_ctx* ctx, const wk_table* in, const int32_t* bound_cols, int32_t n_bound,
+                          wk_table* out);
 /* Device address of the table's first element (for callers that keep data on the GPU). */
 int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dptr);
 

@@ -240,3 +240,17 @@ def final_process(table, keep_cols, distinct=False, offset=0, limit=-1):
         rows = rows[:limit]
     out = np.array([[r[c] for c in keep_cols] for r in rows], dtype=np.int32).reshape(-1, len(keep_cols))
     return out.view(np.uint32)
+
+
+BLANK_ID = 0xFFFFFFFF
+
+
+def bound_filter(table, bound_cols):
+    """The BOUND filters of a query: SPARQLEngine::bound_filter (sparql.hpp:1222-1234) for each
+    column, ANDed as execute_filter applies them (sparql.hpp:1356-1376): a row is kept when none
+    of the columns holds BLANK_ID; kept rows keep their order."""
+    t = np.asarray(table, dtype=np.uint32)
+    keep = np.ones(t.shape[0], bool)
+    for c in bound_cols:
+        keep &= t[:, c] != BLANK_ID
+    return t[keep]

@@ -113,6 +113,46 @@ int wkref_query(void* g, const int32_t* pats, int n, int nvars, const int32_t* r
     return SUCCESS;
 }
 
+// The engine's filter stage on a given table (rows x cols, variable -(c+1) in column c): one
+// BOUND(?x) filter per column in bound_cols (Filter::Builtin_bound over a Variable argument),
+// run through execute_sparql_query with no patterns, so execute_filter and then final_process
+// (identity projection) apply.  *out (malloc'd) receives the kept rows.
+int wkref_filter_bound(const uint32_t* table, uint64_t rows, int cols, const int32_t* bound_cols, int nb,
+                       uint32_t** out, uint64_t* out_rows) {
+    SPARQLQuery::PatternGroup group;
+    for (int k = 0; k < nb; ++k) {
+        SPARQLQuery::Filter f;
+        f.type = SPARQLQuery::Filter::Type::Builtin_bound;
+        f.arg1 = new SPARQLQuery::Filter();
+        f.arg1->type = SPARQLQuery::Filter::Type::Variable;
+        f.arg1->valueArg = -(bound_cols[k] + 1);
+        group.filters.push_back(f);
+    }
+    std::vector<ssid_t> req;
+    for (int c = 0; c < cols; ++c) req.push_back(-(c + 1));
+    SPARQLQuery q(group, cols, req);
+    for (int c = 0; c < cols; ++c) q.result.add_var2col(-(c + 1), c);
+    q.result.set_col_num(cols);
+    q.result.result_table.assign(table, table + rows * (uint64_t)cols);
+    q.result.update_nrows();
+    q.pqid = 0;
+    Coder coder(0, 1);
+    Messenger msgr;
+    StringMapping str;
+    SPARQLEngine engine(0, 1, &str, nullptr, &coder, &msgr);
+    engine.execute_sparql_query(q);
+    if (msgr.replies.size() != 1) return UNKNOWN_ERROR;
+    SPARQLQuery& r = msgr.replies[0];
+    if (r.result.get_status_code() != SUCCESS) return r.result.get_status_code();
+    const uint64_t nr = r.result.get_row_num();
+    uint32_t* o = (uint32_t*)std::malloc(std::max<uint64_t>(nr * cols, 1) * sizeof(uint32_t));
+    if (!o) return UNKNOWN_ERROR;
+    for (uint64_t i = 0; i < nr * (uint64_t)cols; ++i) o[i] = r.result.result_table[i];
+    *out = o;
+    *out_rows = nr;
+    return SUCCESS;
+}
+
 void wkref_free(void* p) { std::free(p); }
 
 }  // extern "C"

@@ -31,6 +31,8 @@ def lib():
                                   C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_int), P]
         L.wkref_free.argtypes = [P]
+        L.wkref_filter_bound.argtypes = [P, C.c_uint64, C.c_int, P, C.c_int,
+                                         C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]
         _lib = L
     return _lib
 
@@ -113,3 +115,21 @@ def bound_vars(query_flat):
         if o < 0 and o not in bound:
             bound.append(int(o))
     return bound
+
+
+def filter_bound(table, bound_cols):
+    """The reference engine's filter stage with one BOUND filter per column of bound_cols, on a
+    given row-major uint32 table (execute_filter, sparql.hpp:1356-1376)."""
+    t = np.ascontiguousarray(table, dtype=np.uint32)
+    cols = np.array(bound_cols, np.int32)
+    out = C.POINTER(C.c_uint32)()
+    rows = C.c_uint64()
+    rc = lib().wkref_filter_bound(_p(t), t.shape[0], t.shape[1], _p(cols), cols.size, C.byref(out),
+                                  C.byref(rows))
+    if rc:
+        raise RuntimeError("reference filter status %d" % rc)
+    n = rows.value * t.shape[1]
+    try:
+        return np.ctypeslib.as_array(out, shape=(max(n, 1),))[:n].copy().reshape(rows.value, t.shape[1])
+    finally:
+        lib().wkref_free(out)

@@ -6,7 +6,8 @@ headers it includes, compiled unmodified from the reference tree (oracle/Makefil
 "ref") against stand-ins for the Boost / TBB / network names the pattern operators do not use.
 Each query runs through SPARQLEngine::execute_sparql_query, so the patterns go through the
 reference's own dispatch and operators (sparql.hpp:197-552, 932-1055) and the modifiers through
-its own final_process (:1419-1546).  The engine reads a graph that serves, for every key, the
+its own final_process (:1419-1546); tables with planted BLANK_IDs go through its filter stage
+with BOUND filters (execute_filter, :1356-1376).  The engine reads a graph that serves, for every key, the
 list the oracle's store holds (the store's construction is pinned separately by the reference's
 tests/test_graph.cc answers, tests/test_oracle_known_answers.py).
 
@@ -75,6 +76,29 @@ def final_cases(v, inst):
             ("star_distinct_limit_offset", star, [-3, -2], True, 25, 10)]
 
 
+def bound_cases(o, v, inst):
+    """(name, table, bound columns) for the BOUND filter: tables of real rows with BLANK_ID
+    (an unbound variable, as OPTIONAL leaves it) planted at seeded random places."""
+    import workloads
+    rng = np.random.default_rng(11)
+    units = inst[v["t_unit"]]
+    _, chain, _ = o.run(workloads.small_chain(v, int(units[1])).flat(), 2)
+    base = np.concatenate([chain[:90], chain[:90, :1]], axis=1).astype(np.uint32)   # 3 columns
+    blank = 0xFFFFFFFF
+    t1 = base.copy()
+    t1[rng.random(t1.shape) < 0.15] = blank
+    t2 = base.copy()
+    t2[:, 2] = blank
+    t3 = base[:0].copy()
+    return [("one_column", t1, [1]),
+            ("two_columns", t1, [0, 2]),
+            ("every_column", t1, [0, 1, 2]),
+            ("column_all_blank", t2, [2]),
+            ("column_all_blank_not_asked", t2, [0]),
+            ("no_filter_columns", t1, []),
+            ("empty_table", t3, [0])]
+
+
 def main():
     import oracle
     import refengine
@@ -108,9 +132,16 @@ def main():
                              "limit": limit, "offset": offset, "rows": int(rows.shape[0]),
                              "cols": int(rows.shape[1]), "table_sha256": digest(rows),
                              "head": rows[:3].tolist()})
+    doc["bound"] = []
+    for name, table, bcols in bound_cases(o, v, inst):
+        got = refengine.filter_bound(table, bcols)
+        doc["bound"].append({"name": name, "table": table.tolist(), "cols": int(table.shape[1]),
+                             "bound_cols": bcols, "rows": int(got.shape[0]),
+                             "table_sha256": digest(got)})
     with open(OUT, "w") as f:
         json.dump(doc, f, indent=1)
-    print("wrote", OUT, len(doc["queries"]), "queries,", len(doc["final"]), "final-stage cases")
+    print("wrote", OUT, len(doc["queries"]), "queries,", len(doc["final"]), "final-stage cases,",
+          len(doc["bound"]), "BOUND cases")
 
 
 if __name__ == "__main__":

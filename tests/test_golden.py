@@ -152,3 +152,45 @@ def test_gpu_final_stage_reproduces_reference(ctx, golden):
         assert _digest(got) == g["table_sha256"], g["name"]
         out.free()
         tin.free()
+
+
+def test_oracle_bound_filter_reproduces_reference(built, golden):
+    import oracle
+    for g in golden["bound"]:
+        t = np.array(g["table"], np.uint32).reshape(-1, g["cols"])
+        got = oracle.bound_filter(t, g["bound_cols"])
+        assert got.shape[0] == g["rows"], g["name"]
+        assert _digest(got) == g["table_sha256"], g["name"]
+
+
+@pytest.mark.gpu
+def test_gpu_bound_filter_reproduces_reference(ctx, golden):
+    for g in golden["bound"]:
+        t = np.array(g["table"], np.uint32).reshape(-1, g["cols"])
+        tin = ctx.table(t, capacity=max(t.size, 1))
+        for _ in range(2):   # a second call on the same context gives the same rows
+            out = tin.filter_bound(g["bound_cols"])
+            got = out.download()
+            assert got.shape == (g["rows"], g["cols"]), g["name"]
+            assert _digest(got) == g["table_sha256"], g["name"]
+            out.free()
+        tin.free()
+
+
+@pytest.mark.gpu
+def test_gpu_bound_filter_large_and_refusals(ctx):
+    """Many CTAs' chunks (order kept across them), and the refusals."""
+    import oracle
+    import wukong_b200 as wk
+    rng = np.random.default_rng(5)
+    t = rng.integers(1 << 17, 1 << 20, size=(300_000, 4), dtype=np.uint32)
+    t[rng.random(t.shape) < 0.3] = 0xFFFFFFFF
+    want = oracle.bound_filter(t, [1, 3])
+    tin = ctx.table(t, capacity=t.size)
+    out = tin.filter_bound([1, 3])
+    assert np.array_equal(out.download(), want)
+    with pytest.raises(wk.WukongError) as e:
+        tin.filter_bound([4])
+    assert e.value.code == wk.E_BADARG
+    out.free()
+    tin.free()

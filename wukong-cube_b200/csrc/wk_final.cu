@@ -190,6 +190,70 @@ __global__ void __launch_bounds__(kFinThreads) project_kernel(const uint32_t* ta
     if (blockIdx.x == 0 && threadIdx.x == 0) *out_rows = count;
 }
 
+// ---------------------------------------------------------------- BOUND filter
+// SPARQLEngine::bound_filter (sparql.hpp:1222-1234) for every BOUND(?x) of a query at once, as
+// execute_filter ANDs them (:1356-1376): a row survives when none of the named columns holds
+// BLANK_ID, and the survivors keep their order (append_row_to in row order).
+struct BoundArgs {
+    const uint32_t* table;
+    int cols;
+    const int32_t* bcols;   // columns that must be bound
+    int nb;
+    uint32_t n;
+    uint32_t* part;         // [grid + 1] survivors per CTA, then their exclusive scan
+    uint32_t* out;
+};
+
+__device__ __forceinline__ bool row_bound(const BoundArgs& a, uint32_t i) {
+    const uint32_t* r = a.table + (uint64_t)i * a.cols;
+    for (int k = 0; k < a.nb; ++k)
+        if (__ldg(r + a.bcols[k]) == kBlankId) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(kFinThreads) bound_count_kernel(const BoundArgs a) {
+    __shared__ uint64_t s_warp[kFinThreads / 32];
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    uint64_t c = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads) c += row_bound(a, i);
+    const uint64_t ex = block_exclusive_sum<kFinThreads>(c, s_warp);
+    if (threadIdx.x == kFinThreads - 1) a.part[blockIdx.x] = (uint32_t)(ex + c);
+}
+
+// Each CTA walks its chunk 256 rows at a time; a surviving row goes to its CTA's offset plus the
+// survivors before it, and its words are copied by consecutive threads.
+__global__ void __launch_bounds__(kFinThreads) bound_place_kernel(const BoundArgs a) {
+    __shared__ uint64_t s_warp[kFinThreads / 32];
+    __shared__ uint64_t s_carry;
+    __shared__ uint32_t s_src[kFinThreads], s_dst[kFinThreads];
+    __shared__ uint32_t s_m;
+    uint32_t lo, hi;
+    chunk(a.n, &lo, &hi);
+    if (threadIdx.x == 0) s_carry = a.part[blockIdx.x];
+    __syncthreads();
+    for (uint32_t base = lo; base < hi; base += kFinThreads) {
+        const uint32_t i = base + threadIdx.x;
+        const uint64_t m = i < hi ? row_bound(a, i) : 0;
+        const uint64_t ex = block_exclusive_sum<kFinThreads>(m, s_warp);
+        const uint64_t carry = s_carry;
+        if (m) {
+            s_src[ex] = i;
+            s_dst[ex] = (uint32_t)(carry + ex);
+        }
+        if (threadIdx.x == kFinThreads - 1) s_m = (uint32_t)(ex + m);
+        __syncthreads();
+        const uint32_t cnt = s_m;
+        for (uint32_t e = threadIdx.x; e < cnt * (uint32_t)a.cols; e += kFinThreads) {
+            const uint32_t j = e / a.cols, c = e - j * a.cols;
+            a.out[(uint64_t)s_dst[j] * a.cols + c] = __ldg(a.table + (uint64_t)s_src[j] * a.cols + c);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry = carry + cnt;
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 cudaError_t final_kernel_attrs() {
@@ -200,6 +264,8 @@ cudaError_t final_kernel_attrs() {
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_count_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_place_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(project_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(bound_count_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(bound_place_kernel);
     return e;
 }
 
@@ -294,5 +360,63 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     project_kernel<<<pgrid, kFinThreads, 0, s>>>(in->d, cols, d_keep, n_keep, idx, start, count, out->d,
                                                  out->d_rows);
     if ((e = cudaGetLastError()) != cudaSuccess) return done(ctx->cuda_fail(e, "projection launch"));
+    return done(WK_SUCCESS);
+}
+
+extern "C" int wk_table_filter_bound(wk_ctx* ctx, const wk_table* in, const int32_t* bound_cols,
+                                     int32_t n_bound, wk_table* out) {
+    using namespace wk;
+    if (!ctx || !in || !out || in == out || (!bound_cols && n_bound) || n_bound < 0) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n_bound > 64) return ctx->fail(WK_E_BADARG, "at most 64 bound columns");
+    const int cols = in->cols;
+    cudaStream_t s = ctx->stream;
+    WKF_CUDA(ctx, cudaMemcpyAsync(ctx->h_rows, in->d_rows, 8, cudaMemcpyDeviceToHost, s));
+    WKF_CUDA(ctx, cudaStreamSynchronize(s));
+    const uint64_t R = ctx->h_rows[0];
+    if (cols > 0 && R > in->cap / (uint64_t)cols)
+        return ctx->fail(WK_E_CORRUPT, "row count beyond table capacity");
+    for (int k = 0; k < n_bound; ++k)
+        if (bound_cols[k] < 0 || bound_cols[k] >= cols) return ctx->fail(WK_E_BADARG, "bound column out of range");
+    if (R >= (1ull << 32)) return ctx->fail(WK_E_CAPACITY, "table too long for the filter stage");
+    int rc = ctx->table_reserve(out, std::max<uint64_t>(R * (uint64_t)std::max(cols, 1), 1));
+    if (rc) return rc;
+    out->cols = cols;
+    if (R == 0 || n_bound == 0) {   // nothing to drop: the table as it is
+        if (R) WKF_CUDA(ctx, cudaMemcpyAsync(out->d, in->d, R * (uint64_t)cols * 4, cudaMemcpyDeviceToDevice, s));
+        WKF_CUDA(ctx, cudaMemcpyAsync(out->d_rows, in->d_rows, 8, cudaMemcpyDeviceToDevice, s));
+        WKF_CUDA(ctx, cudaStreamSynchronize(s));
+        return WK_SUCCESS;
+    }
+    const uint32_t n = (uint32_t)R;
+    const int grid = std::max(1, std::min<int>(ctx->sm_count * 4, (int)((n + 2047) / 2048)));
+    const size_t bytes = 256 + ((size_t)grid + 2) * 4 + 64;
+    char* scratch = nullptr;
+    if (wk::dev_malloc(&scratch, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return ctx->fail(WK_E_OOM, "filter scratch");
+    }
+    auto done = [&](int code) {
+        cudaStreamSynchronize(s);
+        cudaFree(scratch);
+        return code;
+    };
+    int32_t* d_cols = reinterpret_cast<int32_t*>(scratch);
+    uint32_t* part = reinterpret_cast<uint32_t*>(scratch + 256);
+    uint32_t* d_total = part + grid + 1;
+    cudaError_t e = cudaMemcpyAsync(d_cols, bound_cols, (size_t)n_bound * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return done(ctx->cuda_fail(e, "filter columns"));
+    BoundArgs b{in->d, cols, d_cols, n_bound, n, part, out->d};
+    bound_count_kernel<<<grid, kFinThreads, 0, s>>>(b);
+    scan_kernel<<<1, 1024, 0, s>>>(part, (uint32_t)grid, d_total);
+    bound_place_kernel<<<grid, kFinThreads, 0, s>>>(b);
+    if ((e = cudaGetLastError()) != cudaSuccess) return done(ctx->cuda_fail(e, "filter launches"));
+    uint32_t h_total = 0;
+    if ((e = cudaMemcpyAsync(&h_total, d_total, 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return done(ctx->cuda_fail(e, "filter count"));
+    ctx->h_rows[1] = h_total;
+    e = cudaMemcpyAsync(out->d_rows, ctx->h_rows + 1, 8, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return done(ctx->cuda_fail(e, "filter row count"));
     return done(WK_SUCCESS);
 }

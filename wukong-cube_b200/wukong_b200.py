@@ -148,6 +148,7 @@ _SIGS = {
     "wk_table_final_process": (C.c_int, [_P, _P, C.POINTER(C.c_int32), C.c_int32, C.c_int32,
                                          C.c_int64, C.c_int64, _P]),
     "wk_table_download": (C.c_int, [_P, _P, _P, C.c_uint64]),
+    "wk_table_filter_bound": (C.c_int, [_P, _P, C.POINTER(C.c_int32), C.c_int32, _P]),
     "wk_table_shape": (C.c_int, [_P, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_int32)]),
     "wk_table_device_ptr": (C.c_int, [_P, _P, C.POINTER(_P)]),
     "wk_step_index_to_unknown": (C.c_int, [_P, C.c_uint32, C.c_int32, C.c_int32, C.c_int32, _P]),
@@ -440,6 +441,14 @@ class Table:
         keep = (C.c_int32 * max(len(keep_cols), 1))(*[int(c) for c in keep_cols])
         _check(lib().wk_table_final_process(self.ctx.h, self.h, keep, len(keep_cols),
                                             1 if distinct else 0, offset, limit, out.h), self.ctx.h)
+        return out
+
+    def filter_bound(self, bound_cols):
+        """The BOUND filters on the device (wk_table_filter_bound) into a new Table."""
+        out = Table(self.ctx)
+        cols = (C.c_int32 * max(len(bound_cols), 1))(*[int(c) for c in bound_cols])
+        _check(lib().wk_table_filter_bound(self.ctx.h, self.h, cols, len(bound_cols), out.h),
+               self.ctx.h)
         return out
 
 
