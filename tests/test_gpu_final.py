@@ -63,3 +63,20 @@ def test_empty_and_refusals(ctx):
             t.final_process(keep)
         assert e.value.code == code
     t.free()
+
+
+@pytest.mark.parametrize("cols,span", [(5, 2**32), (3, 2**22), (4, 3), (2, 1)])
+def test_packed_key_chunks(ctx, cols, span):
+    """Columns whose ranges need up to 32 bits each (five full-range columns: 160 bits, three
+    64-bit key chunks), narrow ones that share one chunk, and constant ones that need none;
+    offsets from each column's smallest value in signed order."""
+    rng = np.random.default_rng(cols * 7 + 1)
+    rows = 50_000
+    base = rng.integers(0, 2**32 - span + 1, size=cols, dtype=np.uint64)
+    table = (base + rng.integers(0, span, size=(rows, cols), dtype=np.uint64)).astype(np.uint32)
+    table[rng.integers(0, rows, size=rows // 3)] = table[:rows // 3]   # repeated rows
+    for keep in ([cols - 1], list(range(cols))[::-1], [0]):
+        for offset, limit in ((0, -1), (11, 1000)):
+            got = _run(ctx, table, keep, True, offset, limit)
+            want = oracle.final_process(table, keep, True, offset, limit)
+            assert np.array_equal(got, want), (keep, offset, limit)

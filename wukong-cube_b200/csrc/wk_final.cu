@@ -6,8 +6,8 @@
 // DISTINCT follows the reference step for step: the rows are sorted by all their columns,
 // compared as signed 32-bit values (ReduceCmp over an int table, sparql.hpp:1403-1417), then
 // of each run of neighbours equal on the required columns the first is kept.  The sort is an
-// LSD radix sort of row indices, one stable 8-bit counting pass per byte of every column from
-// the last column to the first; rows equal in every column are interchangeable, so the result
+// LSD radix sort of (packed key, row index) pairs over only the bits in which the rows differ
+// (see "DISTINCT sort" below); rows equal in every column are interchangeable, so the result
 // does not depend on how the reference's std::sort orders them.
 #include <cuda_runtime.h>
 
@@ -30,20 +30,91 @@ using namespace dev;
 constexpr int kFinThreads = 256;
 constexpr int kDigits = 256;
 
+// ---------------------------------------------------------------- DISTINCT sort
+// The sort orders rows by all their columns as signed 32-bit values.  A column is first mapped
+// to its offset from the column's smallest value (in signed order), so a column spanning d
+// distinct-order values needs only ceil(log2(d)) bits, and a constant column none.  Columns are
+// packed, last column in the lowest bits, into 64-bit keys ("chunks" of consecutive columns that
+// fit in 64 bits); the LSD sort runs the chunks from the last columns to the first, and within a
+// chunk one stable 8-bit counting pass per byte of the chunk's bits.  Every pass reads the keys
+// and row indices with coalesced loads; the table itself is read once per chunk, to build its
+// keys.
+
+// Smallest and largest value of every column (signed order, stored with the sign bit flipped).
+__global__ void __launch_bounds__(kFinThreads) minmax_kernel(const uint32_t* table, uint64_t elems, int cols,
+                                                             uint32_t* mm /* [2 * cols] */) {
+    __shared__ uint32_t s_lo[64], s_hi[64];
+    for (int c = threadIdx.x; c < cols; c += kFinThreads) {
+        s_lo[c] = 0xFFFFFFFFu;
+        s_hi[c] = 0;
+    }
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * kFinThreads;
+    uint64_t e = blockIdx.x * (uint64_t)kFinThreads + threadIdx.x;
+    int c = (int)(e % cols);
+    const int step = (int)(stride % cols);
+    uint32_t lo = 0xFFFFFFFFu, hi = 0;
+    int cur = c;
+    for (; e < elems; e += stride) {
+        const uint32_t v = __ldg(table + e) ^ 0x80000000u;
+        if (c != cur) {   // column changed: fold the run so far into shared memory
+            atomicMin(&s_lo[cur], lo);
+            atomicMax(&s_hi[cur], hi);
+            lo = 0xFFFFFFFFu;
+            hi = 0;
+            cur = c;
+        }
+        lo = min(lo, v);
+        hi = max(hi, v);
+        c += step;
+        if (c >= cols) c -= cols;
+    }
+    if (lo <= hi) {
+        atomicMin(&s_lo[cur], lo);
+        atomicMax(&s_hi[cur], hi);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < cols; k += kFinThreads) {
+        if (s_lo[k] <= s_hi[k]) {
+            atomicMin(&mm[2 * k], s_lo[k]);
+            atomicMax(&mm[2 * k + 1], s_hi[k]);
+        }
+    }
+}
+
+// One chunk's key layout: columns ccol[0..nc), most significant first, ccol[j] in cbits[j]
+// bits above the next, offset by cmin[j].
+struct ChunkDesc {
+    int nc;
+    int ccol[32];
+    int cbits[32];
+    uint32_t cmin[32];
+};
+
+// keys[i] = the chunk key of row idx_in[i] (row i when idx_in is null); idx_out[i] = that row.
+__global__ void __launch_bounds__(kFinThreads) key_kernel(const uint32_t* table, int cols, ChunkDesc cd,
+                                                          const uint32_t* idx_in, uint32_t n,
+                                                          unsigned long long* keys, uint32_t* idx_out) {
+    for (uint32_t i = blockIdx.x * kFinThreads + threadIdx.x; i < n; i += gridDim.x * kFinThreads) {
+        const uint32_t r = idx_in ? idx_in[i] : i;
+        const uint32_t* row = table + (uint64_t)r * cols;
+        unsigned long long k = 0;
+        for (int j = 0; j < cd.nc; ++j)
+            k = (k << cd.cbits[j]) | (unsigned long long)((__ldg(row + cd.ccol[j]) ^ 0x80000000u) - cd.cmin[j]);
+        keys[i] = k;
+        idx_out[i] = r;
+    }
+}
+
 struct SortPass {
-    const uint32_t* table;   // row-major, `cols` words per row
-    int cols, col, shift;
+    const unsigned long long* key_in;
     const uint32_t* idx_in;
+    unsigned long long* key_out;
     uint32_t* idx_out;
+    int shift;
     uint32_t n;
     uint32_t* hist;          // [kDigits][grid]: digit-major, so one scan gives the offsets
 };
-
-__device__ __forceinline__ uint32_t digit_of(const SortPass& a, uint32_t row) {
-    // signed order: flipping the sign bit makes the unsigned order the signed one
-    const uint32_t v = a.table[(uint64_t)row * a.cols + a.col] ^ 0x80000000u;
-    return (v >> a.shift) & 0xFFu;
-}
 
 __device__ __forceinline__ void chunk(uint32_t n, uint32_t* lo, uint32_t* hi) {
     const uint32_t c = (n + gridDim.x - 1) / gridDim.x;
@@ -61,7 +132,8 @@ __global__ void __launch_bounds__(kFinThreads) hist_kernel(const SortPass a) {
     __syncthreads();
     uint32_t lo, hi;
     chunk(a.n, &lo, &hi);
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads) atomicAdd(&s_h[digit_of(a, a.idx_in[i])], 1u);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads)
+        atomicAdd(&s_h[(uint32_t)(a.key_in[i] >> a.shift) & 0xFFu], 1u);
     __syncthreads();
     a.hist[threadIdx.x * gridDim.x + blockIdx.x] = s_h[threadIdx.x];
 }
@@ -101,8 +173,9 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
         __syncthreads();
         const uint32_t i = base + threadIdx.x;
         const bool live = i < hi;
+        const unsigned long long key = live ? a.key_in[i] : 0;
         const uint32_t row = live ? a.idx_in[i] : 0;
-        const uint32_t dg = live ? digit_of(a, row) : kDigits + lane;   // lone sentinel
+        const uint32_t dg = live ? (uint32_t)(key >> a.shift) & 0xFFu : kDigits + lane;   // lone sentinel
         const unsigned peers = __match_any_sync(0xffffffffu, dg);
         const int rank = __popc(peers & ((1u << lane) - 1));
         if (live && rank == 0) s_cnt[warp][dg] = __popc(peers);
@@ -117,7 +190,11 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
             s_tile[threadIdx.x] = acc;
         }
         __syncthreads();
-        if (live) a.idx_out[s_run[dg] + s_cnt[warp][dg] + rank] = row;
+        if (live) {
+            const uint32_t at = s_run[dg] + s_cnt[warp][dg] + rank;
+            a.key_out[at] = key;
+            a.idx_out[at] = row;
+        }
         __syncthreads();
         s_run[threadIdx.x] += s_tile[threadIdx.x];
         __syncthreads();
@@ -258,6 +335,8 @@ __global__ void __launch_bounds__(kFinThreads) bound_place_kernel(const BoundArg
 
 cudaError_t final_kernel_attrs() {
     cudaError_t e = use_max_shared_carveout(iota_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(minmax_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(key_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(hist_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scan_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scatter_kernel);
@@ -302,11 +381,14 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     if (R >= (1ull << 32)) return ctx->fail(WK_E_CAPACITY, "table too long for the post-pattern stage");
     const uint32_t n = (uint32_t)R;
     const int grid = std::max(1, std::min<int>(ctx->sm_count * 4, (int)((n + 2047) / 2048)));
-    // scratch: the required columns, two index arrays, the digit histogram, the CTA counts and
-    // the distinct total
+    // scratch: the required columns, two index arrays, two key arrays (DISTINCT only), the
+    // digit histogram, the CTA counts and the distinct total, the column ranges
+    const bool sort = distinct && n > 1;
     const size_t keep_bytes = ((size_t)n_keep * 4 + 255) & ~(size_t)255;
-    const size_t bytes = keep_bytes + 2 * (size_t)n * 4 + (size_t)kDigits * grid * 4 +
-                         ((size_t)grid + 2) * 4 + 64;
+    const size_t idx_bytes = ((2 * (size_t)n * 4) + 255) & ~(size_t)255;
+    const size_t key_bytes = sort ? 2 * (size_t)n * 8 : 0;
+    const size_t bytes = keep_bytes + idx_bytes + key_bytes + (size_t)kDigits * grid * 4 +
+                         ((size_t)grid + 2) * 4 + (size_t)cols * 8 + 64;
     char* scratch = nullptr;
     if (wk::dev_malloc(&scratch, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -320,26 +402,84 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     int32_t* d_keep = reinterpret_cast<int32_t*>(scratch);
     uint32_t* idx0 = reinterpret_cast<uint32_t*>(scratch + keep_bytes);
     uint32_t* idx1 = idx0 + n;
-    uint32_t* hist = idx1 + n;
+    unsigned long long* key0 = reinterpret_cast<unsigned long long*>(scratch + keep_bytes + idx_bytes);
+    unsigned long long* key1 = key0 + (sort ? n : 0);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(scratch + keep_bytes + idx_bytes + key_bytes);
     uint32_t* part = hist + (size_t)kDigits * grid;
     uint32_t* d_total = part + grid + 1;
+    uint32_t* d_mm = d_total + 1;
     cudaError_t e = cudaMemcpyAsync(d_keep, keep_cols, (size_t)n_keep * 4, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return done(ctx->cuda_fail(e, "post-pattern columns"));
     const uint32_t* idx = nullptr;   // null: rows in table order
     uint64_t m = n;
-    if (distinct && n > 1) {
-        iota_kernel<<<grid, kFinThreads, 0, s>>>(idx0, n);
-        uint32_t* a = idx0;
-        uint32_t* b = idx1;
-        for (int c = cols - 1; c >= 0; --c)
-            for (int shift = 0; shift < 32; shift += 8) {
-                SortPass p{in->d, cols, c, shift, a, b, n, hist};
+    if (sort) {
+        // each column's range, in signed order
+        std::vector<uint32_t> mm(2 * (size_t)cols);
+        for (int c = 0; c < cols; ++c) {
+            mm[2 * c] = 0xFFFFFFFFu;
+            mm[2 * c + 1] = 0;
+        }
+        if ((e = cudaMemcpyAsync(d_mm, mm.data(), mm.size() * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return done(ctx->cuda_fail(e, "column ranges"));
+        minmax_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256))),
+                        kFinThreads, 0, s>>>(in->d, (uint64_t)n * cols, cols, d_mm);
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpyAsync(mm.data(), d_mm, mm.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess)
+            return done(ctx->cuda_fail(e, "column ranges"));
+        // chunks of columns, last column first; a constant column orders nothing and is left out
+        std::vector<ChunkDesc> chunks;
+        std::vector<int> chunk_bits;
+        ChunkDesc cur{};
+        int cur_bits = 0;
+        auto flush = [&]() {
+            if (!cur.nc) return;
+            // columns were added least significant first; the key wants the most significant first
+            std::reverse(cur.ccol, cur.ccol + cur.nc);
+            std::reverse(cur.cbits, cur.cbits + cur.nc);
+            std::reverse(cur.cmin, cur.cmin + cur.nc);
+            chunks.push_back(cur);
+            chunk_bits.push_back(cur_bits);
+            cur = ChunkDesc{};
+            cur_bits = 0;
+        };
+        for (int c = cols - 1; c >= 0; --c) {
+            const uint32_t lo = mm[2 * c], hi = mm[2 * c + 1];
+            if (lo >= hi) continue;
+            const int b = 32 - __builtin_clz(hi - lo);
+            if (cur_bits + b > 64) flush();
+            cur.ccol[cur.nc] = c;
+            cur.cbits[cur.nc] = b;
+            cur.cmin[cur.nc] = lo;
+            cur.nc++;
+            cur_bits += b;
+        }
+        flush();
+        const int kgrid = std::max(1, std::min(ctx->sm_count * 8, (int)((n + 255) / 256)));
+        uint32_t* ia = idx0;
+        uint32_t* ib = idx1;
+        unsigned long long* ka = key0;
+        unsigned long long* kb = key1;
+        const uint32_t* sorted = nullptr;
+        for (size_t k = 0; k < chunks.size(); ++k) {
+            key_kernel<<<kgrid, kFinThreads, 0, s>>>(in->d, cols, chunks[k], sorted, n, ka, ia);
+            for (int shift = 0; shift < chunk_bits[k]; shift += 8) {
+                SortPass p{ka, ia, kb, ib, shift, n, hist};
                 hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
                 scan_kernel<<<1, 1024, 0, s>>>(hist, (uint32_t)(kDigits * grid), nullptr);
                 scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
-                std::swap(a, b);
+                std::swap(ka, kb);
+                std::swap(ia, ib);
             }
-        UniqueArgs u{in->d, cols, d_keep, n_keep, a, n, part, b};
+            sorted = ia;
+            std::swap(ia, ib);   // the next chunk's keys go to the other index array
+        }
+        if (!sorted) {   // every column constant: every row is equal, the table order stands
+            iota_kernel<<<kgrid, kFinThreads, 0, s>>>(idx0, n);
+            sorted = idx0;
+        }
+        uint32_t* kept = sorted == idx0 ? idx1 : idx0;
+        UniqueArgs u{in->d, cols, d_keep, n_keep, sorted, n, part, kept};
         unique_count_kernel<<<grid, kFinThreads, 0, s>>>(u);
         scan_kernel<<<1, 1024, 0, s>>>(part, (uint32_t)grid, d_total);
         unique_place_kernel<<<grid, kFinThreads, 0, s>>>(u);
@@ -349,7 +489,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             (e = cudaStreamSynchronize(s)) != cudaSuccess)
             return done(ctx->cuda_fail(e, "distinct count"));
         m = h_total;
-        idx = b;
+        idx = kept;
     }
     const uint64_t start = std::min<uint64_t>((uint64_t)offset, m);
     const uint64_t count = limit < 0 ? m - start : std::min<uint64_t>((uint64_t)limit, m - start);
