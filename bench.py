@@ -534,9 +534,9 @@ def run_ours(args, world, rank, local_rank):
             "batch_other_ms": overheads,
             "autotune": tune,
             "serving": serving,
-            # per batch: one launch per level (four where the level runs the flat passes),
+            # per batch: one launch per level (three where the level runs the flat passes),
             # result scan, gather
-            "gpu_launches": args.steps * (sum(4 if (tune.get("batch_flat", 0) >> k) & 1 else 1
+            "gpu_launches": args.steps * (sum(3 if (tune.get("batch_flat", 0) >> k) & 1 else 1
                                               for k in range(len(levels))) + 2),
             "clocks": clk.summary()}
     if rank == 0:

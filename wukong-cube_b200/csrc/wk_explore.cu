@@ -419,6 +419,11 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     }
     const uint64_t obase = a.out_base_rows ? *(volatile const uint64_t*)a.out_base_rows : 0;
     if (ntiles == 0 && !handed_off && blockIdx.x == 0 && threadIdx.x == 0) *a.out_rows = obase;
+    // Nothing to do (an empty input, or the flat passes run this step): leave at once.  No CTA
+    // claims a tile or a slice or publishes a status word, so the counters stay as the last
+    // launch reset them and the epoch need not move (it tags only published words).  A launch
+    // that returns at once costs a few microseconds instead of every CTA's counter atomics.
+    if (ntiles == 0) return;
     WK_PH_DECL
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);

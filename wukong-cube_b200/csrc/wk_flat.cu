@@ -3,22 +3,23 @@
 // The tile launch (wk_explore.cu) keeps a whole step in one persistent launch, which suits the
 // many small tables of a batch but pays per-tile barriers and look-back waits, and runs at
 // the occupancy its shared memory allows.  For one large table (index-start queries: 1e5 to
-// 1e8 rows) the same step runs here as four short launches at full occupancy, each a
+// 1e8 rows) the same step runs here as three short launches at full occupancy, each a
 // streaming pass except for the probes themselves:
 //   1. count: one thread per input row probes the key table (two 16-byte slots per load, the
 //      chain followed through slot 7), records the row's output count (list size for
 //      known_to_unknown, 0/1 membership for known_to_known / known_to_const) and its list offset;
 //      each CTA owns a contiguous chunk of rows and publishes the chunk total;
-//   2. scan: one CTA scans the chunk totals, checks the output capacity (overflow sets
-//      kErrOverflow and the rows needed, as the tile launch does) and sets the row count;
+//   2. scan: the last count CTA to finish scans the chunk totals, checks the output capacity
+//      (overflow sets kErrOverflow and the rows needed, as the tile launch does) and sets the
+//      row count;
 //   3. place: each CTA scans its chunk into per-row output positions; filters copy their
 //      surviving rows straight to the output here (a chunk without survivors returns at once);
 //   4. expand (known_to_unknown only): the output rows are split evenly over the CTAs; each CTA
 //      finds its first input row by a 32-way search of the positions and writes its rows in
 //      row-major then edge order (sparql.hpp:328-370), consecutive threads on consecutive rows.
 // When every input row of a known_to_unknown step has exactly one output row (a functional
-// predicate such as memberOf), output row r is input row r: place returns at once and expand
-// copies row by row without positions.
+// predicate such as memberOf), output row r is input row r: the count pass writes it as it
+// goes (every row with one output row does, speculatively), and place and expand return at once.
 // Row counts are read on the device, so the launches chain without a host round trip and can
 // be captured in a graph.  Every launch returns at once unless the input has at least
 // `min_rows` rows; the tile launch of the same step is given the complementary bound, so
@@ -110,6 +111,59 @@ __device__ __forceinline__ uint64_t block_sum(uint64_t x, uint64_t* s_warp) {
     return t;
 }
 
+// Scan of the count CTAs' chunk totals, run by the last count CTA to finish (its kFlatThreads
+// threads): part[] becomes the exclusive scan, part[nparts] the total, part[nparts + 1] the
+// one-to-one flag; the capacity check sets the output row count or the overflow bit.  The
+// totals of other CTAs are read from L2 (they were written by other SMs).
+__device__ void flat_scan_parts(const FlatArgs& a, uint32_t nparts, uint64_t R, uint64_t* s_warp) {
+    __shared__ uint64_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    bool not_ones = false;
+    for (uint32_t r0 = 0; r0 < nparts; r0 += kFlatThreads) {
+        const uint32_t i = r0 + threadIdx.x;
+        const uint64_t pv = i < nparts ? __ldcg((const unsigned long long*)a.part + i) : 0;
+        not_ones |= (pv & kNotOneToOne) != 0;
+        const uint64_t x = pv & ~kNotOneToOne;
+        const uint64_t ex = block_exclusive_sum<kFlatThreads>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < nparts) a.part[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == kFlatThreads - 1) s_carry = carry + ex + x;
+        __syncthreads();
+    }
+    const bool one_to_one = !__syncthreads_or(not_ones);
+    if (threadIdx.x == 0) {
+        const uint64_t total = s_carry;
+        a.part[nparts] = total;
+        a.part[nparts + 1] = one_to_one ? 1 : 0;
+        a.pos[R] = total;
+        if (total > a.out_cap_rows) {
+            atomicOr(&a.ctl->err, kErrOverflow);
+            atomicMax(&a.ctl->need, (unsigned long long)total);
+            *a.out_rows = 0;
+        } else {
+            *a.out_rows = total;
+            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(total * a.step.cout * 4ull));
+        }
+    }
+}
+
+// Called by every thread of a count CTA once its chunk total is in part[blockIdx.x]: true in the
+// last CTA to get here, which then runs the scan (and leaves the counter at 0 for the next pass).
+__device__ __forceinline__ bool last_count_cta(StepCtl* ctl) {
+    __shared__ int s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_last = atomicAdd(&ctl->flat_done, 1u) == gridDim.x - 1;
+        if (s_last) ctl->flat_done = 0;
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last != 0;
+}
+
 // Registers capped for 8 CTAs per SM (2,048 threads, one probe each in flight).
 __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
@@ -121,6 +175,7 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
     const bool filt = d.op == kXK2K || d.op == kXK2C;
     uint64_t sum = 0, sd = 0, nvalid = 0;
     bool ones = true;   // every row of this thread has exactly one output row
+    const bool spec = R <= a.out_cap_rows;   // output row r exists: one-to-one rows written here
     // the next round's row words are loaded while this round's probe is out (3-7% per step on
     // the heavy queries)
     uint32_t nxt_cur = 0, nxt_tgt = d.end_const;
@@ -180,7 +235,18 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
         if (!valid) c = 0;
         a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
         if (c != 1) ones = false;
-        if (!filt) a.off[r] = off;
+        if (!filt) {
+            a.off[r] = off;
+            // A row with exactly one output row writes it now, at output row r: when every row
+            // has one (a functional predicate), that is the step's output and the place and
+            // expand passes return at once; otherwise expand overwrites these rows.
+            if (c == 1 && spec) {
+                const uint32_t* src = a.in + r * (uint64_t)a.w_in;
+                uint32_t* dst = a.out + r * (uint64_t)a.w_out;
+                for (int k = 0; k < d.cin; ++k) dst[k] = __ldg(src + k);
+                dst[d.cin] = __ldg(a.store.edges + off);
+            }
+        }
         sum += c;
         if (valid) {
             sd += deg;
@@ -198,42 +264,7 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
             atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(nvalid * (d.cin * 4ull + 16) + sd * 4));
         }
     }
-}
-
-__global__ void __launch_bounds__(1024) flat_scan_kernel(const FlatArgs a, uint32_t nparts) {
-    __shared__ uint64_t s_warp[32];
-    __shared__ uint64_t s_carry;
-    const uint64_t R = flat_rows(a);
-    if (R < a.min_rows) return;
-    if (threadIdx.x == 0) s_carry = 0;
-    bool not_ones = false;
-    for (uint32_t r0 = 0; r0 < nparts; r0 += 1024) {
-        const uint32_t i = r0 + threadIdx.x;
-        const uint64_t pv = i < nparts ? a.part[i] : 0;
-        not_ones |= (pv & kNotOneToOne) != 0;
-        const uint64_t x = pv & ~kNotOneToOne;
-        const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
-        const uint64_t carry = s_carry;
-        if (i < nparts) a.part[i] = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 1023) s_carry = carry + ex + x;
-        __syncthreads();
-    }
-    const bool one_to_one = !__syncthreads_or(not_ones);
-    if (threadIdx.x == 0) {
-        const uint64_t total = s_carry;
-        a.part[nparts] = total;
-        a.part[nparts + 1] = one_to_one ? 1 : 0;
-        a.pos[R] = total;
-        if (total > a.out_cap_rows) {
-            atomicOr(&a.ctl->err, kErrOverflow);
-            atomicMax(&a.ctl->need, (unsigned long long)total);
-            *a.out_rows = 0;
-        } else {
-            *a.out_rows = total;
-            atomicAdd(&a.ctl->alg_bytes, (unsigned long long)(total * a.step.cout * 4ull));
-        }
-    }
+    if (last_count_cta(a.ctl)) flat_scan_parts(a, gridDim.x, R, s_warp);
 }
 
 __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs a, uint32_t nparts) {
@@ -278,17 +309,9 @@ __global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArg
     if (R < a.min_rows) return;
     const uint64_t total = a.pos[R];
     if (total > a.out_cap_rows || total == 0) return;
-    if (a.part[nparts + 1] == 1) {   // one output row per input row: row r is the output's row r
-        const int wo = a.w_out, ecol = a.step.cin;
-        for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < R;
-             r += (uint64_t)gridDim.x * blockDim.x) {
-            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
-            uint32_t* dst = a.out + r * (uint64_t)wo;
-            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
-            dst[ecol] = __ldg(a.store.edges + a.off[r]);
-        }
-        return;
-    }
+    // one output row per input row: the count pass wrote output row r for input row r (the
+    // total fits, so R does too)
+    if (a.part[nparts + 1] == 1) return;
     const uint64_t per = (total + gridDim.x - 1) / gridDim.x;
     const uint64_t j0 = min(total, (uint64_t)blockIdx.x * per), j1 = min(total, j0 + per);
     if (j0 >= j1) return;
@@ -351,6 +374,36 @@ __device__ __forceinline__ uint64_t level_rows(const FlatLevelArgs& a) {
 
 __device__ __forceinline__ uint32_t level_owner(const FlatLevelArgs& a, uint64_t r) {
     return a.virtual_rows ? (uint32_t)r : __ldg(a.owner_in + r);
+}
+
+// The level pass's scan of the chunk totals, run by the last count CTA (as flat_scan_parts).
+__device__ void flat_level_scan_parts(const FlatLevelArgs& a, uint32_t nparts, uint64_t R,
+                                      uint64_t* s_warp) {
+    __shared__ uint64_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t r0 = 0; r0 < nparts; r0 += kFlatThreads) {
+        const uint32_t i = r0 + threadIdx.x;
+        const uint64_t x = i < nparts ? __ldcg((const unsigned long long*)a.part + i) : 0;
+        const uint64_t ex = block_exclusive_sum<kFlatThreads>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (i < nparts) a.part[i] = carry + ex;
+        __syncthreads();
+        if (threadIdx.x == kFlatThreads - 1) s_carry = carry + ex + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint64_t total = s_carry;
+        a.part[nparts] = total;
+        a.pos[R] = total;
+        if (total > a.out_cap_rows) {
+            atomicOr(&a.ctl->err, kErrOverflow);
+            atomicMax(&a.ctl->need, (unsigned long long)total);
+            *a.out_rows = 0;
+        } else {
+            *a.out_rows = total;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const FlatLevelArgs a) {
@@ -416,35 +469,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const Fl
             atomicAdd(&a.ctl->alg_bytes, (unsigned long long)alg);
         }
     }
-}
-
-__global__ void __launch_bounds__(1024) flat_level_scan_kernel(const FlatLevelArgs a, uint32_t nparts) {
-    __shared__ uint64_t s_warp[32];
-    __shared__ uint64_t s_carry;
-    const uint64_t R = level_rows(a);
-    if (threadIdx.x == 0) s_carry = 0;
-    for (uint32_t r0 = 0; r0 < nparts; r0 += 1024) {
-        const uint32_t i = r0 + threadIdx.x;
-        const uint64_t x = i < nparts ? a.part[i] : 0;
-        const uint64_t ex = block_exclusive_sum<1024>(x, s_warp);
-        const uint64_t carry = s_carry;
-        if (i < nparts) a.part[i] = carry + ex;
-        __syncthreads();
-        if (threadIdx.x == 1023) s_carry = carry + ex + x;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const uint64_t total = s_carry;
-        a.part[nparts] = total;
-        a.pos[R] = total;
-        if (total > a.out_cap_rows) {
-            atomicOr(&a.ctl->err, kErrOverflow);
-            atomicMax(&a.ctl->need, (unsigned long long)total);
-            *a.out_rows = 0;
-        } else {
-            *a.out_rows = total;
-        }
-    }
+    if (last_count_cta(a.ctl)) flat_level_scan_parts(a, gridDim.x, R, s_warp);
 }
 
 __global__ void __launch_bounds__(kFlatThreads) flat_level_place_kernel(const FlatLevelArgs a, uint32_t nparts) {
@@ -558,16 +583,14 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
 int flat_grid(int sm_count) { return sm_count * (2048 / kFlatThreads); }
 
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
-    flat_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);
-    flat_scan_kernel<<<1, 1024, 0, s>>>(a, (uint32_t)grid);
+    flat_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);   // its last CTA scans the totals
     flat_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     return cudaGetLastError();
 }
 
 cudaError_t launch_flat_level(const FlatLevelArgs& a, int grid, cudaStream_t s) {
-    flat_level_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);
-    flat_level_scan_kernel<<<1, 1024, 0, s>>>(a, (uint32_t)grid);
+    flat_level_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);   // its last CTA scans the totals
     flat_level_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     flat_level_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a);
     return cudaGetLastError();
@@ -576,11 +599,9 @@ cudaError_t launch_flat_level(const FlatLevelArgs& a, int grid, cudaStream_t s) 
 cudaError_t flat_kernel_attrs() {
     cudaError_t e;
     if ((e = use_max_shared_carveout(flat_count_kernel)) != cudaSuccess) return e;
-    if ((e = use_max_shared_carveout(flat_scan_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_place_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_expand_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_level_count_kernel)) != cudaSuccess) return e;
-    if ((e = use_max_shared_carveout(flat_level_scan_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_level_place_kernel)) != cudaSuccess) return e;
     return use_max_shared_carveout(flat_level_expand_kernel);
 }

@@ -24,7 +24,8 @@ struct StepCtl {
     unsigned int exit_counter;
     unsigned int epoch;          // 1..65535, tags valid status words of the running launch
     unsigned int err;
-    unsigned int pad;
+    unsigned int flat_done;      // count CTAs of a flat pass that have published their chunk
+                                 // total; the last one scans them and resets this to 0
     unsigned long long need;     // largest output (elements) a launch asked for
     unsigned long long status_cap;   // entries in the status array that follows
     unsigned long long sum_deg;  // neighbour-list lengths the probes found (profiling)
