@@ -182,6 +182,16 @@ void wk_free(void* p);
  * fraction of the 7 data slots of a bucket in use (0 < f <= 1; 0 = default 0.1). */
 int wk_gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
                     double load_factor, wk_gstore** out);
+/* The same, and with versatile != 0 also every vertex's predicate list, as the reference's
+ * default (VERSATILE) build inserts it (insert_vp, segment_rdf_dgraph.hpp:365-455): key
+ * [vid|PREDICATE_ID|OUT] lists the distinct predicates of subject vid ascending, key
+ * [vid|PREDICATE_ID|IN] those of object vid (type ids are never IN keys).  A context whose
+ * store holds them runs patterns with an unknown predicate (wk_query_execute and the
+ * wk_step_*_unknown_* steps); without them those patterns are WK_UNKNOWN_PATTERN, as in a
+ * reference build without VERSATILE.  The global sets [0|TYPE_ID|*] and [0|PREDICATE_ID|OUT]
+ * are not built: no pattern operator reads them. */
+int wk_gstore_build_ex(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
+                       double load_factor, int32_t versatile, wk_gstore** out);
 void wk_gstore_free(wk_gstore* g);
 int wk_gstore_info(const wk_gstore* g, uint64_t* n_slots, uint64_t* n_edges, uint32_t* n_segs,
                    uint64_t* n_keys);
@@ -286,6 +296,34 @@ int wk_step_known_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_start, i
 /* ?X P C — GPUEngineCuda::known_to_const (gpu_engine_cuda.hpp:284-363). */
 int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t end_vid,
                            uint32_t pid, int32_t dir, wk_table* out);
+/* C P ?X with ?X known (a column of `in`): SPARQLEngine::const_to_known (sparql.hpp:132-189).
+ * Keeps the rows whose col_end value is in the list of [vid|pid|dir], in order.  (The GPU
+ * engine has no counterpart; the dispatch reaches it for a constant subject whose object an
+ * earlier pattern bound.) */
+int wk_step_const_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_end, uint32_t vid, uint32_t pid,
+                           int32_t dir, wk_table* out);
+/* IDX P ?X with ?X known: SPARQLEngine::index_to_known (sparql.hpp:83-130), the first pattern of
+ * a group that inherited `in` (a union / optional sub-query).  Keeps the rows whose col_end
+ * value is in slice mt_tid of mt_factor of the index list [0|tpid|dir]: equal shares of
+ * length / mt_factor, the last slice with the remainder (sparql.hpp:105-116). */
+int wk_step_index_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_end, uint32_t tpid, int32_t dir,
+                           int32_t mt_tid, int32_t mt_factor, wk_table* out);
+/* The unknown-predicate (versatile) steps, on a store built with wk_gstore_build_ex(versatile):
+ *   ?X ?P ?Y  known_unknown_unknown (sparql.hpp:600-640): each row of `in` times every (p, y) of
+ *             its col_start vertex: the row, then p, then y (two new columns);
+ *   ?X ?P C   known_unknown_const (:649-689): each row times every predicate p of its vertex
+ *             whose list holds end_vid (one new column);
+ *   C ?P ?X   const_unknown_unknown (:559-592): the (p, x) pairs of vid (two columns);
+ *   C1 ?P C2  const_unknown_const (:697-739): the predicates of vid reaching end_vid (one).
+ * Rows come row-major, then in the vertex's predicate order, then in list order.
+ * WK_UNKNOWN_PATTERN on a store without the vertex-predicate lists. */
+int wk_step_known_unknown_unknown(wk_ctx* ctx, const wk_table* in, int32_t col_start, int32_t dir,
+                                  wk_table* out);
+int wk_step_known_unknown_const(wk_ctx* ctx, const wk_table* in, int32_t col_start, uint32_t end_vid,
+                                int32_t dir, wk_table* out);
+int wk_step_const_unknown_unknown(wk_ctx* ctx, uint32_t vid, int32_t dir, wk_table* out);
+int wk_step_const_unknown_const(wk_ctx* ctx, uint32_t vid, uint32_t end_vid, int32_t dir, wk_table* out);
+
 /* known_to_unknown that allocates nothing.  No reference counterpart: the reference allocates
  * its buffers up front (GPUMem) and aborts when they overflow.
  *
@@ -331,6 +369,12 @@ int wk_query_execute(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
  * status the query would end with for a malformed plan, else 0 with the final v2c_map[nvars]
  * and *col_num. */
 int wk_query_validate(const wk_query* q, int32_t max_cols, int32_t* v2c_map, int32_t* col_num);
+/* The same for a store with (versatile != 0) or without the vertex-predicate lists: with them a
+ * pattern with an unknown predicate dispatches to the versatile operators (sparql.hpp:954-1012);
+ * without them it is WK_UNKNOWN_PATTERN (wk_query_validate).  Batches and serving runs refuse
+ * plans with versatile steps (WK_E_UNSUPPORTED): those run as single queries. */
+int wk_query_validate_ex(const wk_query* q, int32_t max_cols, int32_t versatile, int32_t* v2c_map,
+                         int32_t* col_num);
 /* Same, with the final table copied to host memory (the reference's new_table vector). */
 int wk_query_execute_host(wk_ctx* ctx, const wk_query* q, int32_t mode, uint32_t* host_out,
                           uint64_t cap_elems, int32_t* v2c_map, int32_t* col_num, uint64_t* rows);

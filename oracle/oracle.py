@@ -24,6 +24,11 @@ def lib():
         P = C.c_void_p
         L.orc_store_build.restype = P
         L.orc_store_build.argtypes = [P, C.c_uint64, P, C.c_uint64]
+        L.orc_store_build2.restype = P
+        L.orc_store_build2.argtypes = [P, C.c_uint64, P, C.c_uint64, C.c_int]
+        L.orc_pattern.argtypes = [P, P, C.c_uint64, C.c_int, C.c_int, P, C.c_int, C.c_int,
+                                  C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_int), P]
         L.orc_store_free.argtypes = [P]
         L.orc_get_triples.argtypes = [P, C.c_uint32, C.c_uint32, C.c_int,
                                       C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]
@@ -51,10 +56,13 @@ def _p(a):
 class OracleStore:
     """Store built by the reference's construction rules from (s, p, o) triples."""
 
-    def __init__(self, pso, pos=None):
+    def __init__(self, pso, pos=None, versatile=False):
+        """versatile: also the vertex-predicate lists [v|PREDICATE_ID|d] the unknown-predicate
+        operators read (the reference's default VERSATILE build)."""
         pso = np.ascontiguousarray(pso, dtype=np.uint32)
         pos = pso if pos is None else np.ascontiguousarray(pos, dtype=np.uint32)
-        self.h = lib().orc_store_build(_p(pso), pso.shape[0], _p(pos), pos.shape[0])
+        self.versatile = bool(versatile)
+        self.h = lib().orc_store_build2(_p(pso), pso.shape[0], _p(pos), pos.shape[0], int(versatile))
         if not self.h:
             raise RuntimeError("oracle store build failed")
 
@@ -120,6 +128,29 @@ class OracleStore:
         finally:
             lib().orc_free(out)
         return r
+
+    def pattern(self, table, nvars, pattern, mt_tid=0, mt_factor=1):
+        """One pattern (s, p, o, d, pred_type) through the dispatch over a given table whose
+        column i holds variable -(i + 1), as the first pattern of a group that inherited the
+        table.  Returns (status, table, v2c)."""
+        t = np.ascontiguousarray(table, dtype=np.uint32)
+        if t.ndim == 1:
+            t = t.reshape(-1, 1)
+        pat = np.ascontiguousarray(pattern, dtype=np.int32)
+        out = C.POINTER(C.c_uint32)()
+        rows = C.c_uint64()
+        cols = C.c_int()
+        v2c = np.zeros(max(nvars, 1), np.int32)
+        rc = lib().orc_pattern(self.h, _p(t), t.shape[0], t.shape[1], nvars, _p(pat), mt_tid, mt_factor,
+                               C.byref(out), C.byref(rows), C.byref(cols), _p(v2c))
+        if rc:
+            return rc, None, None
+        n = rows.value * cols.value
+        try:
+            r = np.ctypeslib.as_array(out, shape=(max(n, 1),))[:n].copy().reshape(rows.value, cols.value)
+        finally:
+            lib().orc_free(out)
+        return 0, r, list(v2c[:nvars])
 
     def run_many(self, flat_list, nvars_list, threads):
         """Run many queries, one per thread at a time; returns (rows, status) arrays."""

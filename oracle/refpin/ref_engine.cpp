@@ -153,6 +153,48 @@ int wkref_filter_bound(const uint32_t* table, uint64_t rows, int cols, const int
     return SUCCESS;
 }
 
+// One pattern through the engine's dispatch over a given table (rows x cols, variable -(c+1) in
+// column c, nvars variables), as the first pattern of a group that inherited that table (a
+// union / optional sub-query does), so an index pattern with a known object runs
+// index_to_known.  mt_factor > 1 runs slice mt_tid as the engine runs a forked sub-query: it
+// reports to a parent, so the final stage does not run.  *out (malloc'd), *out_rows, *out_cols
+// and v2c[nvars] receive the result; the return is the engine's status.
+int wkref_pattern(void* g, const uint32_t* table, uint64_t rows, int cols, int nvars, const int32_t* pat,
+                  int mt_tid, int mt_factor, uint32_t** out, uint64_t* out_rows, int* out_cols,
+                  int32_t* v2c) {
+    SPARQLQuery::PatternGroup group;
+    SPARQLQuery::Pattern p(pat[0], pat[1], (ssid_t)pat[3], pat[2]);
+    p.pred_type = (char)pat[4];
+    group.patterns.push_back(p);
+    std::vector<ssid_t> req;
+    SPARQLQuery q(group, nvars, req);
+    for (int c = 0; c < cols; ++c) q.result.add_var2col(-(c + 1), c);
+    q.result.set_col_num(cols);
+    q.result.result_table.assign(table, table + rows * (uint64_t)cols);
+    q.result.update_nrows();
+    q.mt_factor = mt_factor < 1 ? 1 : mt_factor;
+    q.mt_tid = mt_tid;
+    q.pqid = 1;   // a sub-query's reply (thread 1 is an engine): no dispatch, no final stage
+    Coder coder(0, 1);
+    Messenger msgr;
+    StringMapping str;
+    SPARQLEngine engine(0, 1, &str, static_cast<ListGraph*>(g), &coder, &msgr);
+    engine.execute_sparql_query(q);
+    if (msgr.replies.size() != 1) return UNKNOWN_ERROR;
+    SPARQLQuery& r = msgr.replies[0];
+    if (r.result.get_status_code() != SUCCESS) return r.result.get_status_code();
+    const uint64_t nr = r.result.get_row_num();
+    const int nc = r.result.get_col_num();
+    uint32_t* o = (uint32_t*)std::malloc(std::max<uint64_t>(nr * nc, 1) * sizeof(uint32_t));
+    if (!o) return UNKNOWN_ERROR;
+    for (uint64_t i = 0; i < nr * (uint64_t)nc; ++i) o[i] = r.result.result_table[i];
+    *out = o;
+    *out_rows = nr;
+    *out_cols = nc;
+    for (int i = 0; i < nvars; ++i) v2c[i] = r.result.var2col(-(i + 1));
+    return SUCCESS;
+}
+
 void wkref_free(void* p) { std::free(p); }
 
 }  // extern "C"

@@ -31,6 +31,9 @@ def lib():
                                   C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_int), P]
         L.wkref_free.argtypes = [P]
+        L.wkref_pattern.argtypes = [P, P, C.c_uint64, C.c_int, C.c_int, P, C.c_int, C.c_int,
+                                    C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_int), P]
         L.wkref_filter_bound.argtypes = [P, C.c_uint64, C.c_int, P, C.c_int,
                                          C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64)]
         _lib = L
@@ -58,6 +61,29 @@ class RefGraph:
 
     __del__ = close
 
+    def pattern(self, table, nvars, pattern, mt_tid=0, mt_factor=1):
+        """One pattern through the engine's dispatch over a given table (column i = variable
+        -(i + 1)), as the first pattern of a group that inherited it.  Returns (status, table,
+        v2c)."""
+        t = np.ascontiguousarray(table, dtype=np.uint32)
+        if t.ndim == 1:
+            t = t.reshape(-1, 1)
+        pat = np.ascontiguousarray(pattern, dtype=np.int32)
+        out = C.POINTER(C.c_uint32)()
+        rows = C.c_uint64()
+        cols = C.c_int()
+        v2c = np.zeros(max(nvars, 1), np.int32)
+        rc = lib().wkref_pattern(self.h, _p(t), t.shape[0], t.shape[1], nvars, _p(pat), mt_tid,
+                                 mt_factor, C.byref(out), C.byref(rows), C.byref(cols), _p(v2c))
+        if rc:
+            return rc, None, None
+        n = rows.value * cols.value
+        try:
+            r = np.ctypeslib.as_array(out, shape=(max(n, 1),))[:n].copy().reshape(rows.value, cols.value)
+        finally:
+            lib().wkref_free(out)
+        return 0, r, list(v2c[:nvars])
+
     def run(self, query_flat, nvars, required=None, distinct=False, limit=-1, offset=0):
         """Run one planned query through SPARQLEngine::execute_sparql_query.
         Returns (status, table, v2c)."""
@@ -82,13 +108,20 @@ class RefGraph:
 def graph_from_store(store, triples, vocab):
     """A RefGraph holding every key of `triples` with the lists `store` (anything with
     get_triples / get_index) answers: normal keys [s|p|OUT], [o|p|IN] (type triples only OUT),
-    the type index [0|t|IN] and the predicate indexes [0|p|IN], [0|p|OUT]."""
+    the type index [0|t|IN] and the predicate indexes [0|p|IN], [0|p|OUT]; and, from a store
+    built versatile, every vertex's predicate lists [v|PREDICATE_ID|OUT], [v|PREDICATE_ID|IN]."""
     g = RefGraph()
     seen = set()
+    versatile = getattr(store, "versatile", False)
     for s, p, o in triples:
         s, p, o = int(s), int(p), int(o)
-        for key in ((s, p, 1), (o, p, 0)):
-            if key[2] == 0 and p == 1:
+        keys = [(s, p, 1), (o, p, 0)]
+        if versatile:
+            keys += [(s, 0, 1), (o, 0, 0)]
+        for key in keys:
+            if key[2] == 0 and 1 < key[0] < (1 << 17):
+                continue   # a type id object is never an IN key
+            if key[2] == 0 and p == 1 and key[1] != 0:
                 continue
             if key not in seen:
                 seen.add(key)
@@ -107,11 +140,14 @@ def graph_from_store(store, triples, vocab):
 
 def bound_vars(query_flat):
     """The variables a planned pattern list binds, in the order their columns are added (the
-    object of an index or constant start, then the object of each known_to_unknown step).
+    object of an index or constant start, the object of each known_to_unknown step, and an
+    unknown predicate's variable before its object's, as the versatile operators add them).
     Asking the final stage for exactly these keeps its projection (sparql.hpp:1500-1529) the
     identity, so the reference's table is the pattern stage's table."""
     bound = []
     for s, p, o, d, t in np.asarray(query_flat).reshape(-1, 5):
+        if p < 0 and p not in bound:
+            bound.append(int(p))
         if o < 0 and o not in bound:
             bound.append(int(o))
     return bound

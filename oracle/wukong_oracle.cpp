@@ -23,9 +23,16 @@
 //     409-510) and start_from_index (:816-838);
 //   * the mt_factor split of an index start (sparql.hpp:213-224, dispatch :1058-1105) with the
 //     sub-results concatenated in sub-query order (Result::append_result, query.hpp:676-707).
-// The reference itself cannot be compiled here (boost/tbb/MPI headers are absent), so no
-// reference binary stands behind this file; it is pinned by the known-answer checks of
-// tests/test_graph.cc re-derived in tests/test_oracle_known_answers.py.
+// The reference's own engine stands behind this file: oracle/Makefile (target "ref") compiles
+// src/core/engine/sparql.hpp and what it includes from the reference tree against small
+// stand-ins for Boost / TBB / the network (oracle/refpin), and tests/golden holds its answers,
+// which this file must reproduce.  The store construction is pinned by the known-answer checks
+// of tests/test_graph.cc re-derived in tests/test_oracle_known_answers.py.
+//   * VERSATILE (the reference's default build, CMakeLists.txt USE_VERSATILE ON): the
+//     vertex-predicate lists (insert_vp, segment_rdf_dgraph.hpp:365-455) when the store is
+//     built with them, and the unknown-predicate operators (sparql.hpp:554-739) plus
+//     index_to_known / const_to_known (:83-189).  The global sets [0|TYPE_ID|IN/OUT] and
+//     [0|PREDICATE_ID|OUT] (:333-346) are not built: no pattern operator reads them.
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
@@ -157,8 +164,8 @@ static void par_sort(std::vector<T>& v, Cmp cmp) {
         for (auto& t : th) t.join();
     }
 }
-enum { SUCCESS = 0, UNKNOWN_PATTERN = 3, OBJ_ERROR = 7, VERTEX_INVALID = 8, UNKNOWN_SUB = 9,
-       FIRST_PATTERN_ERROR = 11, STORE_ERROR = 106 };
+enum { SUCCESS = 0, UNKNOWN_ERROR = 1, UNKNOWN_PATTERN = 3, OBJ_ERROR = 7, VERTEX_INVALID = 8,
+       UNKNOWN_SUB = 9, FIRST_PATTERN_ERROR = 11, STORE_ERROR = 106 };
 #define ORACLE_ASSERT(c, code) \
     do {                       \
         if (!(c)) throw error_code(code); \
@@ -179,6 +186,11 @@ public:
     static const int ASSOCIATIVITY = 8;
     static const int est_load_factor = 55;   // global.hpp:127
     std::map<uint32_t, std::vector<uint32_t>> pidx_in_map, pidx_out_map, tidx_map;
+    // VERSATILE builds (segment_rdf_dgraph.hpp:365-455): every vertex's predicates, key
+    // [vid|PREDICATE_ID|OUT] for the subjects of pso, [vid|PREDICATE_ID|IN] for the objects of
+    // pos that are not type ids; each list ascending (the loader sorts by spo / ops there).
+    bool versatile = false;
+    std::map<uint32_t, std::vector<uint32_t>> vp_out, vp_in;
 
     // kvstore.hpp:446-457: extension buckets live after the main-header region
     uint64_t alloc_ext_buckets(uint64_t n) {
@@ -444,6 +456,20 @@ public:
             order.push_back(&out_seg);
             order.push_back(&in_seg);
         }
+        if (versatile) {   // :837-851: the vid-predicate segments
+            rdf_seg_meta_t& pout = seg_map[segid_t(0, PREDICATE_ID, OUT)];
+            rdf_seg_meta_t& pin = seg_map[segid_t(0, PREDICATE_ID, IN)];
+            for (auto& e : vp_out) pout.num_edges += e.second.size();
+            for (auto& e : vp_in) pin.num_edges += e.second.size();
+            pout.num_keys = vp_out.size();
+            pin.num_keys = vp_in.size();
+            pout.edge_start = alloc_entries(pout.num_edges);
+            pin.edge_start = alloc_entries(pin.num_edges);
+            alloc_buckets_to_seg(pout);
+            alloc_buckets_to_seg(pin);
+            order.push_back(&pout);
+            order.push_back(&pin);
+        }
         idx_out_seg.edge_start = alloc_entries(idx_out_seg.num_edges);
         idx_out_seg.num_keys += edge_predicates.empty() ? 0 : edge_predicates.size() - 1;
         alloc_buckets_to_seg(idx_out_seg);
@@ -488,6 +514,16 @@ public:
         ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
         predicates = ids;
 
+        if (versatile) {
+            // distinct (s, p) of pso in (p, s) order: appending p per s gives each s's
+            // predicates ascending; likewise (o, p) of pos, type-id objects skipped (:404-411)
+            for (size_t i = 0; i < pso.size(); ++i)
+                if (i == 0 || pso[i].p != pso[i - 1].p || pso[i].s != pso[i - 1].s)
+                    vp_out[pso[i].s].push_back(pso[i].p);
+            for (size_t i = 0; i < pos.size(); ++i)
+                if (!is_tpid(pos[i].o) && (i == 0 || pos[i].p != pos[i - 1].p || pos[i].o != pos[i - 1].o))
+                    vp_in[pos[i].o].push_back(pos[i].p);
+        }
         init_seg_metas(pso, pos);
 
         std::map<uint32_t, size_t> out_map, in_map;   // init_triple_map: first row of each pid
@@ -501,6 +537,17 @@ public:
         }
         insert_idx(pidx_in_map, IN);
         insert_idx(pidx_out_map, OUT);
+        if (versatile) {   // insert_vp (:371-455)
+            for (int d = 0; d < 2; ++d) {
+                auto& vp = d == OUT ? vp_out : vp_in;
+                rdf_seg_meta_t& seg = seg_map[segid_t(0, PREDICATE_ID, d)];
+                uint64_t off = seg.edge_start;
+                for (auto& e : vp) {
+                    insert_key_to_seg(ikey_t(e.first, PREDICATE_ID, d), iptr_t(e.second.size(), off));
+                    for (uint32_t v : e.second) values[off++] = v;
+                }
+            }
+        }
     }
 };
 
@@ -532,12 +579,12 @@ struct Result {
         ORACLE_ASSERT(idx < nvars && idx >= 0, VERTEX_INVALID);
         return v2c_map[idx] & 0xFFFF;
     }
-    void add_var2col(int32_t vid, int col) {   // :443-459
-        ORACLE_ASSERT(vid < 0 && col >= 0, VERTEX_INVALID);
+    void add_var2col(int32_t vid, int col) {   // :443-459 (plain ASSERTs: UNKNOWN_ERROR)
+        ORACLE_ASSERT(vid < 0 && col >= 0, UNKNOWN_ERROR);
         if (v2c_map.empty()) v2c_map.assign(nvars, NO_RESULT);
         int idx = -(vid + 1);
-        ORACLE_ASSERT(idx < nvars && idx >= 0, VERTEX_INVALID);
-        ORACLE_ASSERT(v2c_map[idx] == NO_RESULT, VERTEX_INVALID);
+        ORACLE_ASSERT(idx < nvars && idx >= 0, UNKNOWN_ERROR);
+        ORACLE_ASSERT(v2c_map[idx] == NO_RESULT, UNKNOWN_ERROR);   // a variable is set once
         v2c_map[idx] = col;   // col2ext(col, SID_t)
     }
     uint64_t get_row_num() const { return col_num == 0 ? 0 : result_table.size() / col_num; }
@@ -711,17 +758,195 @@ public:
         req.pattern_step++;
     }
 
-    void execute_one_pattern(Query& req) {   // :932-1055 (no VERSATILE)
+    // :83-130 (BASIC): keep the rows whose `end` value is in the index list (its mt slice)
+    void index_to_known(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        int32_t tpid = pattern.subject, id01 = pattern.predicate, end = pattern.object;
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        int col = res.var2col(end);
+        ORACLE_ASSERT(col != NO_RESULT, VERTEX_INVALID);
+        ORACLE_ASSERT(id01 == PREDICATE_ID || id01 == TYPE_ID, OBJ_ERROR);
+        uint64_t sz = 0;
+        const uint32_t* edges = graph->get_index((uint32_t)tpid, pattern.direction, sz);
+        int start = req.mt_tid % req.mt_factor;
+        uint64_t length = sz / req.mt_factor;
+        std::vector<uint32_t> set;
+        for (uint64_t k = start * length; k < (start + 1) * length; k++) set.push_back(edges[k]);
+        if (start == req.mt_factor - 1)
+            for (uint64_t k = (start + 1) * length; k < sz; k++) set.push_back(edges[k]);
+        std::sort(set.begin(), set.end());
+        std::vector<uint32_t> updated;
+        uint64_t nrows = res.get_row_num();
+        for (uint64_t i = 0; i < nrows; i++)
+            if (std::binary_search(set.begin(), set.end(), res.get_row_col(i, col)))
+                res.append_row_to(i, updated);
+        res.result_table.swap(updated);
+        req.pattern_step++;
+    }
+
+    // :132-189 (BASIC): keep the rows whose `end` value is a neighbour of the constant
+    void const_to_known(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        int col = res.var2col(pattern.object);
+        ORACLE_ASSERT(col != NO_RESULT, VERTEX_INVALID);
+        uint64_t sz = 0;
+        const uint32_t* vids = graph->get_triples((uint32_t)pattern.subject, (uint32_t)pattern.predicate,
+                                                  pattern.direction, sz);
+        std::vector<uint32_t> set(vids, vids + sz);
+        std::sort(set.begin(), set.end());
+        std::vector<uint32_t> updated;
+        uint64_t nrows = res.get_row_num();
+        for (uint64_t i = 0; i < nrows; i++)
+            if (std::binary_search(set.begin(), set.end(), res.get_row_col(i, col)))
+                res.append_row_to(i, updated);
+        res.result_table.swap(updated);
+        req.pattern_step++;
+    }
+
+    // The versatile operators (:554-739) read the vertex's predicate list [v|PREDICATE_ID|d]
+    // and then the vertex's list for each of those predicates.
+    // C ?P ?X (:559-592): a (p, x) row for every predicate p of C and neighbour x over p.
+    void const_unknown_unknown(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        const uint32_t start = (uint32_t)pattern.subject;
+        const int d = pattern.direction;
+        uint64_t npids = 0;
+        const uint32_t* pids = graph->get_triples(start, PREDICATE_ID, d, npids);
+        std::vector<uint32_t> tpids(pids, pids + npids), updated;
+        for (uint32_t p : tpids) {
+            uint64_t sz = 0;
+            const uint32_t* vids = graph->get_triples(start, p, d, sz);
+            for (uint64_t k = 0; k < sz; k++) {
+                updated.push_back(p);
+                updated.push_back(vids[k]);
+            }
+        }
+        res.result_table.swap(updated);
+        res.col_num = 2;
+        res.add_var2col(pattern.predicate, 0);
+        res.add_var2col(pattern.object, 1);
+        req.pattern_step++;
+    }
+
+    // ?X ?P ?Y (:600-640): every known row times its start's (p, y) pairs.
+    void known_unknown_unknown(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        const int d = pattern.direction;
+        std::vector<uint32_t> updated;
+        uint64_t nrows = res.get_row_num();
+        int cs = res.var2col(pattern.subject);
+        for (uint64_t i = 0; i < nrows; i++) {
+            uint32_t cur = res.get_row_col(i, cs);
+            uint64_t npids = 0;
+            const uint32_t* pids = graph->get_triples(cur, PREDICATE_ID, d, npids);
+            std::vector<uint32_t> tpids(pids, pids + npids);
+            for (uint32_t p : tpids) {
+                uint64_t sz = 0;
+                const uint32_t* vids = graph->get_triples(cur, p, d, sz);
+                for (uint64_t k = 0; k < sz; k++) {
+                    res.append_row_to(i, updated);
+                    updated.push_back(p);
+                    updated.push_back(vids[k]);
+                }
+            }
+        }
+        res.result_table.swap(updated);
+        res.add_var2col(pattern.predicate, res.col_num);
+        res.add_var2col(pattern.object, res.col_num + 1);
+        res.col_num += 2;
+        req.pattern_step++;
+    }
+
+    // ?X ?P C (:649-689): a row times every predicate of its start that reaches C.
+    void known_unknown_const(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        const int d = pattern.direction;
+        const uint32_t end = (uint32_t)pattern.object;
+        std::vector<uint32_t> updated;
+        uint64_t nrows = res.get_row_num();
+        int cs = res.var2col(pattern.subject);
+        for (uint64_t i = 0; i < nrows; i++) {
+            uint32_t prev = res.get_row_col(i, cs);
+            uint64_t npids = 0;
+            const uint32_t* pids = graph->get_triples(prev, PREDICATE_ID, d, npids);
+            std::vector<uint32_t> tpids(pids, pids + npids);
+            for (uint32_t p : tpids) {
+                uint64_t sz = 0;
+                const uint32_t* vids = graph->get_triples(prev, p, d, sz);
+                for (uint64_t k = 0; k < sz; k++)
+                    if (vids[k] == end) {
+                        res.append_row_to(i, updated);
+                        updated.push_back(p);
+                        break;
+                    }
+            }
+        }
+        res.result_table.swap(updated);
+        res.add_var2col(pattern.predicate, res.col_num);
+        res.col_num += 1;
+        req.pattern_step++;
+    }
+
+    // C1 ?P C2 (:697-739): every predicate of C1 that reaches C2; first pattern only.
+    void const_unknown_const(Query& req) {
+        Pattern& pattern = req.patterns[req.pattern_step];
+        ORACLE_ASSERT(pattern.pred_type == 0, UNKNOWN_PATTERN);
+        Result& res = req.result;
+        ORACLE_ASSERT(res.col_num == 0, FIRST_PATTERN_ERROR);
+        const uint32_t start = (uint32_t)pattern.subject, end = (uint32_t)pattern.object;
+        const int d = pattern.direction;
+        uint64_t npids = 0;
+        const uint32_t* pids = graph->get_triples(start, PREDICATE_ID, d, npids);
+        std::vector<uint32_t> tpids(pids, pids + npids), updated;
+        for (uint32_t p : tpids) {
+            uint64_t sz = 0;
+            const uint32_t* vids = graph->get_triples(start, p, d, sz);
+            for (uint64_t k = 0; k < sz; k++)
+                if (vids[k] == end) {
+                    updated.push_back(p);
+                    break;
+                }
+        }
+        res.result_table.swap(updated);
+        res.col_num = 1;
+        res.add_var2col(pattern.predicate, 0);
+        req.pattern_step++;
+    }
+
+    void execute_one_pattern(Query& req) {   // :932-1055
         Pattern& pattern = req.patterns[req.pattern_step];
         int32_t start = pattern.subject, predicate = pattern.predicate, end = pattern.object;
         if (req.pattern_step == 0 && req.start_from_index()) {
-            // index_to_known is not part of the path
-            ORACLE_ASSERT(req.result.var2col(end) == NO_RESULT, UNKNOWN_PATTERN);
-            index_to_unknown(req);
+            if (req.result.var2col(end) != NO_RESULT)
+                index_to_known(req);
+            else
+                index_to_unknown(req);
             return;
         }
-        ORACLE_ASSERT(req.result.var_stat(predicate) == CONST_VAR, UNKNOWN_PATTERN);
+        if (req.result.var_stat(predicate) != CONST_VAR) {
+            // an unknown (or earlier bound) predicate: the VERSATILE operators, on a store that
+            // holds the vertex-predicate lists; without them the pattern is unsupported
+            ORACLE_ASSERT(graph->versatile, UNKNOWN_PATTERN);
+            switch (const_pair(req.result.var_stat(start), req.result.var_stat(end))) {
+            case const_pair(CONST_VAR, UNKNOWN_VAR): const_unknown_unknown(req); break;
+            case const_pair(CONST_VAR, CONST_VAR): const_unknown_const(req); break;
+            case const_pair(KNOWN_VAR, UNKNOWN_VAR): known_unknown_unknown(req); break;
+            case const_pair(KNOWN_VAR, CONST_VAR): known_unknown_const(req); break;
+            default: throw error_code(UNKNOWN_PATTERN);   // [C|?|K], [K|?|K], [U|?|*]
+            }
+            return;
+        }
         switch (const_pair(req.result.var_stat(start), req.result.var_stat(end))) {
+        case const_pair(CONST_VAR, KNOWN_VAR): const_to_known(req); break;
         case const_pair(CONST_VAR, UNKNOWN_VAR): const_to_unknown(req); break;
         case const_pair(KNOWN_VAR, CONST_VAR): known_to_const(req); break;
         case const_pair(KNOWN_VAR, KNOWN_VAR): known_to_known(req); break;
@@ -729,7 +954,7 @@ public:
         case const_pair(UNKNOWN_VAR, CONST_VAR):
         case const_pair(UNKNOWN_VAR, KNOWN_VAR):
         case const_pair(UNKNOWN_VAR, UNKNOWN_VAR): throw error_code(UNKNOWN_SUB);
-        default: throw error_code(UNKNOWN_PATTERN);   // CONST|CONST, CONST|KNOWN (const_to_known)
+        default: throw error_code(UNKNOWN_PATTERN);   // CONST|CONST
         }
     }
 
@@ -754,9 +979,12 @@ struct OracleStore {
 
 extern "C" {
 
-// Build the store from n x 3 (s, p, o) triples for each direction.
-void* orc_store_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos) {
+// Build the store from n x 3 (s, p, o) triples for each direction; versatile adds the
+// vertex-predicate lists the unknown-predicate operators read.
+void* orc_store_build2(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
+                       int versatile) {
     auto* h = new OracleStore();
+    h->store.versatile = versatile != 0;
     std::vector<triple_t> a(n_pso), b(n_pos);
     for (uint64_t i = 0; i < n_pso; ++i) a[i] = {pso[3 * i], pso[3 * i + 1], pso[3 * i + 2]};
     for (uint64_t i = 0; i < n_pos; ++i) b[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
@@ -767,6 +995,10 @@ void* orc_store_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, 
         return nullptr;
     }
     return h;
+}
+
+void* orc_store_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos) {
+    return orc_store_build2(pso, n_pso, pos, n_pos, 0);
 }
 
 void orc_store_free(void* h) { delete (OracleStore*)h; }
@@ -931,6 +1163,37 @@ int orc_step(void* h, int op, const uint32_t* table, uint64_t rows, int cols, in
     *out = buf;
     *out_cols = q.result.col_num;
     *out_rows = q.result.col_num ? t.size() / q.result.col_num : 0;
+    return 0;
+}
+
+// Run one pattern through the dispatch (execute_one_pattern) on a given table: rows x cols,
+// column i holding variable -(i + 1), nvars >= cols variables in all.  pattern: 5 int32 as in
+// orc_query_run.  The table plays the result a pattern group starts with (as a union or
+// optional sub-query inherits one), so the pattern runs as pattern 0: an index pattern whose
+// object is known runs index_to_known, with the given mt slice.  On success *out (malloc'd)
+// is the new table and v2c receives nvars entries.
+int orc_pattern(void* h, const uint32_t* table, uint64_t rows, int cols, int nvars,
+                const int32_t* pattern, int mt_tid, int mt_factor, uint32_t** out, uint64_t* out_rows,
+                int* out_cols, int32_t* v2c) {
+    const Store* st = &((OracleStore*)h)->store;
+    Query q;
+    q.patterns.push_back({pattern[0], pattern[1], pattern[2], pattern[3], pattern[4]});
+    q.mt_tid = mt_tid;
+    q.mt_factor = mt_factor < 1 ? 1 : mt_factor;
+    q.result.nvars = nvars;
+    q.result.col_num = cols;
+    q.result.v2c_map.assign(nvars, NO_RESULT);
+    for (int i = 0; i < cols && i < nvars; ++i) q.result.v2c_map[i] = i;
+    q.result.result_table.assign(table, table + rows * (uint64_t)cols);
+    int rc = Engine(st).run(q);
+    if (rc) return rc;
+    auto& t = q.result.result_table;
+    uint32_t* buf = (uint32_t*)std::malloc(std::max<size_t>(t.size(), 1) * 4);
+    if (!t.empty()) std::memcpy(buf, t.data(), t.size() * 4);
+    *out = buf;
+    *out_cols = q.result.col_num;
+    *out_rows = q.result.col_num ? t.size() / q.result.col_num : 0;
+    for (int i = 0; i < nvars; ++i) v2c[i] = q.result.v2c_map[i];
     return 0;
 }
 

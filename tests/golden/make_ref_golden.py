@@ -99,6 +99,53 @@ def bound_cases(o, v, inst):
             ("empty_table", t3, [0])]
 
 
+def versatile_queries(v, inst):
+    """Queries with an unknown predicate (the versatile operators, sparql.hpp:554-739) and with a
+    constant start whose object is already known (const_to_known, :132-189)."""
+    import wukong_b200 as wk
+    units, persons, courses = inst[v["t_unit"]], inst[v["t_person_a"]], inst[v["t_course"]]
+    u0, u1, p0, c0 = int(units[0]), int(units[1]), int(persons[3]), int(courses[2])
+    m, t, s = v["p_member_of"], v["p_takes"], v["p_sub_org_of"]
+    Q = wk.Query
+    return [
+        ("v_const_unknown_unknown_out", Q([(p0, -1, wk.OUT, -2)], nvars=2)),
+        ("v_const_unknown_unknown_in", Q([(u0, -1, wk.IN, -2)], nvars=2)),
+        ("v_const_unknown_const", Q([(p0, -1, wk.OUT, u0)], nvars=1)),
+        ("v_const_unknown_const_none", Q([(p0, -1, wk.OUT, u1)], nvars=1)),
+        ("v_known_unknown_unknown", Q([(u0, m, wk.IN, -1), (-1, -2, wk.OUT, -3)], nvars=3)),
+        ("v_known_unknown_unknown_in", Q([(u0, m, wk.IN, -1), (-1, t, wk.OUT, -2), (-2, -3, wk.IN, -4)], nvars=4)),
+        ("v_known_unknown_const", Q([(u0, m, wk.IN, -1), (-1, -2, wk.OUT, u0)], nvars=2)),
+        ("v_chain_after_versatile", Q([(p0, -1, wk.OUT, -2), (-2, -3, wk.OUT, -4)], nvars=4)),
+        ("v_known_pred_var", Q([(u0, m, wk.IN, -1), (-1, -2, wk.OUT, -3), (-3, -2, wk.OUT, -4)], nvars=4)),
+        ("v_unknown_start", Q([(-1, -2, wk.OUT, -3)], nvars=3)),
+        ("v_const_unknown_known", Q([(u0, m, wk.IN, -1), (u0, -2, wk.IN, -1)], nvars=2)),
+        ("const_to_known", Q([(u0, m, wk.IN, -1), (-1, t, wk.OUT, -2), (c0, t, wk.IN, -1)], nvars=2)),
+        ("const_to_known_index_const", Q([(u0, m, wk.IN, -1), (v["t_person_a"], 1, wk.IN, -1)], nvars=1)),
+        ("const_to_known_type", Q([(u0, m, wk.IN, -1), (-1, 1, wk.OUT, -2), (p0, 1, wk.OUT, -2)], nvars=2)),
+        ("const_to_known_second_pred", Q([(u1, m, wk.IN, -1), (u0, s, wk.OUT, -2), (u1, m, wk.IN, -1)], nvars=2)),
+    ]
+
+
+def pattern_cases(o, v, inst):
+    """(name, table, nvars, pattern, mt_tid, mt_factor): one pattern over a given table, as the
+    first pattern of a group that inherited it (index_to_known runs only there)."""
+    import wukong_b200 as wk
+    persons, courses, units = inst[v["t_person_a"]], inst[v["t_course"]], inst[v["t_unit"]]
+    mixed = np.concatenate([persons[:300], courses[:80], persons[-40:]]).reshape(-1, 1).astype(np.uint32)
+    two = np.stack([persons[:60], np.resize(units, 60)], axis=1).astype(np.uint32)
+    cases = [("c2k", mixed, 1, [int(units[0]), v["p_member_of"], -1, wk.IN, 0], 0, 1),
+             ("c2k_second_col", two, 2, [int(persons[5]), v["p_member_of"], -2, wk.OUT, 0], 0, 1),
+             ("kuu_out", mixed[:50], 3, [-1, -2, -3, wk.OUT, 0], 0, 1),
+             ("kuu_in", np.resize(courses, 40).reshape(-1, 1).astype(np.uint32), 3, [-1, -2, -3, wk.IN, 0], 0, 1),
+             ("kuc", two, 3, [-1, -3, int(units[0]), wk.OUT, 0], 0, 1),
+             ("kuc_second_col", two, 3, [-2, -3, int(inst[v["t_org"]][0]), wk.OUT, 0], 0, 1)]
+    for mt in (1, 2, 3):
+        for tid in range(mt):
+            cases.append(("i2k_mt%d_%d" % (mt, tid), mixed, 1, [v["t_person_a"], 1, -1, wk.IN, 0], tid, mt))
+    cases.append(("i2k_predicate_index", mixed, 1, [v["p_takes"], 0, -1, wk.IN, 0], 0, 1))
+    return cases
+
+
 def main():
     import oracle
     import refengine
@@ -132,6 +179,29 @@ def main():
                              "limit": limit, "offset": offset, "rows": int(rows.shape[0]),
                              "cols": int(rows.shape[1]), "table_sha256": digest(rows),
                              "head": rows[:3].tolist()})
+    # the versatile store (the reference's default build): the same graph with every vertex's
+    # predicate lists
+    ov = oracle.OracleStore(tr, versatile=True)
+    gv = refengine.graph_from_store(ov, tr, v)
+    doc["versatile"] = []
+    for name, q in versatile_queries(v, inst):
+        st, rows, v2c = gv.run(q.flat(), q.nvars, required=refengine.bound_vars(q.flat()) or [-1])
+        srt = oracle.sorted_rows(rows) if st == 0 else np.zeros((0, 0), np.uint32)
+        doc["versatile"].append({"name": name, "patterns": [list(map(int, p)) for p in q.patterns],
+                                 "nvars": q.nvars, "status": int(st),
+                                 "v2c": [int(x) for x in v2c] if st == 0 else None,
+                                 "rows": int(srt.shape[0]),
+                                 "cols": int(srt.shape[1]) if srt.ndim == 2 else 0,
+                                 "sorted_sha256": digest(srt), "head": srt[:3].tolist()})
+    doc["patterns"] = []
+    for name, table, nvars, pat, tid, mt in pattern_cases(ov, v, inst):
+        st, rows, v2c = gv.pattern(table, nvars, pat, tid, mt)
+        doc["patterns"].append({"name": name, "table": table.tolist(), "nvars": nvars,
+                                "pattern": [int(x) for x in pat], "mt_tid": tid, "mt_factor": mt,
+                                "status": int(st), "v2c": [int(x) for x in v2c] if st == 0 else None,
+                                "rows": int(rows.shape[0]) if st == 0 else 0,
+                                "cols": int(rows.shape[1]) if st == 0 else 0,
+                                "table_sha256": digest(rows) if st == 0 else None})
     doc["bound"] = []
     for name, table, bcols in bound_cases(o, v, inst):
         got = refengine.filter_bound(table, bcols)
@@ -141,7 +211,8 @@ def main():
     with open(OUT, "w") as f:
         json.dump(doc, f, indent=1)
     print("wrote", OUT, len(doc["queries"]), "queries,", len(doc["final"]), "final-stage cases,",
-          len(doc["bound"]), "BOUND cases")
+          len(doc["bound"]), "BOUND cases,", len(doc["versatile"]), "versatile queries,",
+          len(doc["patterns"]), "single patterns")
 
 
 if __name__ == "__main__":

@@ -194,3 +194,168 @@ def test_gpu_bound_filter_large_and_refusals(ctx):
     assert e.value.code == wk.E_BADARG
     out.free()
     tin.free()
+
+
+@pytest.fixture(scope="module")
+def oracle_versatile(graph20):
+    import oracle
+    return oracle.OracleStore(graph20["triples"], versatile=True)
+
+
+def test_oracle_versatile_queries_reproduce_reference(oracle_versatile, golden):
+    import oracle
+    import wukong_b200 as wk
+    for g in golden["versatile"]:
+        q = wk.Query(g["patterns"], nvars=g["nvars"])
+        st, rows, v2c = oracle_versatile.run(q.flat(), q.nvars)
+        assert st == g["status"], g["name"]
+        if st == 0:
+            s = oracle.sorted_rows(rows)
+            assert s.shape == (g["rows"], g["cols"]), g["name"]
+            assert _digest(s) == g["sorted_sha256"], g["name"]
+            assert list(v2c) == g["v2c"], g["name"]
+
+
+def test_oracle_single_patterns_reproduce_reference(oracle_versatile, golden):
+    for g in golden["patterns"]:
+        t = np.array(g["table"], np.uint32).reshape(len(g["table"]), -1)
+        st, rows, v2c = oracle_versatile.pattern(t, g["nvars"], g["pattern"], g["mt_tid"], g["mt_factor"])
+        assert st == g["status"], g["name"]
+        if st == 0:
+            assert rows.shape == (g["rows"], g["cols"]), g["name"]
+            assert _digest(rows) == g["table_sha256"], g["name"]   # row for row
+            assert list(v2c) == g["v2c"], g["name"]
+
+
+def test_non_versatile_store_refuses_unknown_predicates(graph20, golden):
+    """Without the vertex-predicate lists the unknown-predicate patterns are unsupported, as in
+    a reference build without VERSATILE; const_to_known needs no extra lists."""
+    import wukong_b200 as wk
+    o = graph20["oracle"]
+    for g in golden["versatile"]:
+        q = wk.Query(g["patterns"], nvars=g["nvars"])
+        st, _, _ = o.run(q.flat(), q.nvars)
+        if any(p[1] < 0 for p in g["patterns"]) and g["status"] == 0:
+            assert st == wk.UNKNOWN_PATTERN, g["name"]
+
+
+@pytest.mark.parametrize("versatile", [False, True])
+def test_reference_engine_dispatch_live(built, versatile):
+    """Where the reference engine library was built: seeded random plans (the dispatch test's
+    generator) give the oracle's status, table and column map through the reference's own
+    execute_sparql_query, on a store without and with the vertex-predicate lists."""
+    import oracle
+    import refengine
+    import wukong_b200 as wk
+    if not refengine.available() or not versatile:
+        # the reference library is a VERSATILE build: it runs unknown predicates either way,
+        # so only the versatile store can be compared with it
+        pytest.skip("needs the reference engine library and a versatile store")
+    V = 1 << 17
+    tr = np.array([(V + 1, 5, V + 2), (V + 2, 6, V + 3), (V + 1, 1, 7), (V + 3, 5, V + 1),
+                   (V + 2, 1, 7), (V + 3, 6, V + 2)], np.uint32)
+    o = oracle.OracleStore(tr, versatile=True)
+    g = refengine.graph_from_store(o, tr, None)
+    rng = np.random.default_rng(29)
+    consts = [V + 1, V + 2, V + 3, 7]
+    for _ in range(400):
+        nvars = int(rng.integers(1, 4))
+        pats = []
+        for k in range(int(rng.integers(1, 5))):
+            def term():
+                if rng.random() < 0.5:
+                    return -int(rng.integers(1, nvars + 1))   # in range: the engine asserts otherwise
+                return int(rng.choice(consts))
+            pats.append((term(), int(rng.choice([5, 6, wk.TYPE_ID, -1])), int(rng.integers(0, 2)), term()))
+        q = wk.Query(pats, nvars=nvars)
+        st, tab, v2c = o.run(q.flat(), q.nvars)
+        rst, rtab, rv2c = g.run(q.flat(), q.nvars, required=refengine.bound_vars(q.flat()) or [-1])
+        if st == 0 and rst == 0 and len(refengine.bound_vars(q.flat())) != tab.shape[1]:
+            continue   # a table replaced mid-plan: the projection is not the identity
+        assert st == rst, (pats, st, rst)
+        if st == 0:
+            assert np.array_equal(oracle.sorted_rows(tab), oracle.sorted_rows(rtab)), pats
+            assert list(v2c) == list(rv2c), pats
+
+
+@pytest.fixture(scope="module")
+def ctx_versatile(graph20):
+    """A context holding the 20-organisation store built with the vertex-predicate lists."""
+    import wukong_b200 as wk
+    g = wk.GStore(graph20["triples"], versatile=True)
+    c = wk.Context(0)
+    c.upload_gstore(g)
+    yield c
+    c.close()
+    g.close()
+
+
+@pytest.mark.gpu
+def test_gpu_versatile_queries_reproduce_reference(ctx_versatile, golden):
+    import oracle
+    import wukong_b200 as wk
+    for mode in (wk.MODE_PLAIN, wk.MODE_RESIDENT, wk.MODE_GRAPH):
+        for g in golden["versatile"]:
+            q = wk.Query(g["patterns"], nvars=g["nvars"])
+            if g["status"]:
+                with pytest.raises(wk.WukongError) as e:
+                    ctx_versatile.execute(q, mode)
+                assert e.value.code == g["status"], (g["name"], mode)
+                continue
+            t, v2c = ctx_versatile.execute(q, mode)
+            s = oracle.sorted_rows(t)
+            assert s.shape == (g["rows"], g["cols"]), (g["name"], mode)
+            assert _digest(s) == g["sorted_sha256"], (g["name"], mode)
+            assert v2c == g["v2c"], (g["name"], mode)
+
+
+@pytest.mark.gpu
+def test_gpu_single_patterns_reproduce_reference(ctx_versatile, golden):
+    """const_to_known, index_to_known (every mt slice) and the known-start versatile steps
+    through their own entry points, row for row against the reference engine."""
+    import wukong_b200 as wk
+    c = ctx_versatile
+    for g in golden["patterns"]:
+        t = np.array(g["table"], np.uint32).reshape(len(g["table"]), -1)
+        s, p, o, d, _ = g["pattern"]
+        tin = c.table(t, capacity=t.size)
+        out = c.table(capacity=1)
+        name = g["name"]
+        if name.startswith("c2k"):
+            c.const_to_known(tin, -o - 1, s, p, d, out)
+        elif name.startswith("i2k"):
+            c.index_to_known(tin, -o - 1, s, d, out, g["mt_tid"], g["mt_factor"])
+        elif name.startswith("kuu"):
+            c.known_unknown_unknown(tin, -s - 1, d, out)
+        elif name.startswith("kuc"):
+            c.known_unknown_const(tin, -s - 1, o, d, out)
+        got = out.download()
+        assert g["status"] == 0 and got.shape == (g["rows"], g["cols"]), name
+        assert _digest(got) == g["table_sha256"], name
+        tin.free()
+        out.free()
+
+
+@pytest.mark.gpu
+def test_gpu_constant_versatile_steps_and_refusals(ctx, ctx_versatile, golden):
+    """The constant forms' entry points give the whole-query answers; a store without the
+    vertex-predicate lists refuses unknown predicates; batches refuse versatile plans."""
+    import oracle
+    import wukong_b200 as wk
+    byname = {g["name"]: g for g in golden["versatile"]}
+    for name, call in (("v_const_unknown_unknown_out", "uu"), ("v_const_unknown_const", "uc")):
+        g = byname[name]
+        s, p, d, o = g["patterns"][0]
+        out = ctx_versatile.table(capacity=1)
+        if call == "uu":
+            ctx_versatile.const_unknown_unknown(s, d, out)
+        else:
+            ctx_versatile.const_unknown_const(s, o, d, out)
+        assert _digest(oracle.sorted_rows(out.download())) == g["sorted_sha256"], name
+        out.free()
+    q = wk.Query(byname["v_known_unknown_unknown"]["patterns"], nvars=3)
+    with pytest.raises(wk.WukongError) as e:
+        ctx.execute(q, wk.MODE_RESIDENT)
+    assert e.value.code == wk.UNKNOWN_PATTERN
+    res = ctx_versatile.batch([q])
+    assert res[0][1] == wk.E_UNSUPPORTED

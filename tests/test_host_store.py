@@ -126,16 +126,18 @@ def test_capi_exports_every_declared_symbol(built):
     assert set(wk.exported_symbols()) <= names
 
 
-def test_random_plans_dispatch_like_the_oracle(built):
+@pytest.mark.parametrize("versatile", [False, True])
+def test_random_plans_dispatch_like_the_oracle(built, versatile):
     """Seeded random pattern lists (constants, variables bound or not, index starts, both
     directions, out-of-range variables, unknown predicates): the library's host-side dispatch
-    (wk_query_validate) gives the oracle's status and, on success, its column map."""
+    (wk_query_validate_ex) gives the oracle's status and, on success, its column map, for a
+    store without and with the vertex-predicate lists."""
     import oracle
     import wukong_b200 as wk
     V = 1 << 17
     tr = np.array([(V + 1, 5, V + 2), (V + 2, 6, V + 3), (V + 1, 1, 7), (V + 3, 5, V + 1),
                    (V + 2, 1, 7), (V + 3, 6, V + 2)], np.uint32)
-    o = oracle.OracleStore(tr)
+    o = oracle.OracleStore(tr, versatile=versatile)
     rng = np.random.default_rng(11)
     consts = [V + 1, V + 2, V + 3, 7]
     seen = set()
@@ -152,7 +154,7 @@ def test_random_plans_dispatch_like_the_oracle(built):
             d = int(rng.integers(0, 2))
             pats.append((s, p, d, term()))
         q = wk.Query(pats, nvars=nvars)
-        rc, v2c, cols = wk.validate(q)
+        rc, v2c, cols = wk.validate(q, versatile=versatile)
         st, tab, ov2c = o.run(q.flat(), q.nvars)
         assert rc == st, (pats, nvars, rc, st)
         if st == 0:

@@ -270,6 +270,7 @@ int build_plan(wk_ctx* ctx, BatchState* b, const wk_query* queries, uint32_t n, 
     P.steps.resize((size_t)n * kMaxBatchLevels);
     P.nsteps.assign(n, 0);
     const int max_cols = ctx->cfg.max_cols;
+    const bool versatile = ctx->versatile;
 #pragma omp parallel if (n >= 2048)
     {
         std::vector<wk::PlanStep> st;
@@ -279,8 +280,11 @@ int build_plan(wk_ctx* ctx, BatchState* b, const wk_query* queries, uint32_t n, 
         for (int64_t qi = 0; qi < (int64_t)n; ++qi) {
             const uint32_t q = (uint32_t)qi;
             wk::ColMap cm(queries[q].nvars);
-            int rc = wk::resolve_plan(queries[q], max_cols, st, cm);
+            int rc = wk::resolve_plan(queries[q], max_cols, st, cm, versatile);
             if (rc == WK_SUCCESS && (int)st.size() > kMaxBatchLevels) rc = WK_E_CAPACITY;
+            // the unknown-predicate operators walk several lists per row: single queries only
+            for (auto& x : st)
+                if (rc == WK_SUCCESS && wk::is_versatile_step(x.kind)) rc = WK_E_UNSUPPORTED;
             if (rc == WK_SUCCESS && queries[q].mt_factor != 1) rc = WK_E_UNSUPPORTED;
             if (rc) {
                 P.status[q] = rc;

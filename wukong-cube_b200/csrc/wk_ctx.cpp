@@ -190,7 +190,8 @@ int wk_ctx::clear_ctl_err() {
 // ---------------------------------------------------------------- plan resolution
 namespace wk {
 
-int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm) {
+int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm,
+                 bool versatile) {
     steps.clear();
     if (q.n_patterns < 0 || q.nvars < 0 || (q.n_patterns > 0 && !q.patterns)) return WK_E_BADARG;
     for (int i = 0; i < q.n_patterns; ++i) {
@@ -199,12 +200,14 @@ int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, 
         PlanStep st{};
         st.dir = p.direction;
         if (i == 0 && is_tpid(p.subject)) {
-            // start_from_index (query.hpp:816-838) -> index_to_unknown (gpu_engine.hpp:65-100)
+            // start_from_index (query.hpp:816-838) -> index_to_unknown (sparql.hpp:197-234)
             if (p.predicate != WK_PREDICATE_ID && p.predicate != WK_TYPE_ID) return WK_OBJ_ERROR;
-            if (p.pred_type != 0) return WK_UNKNOWN_PATTERN;
             int vs = cm.var_stat(p.object);
             if (vs < 0 || vs == 2) return WK_VERTEX_INVALID;
-            if (vs == 0) return WK_UNKNOWN_PATTERN;   // index_to_known: not on the GPU path
+            // index_to_known needs a known object, and nothing is bound before the first
+            // pattern; the single step wk_step_index_to_known runs it over a given table
+            if (vs == 0) return WK_UNKNOWN_PATTERN;
+            if (p.pred_type != 0) return WK_UNKNOWN_PATTERN;
             st.kind = PlanStep::kIndex;
             st.start_const = (uint32_t)p.subject;
             st.in_cols = 0;
@@ -214,10 +217,59 @@ int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, 
             steps.push_back(st);
             continue;
         }
-        if (p.predicate < 0) return WK_UNKNOWN_PATTERN;   // versatile (unknown predicate)
+        const int vs = cm.var_stat(p.subject), ve = cm.var_stat(p.object);
+        if (p.predicate < 0) {
+            // an unknown (or earlier bound) predicate: the versatile operators (sparql.hpp:
+            // 554-739, dispatch :954-1012); they read the vertex-predicate lists
+            const int vp = cm.var_stat(p.predicate);
+            if (vp < 0) return WK_VERTEX_INVALID;
+            if (!versatile) return WK_UNKNOWN_PATTERN;
+            if (vs < 0 || ve < 0) return WK_VERTEX_INVALID;
+            if (p.pred_type != 0) return WK_UNKNOWN_PATTERN;
+            if (vs == 2 && ve == 1) {            // C ?P ?X: the table becomes (p, x) rows
+                st.kind = PlanStep::kCUU;
+                st.start_const = (uint32_t)p.subject;
+                st.in_cols = 0;
+                st.out_cols = 2;
+                cm.col_num = 2;
+                // add_var2col asserts (UNKNOWN_ERROR) on a variable already bound, the
+                // predicate's first, then the object's (which may be the same variable)
+                if (!cm.bind_new(p.predicate, 0) || !cm.bind_new(p.object, 1)) return WK_UNKNOWN_ERROR;
+            } else if (vs == 2 && ve == 2) {     // C1 ?P C2
+                if (cm.col_num != 0) return WK_FIRST_PATTERN_ERROR;
+                st.kind = PlanStep::kCUC;
+                st.start_const = (uint32_t)p.subject;
+                st.end_const = (uint32_t)p.object;
+                st.in_cols = 0;
+                st.out_cols = 1;
+                cm.col_num = 1;
+                if (!cm.bind_new(p.predicate, 0)) return WK_UNKNOWN_ERROR;
+            } else if (vs == 0 && ve == 1) {     // ?X ?P ?Y
+                st.kind = PlanStep::kKUU;
+                st.cs = cm.col(p.subject);
+                st.in_cols = cm.col_num;
+                st.out_cols = cm.col_num + 2;
+                if (st.out_cols > max_cols) return WK_E_CAPACITY;
+                if (!cm.bind_new(p.predicate, cm.col_num) || !cm.bind_new(p.object, cm.col_num + 1))
+                    return WK_UNKNOWN_ERROR;
+                cm.col_num += 2;
+            } else if (vs == 0 && ve == 2) {     // ?X ?P C
+                st.kind = PlanStep::kKUC;
+                st.cs = cm.col(p.subject);
+                st.end_const = (uint32_t)p.object;
+                st.in_cols = cm.col_num;
+                st.out_cols = cm.col_num + 1;
+                if (st.out_cols > max_cols) return WK_E_CAPACITY;
+                if (!cm.bind_new(p.predicate, cm.col_num)) return WK_UNKNOWN_ERROR;
+                cm.col_num += 1;
+            } else {
+                return WK_UNKNOWN_PATTERN;   // [C|?|K], [K|?|K], [U|?|*]
+            }
+            steps.push_back(st);
+            continue;
+        }
         if (p.pred_type != 0) return WK_ATTR_DISABLE;
         st.pid = (uint32_t)p.predicate;
-        const int vs = cm.var_stat(p.subject), ve = cm.var_stat(p.object);
         if (vs < 0 || ve < 0) return WK_VERTEX_INVALID;
         if (vs == 2 && ve == 1) {
             if (cm.col_num != 0) return WK_FIRST_PATTERN_ERROR;
@@ -227,6 +279,12 @@ int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, 
             st.out_cols = 1;
             cm.bind(p.object, 0);
             cm.col_num = 1;
+        } else if (vs == 2 && ve == 0) {
+            // C P ?X with ?X known: const_to_known (sparql.hpp:132-189)
+            st.kind = PlanStep::kC2K;
+            st.start_const = (uint32_t)p.subject;
+            st.ce = cm.col(p.object);
+            st.in_cols = st.out_cols = cm.col_num;
         } else if (vs == 0 && ve == 2) {
             st.kind = PlanStep::kK2C;
             st.cs = cm.col(p.subject);
@@ -248,7 +306,7 @@ int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, 
         } else if (vs == 1) {
             return WK_UNKNOWN_SUB;
         } else {
-            return WK_UNKNOWN_PATTERN;   // CONST|CONST, CONST|KNOWN
+            return WK_UNKNOWN_PATTERN;   // CONST|CONST
         }
         steps.push_back(st);
     }
@@ -282,6 +340,42 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
         if (grid_override > 0) grid = grid_override;
         cudaError_t e = launch_list(a, grid, s);
         if (e != cudaSuccess) return ctx->cuda_fail(e, "list kernel launch");
+        return WK_SUCCESS;
+    }
+    if (is_versatile_step(st.kind)) {
+        // one virtual row for the constant forms; the flat scratch holds the per-row counts
+        const bool virt = st.kind == PlanStep::kCUU || st.kind == PlanStep::kCUC;
+        if (!virt && (!in || st.in_cols <= 0)) return WK_E_BADARG;
+        if (!ctx->d_flat) return ctx->fail(WK_E_BADARG, "versatile step without its scratch");
+        VersArgs v{};
+        v.store = ctx->dev_store();
+        v.vp_seg = ctx->seg_of(1, kPredicateId, st.dir);
+        v.pseg = ctx->d_pseg;
+        v.n_pseg = ctx->n_pseg;
+        v.op = st.kind == PlanStep::kKUU ? kVKUU : st.kind == PlanStep::kKUC ? kVKUC
+             : st.kind == PlanStep::kCUU ? kVCUU : kVCUC;
+        v.dir = st.dir;
+        v.virtual_row = virt ? 1 : 0;
+        v.start_const = st.start_const;
+        v.end_const = st.end_const;
+        v.cs = st.cs;
+        v.cin = virt ? 0 : st.in_cols;
+        v.in_rows = in ? in->d_rows : nullptr;
+        v.in = in ? in->d : nullptr;
+        v.w_in = virt ? 0 : st.in_cols;
+        v.in_cap_rows = virt ? 1 : in->cap / st.in_cols;
+        if (!virt && v.in_cap_rows > ctx->flat_cap_rows)
+            return ctx->fail(WK_E_BADARG, "versatile step scratch smaller than its input");
+        v.out = out->d;
+        v.w_out = st.out_cols;
+        v.out_cap_rows = out->cap / st.out_cols;
+        v.out_rows = out->d_rows;
+        v.pos = reinterpret_cast<uint64_t*>(ctx->d_flat);
+        v.part = v.pos + 2 * ctx->flat_cap_rows + 1;
+        v.ctl = ctx->d_ctl;
+        v.sorted_lists = ctx->sorted_lists;
+        cudaError_t e = launch_versatile(v, vers_grid(virt ? 1 : v.in_cap_rows, ctx->sm_count), s);
+        if (e != cudaSuccess) return ctx->cuda_fail(e, "versatile step launch");
         return WK_SUCCESS;
     }
     if (!in || st.in_cols <= 0) return WK_E_BADARG;
@@ -382,6 +476,17 @@ StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s) {
         d.op = kXK2K;
         d.seg = ctx->seg_of(1, s.pid, s.dir);
         break;
+    case PlanStep::kC2K:
+        d.op = kXC2K;
+        d.start_key = make_key(s.start_const, s.pid, s.dir);
+        d.seg = ctx->seg_of(s.start_const, s.pid, s.dir);
+        break;
+    case PlanStep::kI2K:
+        d.op = kXI2K;
+        d.start_key = make_key(0, s.start_const, s.dir);
+        d.seg = ctx->seg_of(0, s.start_const, s.dir);
+        d.mt = (uint32_t)(s.mt_tid & 0xFFFF) | ((uint32_t)(s.mt_factor & 0xFFFF) << 16);
+        break;
     default:
         d.op = kXK2C;
         d.seg = ctx->seg_of(1, s.pid, s.dir);
@@ -445,6 +550,9 @@ int wk::ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas
     ctx->segs = parent->segs;
     ctx->index = parent->index;
     ctx->has_store = parent->has_store;
+    ctx->versatile = parent->versatile;
+    ctx->d_pseg = parent->d_pseg;
+    ctx->n_pseg = parent->n_pseg;
     ctx->borrowed_store = true;
     ctx->sorted_lists = parent->sorted_lists;
     ctx->default_lanes = parent->default_lanes;
@@ -477,6 +585,7 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     if (e == cudaSuccess) e = wk::serve_kernel_attrs();
     if (e == cudaSuccess) e = wk::flat_kernel_attrs();
     if (e == cudaSuccess) e = wk::final_kernel_attrs();
+    if (e == cudaSuccess) e = wk::versatile_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
     e = wk::dev_malloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
@@ -507,6 +616,7 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     }
     if (ctx->d_slots && !ctx->borrowed_store) cudaFree(ctx->d_slots);
     if (ctx->d_edges && !ctx->borrowed_store) cudaFree(ctx->d_edges);
+    if (ctx->d_pseg && !ctx->borrowed_store) cudaFree(ctx->d_pseg);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_heavy) cudaFree(ctx->d_heavy);
     if (ctx->d_flat) cudaFree(ctx->d_flat);
@@ -568,6 +678,29 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
     ctx->n_edges = n_edges;
     ctx->segs.assign(segs, segs + n_segs);
     ctx->index.build(ctx->segs.data(), n_segs);
+    {
+        // the predicate segments by pid * 2 + dir, for the versatile steps' list walks; a
+        // vertex-predicate segment (pid PREDICATE_ID) makes the store versatile
+        std::vector<wk::PredSeg> ps;
+        ctx->versatile = false;
+        for (uint32_t i = 0; i < n_segs; ++i) {
+            const wk_seg_meta& m = segs[i];
+            if (m.index || m.pid >= (1u << wk::kNbitsIdx)) continue;
+            if (m.pid == wk::kPredicateId) ctx->versatile = true;
+            ps.push_back(wk::PredSeg{m.pid * 2 + (uint32_t)m.dir, 0, wk::to_desc(m)});
+        }
+        std::sort(ps.begin(), ps.end(), [](const wk::PredSeg& a, const wk::PredSeg& b) { return a.key < b.key; });
+        if (ctx->d_pseg) cudaFree(ctx->d_pseg);
+        ctx->d_pseg = nullptr;
+        ctx->n_pseg = 0;
+        if (wk::dev_malloc(&ctx->d_pseg, std::max<size_t>(ps.size(), 1) * sizeof(wk::PredSeg)) != cudaSuccess) {
+            cudaGetLastError();
+            return ctx->fail(WK_E_OOM, "predicate segment table");
+        }
+        if (!ps.empty())
+            WK_CUDA(ctx, cudaMemcpy(ctx->d_pseg, ps.data(), ps.size() * sizeof(wk::PredSeg), cudaMemcpyHostToDevice));
+        ctx->n_pseg = (uint32_t)ps.size();
+    }
     ctx->has_store = true;
     {
         // are all lists ascending + unique?  (lets the filters binary-search long lists)
@@ -693,8 +826,14 @@ extern "C" int wk_table_device_ptr(wk_ctx* ctx, const wk_table* t, uint32_t** dp
 static int run_step_sync(wk_ctx* ctx, const wk::PlanStep& st, const wk_table* in, wk_table* out,
                          int32_t mt_tid, int32_t mt_factor) {
     if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    if (wk::is_versatile_step(st.kind)) {
+        if (!ctx->versatile)
+            return ctx->fail(WK_UNKNOWN_PATTERN, "the store holds no vertex-predicate lists (build it versatile)");
+        int rc = ctx->ensure_flat(in && in->cols > 0 ? in->cap / in->cols : 1);
+        if (rc) return rc;
+    }
     int flat = wk::kTileOnly;
-    if (in && in->cols > 0) {
+    if (in && in->cols > 0 && !wk::is_versatile_step(st.kind)) {
         int rc = ctx->ensure_status(in->cap / in->cols / wk::kTileRows + 2);
         if (rc) return rc;
         // the host syncs after every step here anyway, so it picks the launch by the row count
@@ -817,6 +956,88 @@ extern "C" int wk_step_known_to_const(wk_ctx* ctx, const wk_table* in, int32_t c
     return run_step_sync(ctx, st, in, out, 0, 1);
 }
 
+// C P ?X with ?X known: const_to_known (sparql.hpp:132-189).
+extern "C" int wk_step_const_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_end, uint32_t vid,
+                                      uint32_t pid, int32_t dir, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || in == out) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc = check_in(ctx, in, col_end, col_end);
+    if (rc) return rc;
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kC2K;
+    st.start_const = vid;
+    st.pid = pid;
+    st.dir = dir;
+    st.ce = col_end;
+    st.in_cols = st.out_cols = in->cols;
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+// IDX P ?X with ?X known: index_to_known (sparql.hpp:83-130), slice mt_tid of mt_factor.
+extern "C" int wk_step_index_to_known(wk_ctx* ctx, const wk_table* in, int32_t col_end, uint32_t tpid,
+                                      int32_t dir, int32_t mt_tid, int32_t mt_factor, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || in == out || mt_factor < 1 || mt_tid < 0 ||
+        mt_factor > 0xFFFF)
+        return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    int rc = check_in(ctx, in, col_end, col_end);
+    if (rc) return rc;
+    wk::PlanStep st{};
+    st.kind = wk::PlanStep::kI2K;
+    st.start_const = tpid;
+    st.dir = dir;
+    st.ce = col_end;
+    st.mt_tid = mt_tid % mt_factor;
+    st.mt_factor = mt_factor;
+    st.in_cols = st.out_cols = in->cols;
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+// The unknown-predicate steps (sparql.hpp:554-739) on a versatile store.
+static int versatile_step(wk_ctx* ctx, wk::PlanStep::Kind kind, const wk_table* in, int32_t col_start,
+                          uint32_t start_vid, uint32_t end_vid, int32_t dir, wk_table* out) {
+    if (!ctx || !out || (dir != WK_IN && dir != WK_OUT) || (in && in == out)) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    wk::PlanStep st{};
+    st.kind = kind;
+    st.dir = dir;
+    st.start_const = start_vid;
+    st.end_const = end_vid;
+    if (kind == wk::PlanStep::kKUU || kind == wk::PlanStep::kKUC) {
+        int rc = check_in(ctx, in, col_start, col_start);
+        if (rc) return rc;
+        st.cs = col_start;
+        st.in_cols = in->cols;
+        st.out_cols = in->cols + (kind == wk::PlanStep::kKUU ? 2 : 1);
+        if (st.out_cols > ctx->cfg.max_cols) return ctx->fail(WK_E_CAPACITY, "too many columns");
+    } else {
+        in = nullptr;
+        st.out_cols = kind == wk::PlanStep::kCUU ? 2 : 1;
+    }
+    return run_step_sync(ctx, st, in, out, 0, 1);
+}
+
+extern "C" int wk_step_known_unknown_unknown(wk_ctx* ctx, const wk_table* in, int32_t col_start,
+                                             int32_t dir, wk_table* out) {
+    if (!in) return WK_E_BADARG;
+    return versatile_step(ctx, wk::PlanStep::kKUU, in, col_start, 0, 0, dir, out);
+}
+
+extern "C" int wk_step_known_unknown_const(wk_ctx* ctx, const wk_table* in, int32_t col_start,
+                                           uint32_t end_vid, int32_t dir, wk_table* out) {
+    if (!in) return WK_E_BADARG;
+    return versatile_step(ctx, wk::PlanStep::kKUC, in, col_start, 0, end_vid, dir, out);
+}
+
+extern "C" int wk_step_const_unknown_unknown(wk_ctx* ctx, uint32_t vid, int32_t dir, wk_table* out) {
+    return versatile_step(ctx, wk::PlanStep::kCUU, nullptr, 0, vid, 0, dir, out);
+}
+
+extern "C" int wk_step_const_unknown_const(wk_ctx* ctx, uint32_t vid, uint32_t end_vid, int32_t dir,
+                                           wk_table* out) {
+    return versatile_step(ctx, wk::PlanStep::kCUC, nullptr, 0, vid, end_vid, dir, out);
+}
+
 // ---------------------------------------------------------------- whole queries
 static std::string plan_key(const std::vector<wk::PlanStep>& steps, const wk_query& q,
                             const wk_ctx* ctx) {
@@ -844,11 +1065,14 @@ static int plan_flat_mode(const std::vector<wk::PlanStep>& steps) {
 
 // Flat scratch for every step input of a plan (the rbuf capacities bound the row counts).
 static int plan_ensure_flat(wk_ctx* ctx, const std::vector<wk::PlanStep>& steps) {
-    if (plan_flat_mode(steps) == wk::kTileOnly || !ctx->flat_min_rows) return WK_SUCCESS;
-    uint64_t rows = 0;
+    bool vers = false;
+    for (auto& s : steps) vers |= wk::is_versatile_step(s.kind);
+    if (!vers && (plan_flat_mode(steps) == wk::kTileOnly || !ctx->flat_min_rows)) return WK_SUCCESS;
+    uint64_t rows = 1;
     for (size_t i = 1; i < steps.size(); ++i)
         if (steps[i].in_cols > 0) rows = std::max<uint64_t>(rows, ctx->rbuf[(i - 1) & 1].cap / steps[i].in_cols);
-    return rows >= ctx->flat_min_rows ? ctx->ensure_flat(rows) : WK_SUCCESS;
+    // the versatile steps always use the scratch; the flat passes only from their threshold on
+    return (vers || rows >= ctx->flat_min_rows) ? ctx->ensure_flat(rows) : WK_SUCCESS;
 }
 
 static int enqueue_plan(wk_ctx* ctx, const std::vector<wk::PlanStep>& steps, const wk_query& q) {
@@ -867,7 +1091,7 @@ static int query_run(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_tabl
     if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
     std::vector<wk::PlanStep> steps;
     wk::ColMap cm(q->nvars);
-    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm, ctx->versatile);
     if (rc) return ctx->fail(rc, wk_strerror(rc));
     if (q->mt_factor < 1 || q->mt_tid < 0) return ctx->fail(WK_E_BADARG, "mt_factor");
     for (auto& t : ctx->rbuf) {
@@ -1012,7 +1236,7 @@ extern "C" int wk_query_enqueue(wk_ctx* ctx, const wk_query* q, int32_t mode) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     std::vector<wk::PlanStep> steps;
     wk::ColMap cm(q->nvars);
-    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm, ctx->versatile);
     if (rc) return rc;
     if (mode == WK_MODE_GRAPH) {
         auto it = ctx->graphs.find(plan_key(steps, *q, ctx));
@@ -1041,11 +1265,16 @@ extern "C" int wk_ctx_check(wk_ctx* ctx) {
 
 extern "C" int wk_query_validate(const wk_query* q, int32_t max_cols, int32_t* v2c_map,
                                  int32_t* col_num) {
+    return wk_query_validate_ex(q, max_cols, 0, v2c_map, col_num);
+}
+
+extern "C" int wk_query_validate_ex(const wk_query* q, int32_t max_cols, int32_t versatile,
+                                    int32_t* v2c_map, int32_t* col_num) {
     if (!q) return WK_E_BADARG;
     if (max_cols <= 0) max_cols = 32;
     std::vector<wk::PlanStep> steps;
     wk::ColMap cm(q->nvars);
-    int rc = wk::resolve_plan(*q, max_cols, steps, cm);
+    int rc = wk::resolve_plan(*q, max_cols, steps, cm, versatile != 0);
     if (rc) return rc;
     if (col_num) *col_num = cm.col_num;
     if (v2c_map)
@@ -1059,7 +1288,7 @@ extern "C" int wk_query_profile(wk_ctx* ctx, const wk_query* q, int32_t iters, w
     std::lock_guard<std::mutex> lk(ctx->mu);
     std::vector<wk::PlanStep> steps;
     wk::ColMap cm(q->nvars);
-    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm);
+    int rc = wk::resolve_plan(*q, ctx->cfg.max_cols, steps, cm, ctx->versatile);
     if (rc) return ctx->fail(rc, wk_strerror(rc));
     if ((int)steps.size() > max_steps) return ctx->fail(WK_E_CAPACITY, "profile array too small");
     const wk_table* t = nullptr;

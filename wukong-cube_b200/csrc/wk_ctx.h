@@ -11,6 +11,7 @@
 #include "wk_explore.h"
 #include "wk_flat.h"
 #include "wk_kernels.h"
+#include "wk_versatile.h"
 
 // A device result table (the reference's rbuf + GPUResult, query.hpp:311-362).
 struct wk_table {
@@ -37,22 +38,39 @@ struct ColMap {
     }
     int col(int32_t id) const { return v2c[-(id + 1)]; }
     void bind(int32_t id, int c) { v2c[-(id + 1)] = c; }
+    // bind an unbound variable; false if it is bound already (add_var2col's assertion)
+    bool bind_new(int32_t id, int c) {
+        if (v2c[-(id + 1)] != WK_NO_RESULT) return false;
+        v2c[-(id + 1)] = c;
+        return true;
+    }
 };
 
 // One resolved exploration step of a plan.
+//   kIndex index_to_unknown, kConst const_to_unknown, kK2U / kK2K / kK2C known_to_*,
+//   kC2K const_to_known, kI2K index_to_known (single steps only: a query starts unbound),
+//   kCUU / kCUC / kKUU / kKUC the unknown-predicate (versatile) operators.
 struct PlanStep {
-    enum Kind { kIndex, kConst, kK2U, kK2K, kK2C } kind;
+    enum Kind { kIndex, kConst, kK2U, kK2K, kK2C, kC2K, kI2K, kCUU, kCUC, kKUU, kKUC } kind;
     uint32_t pid = 0;
     int32_t dir = 0;
     uint32_t start_const = 0;   // kIndex: tpid; kConst: start vertex
     int32_t cs = 0, ce = 0;     // input columns
-    uint32_t end_const = 0;     // kK2C
+    uint32_t end_const = 0;     // kK2C, kKUC, kCUC
     int32_t in_cols = 0, out_cols = 0;
+    int32_t mt_tid = 0, mt_factor = 1;   // kI2K: the slice of the index list
 };
 
-// Resolve a planned pattern list into steps, as GPUEngine::execute_one_pattern dispatches
-// (gpu_engine.hpp:265-338).  Returns a WK_* status; fills v2c_map / col_num of the result.
-int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm);
+// Resolve a planned pattern list into steps, as SPARQLEngine::execute_one_pattern dispatches
+// (sparql.hpp:932-1055; the GPU engine's gpu_engine.hpp:265-338 is its subset).  With
+// `versatile` (the store holds the vertex-predicate lists) an unknown predicate goes to the
+// versatile operators, else it is WK_UNKNOWN_PATTERN.  Returns a WK_* status; fills v2c_map /
+// col_num of the result.
+int resolve_plan(const wk_query& q, int max_cols, std::vector<PlanStep>& steps, ColMap& cm,
+                 bool versatile = false);
+inline bool is_versatile_step(int kind) {
+    return kind == PlanStep::kCUU || kind == PlanStep::kCUC || kind == PlanStep::kKUU || kind == PlanStep::kKUC;
+}
 
 }  // namespace wk
 
@@ -71,6 +89,9 @@ struct wk_ctx {
     std::vector<wk_seg_meta> segs;
     wk::SegIndex index;
     bool has_store = false;
+    bool versatile = false;           // the store holds the vertex-predicate lists
+    wk::PredSeg* d_pseg = nullptr;    // predicate segments by pid * 2 + dir (versatile steps)
+    uint32_t n_pseg = 0;
     bool borrowed_store = false;   // a serving lane: the store belongs to its parent context
     wk::CtaUse beside_use{0, 0, 0};   // a serving lane leaves room on every SM for this many
     int beside_ctas = 0;              // resident CTAs of this size (the iteration launches)

@@ -158,6 +158,54 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
     }
 }
 
+// Probe one key by one thread: the home bucket's slots two at a time (one 32-byte sector),
+// then the chain through slot 7.  Returns the pointer word, 0 when absent.  `first` skips the
+// home bucket's slots a caller has already compared (0 or an even slot).
+__device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t key, uint64_t bucket,
+                                                 unsigned* err, int first = 0) {
+    for (int hop = 0; hop < kMaxProbeIters; ++hop) {
+        if (bucket >= st.n_buckets) {
+            atomicOr(err, kErrCorrupt);
+            return 0;
+        }
+        const Slot* b = st.slots + bucket * kAssoc;
+#pragma unroll
+        for (int s = 0; s < kAssoc - 1; s += 2) {
+            if (hop == 0 && s < first) continue;
+            const ulonglong2 s0 = load_slot(b + s);   // both slots: one 32-byte sector
+            const ulonglong2 s1 = load_slot(b + s + 1);
+            if (s0.x == key) return s0.y;
+            if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
+            if (s + 1 == kAssoc - 1) {   // slot 7: the chain link
+                if (s1.x == 0) return 0;
+                bucket = key_vid(s1.x);
+                break;
+            }
+            if (s1.x == key) return s1.y;
+            if (s1.x == 0) return 0;
+        }
+    }
+    atomicOr(err, kErrCorrupt);
+    return 0;
+}
+
+// Is `target` in the list edges[off, off + deg)?  Binary search when lists are sorted.
+__device__ __forceinline__ bool thread_member(const uint32_t* edges, uint64_t off, uint64_t deg,
+                                              uint32_t target, bool sorted) {
+    const uint32_t* p = edges + off;
+    if (sorted) {
+        uint64_t lo = 0, hi = deg;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (__ldg(p + mid) < target) lo = mid + 1; else hi = mid;
+        }
+        return lo < deg && __ldg(p + lo) == target;
+    }
+    for (uint64_t k = 0; k < deg; ++k)
+        if (__ldg(p + k) == target) return true;
+    return false;
+}
+
 // Exclusive block scan of s_cnt[0..n) into s_pre[0..n]; returns the tile total.
 __device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* s_pre, int n,
                                                uint64_t* s_warp) {

@@ -182,6 +182,10 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
                 uint64_t key = 0;
                 if (op == kXStart) {
                     key = d->start_key;
+                } else if (valid && (op == kXC2K || op == kXI2K)) {
+                    // const_to_known / index_to_known: every row looks up the same list
+                    key = d->start_key;
+                    target = B.in[row * wi + d->ce];   // shared memory: plain loads
                 } else if (valid) {
                     const uint32_t* rin = B.in + row * wi;   // shared memory: plain loads
                     const uint32_t cur = rin[d->cs];
@@ -235,7 +239,13 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
                 if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg[u] = 0;
             }
-            has[u] = valid[u] && deg[u] > 0 && (op == kXK2K || op == kXK2C);
+            if (op == kXI2K && valid[u]) {   // index_to_known reads its mt slice of the list
+                uint64_t lo, hi;
+                mt_slice(step_desc(a, B.q[row[u]])->mt, deg[u], &lo, &hi);
+                off[u] += lo;
+                deg[u] = hi - lo;
+            }
+            has[u] = valid[u] && deg[u] > 0 && is_filter_op(op);
             any_filter |= has[u];
             found[u] = false;
         }
@@ -248,7 +258,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
             for (int u = 0; u < kUnroll; ++u)
                 if (valid[u]) {
                     const uint32_t op = flag[u] & 0xFFu;
-                    const bool filt = op == kXK2K || op == kXK2C;
+                    const bool filt = is_filter_op(op);
                     const uint32_t cnt = filt ? (found[u] ? 1u : 0u) : (uint32_t)deg[u];
                     B.off[row[u]] = off[u];
                     B.cnt[row[u]] = cnt;

@@ -11,7 +11,13 @@
 
 namespace wk {
 
-enum ExploreOp : uint8_t { kXStart = 0, kXK2U = 1, kXK2K = 2, kXK2C = 3, kXDone = 4 };
+// kXC2K: const_to_known, kXI2K: index_to_known (the row survives when its `ce` value is in the
+// constant's / index's list, the index list cut to the step's mt slice).
+enum ExploreOp : uint8_t { kXStart = 0, kXK2U = 1, kXK2K = 2, kXK2C = 3, kXDone = 4, kXC2K = 5, kXI2K = 6 };
+
+__host__ __device__ inline bool is_filter_op(uint32_t op) {
+    return op == kXK2K || op == kXK2C || op == kXC2K || op == kXI2K;
+}
 
 // One query's step at one level (64 bytes).
 struct StepDesc {
@@ -21,8 +27,17 @@ struct StepDesc {
     uint32_t end_const;     // kXK2C
     uint8_t op, dir, cin, cout;
     uint8_t cs, ce, type_index, pad;
-    uint32_t pad2;
+    uint32_t mt;            // kXI2K: mt_tid | mt_factor << 16, the slice of the index list
 };
+
+// The part of a list of `deg` entries that slice mt_tid of mt_factor reads (sparql.hpp:105-116,
+// 213-224): equal shares of deg / mt_factor, the last slice also taking the remainder.
+__host__ __device__ inline void mt_slice(uint32_t mt, uint64_t deg, uint64_t* lo, uint64_t* hi) {
+    const uint64_t tid = mt & 0xFFFF, factor = (mt >> 16) ? (mt >> 16) : 1;
+    const uint64_t len = deg / factor;
+    *lo = (tid % factor) * len;
+    *hi = (tid % factor) == factor - 1 ? deg : *lo + len;
+}
 static_assert(sizeof(StepDesc) == 64, "StepDesc is 64 bytes");
 
 // A slice of a long neighbour list.  Rows whose count exceeds kHeavyRows are not written by

@@ -47,54 +47,6 @@ __device__ __forceinline__ uint64_t flat_rows(const FlatArgs& a) {
     return R > a.in_cap_rows ? 0 : R;   // past capacity: the step before overflowed
 }
 
-// Probe one key by one thread: the home bucket's slots two at a time (one 32-byte sector),
-// then the chain through slot 7.  Returns the pointer word, 0 when absent.  `first` skips the
-// home bucket's slots a caller has already compared (0 or an even slot).
-__device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t key, uint64_t bucket,
-                                                 unsigned* err, int first = 0) {
-    for (int hop = 0; hop < kMaxProbeIters; ++hop) {
-        if (bucket >= st.n_buckets) {
-            atomicOr(err, kErrCorrupt);
-            return 0;
-        }
-        const Slot* b = st.slots + bucket * kAssoc;
-#pragma unroll
-        for (int s = 0; s < kAssoc - 1; s += 2) {
-            if (hop == 0 && s < first) continue;
-            const ulonglong2 s0 = load_slot(b + s);   // both slots: one 32-byte sector
-            const ulonglong2 s1 = load_slot(b + s + 1);
-            if (s0.x == key) return s0.y;
-            if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
-            if (s + 1 == kAssoc - 1) {   // slot 7: the chain link
-                if (s1.x == 0) return 0;
-                bucket = key_vid(s1.x);
-                break;
-            }
-            if (s1.x == key) return s1.y;
-            if (s1.x == 0) return 0;
-        }
-    }
-    atomicOr(err, kErrCorrupt);
-    return 0;
-}
-
-// Is `target` in the list edges[off, off + deg)?  Binary search when lists are sorted.
-__device__ __forceinline__ bool thread_member(const uint32_t* edges, uint64_t off, uint64_t deg,
-                                              uint32_t target, bool sorted) {
-    const uint32_t* p = edges + off;
-    if (sorted) {
-        uint64_t lo = 0, hi = deg;
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (__ldg(p + mid) < target) lo = mid + 1; else hi = mid;
-        }
-        return lo < deg && __ldg(p + lo) == target;
-    }
-    for (uint64_t k = 0; k < deg; ++k)
-        if (__ldg(p + k) == target) return true;
-    return false;
-}
-
 __device__ __forceinline__ void chunk_of(uint64_t R, uint64_t* lo, uint64_t* hi) {
     const uint64_t chunk = (R + gridDim.x - 1) / gridDim.x;
     *lo = min(R, (uint64_t)blockIdx.x * chunk);
@@ -172,7 +124,9 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
     const StepDesc& d = a.step;
-    const bool filt = d.op == kXK2K || d.op == kXK2C;
+    const bool filt = is_filter_op(d.op);
+    const bool from_const = d.op == kXC2K || d.op == kXI2K;   // every row looks up one list
+    const int tcol = (d.op == kXK2K || from_const) ? d.ce : -1;   // the row's membership target
     uint64_t sum = 0, sd = 0, nvalid = 0;
     bool ones = true;   // every row of this thread has exactly one output row
     const bool spec = R <= a.out_cap_rows;   // output row r exists: one-to-one rows written here
@@ -184,7 +138,7 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
         if (r < hi) {
             const uint32_t* row = a.in + r * (uint64_t)a.w_in;
             nxt_cur = __ldg(row + d.cs);
-            if (d.op == kXK2K) nxt_tgt = __ldg(row + d.ce);
+            if (tcol >= 0) nxt_tgt = __ldg(row + tcol);
         }
     }
     for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
@@ -193,12 +147,14 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
         if (r + kFlatThreads < hi) {
             const uint32_t* row = a.in + (r + kFlatThreads) * (uint64_t)a.w_in;
             nxt_cur = __ldg(row + d.cs);
-            if (d.op == kXK2K) nxt_tgt = __ldg(row + d.ce);
+            if (tcol >= 0) nxt_tgt = __ldg(row + tcol);
         }
         uint64_t key;
         SegDesc sg = d.seg;   // by value: registers, not a pointer into the parameter block
-        bool valid = cur != kBlankId;
-        if (d.op == kXK2U && d.type_index) {
+        bool valid = from_const || cur != kBlankId;
+        if (from_const) {
+            key = d.start_key;
+        } else if (d.op == kXK2U && d.type_index) {
             // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
             key = make_key(0, cur, kIn);
             sg = a.seg_index[kIn];
@@ -228,6 +184,12 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatA
             if (off + deg > a.store.n_edges) {
                 if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg = 0;
+            }
+            if (d.op == kXI2K) {   // index_to_known reads its mt slice of the list
+                uint64_t lo, hi;
+                mt_slice(d.mt, deg, &lo, &hi);
+                off += lo;
+                deg = hi - lo;
             }
         }
         uint32_t c = (uint32_t)deg;
@@ -274,7 +236,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs
     if (R < a.min_rows || a.part[nparts] > a.out_cap_rows) return;
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
-    const bool filt = a.step.op == kXK2K || a.step.op == kXK2C;
+    const bool filt = is_filter_op(a.step.op);
     if (!filt && a.part[nparts + 1] == 1) return;   // one output row per input row, in order
     // a filter's chunk without survivors has nothing to copy (part holds the exclusive scan of
     // the chunk totals, part[nparts] the total)
@@ -421,6 +383,10 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const Fl
         uint32_t target = d->end_const, cin = 0;
         if (valid && op == kXStart) {
             key = d->start_key;
+        } else if (valid && (op == kXC2K || op == kXI2K)) {   // one list for every row
+            cin = d->cin;
+            key = d->start_key;
+            target = __ldg(a.in + r * (uint64_t)a.w_in + d->ce);
         } else if (valid) {
             cin = d->cin;
             const uint32_t* row = a.in + r * (uint64_t)a.w_in;
@@ -446,8 +412,14 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const Fl
                 if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg = 0;
             }
+            if (op == kXI2K) {
+                uint64_t lo, hi;
+                mt_slice(d->mt, deg, &lo, &hi);
+                off += lo;
+                deg = hi - lo;
+            }
         }
-        const bool filt = op == kXK2K || op == kXK2C;
+        const bool filt = is_filter_op(op);
         uint32_t c = (uint32_t)deg;
         if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
         if (!valid) c = 0;
@@ -498,7 +470,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_place_kernel(const Fl
             }
             if (last) atomicAdd(a.qcount + q, (unsigned long long)(p + c));
             const uint32_t op = a.desc[q].op;
-            if (c && (op == kXK2K || op == kXK2C)) {   // a surviving row keeps its columns
+            if (c && is_filter_op(op)) {   // a surviving row keeps its columns
                 const int cin = a.desc[q].cin;
                 const uint32_t* src = a.in + r * (uint64_t)a.w_in;
                 uint32_t* dst = a.out + p * (uint64_t)a.w_out;
@@ -553,7 +525,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
             s_q[t] = q;
             const StepDesc* d = a.desc + q;
             const uint32_t op = d->op;
-            s_ecol[t] = op == kXStart ? 0 : op == kXK2U ? (int32_t)d->cin : -1;
+            s_ecol[t] = op == kXStart ? 0 : op == kXK2U ? (int32_t)d->cin : -1;   // filters: -1
         }
         __syncthreads();
         const uint64_t wend = min(j1, s_pos[n]);

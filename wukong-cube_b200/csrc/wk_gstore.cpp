@@ -10,7 +10,10 @@
 //     [0|pid|OUT] = objects of pid, and the type index [0|type|IN] = instances
 //     (collect_idx_info :951-994, insert_idx :284-347), predicate lists first, then types;
 //   * keys go to bucket_start + hash(key) % num_buckets, into the first empty slot of 0..6,
-//     overflowing through slot 7 into extension buckets (insert_key_to_seg :203-271).
+//     overflowing through slot 7 into extension buckets (insert_key_to_seg :203-271);
+//   * a versatile build (the reference's default, VERSATILE) adds each vertex's predicate list:
+//     keys [vid|PREDICATE_ID|OUT] / [vid|PREDICATE_ID|IN] in two more normal segments, the
+//     predicates ascending (insert_vp :365-455).
 // How many buckets a segment gets is this builder's own choice (the reference derives it from
 // the configured memory size, :117-163): enough for a mean fill of load_factor of the 7 data
 // slots, so chains stay rare and most probes touch only the bucket's first sector.
@@ -134,8 +137,27 @@ uint64_t buckets_for(uint64_t keys, double load) {
 
 }  // namespace
 
+// The vertex-predicate lists of a VERSATILE build (insert_vp, segment_rdf_dgraph.hpp:365-455):
+// for every key vertex of one direction, its distinct predicates in ascending order.  `L`
+// holds that direction's (vid << 32 | value) pairs grouped by ascending predicate.  Returns
+// (vid << 32 | pid) pairs sorted by vertex, then predicate.
+std::vector<uint64_t> vertex_predicates(const DirLists& L) {
+    const size_t np = (size_t)1 << kNbitsIdx;
+    std::vector<uint64_t> vp;
+    for (size_t p = 0; p < np; ++p) {
+        uint64_t last = ~0ull;
+        for (uint64_t i = L.pred_begin[p]; i < L.pred_begin[p + 1]; ++i) {
+            const uint64_t v = L.pairs[i] >> 32;
+            if (v != last) vp.push_back(v << 32 | p);
+            last = v;
+        }
+    }
+    __gnu_parallel::sort(vp.begin(), vp.end());
+    return vp;
+}
+
 int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint64_t n_pos,
-                 double load, wk_gstore& g) {
+                 double load, bool versatile, wk_gstore& g) {
     // Default: about 0.7 keys per bucket.  A key's slot is its insertion rank in the bucket, so
     // at this fill about 94% of keys sit in the first 32-byte sector (slots 0-1) and their probe
     // is one request (at 1.4 keys per bucket it was 83%); HBM is plentiful, latency is not.
@@ -189,7 +211,24 @@ int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint6
     for (size_t t = 0; t < np; ++t)
         if (!type_inst[t].empty()) idx_in.emplace_back((uint32_t)t, std::move(type_inst[t]));
 
-    // Segment table: (p, OUT), (p, IN) for every predicate, then index OUT, index IN.
+    // VERSATILE: [v|PREDICATE_ID|OUT] for every subject, [v|PREDICATE_ID|IN] for every object
+    // that is not a type id (the IN lists already leave those out)
+    std::vector<uint64_t> vp_out, vp_in;
+    if (versatile) {
+        vp_out = vertex_predicates(outl);
+        vp_in = vertex_predicates(inl);
+    }
+    auto vp_keys = [](const std::vector<uint64_t>& vp) {
+        uint64_t k = 0, last = ~0ull;
+        for (uint64_t x : vp) {
+            if ((x >> 32) != last) ++k;
+            last = x >> 32;
+        }
+        return k;
+    };
+
+    // Segment table: (PREDICATE_ID, OUT), (PREDICATE_ID, IN) in a versatile build, then (p, OUT),
+    // (p, IN) for every predicate, then index OUT, index IN.
     g.segs.clear();
     uint64_t bucket_off = 0, edge_off = 0;
     auto add_seg = [&](int index, uint32_t pid, int dir, uint64_t keys, uint64_t edges) {
@@ -206,6 +245,10 @@ int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint6
         edge_off += edges;
         g.segs.push_back(m);
     };
+    if (versatile) {
+        add_seg(0, kPredicateId, kOut, vp_keys(vp_out), vp_out.size());
+        add_seg(0, kPredicateId, kIn, vp_keys(vp_in), vp_in.size());
+    }
     for (uint32_t p : preds) {
         add_seg(0, p, kOut, count_keys(outl, p), outl.pred_begin[p + 1] - outl.pred_begin[p]);
         add_seg(0, p, kIn, count_keys(inl, p), inl.pred_begin[p + 1] - inl.pred_begin[p]);
@@ -223,6 +266,23 @@ int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint6
 
     // Normal segments: keys in (vid) order, values ascending.
     size_t si = 0;
+    if (versatile) {
+        for (int d = 0; d < 2; ++d, ++si) {
+            const std::vector<uint64_t>& vp = d == 0 ? vp_out : vp_in;
+            const int dir = d == 0 ? kOut : kIn;
+            wk_seg_meta& m = g.segs[si];
+            uint64_t w = m.edge_start, ext0 = b.ext_used, i = 0;
+            while (i < vp.size()) {
+                const uint64_t vid = vp[i] >> 32, start = w;
+                uint64_t j = i;
+                while (j < vp.size() && (vp[j] >> 32) == vid) g.edges[w++] = (uint32_t)vp[j++];
+                b.insert(m, make_key(vid, kPredicateId, dir), make_ptr(j - i, start));
+                g.n_keys++;
+                i = j;
+            }
+            m.ext_num = b.ext_used - ext0;
+        }
+    }
     for (uint32_t p : preds) {
         for (int d = 0; d < 2; ++d, ++si) {
             const DirLists& L = (d == 0) ? outl : inl;
@@ -271,11 +331,17 @@ int gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos, uint6
 
 extern "C" int wk_gstore_build(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos,
                                uint64_t n_pos, double load_factor, wk_gstore** out) {
+    return wk_gstore_build_ex(pso, n_pso, pos, n_pos, load_factor, 0, out);
+}
+
+extern "C" int wk_gstore_build_ex(const uint32_t* pso, uint64_t n_pso, const uint32_t* pos,
+                                  uint64_t n_pos, double load_factor, int32_t versatile,
+                                  wk_gstore** out) {
     if (!out || (!pso && n_pso) || (!pos && n_pos)) return WK_E_BADARG;
     wk_gstore* g = nullptr;
     try {
         g = new wk_gstore();
-        int rc = wk::gstore_build(pso, n_pso, pos, n_pos, load_factor, *g);
+        int rc = wk::gstore_build(pso, n_pso, pos, n_pos, load_factor, versatile != 0, *g);
         if (rc != WK_SUCCESS) {
             delete g;
             return rc;

@@ -451,8 +451,11 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     bool any_heavy = false;
     for (uint32_t i = 0; i < n; ++i) {
         wk::ColMap cm(queries[i].nvars);
-        int rc = wk::resolve_plan(queries[i], ctx->cfg.max_cols, plans[i], cm);
+        int rc = wk::resolve_plan(queries[i], ctx->cfg.max_cols, plans[i], cm, ctx->versatile);
         if (rc == WK_SUCCESS && (int)plans[i].size() > wk::kMaxSteps) rc = WK_E_CAPACITY;
+        // the unknown-predicate operators walk several lists per row: single queries only
+        for (auto& x : plans[i])
+            if (rc == WK_SUCCESS && wk::is_versatile_step(x.kind)) rc = WK_E_UNSUPPORTED;
         if (rc == WK_SUCCESS && queries[i].mt_factor != 1) rc = WK_E_UNSUPPORTED;
         if (rc) {
             status[i] = rc;

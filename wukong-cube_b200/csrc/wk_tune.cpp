@@ -117,7 +117,10 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
     for (uint32_t i = 0; i < n; ++i) {
         std::vector<wk::PlanStep> steps;
         wk::ColMap cm(queries[i].nvars);
-        if (wk::resolve_plan(queries[i], ctx->cfg.max_cols, steps, cm) || steps.empty()) continue;
+        if (wk::resolve_plan(queries[i], ctx->cfg.max_cols, steps, cm, ctx->versatile) || steps.empty()) continue;
+        bool vers = false;
+        for (auto& x : steps) vers |= wk::is_versatile_step(x.kind);
+        if (vers) continue;   // not a tile-schedule workload
         const bool is_heavy = steps[0].kind == wk::PlanStep::kIndex;
         (is_heavy ? heavy : light).push_back(queries[i]);
         if (!is_heavy) light_levels = std::max(light_levels, std::min((int)steps.size(), wk::kMaxBatchLevels));

@@ -126,6 +126,7 @@ _SIGS = {
     "wk_plan_apply_fmt": (C.c_int, [C.POINTER(Pattern), C.c_int32, C.c_char_p, C.POINTER(Pattern),
                                     C.c_int32, C.POINTER(C.c_int32)]),
     "wk_gstore_build": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.c_double, C.POINTER(_P)]),
+    "wk_gstore_build_ex": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64, C.c_double, C.c_int32, C.POINTER(_P)]),
     "wk_gstore_free": (None, [_P]),
     "wk_gstore_info": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
@@ -157,6 +158,14 @@ _SIGS = {
     "wk_step_known_to_known": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_uint32, C.c_int32, _P]),
     "wk_step_known_to_const": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, _P]),
     "wk_step_known_to_unknown_noalloc": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _P]),
+    "wk_step_const_to_known": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_uint32, C.c_int32, _P]),
+    "wk_step_index_to_known": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, C.c_int32, C.c_int32, _P]),
+    "wk_step_known_unknown_unknown": (C.c_int, [_P, _P, C.c_int32, C.c_int32, _P]),
+    "wk_step_known_unknown_const": (C.c_int, [_P, _P, C.c_int32, C.c_uint32, C.c_int32, _P]),
+    "wk_step_const_unknown_unknown": (C.c_int, [_P, C.c_uint32, C.c_int32, _P]),
+    "wk_step_const_unknown_const": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_int32, _P]),
+    "wk_query_validate_ex": (C.c_int, [C.POINTER(QueryC), C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32)]),
     "wk_query_execute": (C.c_int, [_P, C.POINTER(QueryC), C.c_int32, C.POINTER(_P),
                                    C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                    C.POINTER(C.c_uint64)]),
@@ -293,14 +302,17 @@ def plan_fmt(written, fmt_text, nvars=None):
 class GStore:
     """Host-built static segment store (SegmentRDFGraph::init_gstore layout)."""
 
-    def __init__(self, pso, pos=None, load_factor=0.0):
+    def __init__(self, pso, pos=None, load_factor=0.0, versatile=False):
+        """versatile: also every vertex's predicate lists (wk_gstore_build_ex), which the
+        unknown-predicate patterns read."""
         L = lib()
         pso = np.ascontiguousarray(pso, dtype=np.uint32)
         pos = pso if pos is None else np.ascontiguousarray(pos, dtype=np.uint32)
         h = C.c_void_p()
-        _check(L.wk_gstore_build(_ptr(pso), pso.shape[0], _ptr(pos), pos.shape[0],
-                                 load_factor, C.byref(h)))
+        _check(L.wk_gstore_build_ex(_ptr(pso), pso.shape[0], _ptr(pos), pos.shape[0],
+                                    load_factor, 1 if versatile else 0, C.byref(h)))
         self.h = h
+        self.versatile = bool(versatile)
 
     def close(self):
         if self.h:
@@ -385,12 +397,13 @@ def phase_cycles(reset=True):
     return dict(zip(PHASES, list(arr)))
 
 
-def validate(q, max_cols=32):
-    """Plan check without a device: (status, v2c_map, col_num)."""
+def validate(q, max_cols=32, versatile=False):
+    """Plan check without a device: (status, v2c_map, col_num); versatile: for a store with the
+    vertex-predicate lists (wk_query_validate_ex)."""
     qc = q.as_c()
     v2c = (C.c_int32 * max(q.nvars, 1))()
     cols = C.c_int32()
-    rc = lib().wk_query_validate(C.byref(qc), max_cols, v2c, C.byref(cols))
+    rc = lib().wk_query_validate_ex(C.byref(qc), max_cols, 1 if versatile else 0, v2c, C.byref(cols))
     return rc, list(v2c)[:q.nvars], cols.value
 
 
@@ -541,6 +554,25 @@ class Context:
 
     def known_to_const(self, tin, col_start, end_vid, pid, d, out):
         _check(lib().wk_step_known_to_const(self.h, tin.h, col_start, end_vid, pid, d, out.h), self.h)
+
+    def const_to_known(self, tin, col_end, vid, pid, d, out):
+        _check(lib().wk_step_const_to_known(self.h, tin.h, col_end, vid, pid, d, out.h), self.h)
+
+    def index_to_known(self, tin, col_end, tpid, d, out, mt_tid=0, mt_factor=1):
+        _check(lib().wk_step_index_to_known(self.h, tin.h, col_end, tpid, d, mt_tid, mt_factor, out.h),
+               self.h)
+
+    def known_unknown_unknown(self, tin, col_start, d, out):
+        _check(lib().wk_step_known_unknown_unknown(self.h, tin.h, col_start, d, out.h), self.h)
+
+    def known_unknown_const(self, tin, col_start, end_vid, d, out):
+        _check(lib().wk_step_known_unknown_const(self.h, tin.h, col_start, end_vid, d, out.h), self.h)
+
+    def const_unknown_unknown(self, vid, d, out):
+        _check(lib().wk_step_const_unknown_unknown(self.h, vid, d, out.h), self.h)
+
+    def const_unknown_const(self, vid, end_vid, d, out):
+        _check(lib().wk_step_const_unknown_const(self.h, vid, end_vid, d, out.h), self.h)
 
     def execute(self, q, mode=MODE_RESIDENT):
         """Run a whole planned query; returns (table (rows, cols) uint32, v2c_map list)."""
