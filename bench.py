@@ -289,6 +289,20 @@ def run_ours(args, world, rank, local_rank):
     ctx = wk.Context(local_rank)
     ctx.upload_gstore(g)
     ginfo["device_store_bytes"] = ctx.store_bytes()
+    if not args.no_device_build:
+        # the same store built on the device (wk_store_build_device) from the same triples, in a
+        # second context: wall time of the call (upload of the triples included), against the
+        # host build above; the two stores must hold the same slots and lists
+        with wk.Context(local_rank) as cb:
+            cb.build_store(tr[:1], load_factor=args.load_factor)   # loads the build's kernels
+            t0 = time.time()
+            cb.build_store(tr, load_factor=args.load_factor)
+            ginfo["device_build_s"] = round(time.time() - t0, 3)
+            same = cb.store_bytes() == ginfo["device_store_bytes"]
+            probe = workloads.light_queries(v, inst, 512, seed=args.seed + 3)
+            a = [r[0].shape[0] if r[0] is not None else -1 for r in cb.batch(probe)]
+            b = [r[0].shape[0] if r[0] is not None else -1 for r in ctx.batch(probe)]
+            assert same and a == b, "device-built store differs from the host-built one"
     stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
     cores = os.cpu_count() or 1
@@ -626,6 +640,8 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-device-build", action="store_true",
+                    help="skip timing the store build on the device against the host build")
     ap.add_argument("--heavy-cpu-reps", type=int, default=3,
                     help="timed CPU-engine runs of each heavy query (median reported)")
     ap.add_argument("--serve-rates", type=lambda s: [int(x) for x in s.split(",")],

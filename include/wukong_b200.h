@@ -243,6 +243,20 @@ int wk_ctx_check(wk_ctx* ctx);
 int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_segs, const void* slots,
                     uint64_t n_slots, const uint32_t* edges, uint64_t n_edges);
 int wk_store_upload_gstore(wk_ctx* ctx, const wk_gstore* g);
+/* Build the store on the device from n x 3 (s, p, o) id triples in host memory (used for both
+ * directions, as wk_gstore_build is normally called): the same layout, byte for byte, as
+ * wk_gstore_build_ex with the same load factor and versatile flag, in place of the host build
+ * and upload.  The loader's sort + dedup (base_loader.hpp:481-496) and
+ * SegmentRDFGraph::init_gstore (segment_rdf_dgraph.hpp:1182-1269) run as radix sorts, scans and
+ * a placement pass on the device.  Replaces the context's store.  At most 2^32 - 1 triples;
+ * load_factor 0 takes the default 0.1. */
+int wk_store_build_device(wk_ctx* ctx, const uint32_t* triples, uint64_t n_triples, double load_factor,
+                          int32_t versatile);
+/* Copy the context's store to host memory in wk_store_upload's layout.  With all three array
+ * pointers null only the sizes are returned; otherwise each non-null array must hold its size
+ * (WK_E_CAPACITY).  No reference counterpart. */
+int wk_store_export(wk_ctx* ctx, void* slots, uint64_t slots_cap, uint32_t* edges, uint64_t edges_cap,
+                    wk_seg_meta* segs, uint32_t segs_cap, uint64_t* n_slots, uint64_t* n_edges, uint32_t* n_segs);
 /* Device bytes held by the store (slots + edges + segment table). */
 int wk_store_bytes(const wk_ctx* ctx, uint64_t* bytes);
 

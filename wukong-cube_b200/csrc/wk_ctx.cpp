@@ -586,6 +586,7 @@ static int ctx_init_device(wk_ctx* ctx, bool low_priority) {
     if (e == cudaSuccess) e = wk::flat_kernel_attrs();
     if (e == cudaSuccess) e = wk::final_kernel_attrs();
     if (e == cudaSuccess) e = wk::versatile_kernel_attrs();
+    if (e == cudaSuccess) e = wk::gbuild_kernel_attrs();
     if (e != cudaSuccess) return bail(e, "kernel attributes");
     e = wk::dev_malloc(&ctx->d_ctl, sizeof(wk::StepCtl));
     if (e != cudaSuccess) return bail(e, "control block");
@@ -674,9 +675,23 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
         WK_CUDA(ctx, cudaMemcpy(ctx->d_slots, slots, n_slots * sizeof(wk::Slot), cudaMemcpyHostToDevice));
     if (n_edges)
         WK_CUDA(ctx, cudaMemcpy(ctx->d_edges, edges, n_edges * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    std::vector<wk_seg_meta> sv(segs, segs + n_segs);
+    wk::Slot* ds = ctx->d_slots;
+    uint32_t* de = ctx->d_edges;
+    return wk::store_adopt(ctx, ds, n_slots, de, n_edges, sv);
+}
+
+// Make device arrays the context's store: segment lookup, predicate segment table, the
+// sorted-list check.  The context owns the arrays from here on, on failure too.
+int wk::store_adopt(wk_ctx* ctx, Slot* d_slots, uint64_t n_slots, uint32_t* d_edges, uint64_t n_edges,
+                    const std::vector<wk_seg_meta>& segs) {
+    ctx->d_slots = d_slots;
+    ctx->d_edges = d_edges;
     ctx->n_slots = n_slots;
     ctx->n_edges = n_edges;
-    ctx->segs.assign(segs, segs + n_segs);
+    ctx->has_store = false;
+    const uint32_t n_segs = (uint32_t)segs.size();
+    ctx->segs = segs;
     ctx->index.build(ctx->segs.data(), n_segs);
     {
         // the predicate segments by pid * 2 + dir, for the versatile steps' list walks; a
@@ -720,6 +735,29 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
         ctx->sorted_lists = (flag & 1u) ? 0 : 1;
     }
     ctx->drop_graphs();
+    return WK_SUCCESS;
+}
+
+// A copy of the context's store in host memory, in the layout wk_store_upload takes.
+extern "C" int wk_store_export(wk_ctx* ctx, void* slots, uint64_t slots_cap, uint32_t* edges, uint64_t edges_cap,
+                               wk_seg_meta* segs, uint32_t segs_cap, uint64_t* n_slots, uint64_t* n_edges,
+                               uint32_t* n_segs) {
+    if (!ctx) return WK_E_BADARG;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->has_store) return ctx->fail(WK_E_NOSTORE, "no store uploaded");
+    if (n_slots) *n_slots = ctx->n_slots;
+    if (n_edges) *n_edges = ctx->n_edges;
+    if (n_segs) *n_segs = (uint32_t)ctx->segs.size();
+    if (!slots && !edges && !segs) return WK_SUCCESS;   // sizes only
+    if ((slots && slots_cap < ctx->n_slots) || (edges && edges_cap < ctx->n_edges) ||
+        (segs && segs_cap < ctx->segs.size()))
+        return ctx->fail(WK_E_CAPACITY, "export buffers too small");
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (slots && ctx->n_slots)
+        WK_CUDA(ctx, cudaMemcpy(slots, ctx->d_slots, ctx->n_slots * sizeof(wk::Slot), cudaMemcpyDeviceToHost));
+    if (edges && ctx->n_edges)
+        WK_CUDA(ctx, cudaMemcpy(edges, ctx->d_edges, ctx->n_edges * 4, cudaMemcpyDeviceToHost));
+    if (segs && !ctx->segs.empty()) std::memcpy(segs, ctx->segs.data(), ctx->segs.size() * sizeof(wk_seg_meta));
     return WK_SUCCESS;
 }
 

@@ -203,6 +203,10 @@ int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t*
 int table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host);
 // Size a serving lane's tables and scan scratch for `elems`-element tables up front.
 int lane_prepare(wk_ctx* lane, uint64_t elems);
+// Make device arrays (dev_malloc'd) the context's store; the context owns them from here on.
+int store_adopt(wk_ctx* ctx, Slot* d_slots, uint64_t n_slots, uint32_t* d_edges, uint64_t n_edges,
+                const std::vector<wk_seg_meta>& segs);
+cudaError_t gbuild_kernel_attrs();   // wk_gbuild.cu
 // Lanes for one (explore op, input columns) step of single queries (the autotuner's choice).
 int tune_step_lanes(wk_ctx* ctx, int op, int cols, int lanes);
 }  // namespace wk

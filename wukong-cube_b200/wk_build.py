@@ -24,7 +24,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["wk_kernels.cu", "wk_explore.cu", "wk_batch.cu", "wk_serve.cu", "wk_noalloc.cu", "wk_flat.cu",
-              "wk_final.cu", "wk_versatile.cu"]
+              "wk_final.cu", "wk_versatile.cu", "wk_gbuild.cu"]
 CPP_SOURCES = ["wk_ctx.cpp", "wk_gstore.cpp", "wk_synth.cpp", "wk_tune.cpp", "wk_loader.cpp"]
 HEADERS = ["wk_format.h", "wk_internal.h", "wk_kernels.h", "wk_ctx.h", "wk_batch.h",
            "wk_device.cuh", "wk_explore.h", "wk_flat.h", "wk_versatile.h"]

@@ -143,6 +143,9 @@ _SIGS = {
     "wk_store_upload": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint64, _P, C.c_uint64]),
     "wk_store_upload_gstore": (C.c_int, [_P, _P]),
     "wk_store_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "wk_store_build_device": (C.c_int, [_P, _P, C.c_uint64, C.c_double, C.c_int32]),
+    "wk_store_export": (C.c_int, [_P, _P, C.c_uint64, _P, C.c_uint64, C.POINTER(SegMeta), C.c_uint32,
+                                  C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     "wk_table_alloc": (C.c_int, [_P, C.c_uint64, C.POINTER(_P)]),
     "wk_table_free": (C.c_int, [_P, _P]),
     "wk_table_upload": (C.c_int, [_P, _P, _P, C.c_uint64, C.c_int32]),
@@ -527,6 +530,26 @@ class Context:
         n_segs = len(segs)
         _check(lib().wk_store_upload(self.h, C.cast(segs, C.c_void_p), n_segs, _ptr(slots),
                                      slots.size // 2, _ptr(edges), edges.size), self.h)
+
+    def build_store(self, triples, load_factor=0.0, versatile=False):
+        """Build the store on the device from (n, 3) id triples (wk_store_build_device)."""
+        t = np.ascontiguousarray(triples, dtype=np.uint32).reshape(-1, 3)
+        _check(lib().wk_store_build_device(self.h, _ptr(t), t.shape[0], load_factor, 1 if versatile else 0),
+               self.h)
+
+    def export_store(self):
+        """The context's store as host arrays: (slots uint64[n, 2], edges uint32[m], segs list of
+        dicts), in wk_store_upload's layout (wk_store_export)."""
+        ns, ne, ng = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        L = lib()
+        _check(L.wk_store_export(self.h, None, 0, None, 0, None, 0, C.byref(ns), C.byref(ne), C.byref(ng)), self.h)
+        slots = np.zeros((max(ns.value, 1), 2), np.uint64)
+        edges = np.zeros(max(ne.value, 1), np.uint32)
+        segs = (SegMeta * max(ng.value, 1))()
+        _check(L.wk_store_export(self.h, _ptr(slots), ns.value, _ptr(edges), ne.value, segs, ng.value,
+                                 C.byref(ns), C.byref(ne), C.byref(ng)), self.h)
+        seg_list = [{f: getattr(segs[i], f) for f, _ in SegMeta._fields_} for i in range(ng.value)]
+        return slots[:ns.value], edges[:ne.value], seg_list
 
     def store_bytes(self):
         b = C.c_uint64()
