@@ -135,12 +135,18 @@ typedef struct wk_serve_config {
     uint64_t working_set_cap_bytes;   /* admission cap on projected table bytes (40 GiB) */
     uint64_t arena_bytes;             /* initial bytes of each of the two table arenas (1 GiB);
                                          they grow up to the cap when a step needs more */
-    uint64_t light_proj_bytes;        /* projected bytes of a query that starts from a
-                                         constant (256 KiB) */
-    uint64_t heavy_proj_bytes;        /* projected bytes of one that starts from an index
-                                         (256 MiB) */
+    uint64_t min_proj_bytes;          /* floor of one query's projected bytes (64 KiB).  A
+                                         query's projection is the input + output table bytes of
+                                         its widest step, with rows taken from the store's
+                                         metadata: an index start's exact list length, a mean
+                                         degree (edges / keys of the segment) for a constant
+                                         start and each known_to_unknown step, and unchanged
+                                         rows through a filter step */
+    uint64_t lane_table_bytes;        /* table bytes each lane is sized for before the run
+                                         (0: the largest projection among the run's index-start
+                                         queries, at most 1 GiB) */
     uint32_t max_inflight;            /* constant-start queries resident at once (default 65536) */
-    uint32_t max_heavy_inflight;      /* index-start queries running at once (default 1); each
+    uint32_t max_heavy_inflight;      /* index-start queries running at once (default 4); each
                                          runs whole on its own lane: a stream of the lowest
                                          priority with its own tables, beside the iterations */
     int32_t light_ctas_per_sm;        /* exploration CTAs per SM of the iteration launches; the

@@ -60,7 +60,7 @@ def test_two_lanes_and_a_tight_working_set_cap(ctx, graph20):
     qs = _mix(graph20, 400, seed=24)
     arrivals = np.linspace(0, 500, len(qs))
     res = ctx.serve(qs, arrivals, max_heavy_inflight=2, working_set_cap_bytes=64 << 20,
-                    heavy_proj_bytes=16 << 20, light_proj_bytes=1 << 20, light_ctas_per_sm=1)
+                    lane_table_bytes=16 << 20, min_proj_bytes=1 << 20, light_ctas_per_sm=1)
     _check(graph20["oracle"], qs, res)
 
 

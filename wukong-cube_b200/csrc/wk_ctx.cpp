@@ -716,6 +716,30 @@ int wk::store_adopt(wk_ctx* ctx, Slot* d_slots, uint64_t n_slots, uint32_t* d_ed
             WK_CUDA(ctx, cudaMemcpy(ctx->d_pseg, ps.data(), ps.size() * sizeof(wk::PredSeg), cudaMemcpyHostToDevice));
         ctx->n_pseg = (uint32_t)ps.size();
     }
+    {
+        // the index lists' lengths (the keys [0|tpid|dir] of the two index segments: a few
+        // buckets per predicate and type), which the serving admission projects from
+        ctx->index_len.clear();
+        const uint64_t nb = n_slots / wk::kAssoc;
+        std::vector<wk::Slot> bk;
+        for (int d = 0; d < 2; ++d) {
+            const int32_t i = ctx->index.index_seg[d];
+            if (i < 0) continue;
+            const wk_seg_meta& m = segs[i];
+            const uint64_t ranges[2][2] = {{m.bucket_start, m.num_buckets}, {m.ext_start, m.ext_num}};
+            for (auto& r : ranges) {
+                if (!r[1] || r[0] >= nb || r[1] > nb - r[0]) continue;
+                bk.resize(r[1] * wk::kAssoc);
+                WK_CUDA(ctx, cudaMemcpy(bk.data(), d_slots + r[0] * wk::kAssoc, bk.size() * sizeof(wk::Slot),
+                                        cudaMemcpyDeviceToHost));
+                for (size_t k = 0; k < bk.size(); ++k) {
+                    const uint64_t key = bk[k].key;
+                    if (k % wk::kAssoc == wk::kAssoc - 1 || key == 0 || wk::key_vid(key) != 0) continue;
+                    ctx->index_len[wk::key_pid(key) * 2 + wk::key_dir(key)] = wk::ptr_size(bk[k].ptr);
+                }
+            }
+        }
+    }
     ctx->has_store = true;
     {
         // are all lists ascending + unique?  (lets the filters binary-search long lists)

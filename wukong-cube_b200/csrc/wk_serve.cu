@@ -109,6 +109,37 @@ __global__ void pack_kernel(const StepCtl* ctl, uint64_t* pkt) {
     pkt[1] = ctl->need;
 }
 
+// Projected table bytes of a plan: the input + output table bytes of its widest step, with the
+// rows each step is expected to produce taken from the store's metadata.  An index start has
+// its list's exact length (the index keys read at upload); a constant start and every
+// known_to_unknown step multiply by their segment's mean degree (edges / keys); a filter step
+// keeps its input rows, an upper bound.
+uint64_t plan_projection(const wk_ctx* ctx, const std::vector<PlanStep>& plan) {
+    auto mean_deg = [&](uint32_t pid, int dir) {
+        const int32_t i = ctx->index.find(1, pid, dir);
+        if (i < 0 || ctx->segs[i].num_keys == 0) return 0.0;
+        return (double)ctx->segs[i].num_edges / (double)ctx->segs[i].num_keys;
+    };
+    double rows = 1, peak = 0;
+    int cols = 0;
+    for (const PlanStep& s : plan) {
+        const double in_bytes = rows * cols * 4.0;
+        switch (s.kind) {
+            case PlanStep::kIndex: {
+                auto it = ctx->index_len.find(s.start_const * 2 + (uint32_t)s.dir);
+                rows = it == ctx->index_len.end() ? 0.0 : (double)it->second;
+                break;
+            }
+            case PlanStep::kConst: rows = mean_deg(s.pid, s.dir); break;
+            case PlanStep::kK2U: rows *= mean_deg(s.pid, s.dir); break;
+            default: break;   // filters keep at most their input rows
+        }
+        cols = s.out_cols;
+        peak = std::max(peak, in_bytes + rows * cols * 4.0);
+    }
+    return peak >= 1e18 ? (uint64_t)1e18 : (uint64_t)peak;
+}
+
 struct QSlot {
     uint32_t query;       // index into the caller's query array
     uint32_t admit_iter;
@@ -438,17 +469,18 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     S.cfg = cfg_in ? *cfg_in : wk_serve_config{};
     if (!S.cfg.working_set_cap_bytes) S.cfg.working_set_cap_bytes = 40ull << 30;
     if (!S.cfg.arena_bytes) S.cfg.arena_bytes = 1ull << 30;
-    if (!S.cfg.light_proj_bytes) S.cfg.light_proj_bytes = 256ull << 10;
-    if (!S.cfg.heavy_proj_bytes) S.cfg.heavy_proj_bytes = 256ull << 20;
+    if (!S.cfg.min_proj_bytes) S.cfg.min_proj_bytes = 64ull << 10;
     if (!S.cfg.max_inflight) S.cfg.max_inflight = 65536;
-    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 1;
+    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 4;
     if (S.cfg.light_ctas_per_sm <= 0) S.cfg.light_ctas_per_sm = 2;
 
     // Resolve every plan once (the same dispatch as a single query).
     std::vector<std::vector<wk::PlanStep>> plans(n);
     std::vector<int32_t> status(n, 0);
+    std::vector<uint64_t> proj(n, 0);   // projected bytes of each query
     int width = 1;
     bool any_heavy = false;
+    uint64_t heavy_proj_max = 0;
     for (uint32_t i = 0; i < n; ++i) {
         wk::ColMap cm(queries[i].nvars);
         int rc = wk::resolve_plan(queries[i], ctx->cfg.max_cols, plans[i], cm, ctx->versatile);
@@ -461,8 +493,10 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             status[i] = rc;
             plans[i].clear();
         }
+        proj[i] = std::max<uint64_t>(S.cfg.min_proj_bytes, wk::plan_projection(ctx, plans[i]));
         if (!plans[i].empty() && plans[i][0].kind == wk::PlanStep::kIndex) {
             any_heavy = true;   // runs on a lane, not in the iterations
+            heavy_proj_max = std::max(heavy_proj_max, proj[i]);
             continue;
         }
         for (auto& s : plans[i]) width = std::max(width, s.out_cols);
@@ -508,8 +542,10 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         const wk::CtaUse b = wk::explore_cta_use(0, S.w, ctx->batch_lanes);
         const wk::CtaUse light{std::max(a.smem, b.smem), std::max(a.regs, b.regs),
                                std::max(a.threads, b.threads)};
-        rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, light, S.light_ctas() + 1,
-                     S.cfg.heavy_proj_bytes / 4, [&](wk_ctx* lane, uint32_t q) {
+        const uint64_t lane_bytes =
+            S.cfg.lane_table_bytes ? S.cfg.lane_table_bytes : std::min<uint64_t>(heavy_proj_max, 1ull << 30);
+        rc = H.start(ctx, (int)S.cfg.max_heavy_inflight, light, S.light_ctas() + 1, lane_bytes / 4,
+                     [&](wk_ctx* lane, uint32_t q) {
                          const wk_table* t = nullptr;
                          uint64_t rows = 0, off = 0;
                          wk_qresult& r = results[q];
@@ -555,7 +591,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             }
         }
         S.new_slots.push_back(s);
-        proj_bytes += S.cfg.light_proj_bytes;
+        proj_bytes += proj[q];
     };
     std::vector<uint32_t> lane_done;
     while (done < n) {
@@ -566,9 +602,8 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
             if (H.fatal) return ctx->fail(H.fatal, "serving lane: " + H.fatal_msg);
         }
         for (uint32_t q : lane_done) {
-            (void)q;
             --heavy_inflight;
-            proj_bytes -= S.cfg.heavy_proj_bytes;
+            proj_bytes -= proj[q];
             ++done;
         }
         lane_done.clear();
@@ -588,16 +623,17 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
         // 2. admission, FIFO within each class; a class stops at the first query that does not
         // fit under the working-set cap (unless nothing at all is resident)
         while (!wait_heavy.empty() && heavy_inflight < S.cfg.max_heavy_inflight &&
-               (proj_bytes + S.cfg.heavy_proj_bytes <= S.cfg.working_set_cap_bytes ||
+               (proj_bytes + proj[wait_heavy.front()] <= S.cfg.working_set_cap_bytes ||
                 (active.empty() && !heavy_inflight))) {
-            H.submit(wait_heavy.front());
+            const uint32_t q = wait_heavy.front();
             wait_heavy.pop_front();
             ++heavy_inflight;
-            proj_bytes += S.cfg.heavy_proj_bytes;
+            proj_bytes += proj[q];
+            H.submit(q);
         }
         S.new_slots.clear();
         while (!wait_light.empty() && !free_slots.empty() &&
-               (proj_bytes + S.cfg.light_proj_bytes <= S.cfg.working_set_cap_bytes ||
+               (proj_bytes + proj[wait_light.front()] <= S.cfg.working_set_cap_bytes ||
                 (active.empty() && !heavy_inflight && S.new_slots.empty()))) {
             admit(wait_light.front());
             wait_light.pop_front();
@@ -686,7 +722,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                 } else {
                     r.status = WK_E_CAPACITY;   // the caller's buffer is full
                 }
-                proj_bytes -= S.cfg.light_proj_bytes;
+                proj_bytes -= proj[q];
                 finished.push_back(s);
                 ++done;
             }

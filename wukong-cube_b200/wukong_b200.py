@@ -77,7 +77,7 @@ class SynthVocab(C.Structure):
 
 class ServeConfig(C.Structure):
     _fields_ = [("working_set_cap_bytes", C.c_uint64), ("arena_bytes", C.c_uint64),
-                ("light_proj_bytes", C.c_uint64), ("heavy_proj_bytes", C.c_uint64),
+                ("min_proj_bytes", C.c_uint64), ("lane_table_bytes", C.c_uint64),
                 ("max_inflight", C.c_uint32), ("max_heavy_inflight", C.c_uint32),
                 ("light_ctas_per_sm", C.c_int32), ("blind", C.c_int32), ("reserved", C.c_int32 * 2)]
 
