@@ -20,8 +20,10 @@ shape) on a sample of the same queries.
 degreeFrom triangle), device-resident graph replays.
 `serving`: open-loop Poisson sweep of the 98 % light / 2 % heavy mix through
 wk_serve_run_open_loop (continuous batching), p50/p99/p99.9 per class.
-`--impl reference` times the CPU restatement of the reference engine (oracle/) on all host
-cores on the same light batch (one query per thread, as the CPU engines run light queries).
+`--impl reference` times the reference's own CPU engine (oracle/_ref/libwkref.so:
+sparql.hpp compiled unmodified, over the GStore arrays of the oracle's store) on all host cores
+on the same light batch, one engine per thread taking whole queries, as a server's engine
+threads run light queries; where that library was not built, the oracle's restatement of it.
 """
 import argparse
 import json
@@ -35,6 +37,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "wukong-cube_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "oracle", "refpin"))
 
 import numpy as np  # noqa: E402
 
@@ -140,10 +143,35 @@ def config(args):
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
+class CpuEngine:
+    """The CPU engine the baselines time: the reference's own engine over the oracle store's
+    arrays where oracle/_ref/libwkref.so exists ("reference"), else the oracle's restatement
+    ("port")."""
+
+    def __init__(self, o):
+        import refengine
+        self.o = o
+        self.kind = "reference" if refengine.available() else "port"
+        self.g = refengine.RefGraph(o) if self.kind == "reference" else None
+        self.how = ("the reference's SPARQLEngine (sparql.hpp compiled unmodified) over the "
+                    "oracle's GStore arrays" if self.g else
+                    "the oracle (the reference CPU engine restated)")
+
+    def run_many(self, flat, nv, threads):
+        return (self.g or self.o).run_many(flat, nv, threads)
+
+    def run_heavy(self, q, cores):
+        """Status of one heavy query split into `cores` slices of its index start."""
+        if self.g:
+            return self.g.run_split(q.flat(), q.nvars, cores)[0]
+        return self.o.run(q.flat(), q.nvars, mt_factor=cores)[0]
+
+
 def run_reference(args, world, rank):
-    """CPU arm: the oracle (restated reference CPU engine) on all host cores.  The process loads
-    the generator's own library (libwk_synth.so) and the oracle, not the product library: the
-    graph comes from the generator, the type instances from the oracle's own store."""
+    """CPU arm: the reference's CPU engine on all host cores (CpuEngine).  The process loads the
+    generator's own library (libwk_synth.so), the oracle and the reference engine, not the
+    product library: the graph comes from the generator, the store and the type instances from
+    the oracle."""
     if rank != 0:
         return
     import oracle
@@ -162,12 +190,13 @@ def run_reference(args, world, rank):
     qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
     flat = [q.flat() for q in qs]
     nv = [q.nvars for q in qs]
+    eng = CpuEngine(o)
     for _ in range(args.warmup):
-        o.run_many(flat, nv, cores)
+        eng.run_many(flat, nv, cores)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        _, st = o.run_many(flat, nv, cores)
+        _, st = eng.run_many(flat, nv, cores)
         times.append(time.perf_counter() - t0)
         assert (st == 0).all()
     value = len(qs) * args.steps / sum(times)
@@ -176,9 +205,9 @@ def run_reference(args, world, rank):
             "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": config(args), "graph": ginfo,
-            "cpu_baseline": {"value": value, "unit": "light queries/s", "cores": cores, "kind": "port",
-                             "sample": "%d steps x %d light queries, one query per thread" %
-                                       (args.steps, len(qs))},
+            "cpu_baseline": {"value": value, "unit": "light queries/s", "cores": cores, "kind": eng.kind,
+                             "sample": "%d steps x %d light queries after %d warm-up steps, one "
+                                       "query per thread; %s" % (args.steps, len(qs), args.warmup, eng.how)},
             "e2e": {"value": value, "unit": "light queries/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -319,6 +348,7 @@ def run_ours(args, world, rank, local_rank):
     flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
     cores = os.cpu_count() or 1
     o = oracle.OracleStore(tr) if rank == 0 else None
+    eng = CpuEngine(o) if o is not None else None
 
     # ---- light batch: correctness gate, then timing.  With N GPUs (replicas) the query stream
     # holds N batches and each rank answers its own share of it.
@@ -429,12 +459,13 @@ def run_ours(args, world, rank, local_rank):
             assert st == 0 and np.array_equal(oracle.sorted_rows(got), oracle.sorted_rows(want))
         if o is not None and not args.no_cpu:
             # the CPU engine on every host core, split as the reference splits an index start
-            # (mt_factor slices of the index list, one per thread; sparql.hpp:213-224); the
-            # correctness run above warmed it
+            # (mt_factor slices of the index list, one per thread; sparql.hpp:213-224), after
+            # one warm run
+            eng.run_heavy(q, cores)
             cpu_t = []
             for _ in range(args.heavy_cpu_reps):
                 t0 = time.perf_counter()
-                st, _, _ = o.run(q.flat(), q.nvars, mt_factor=cores)
+                st = eng.run_heavy(q, cores)
                 cpu_t.append((time.perf_counter() - t0) * 1000)
                 assert st == 0
             heavy_cpu[name] = statistics.median(cpu_t) if cpu_t else None
@@ -449,8 +480,8 @@ def run_ours(args, world, rank, local_rank):
         heavy[name] = {"ms": statistics.median(ms), "rows": heavy_rows[len(heavy)],
                        "plain_ms": plain_ms, "profile": ctx.profile(q, iters=3),
                        "cpu_ms": heavy_cpu.get(name), "cpu_cores": cores,
-                       "cpu_how": "oracle (the reference CPU engine restated), mt_factor = cores, "
-                                  "median of %d runs after a warm run" % args.heavy_cpu_reps}
+                       "cpu_how": "%s, mt_factor = cores, median of %d runs after a warm run"
+                                  % (eng.how if eng else "", args.heavy_cpu_reps)}
         if heavy_cpu.get(name):
             heavy[name]["speedup_vs_cpu"] = heavy_cpu[name] / heavy[name]["ms"]
 
@@ -570,17 +601,18 @@ def run_ours(args, world, rank, local_rank):
             # the reference arm's method: warm-up runs, then --steps timed runs of the same batch
             flat, nv = [q.flat() for q in qs], [q.nvars for q in qs]
             for _ in range(args.warmup):
-                o.run_many(flat, nv, cores)
+                eng.run_many(flat, nv, cores)
             cpu_t = []
             for _ in range(args.steps):
                 t0 = time.perf_counter()
-                _, st = o.run_many(flat, nv, cores)
+                _, st = eng.run_many(flat, nv, cores)
                 cpu_t.append(time.perf_counter() - t0)
                 assert (st == 0).all()
             line["cpu_baseline"] = {"value": len(qs) * len(cpu_t) / sum(cpu_t), "unit": "light queries/s",
-                                    "cores": cores, "kind": "port",
+                                    "cores": cores, "kind": eng.kind,
                                     "sample": "%d steps x %d light queries after %d warm-up steps, one "
-                                              "query per thread" % (args.steps, len(qs), args.warmup)}
+                                              "query per thread; %s" % (args.steps, len(qs), args.warmup,
+                                                                        eng.how)}
         print(json.dumps(line))
     ctx.close()
 

@@ -37,6 +37,7 @@ def lib():
         L.orc_store_sizes.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_uint64)]
         L.orc_store_export.argtypes = [P, P, P, P]
+        L.orc_store_arrays.argtypes = [P, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
         L.orc_query_run.argtypes = [P, P, C.c_int, C.c_int, C.c_int,
                                     C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_int), P]
@@ -83,6 +84,17 @@ class OracleStore:
 
     def get_index(self, pid, d):
         return self.get_triples(0, pid, d)
+
+    def arrays(self):
+        """The store in place, borrowed (valid while this store lives): (slots pointer, slot
+        count, edges pointer, segs uint64[k,10])."""
+        ns, ne, ng = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib().orc_store_sizes(self.h, C.byref(ns), C.byref(ne), C.byref(ng))
+        segs = np.zeros((ng.value, 10), np.uint64)
+        lib().orc_store_export(self.h, None, None, _p(segs))
+        sp, ep = C.c_void_p(), C.c_void_p()
+        lib().orc_store_arrays(self.h, C.byref(sp), C.byref(ep))
+        return sp.value, ns.value, ep.value, segs
 
     def export(self):
         """(slots uint64[n,2], edges uint32[m], segs uint64[k,10]) in the store's own layout."""

@@ -2,8 +2,9 @@
 the reference's own CPU engine (src/core/engine/sparql.hpp and the headers it includes, compiled
 unmodified from the reference tree by oracle/Makefile against oracle/refpin/stubs).
 
-Only the golden-fixture script (tests/golden/make_ref_golden.py) and tests use it.  The library
-exists only where the reference tree was present when it was built.
+The golden-fixture script (tests/golden/make_ref_golden.py), tests and bench.py's reference arm
+use it.  The library exists only where the reference tree was present when it was built (it
+travels with the repository to a machine without that tree).
 """
 import ctypes as C
 import os
@@ -31,6 +32,10 @@ def lib():
                                   C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_int), P]
         L.wkref_free.argtypes = [P]
+        L.wkref_graph_from_store.restype = P
+        L.wkref_graph_from_store.argtypes = [P, C.c_uint64, P, P, C.c_uint64]
+        L.wkref_query_many.argtypes = [P, P, P, P, C.c_uint32, C.c_int, P, P]
+        L.wkref_query_mt.argtypes = [P, P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64)]
         L.wkref_pattern.argtypes = [P, P, C.c_uint64, C.c_int, C.c_int, P, C.c_int, C.c_int,
                                     C.POINTER(C.POINTER(C.c_uint32)), C.POINTER(C.c_uint64),
                                     C.POINTER(C.c_int), P]
@@ -45,10 +50,45 @@ def _p(a):
 
 
 class RefGraph:
-    """A graph the reference engine reads: every key's list as given (get_triples / get_index)."""
+    """A graph the reference engine reads: every key's list as given (get_triples / get_index),
+    or, with `store` (an oracle.OracleStore, kept alive here), that GStore's arrays in place,
+    probed the way the reference's store probes them."""
 
-    def __init__(self):
-        self.h = lib().wkref_graph_new()
+    def __init__(self, store=None, arrays=None):
+        """store: an oracle.OracleStore; arrays: (slots pointer, slot count, edges pointer,
+        segment rows uint64[k,10]) of any store in the GStore layout, whose owner the caller
+        keeps alive."""
+        self.store = store
+        if store is not None:
+            arrays = store.arrays()
+        if arrays is None:
+            self.h = lib().wkref_graph_new()
+        else:
+            sp, ns, ep, segs = arrays
+            self._segs = np.ascontiguousarray(segs, dtype=np.uint64)
+            self.h = lib().wkref_graph_from_store(sp, ns, ep, _p(self._segs), self._segs.shape[0])
+
+    def run_split(self, query_flat, nvars, mt_factor):
+        """One query with its index start split into mt_factor sub-queries, each on its own
+        engine and host thread, merged by the first engine's reply map.  Returns (status,
+        rows of the final table)."""
+        q = np.ascontiguousarray(query_flat, dtype=np.int32)
+        rows = C.c_uint64()
+        rc = lib().wkref_query_mt(self.h, _p(q), q.size // 5, nvars, mt_factor, C.byref(rows))
+        return rc, rows.value
+
+    def run_many(self, flat_list, nvars_list, threads):
+        """Queries through execute_sparql_query on `threads` threads, one engine each.  Returns
+        (row counts, statuses)."""
+        pats = np.ascontiguousarray(np.concatenate([np.asarray(f, np.int32).reshape(-1) for f in flat_list]),
+                                    dtype=np.int32)
+        offs = np.zeros(len(flat_list) + 1, np.int32)
+        offs[1:] = np.cumsum([np.asarray(f).size // 5 for f in flat_list])
+        nv = np.ascontiguousarray(nvars_list, dtype=np.int32)
+        rows = np.zeros(len(flat_list), np.uint64)
+        st = np.zeros(len(flat_list), np.int32)
+        lib().wkref_query_many(self.h, _p(pats), _p(offs), _p(nv), len(flat_list), threads, _p(rows), _p(st))
+        return rows, st
 
     def put(self, vid, pid, d, vals):
         vals = np.ascontiguousarray(vals, dtype=np.uint32)

@@ -1027,10 +1027,18 @@ void orc_store_sizes(void* h, uint64_t* n_slots, uint64_t* n_edges, uint64_t* n_
     *n_segs = s.seg_map.size();
 }
 
+// The store's slot and value arrays in place (borrowed: valid until orc_store_free).
+void orc_store_arrays(void* h, const void** slots, const uint32_t** edges) {
+    Store& s = ((OracleStore*)h)->store;
+    *slots = s.slots.data();
+    *edges = s.values.data();
+}
+
+// slots / edges may be null: only the segment rows are written.
 void orc_store_export(void* h, void* slots, uint32_t* edges, uint64_t* seg_out) {
     Store& s = ((OracleStore*)h)->store;
-    std::memcpy(slots, s.slots.data(), s.slots.size() * sizeof(slot_t));
-    if (!s.values.empty()) std::memcpy(edges, s.values.data(), s.values.size() * 4);
+    if (slots) std::memcpy(slots, s.slots.data(), s.slots.size() * sizeof(slot_t));
+    if (edges && !s.values.empty()) std::memcpy(edges, s.values.data(), s.values.size() * 4);
     uint64_t i = 0;
     for (auto& kv : s.seg_map) {
         const segid_t& id = kv.first;

@@ -359,3 +359,39 @@ def test_gpu_constant_versatile_steps_and_refusals(ctx, ctx_versatile, golden):
     assert e.value.code == wk.UNKNOWN_PATTERN
     res = ctx_versatile.batch([q])
     assert res[0][1] == wk.E_UNSUPPORTED
+
+
+def _product_store_arrays(g):
+    """The host GStore's arrays (wk_gstore_arrays) as RefGraph takes them."""
+    slots, edges, segs = g.arrays()
+    rows = np.array([[m.index, m.pid, m.dir, m.num_keys, m.num_buckets, m.bucket_start, m.num_edges,
+                      m.edge_start, m.ext_start, m.ext_num] for m in segs], np.uint64)
+    return slots.ctypes.data, slots.shape[0], edges.ctypes.data, rows
+
+
+@pytest.mark.parametrize("which", ["oracle", "product"])
+def test_reference_engine_over_gstore_arrays(graph20, golden, which):
+    """The reference engine reading a GStore in place (SlotGraph: the reference's ikey_t, its
+    hash and its bucket walk over the slot array), once over the oracle's store and once over
+    the library's own host-built store, answers like the oracle: light queries in parallel
+    (row counts and statuses), the fixture queries, and the heavy star and triangle split over
+    engine threads the way the reference splits an index start."""
+    import refengine
+    import workloads
+    if not refengine.available():
+        pytest.skip("the reference engine library was not built here")
+    o, v = graph20["oracle"], graph20["vocab"]
+    if which == "oracle":
+        rg = refengine.RefGraph(o)
+    else:
+        rg = refengine.RefGraph(arrays=_product_store_arrays(graph20["gstore"]))
+    qs = [q for _, q in _queries(golden)] + workloads.light_queries(v, graph20["instances"], 400, seed=29)
+    rows, st = rg.run_many([q.flat() for q in qs], [q.nvars for q in qs], 4)
+    orows, ost = o.run_many([q.flat() for q in qs], [q.nvars for q in qs], 4)
+    assert np.array_equal(st, ost)
+    assert np.array_equal(rows[st == 0].astype(np.int64), orows[st == 0].astype(np.int64))
+    for q in (workloads.heavy_star(v), workloads.heavy_triangle(v)):
+        want_st, want, _ = o.run(q.flat(), q.nvars)
+        for f in (1, 3, 8):
+            got_st, got_rows = rg.run_split(q.flat(), q.nvars, f)
+            assert got_st == want_st == 0 and got_rows == want.shape[0]
