@@ -116,103 +116,137 @@ __device__ __forceinline__ bool last_count_cta(StepCtl* ctl) {
     return s_last != 0;
 }
 
-// Registers capped for 8 CTAs per SM (2,048 threads, one probe each in flight).
-__global__ void __launch_bounds__(kFlatThreads, 8) flat_count_kernel(const FlatArgs a) {
+// Key of a row of the count pass: the step's start key (const_to_known / index_to_known) or
+// [cur|pid|dir] (the index key of get_index for the TYPE_ID/IN form, and for vid 0); *look is
+// false where there is nothing to probe.
+__device__ __forceinline__ uint64_t count_key(const FlatArgs& a, const StepDesc& d, bool from_const, uint32_t cur,
+                                              bool* valid, bool* look, uint64_t* bucket) {
+    uint64_t key;
+    SegDesc sg = d.seg;   // by value: registers, not a pointer into the parameter block
+    *valid = from_const || cur != kBlankId;
+    if (from_const) {
+        key = d.start_key;
+    } else if (d.op == kXK2U && d.type_index) {
+        // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+        key = make_key(0, cur, kIn);
+        sg = a.seg_index[kIn];
+        if (cur >= (1u << kNbitsIdx)) *valid = false;
+    } else {
+        key = make_key(cur, d.pid, d.dir);
+        if (cur == 0) sg = a.seg_index[d.dir & 1];   // vid 0 names the index
+    }
+    *look = *valid && sg.num_buckets != 0 && key != 0;
+    *bucket = *look ? bucket_of(key, sg) : 0;
+    if (*look && *bucket >= a.store.n_buckets) {
+        atomicOr(&a.ctl->err, kErrCorrupt);
+        *look = false;
+    }
+    return key;
+}
+
+// Pointer word of `key` given its home bucket's slot 0 (already loaded): slot 1 shares slot 0's
+// 32-byte sector, so its load hits L1; the rest walk on from slot 2.
+__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0) {
+    if (s0.x == key) return s0.y;
+    if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
+    const ulonglong2 s1 = load_slot(a.store.slots + b * kAssoc + 1);
+    if (s1.x == key) return s1.y;
+    if (s1.x == 0) return 0;
+    return thread_probe(a.store, key, b, &a.ctl->err, 2);
+}
+
+// kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
+// loaded before any is compared, and the neighbour words of their one-to-one rows are loaded
+// before any output row is written, so a thread has that many random reads in flight.
+// Registers are capped for kCountCtas CTAs per SM.  kFilter: the membership steps
+// (known_to_known, known_to_const, const_to_known, index_to_known); the other instance (starts
+// and known_to_unknown) carries no membership search.
+constexpr int kRowsPerThread = 4;
+constexpr int kCountCtas = 4;
+
+template <bool kFilter>
+__global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(const FlatArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
     const uint64_t R = flat_rows(a);
     if (R < a.min_rows) return;
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
     const StepDesc& d = a.step;
-    const bool filt = is_filter_op(d.op);
     const bool from_const = d.op == kXC2K || d.op == kXI2K;   // every row looks up one list
     const int tcol = (d.op == kXK2K || from_const) ? d.ce : -1;   // the row's membership target
     uint64_t sum = 0, sd = 0, nvalid = 0;
     bool ones = true;   // every row of this thread has exactly one output row
     const bool spec = R <= a.out_cap_rows;   // output row r exists: one-to-one rows written here
-    // the next round's row words are loaded while this round's probe is out (3-7% per step on
-    // the heavy queries)
-    uint32_t nxt_cur = 0, nxt_tgt = d.end_const;
-    {
-        const uint64_t r = lo + threadIdx.x;
-        if (r < hi) {
-            const uint32_t* row = a.in + r * (uint64_t)a.w_in;
-            nxt_cur = __ldg(row + d.cs);
-            if (tcol >= 0) nxt_tgt = __ldg(row + tcol);
+    constexpr int K = kRowsPerThread;
+    constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
+    for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
+        uint64_t key[K], bkt[K], p[K];
+        bool valid[K], look[K];
+        ulonglong2 s0[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
+            const uint32_t cur = r < hi ? __ldg(a.in + r * (uint64_t)a.w_in + d.cs) : kBlankId;
+            key[k] = count_key(a, d, from_const, cur, &valid[k], &look[k], &bkt[k]);
+            if (r >= hi) valid[k] = look[k] = false;
         }
-    }
-    for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
-        const uint32_t cur = nxt_cur;
-        uint32_t target = nxt_tgt;
-        if (r + kFlatThreads < hi) {
-            const uint32_t* row = a.in + (r + kFlatThreads) * (uint64_t)a.w_in;
-            nxt_cur = __ldg(row + d.cs);
-            if (tcol >= 0) nxt_tgt = __ldg(row + tcol);
-        }
-        uint64_t key;
-        SegDesc sg = d.seg;   // by value: registers, not a pointer into the parameter block
-        bool valid = from_const || cur != kBlankId;
-        if (from_const) {
-            key = d.start_key;
-        } else if (d.op == kXK2U && d.type_index) {
-            // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-            key = make_key(0, cur, kIn);
-            sg = a.seg_index[kIn];
-            if (cur >= (1u << kNbitsIdx)) valid = false;
-        } else {
-            key = make_key(cur, d.pid, d.dir);
-            if (cur == 0) sg = a.seg_index[d.dir & 1];   // vid 0 names the index
-        }
-        uint64_t off = 0, deg = 0;
-        if (valid && sg.num_buckets != 0 && key != 0) {
-            // the home bucket's first sector (slots 0 and 1, key and pointer) settles most keys;
-            // the rest walk on from slot 2
-            const uint64_t b = bucket_of(key, sg);
-            uint64_t p = 0;
-            if (b >= a.store.n_buckets) {
-                atomicOr(&a.ctl->err, kErrCorrupt);
-            } else {
-                const ulonglong2 s0 = load_slot(a.store.slots + b * kAssoc);
-                const ulonglong2 s1 = load_slot(a.store.slots + b * kAssoc + 1);
-                if (s0.x == key) p = s0.y;
-                else if (s0.x == 0) p = 0;
-                else if (s1.x == key) p = s1.y;
-                else if (s1.x != 0) p = thread_probe(a.store, key, b, &a.ctl->err, 2);
-            }
-            off = ptr_off(p);
-            deg = ptr_size(p);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) p[k] = look[k] ? settle(a, key[k], bkt[k], s0[k]) : 0;
+        // counts and list offsets
+        uint32_t c[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
+            uint64_t off = ptr_off(p[k]), deg = ptr_size(p[k]);
             if (off + deg > a.store.n_edges) {
                 if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
                 deg = 0;
             }
-            if (d.op == kXI2K) {   // index_to_known reads its mt slice of the list
-                uint64_t lo, hi;
-                mt_slice(d.mt, deg, &lo, &hi);
-                off += lo;
-                deg = hi - lo;
+            if (d.op == kXI2K && valid[k]) {   // index_to_known reads its mt slice of the list
+                uint64_t s_lo, s_hi;
+                mt_slice(d.mt, deg, &s_lo, &s_hi);
+                off += s_lo;
+                deg = s_hi - s_lo;
+            }
+            c[k] = (uint32_t)deg;
+            if (kFilter && valid[k] && deg) {
+                // the membership target shares the row's sector with its start column
+                const uint32_t target = tcol >= 0 ? __ldg(a.in + r * (uint64_t)a.w_in + tcol) : d.end_const;
+                c[k] = thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0) ? 1u : 0u;
+            }
+            if (!valid[k]) c[k] = 0;
+            p[k] = off;   // from here on p holds the list offset
+            if (r < hi) {
+                a.pos[r] = c[k];   // the count; flat_place_kernel turns it into the row's position
+                if (!kFilter) a.off[r] = off;
+                if (c[k] != 1) ones = false;
+                sum += c[k];
+            }
+            if (valid[k]) {
+                sd += deg;
+                ++nvalid;
             }
         }
-        uint32_t c = (uint32_t)deg;
-        if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
-        if (!valid) c = 0;
-        a.pos[r] = c;   // the count; flat_place_kernel turns it into the row's position
-        if (c != 1) ones = false;
-        if (!filt) {
-            a.off[r] = off;
+        if (!kFilter && spec) {
             // A row with exactly one output row writes it now, at output row r: when every row
             // has one (a functional predicate), that is the step's output and the place and
-            // expand passes return at once; otherwise expand overwrites these rows.
-            if (c == 1 && spec) {
+            // expand passes return at once; otherwise expand overwrites these rows.  The rows'
+            // neighbour words are all loaded before any row is written.
+            uint32_t nb[K];
+#pragma unroll
+            for (int k = 0; k < K; ++k) nb[k] = c[k] == 1 ? __ldg(a.store.edges + p[k]) : 0;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                if (c[k] != 1) continue;
+                const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
                 const uint32_t* src = a.in + r * (uint64_t)a.w_in;
                 uint32_t* dst = a.out + r * (uint64_t)a.w_out;
-                for (int k = 0; k < d.cin; ++k) dst[k] = __ldg(src + k);
-                dst[d.cin] = __ldg(a.store.edges + off);
+                for (int j = 0; j < d.cin; ++j) dst[j] = __ldg(src + j);
+                dst[d.cin] = nb[k];
             }
-        }
-        sum += c;
-        if (valid) {
-            sd += deg;
-            ++nvalid;
         }
     }
     const bool all_ones = __syncthreads_and(ones);
@@ -555,7 +589,9 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
 int flat_grid(int sm_count) { return sm_count * (2048 / kFlatThreads); }
 
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
-    flat_count_kernel<<<grid, kFlatThreads, 0, s>>>(a);   // its last CTA scans the totals
+    // its last CTA scans the totals
+    if (is_filter_op(a.step.op)) flat_count_kernel<true><<<grid, kFlatThreads, 0, s>>>(a);
+    else flat_count_kernel<false><<<grid, kFlatThreads, 0, s>>>(a);
     flat_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     return cudaGetLastError();
@@ -570,7 +606,8 @@ cudaError_t launch_flat_level(const FlatLevelArgs& a, int grid, cudaStream_t s) 
 
 cudaError_t flat_kernel_attrs() {
     cudaError_t e;
-    if ((e = use_max_shared_carveout(flat_count_kernel)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_count_kernel<true>)) != cudaSuccess) return e;
+    if ((e = use_max_shared_carveout(flat_count_kernel<false>)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_place_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_expand_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_level_count_kernel)) != cudaSuccess) return e;
