@@ -206,9 +206,10 @@ __device__ __forceinline__ bool thread_member(const uint32_t* edges, uint64_t of
     return false;
 }
 
-// Exclusive block scan of s_cnt[0..n) into s_pre[0..n]; returns the tile total.
-__device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* s_pre, int n,
-                                               uint64_t* s_warp) {
+// Exclusive block scan of f(s_cnt[0..n)) into s_pre[0..n]; returns the tile total.
+template <class Out, class F>
+__device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, Out* s_pre, int n, uint64_t* s_warp,
+                                               F f) {
     constexpr int per = kTileRows / kStepThreads;
     constexpr int nwarps = kStepThreads / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -217,7 +218,7 @@ __device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* 
     uint64_t sum = 0;
 #pragma unroll
     for (int i = 0; i < per; ++i) {
-        v[i] = (base + i < n) ? s_cnt[base + i] : 0;
+        v[i] = (base + i < n) ? f(s_cnt[base + i]) : 0;
         sum += v[i];
     }
     uint64_t x = sum;
@@ -241,13 +242,18 @@ __device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* 
     uint64_t run = (warp ? s_warp[warp - 1] : 0) + x - sum;
 #pragma unroll
     for (int i = 0; i < per; ++i) {
-        if (base + i < n) s_pre[base + i] = run;
+        if (base + i < n) s_pre[base + i] = (Out)run;
         run += v[i];
     }
     const uint64_t total = s_warp[nwarps - 1];
-    if (threadIdx.x == 0) s_pre[n] = total;
+    if (threadIdx.x == 0) s_pre[n] = (Out)total;
     __syncthreads();
     return total;
+}
+
+__device__ __forceinline__ uint64_t block_scan(const uint32_t* s_cnt, uint64_t* s_pre, int n,
+                                               uint64_t* s_warp) {
+    return block_scan(s_cnt, s_pre, n, s_warp, [](uint32_t c) { return (uint64_t)c; });
 }
 
 // Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled

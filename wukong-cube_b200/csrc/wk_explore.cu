@@ -70,9 +70,10 @@ __shared__ long long s_ph_t;
 // The step every row of a finished query runs: nothing.
 __constant__ StepDesc c_done = {{0, 0, 0, 0}, 0, 0, 0, kXDone, 0, 0, 0, 0, 0, 0, 0, 0};
 
-// Rows with more output rows than this are written as slices from the queue.
+// Rows with more output rows than this are written as slices from the queue.  At most 2^23, so
+// a tile's short-row outputs (256 rows) stay below 2^31 and their scan fits 32 bits.
 __device__ __forceinline__ uint32_t slice_threshold(const ExploreArgs& a) {
-    return a.slice_rows ? max(a.slice_rows, (uint32_t)kMinSliceRows) : (uint32_t)kHeavyRows;
+    return a.slice_rows ? min(max(a.slice_rows, (uint32_t)kMinSliceRows), 1u << 23) : (uint32_t)kHeavyRows;
 }
 
 // Polls of a bounded wait on another CTA (look-back, slice queue) before it gives up.
@@ -97,14 +98,26 @@ struct TileState {
     int has_heavy;
 };
 
-// Shared-memory arrays of one tile buffer.
+// Words of one tile buffer: its rows (rounded to 16 bytes, the TMA copy's unit), pre and off
+// (64-bit), lpre (kTileRows + 4 words, so the next buffer starts on 16 bytes) and three
+// per-row words.
+__host__ __device__ constexpr size_t tile_buf_words(int wi) {
+    return (((size_t)kTileRows * wi + 3) & ~(size_t)3) + 2 * (kTileRows + 2) + 2 * kTileRows + (kTileRows + 4) +
+           3 * kTileRows;
+}
+static_assert(tile_buf_words(1) % 4 == 0, "tile buffers start on 16 bytes");
+
+// Most rows a tile stages for its writes at once (explore_smem_bytes sizes the staging).
+constexpr int kMaxChunkRows = 512;
+
+// Shared-memory arrays of one tile buffer (tile_buf_words() words).
 struct TileBuf {
     uint32_t* in;     // kTileRows * w_in words (TMA destination)
     uint64_t* pre;    // kTileRows + 2: exclusive scan of cnt, pre[n] = total
-    uint64_t* lpre;   // kTileRows + 2: exclusive scan of lcnt
     uint64_t* off;    // kTileRows: first edge of each row's list
+    uint32_t* lpre;   // kTileRows + 4: exclusive scan of the short rows' counts (0 for a row
+                      // whose list goes to the slice queue); filled only when the tile has one
     uint32_t* cnt;    // kTileRows: output rows of each input row
-    uint32_t* lcnt;   // kTileRows: cnt for short lists, 0 for long ones
     uint32_t* q;      // kTileRows: owner query
     uint32_t* meta;   // kTileRows: op | cin << 8 | cout << 16
 };
@@ -113,11 +126,10 @@ __device__ __forceinline__ TileBuf tile_buf(uint32_t* base, int wi) {
     TileBuf b;
     b.in = base;
     b.pre = reinterpret_cast<uint64_t*>(base + (((size_t)kTileRows * wi + 3) & ~(size_t)3));
-    b.lpre = b.pre + kTileRows + 2;
-    b.off = b.lpre + kTileRows + 2;
-    b.cnt = reinterpret_cast<uint32_t*>(b.off + kTileRows);
-    b.lcnt = b.cnt + kTileRows;
-    b.q = b.lcnt + kTileRows;
+    b.off = b.pre + kTileRows + 2;
+    b.lpre = reinterpret_cast<uint32_t*>(b.off + kTileRows);
+    b.cnt = b.lpre + kTileRows + 4;
+    b.q = b.cnt + kTileRows;
     b.meta = b.q + kTileRows;
     return b;
 }
@@ -271,15 +283,14 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     }
     __syncthreads();
     WK_PH(2);
-    for (int i = threadIdx.x; i < n; i += kStepThreads) {
-        const uint32_t c = B.cnt[i];
-        const bool heavy = c > slice_threshold(a);
-        B.lcnt[i] = heavy ? 0u : c;
-        if (heavy) S.has_heavy = 1;
-    }
+    const uint32_t thr = slice_threshold(a);
+    for (int i = threadIdx.x; i < n; i += kStepThreads)
+        if (B.cnt[i] > thr) S.has_heavy = 1;
     __syncthreads();
     const uint64_t total = block_scan(B.cnt, B.pre, n, s_warp);
-    const uint64_t ltotal = S.has_heavy ? block_scan(B.lcnt, B.lpre, n, s_warp) : total;
+    const uint64_t ltotal =
+        S.has_heavy ? block_scan(B.cnt, B.lpre, n, s_warp, [thr](uint32_t c) { return (uint64_t)(c > thr ? 0u : c); })
+                    : total;
     if (threadIdx.x == 0) {
         S.total = total;
         S.ltotal = ltotal;
@@ -296,6 +307,9 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
                                           uint64_t* bar, unsigned phase, uint64_t ntiles, int wi,
                                           int wo, int chunk_rows, unsigned epoch, uint64_t* s_pos,
                                           uint32_t* s_out, unsigned long long* s_excl, uint64_t obase) {
+    __shared__ uint32_t s_mark[kMaxChunkRows / 32];   // first outputs of rows in the chunk
+    __shared__ uint16_t s_first[kMaxChunkRows];       // the row of each marked output
+    __shared__ int s_carry[2];                        // row of the chunk's last output
     const uint64_t tile = S.tile;
     const int n = S.n;
     const uint64_t total = S.total, ltotal = S.ltotal;
@@ -349,20 +363,36 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
         }
     }
     WK_PH(5);
-    // write the short-list rows (stride w_out)
+    // Write the short-list rows (stride w_out), chunk by chunk of the staging.  Output o of the
+    // tile's short rows belongs to the last row whose first output is at or below o: each
+    // chunk marks its rows' first outputs in a bitmap (s_mark, with the row in s_first), and an
+    // output finds its row from the highest mark at or below it, looking back at most a chunk;
+    // an output before the chunk's first mark continues the row the previous chunk ended in.
     if (fits && ltotal) {
         const bool contiguous = !S.has_heavy;
-        const uint64_t* lp = contiguous ? B.pre : B.lpre;
-        for (uint64_t c0 = 0; c0 < ltotal; c0 += chunk_rows) {
+        int chunk = 0;
+        for (uint64_t c0 = 0; c0 < ltotal; c0 += chunk_rows, ++chunk) {
             const int m = (int)min((uint64_t)chunk_rows, ltotal - c0);
-            for (int j = threadIdx.x; j < m; j += kStepThreads) {
-                const uint64_t o = c0 + j;
-                int lo = 0, hi = n;   // lp[lo] <= o < lp[hi]
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (lp[mid] <= o) lo = mid; else hi = mid;
+            for (int i = threadIdx.x; i < (m + 31) / 32; i += kStepThreads) s_mark[i] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += kStepThreads) {
+                const uint64_t st = contiguous ? B.pre[i] : B.lpre[i];
+                const uint64_t en = contiguous ? B.pre[i + 1] : B.lpre[i + 1];
+                if (en > st && st >= c0 && st < c0 + m) {
+                    const int j = (int)(st - c0);
+                    s_first[j] = (uint16_t)i;
+                    atomicOr(&s_mark[j >> 5], 1u << (j & 31));
                 }
-                const uint64_t k = o - lp[lo];
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < m; j += kStepThreads) {
+                int wd = j >> 5;
+                unsigned w = s_mark[wd] & (0xFFFFFFFFu >> (31 - (j & 31)));
+                while (!w && wd > 0) w = s_mark[--wd];
+                const int lo = w ? (int)s_first[wd * 32 + 31 - __clz(w)] : s_carry[chunk & 1];
+                if (j == m - 1) s_carry[(chunk + 1) & 1] = lo;
+                const uint64_t o = c0 + j;
+                const uint64_t k = o - (contiguous ? B.pre[lo] : (uint64_t)B.lpre[lo]);
                 const uint32_t meta = B.meta[lo];
                 const int opv = meta & 0xFF, cin = (meta >> 8) & 0xFF;
                 uint32_t* dst = s_out + (size_t)j * wo;
@@ -410,8 +440,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     __shared__ TileState s_ts[2];
 
     const int wi = a.virtual_rows ? 0 : a.w_in, wo = a.w_out;
-    const size_t buf_words = (((size_t)kTileRows * wi + 3) & ~(size_t)3) + 4 * (kTileRows + 2) +
-                             2 * kTileRows + 4 * kTileRows;
+    const size_t buf_words = tile_buf_words(wi);
     uint32_t* base = reinterpret_cast<uint32_t*>(smem);
     uint64_t* s_pos = reinterpret_cast<uint64_t*>(base + 2 * buf_words);
     uint32_t* s_out = reinterpret_cast<uint32_t*>(s_pos + chunk_rows);
@@ -559,19 +588,17 @@ cudaError_t set_attr(int bytes) {
 
 size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
     // two tile buffers (rows, two scans, list offsets, four per-row words) + the write staging
-    const size_t buf_words = (((size_t)kTileRows * w_in + 3) & ~(size_t)3) + 4 * (kTileRows + 2) +
-                             2 * kTileRows + 4 * kTileRows;
-    const size_t bufs = 2 * buf_words * 4;
+    const size_t bufs = 2 * tile_buf_words(w_in) * 4;
     // The staging (a position and an output row per staged row) gets what is left once
     // kExploreMinBlocks CTAs fit in an SM's 228 KiB (1 KiB of it reserved per CTA), between 64
     // and 512 rows.  A fixed 8 KiB staging left wide levels at 5 CTAs per SM; sizing it this way
     // took the 16,384-query batch's two widest levels from 0.190 / 0.121 ms to 0.175 / 0.112 ms.
     const size_t per_row = 8 + 4 * (size_t)(w_out > 0 ? w_out : 1);
     const size_t budget = 233472 / kExploreMinBlocks - 1024;
-    int chunk = 512;
+    int chunk = kMaxChunkRows;
     if (bufs + chunk * per_row > budget)
         chunk = budget > bufs ? (int)(((budget - bufs) / per_row) & ~(size_t)31) : 64;
-    if (chunk > 512) chunk = 512;
+    if (chunk > kMaxChunkRows) chunk = kMaxChunkRows;
     if (chunk < 64) chunk = 64;
     size_t bytes = bufs + (size_t)chunk * per_row;
     if (chunk_rows) *chunk_rows = chunk;
