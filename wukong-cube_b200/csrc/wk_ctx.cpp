@@ -648,13 +648,15 @@ extern "C" int wk_store_upload(wk_ctx* ctx, const wk_seg_meta* segs, uint32_t n_
                                uint64_t n_edges) {
     if (!ctx || (!segs && n_segs) || (!slots && n_slots) || (!edges && n_edges)) return WK_E_BADARG;
     if (n_slots % wk::kAssoc) return ctx->fail(WK_E_BADARG, "slot count is not a multiple of 8");
+    // the exploration probe holds bucket ids in 32 bits (2^32 buckets would be 512 GiB)
+    if (n_slots / wk::kAssoc >= (1ull << 32)) return ctx->fail(WK_E_CAPACITY, "2^32 buckets or more");
     std::lock_guard<std::mutex> lk(ctx->mu);
     const uint64_t nb = n_slots / wk::kAssoc;
     for (uint32_t i = 0; i < n_segs; ++i) {
         const wk_seg_meta& m = segs[i];
         if (m.dir != WK_IN && m.dir != WK_OUT)
             return ctx->fail(WK_E_BADARG, "segment direction");
-        if (m.bucket_start + m.num_buckets > nb)
+        if (m.bucket_start > nb || m.num_buckets > nb - m.bucket_start)
             return ctx->fail(WK_E_CORRUPT, "segment buckets outside the slot array");
         if (m.edge_start + m.num_edges > n_edges)
             return ctx->fail(WK_E_CORRUPT, "segment edges outside the edge array");

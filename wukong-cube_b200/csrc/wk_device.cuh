@@ -90,10 +90,12 @@ __device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
 // Probe kUnroll keys per group of L lanes.  Every lane of the warp must call this (ballots and
 // shuffles are warp-wide).  On entry bucket[u] is the key's home bucket and pending[u] says
 // whether to look; on return ptr[u] is the slot's pointer word in every lane of the group, or 0
-// when the key is absent.
-template <int L>
+// when the key is absent.  Bucket ids may be held in 32 bits (BucketT): a device's store has
+// fewer than 2^32 buckets, and a chain link at or past the bucket count is reported as
+// corruption before it is followed.
+template <int L, class BucketT>
 __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&key)[kUnroll],
-                                            uint64_t (&bucket)[kUnroll], bool (&pending)[kUnroll],
+                                            BucketT (&bucket)[kUnroll], bool (&pending)[kUnroll],
                                             uint64_t (&ptr)[kUnroll], unsigned* err) {
     const int lane = threadIdx.x & 31;
     const int h = lane & (L - 1);
@@ -146,8 +148,11 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
                 } else if ((round[u] + 1) * L >= kAssoc) {
                     if (kx == 0) {
                         pending[u] = false;       // no extension bucket
+                    } else if (key_vid(kx) >= st.n_buckets) {
+                        pending[u] = false;       // a link out of range: corrupt chain
+                        if (h == 0) atomicOr(err, kErrCorrupt);
                     } else {
-                        bucket[u] = key_vid(kx);  // follow slot 7 (kvstore.hpp:303-310)
+                        bucket[u] = (BucketT)key_vid(kx);   // follow slot 7 (kvstore.hpp:303-310)
                         round[u] = 0;
                     }
                 } else {

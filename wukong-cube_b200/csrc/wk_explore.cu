@@ -175,8 +175,8 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         // of the batch (descriptor, key, home bucket, filter target), then the group shares
         // them by shuffles, so no row's hash or descriptor is worked out twice.
         // flag: op | valid << 8 | pending << 9 | cin << 16 | cout << 24
-        uint64_t mkey[kOwn], mbkt[kOwn];
-        uint32_t mtgt[kOwn], mflag[kOwn];
+        uint64_t mkey[kOwn];
+        uint32_t mbkt[kOwn], mtgt[kOwn], mflag[kOwn];   // buckets in 32 bits (group_probe)
 #pragma unroll
         for (int j = 0; j < kOwn; ++j) {
             const int u = j * L + h;
@@ -216,13 +216,14 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
                 const bool pending = valid && sg->num_buckets != 0 && key != 0;
                 const uint32_t cin = d->cin, cout = d->cout;
                 mkey[j] = key;
-                mbkt[j] = pending ? bucket_of(key, *sg) : 0;
+                mbkt[j] = pending ? (uint32_t)bucket_of(key, *sg) : 0;
                 mtgt[j] = target;
                 mflag[j] = op | (valid ? 0x100u : 0u) | (pending ? 0x200u : 0u) | (cin << 16) | (cout << 24);
                 B.meta[row] = op | (cin << 8) | (cout << 16);
             }
         }
-        uint64_t key[kUnroll], bucket[kUnroll], ptr[kUnroll];
+        uint64_t key[kUnroll], ptr[kUnroll];
+        uint32_t bucket[kUnroll];
         bool valid[kUnroll], pending[kUnroll];
         int row[kUnroll];
         uint32_t target[kUnroll], flag[kUnroll];
@@ -429,7 +430,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
 
 // Resident CTAs per SM the launch is built for: registers are capped for this many, and the
 // write staging is sized so that shared memory allows as many (explore_smem_bytes).
-constexpr int kExploreMinBlocks = 6;
+constexpr int kExploreMinBlocks = 7;
 
 template <int L>
 __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kernel(const ExploreArgs a, int chunk_rows) {
