@@ -617,6 +617,83 @@ def run_ours(args, world, rank, local_rank):
     ctx.close()
 
 
+def run_scale(args):
+    """The scale configuration on one GPU: the store built on the device straight from the
+    generator's triples (no host store), its footprint, the light batch and the heavy queries
+    timed on it.  With --scale-check N the store is copied back to host memory
+    (wk_store_export) and the reference's CPU engine, reading those arrays in place, answers N
+    of the light queries and both heavy queries: their row counts must equal the device's."""
+    import torch
+
+    import workloads
+    import wukong_b200 as wk
+    t0 = time.time()
+    tr, v = wk.synth_generate(args.orgs, seed=args.seed, zipf=args.zipf, zipf_s=args.zipf_s)
+    gen_s = time.time() - t0
+    info = {"triples": int(tr.shape[0]), "gen_s": round(gen_s, 1), "load_factor": args.load_factor or 0.1}
+    ctx = wk.Context(0)
+    free0, total = torch.cuda.mem_get_info()
+    t0 = time.time()
+    ctx.build_store(tr, load_factor=args.load_factor)
+    info["device_build_s"] = round(time.time() - t0, 2)
+    info["store_bytes"] = ctx.store_bytes()
+    del tr
+    # type instances from the device's index lists (get_index(t, IN))
+    inst = {}
+    t = ctx.table(capacity=1 << 20)
+    for ty in range(v["t_org"], v["t_doc"] + 1):
+        ctx.index_to_unknown(ty, wk.IN, t)
+        inst[ty] = t.download().reshape(-1).copy()
+    qs = workloads.light_queries(v, inst, args.light, seed=args.seed + 1)
+    res = ctx.batch(qs)
+    light_rows = np.array([r[0].shape[0] if r[0] is not None else -1 for r in res], np.int64)
+    assert (light_rows >= 0).all(), "a light query failed"
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+    ctx.batch_device(qs)
+    for _ in range(args.warmup):
+        ctx.batch_replay()
+    ctx.check()
+    with Clocks(0) as clk:
+        step_ms = timed(stream, flush, args.steps, ctx.batch_replay)
+    ctx.check()
+    hq = {"star": workloads.heavy_star(v), "triangle": workloads.heavy_triangle(v)}
+    heavy = {}
+    for name, q in hq.items():
+        got, _ = ctx.execute(q, wk.MODE_GRAPH)
+        ms = timed(stream, flush, args.steps, lambda q=q: ctx.enqueue(q, wk.MODE_GRAPH))
+        ctx.check()
+        heavy[name] = {"ms": statistics.median(ms), "rows": int(got.shape[0])}
+    free1, _ = torch.cuda.mem_get_info()
+    info["device_used_bytes"] = int(free0 - free1)
+    info["device_total_bytes"] = int(total)
+    check = None
+    if args.scale_check:
+        import refengine
+        slots, edges, segs = ctx.export_store()
+        rows = np.array([[m["index"], m["pid"], m["dir"], m["num_keys"], m["num_buckets"], m["bucket_start"],
+                          m["num_edges"], m["edge_start"], m["ext_start"], m["ext_num"]] for m in segs], np.uint64)
+        rg = refengine.RefGraph(arrays=(slots.ctypes.data, slots.shape[0], edges.ctypes.data, rows))
+        cores = os.cpu_count() or 1
+        pick = list(range(0, len(qs), max(1, len(qs) // args.scale_check)))[:args.scale_check]
+        rrows, rst = rg.run_many([qs[i].flat() for i in pick], [qs[i].nvars for i in pick], cores)
+        assert (rst == 0).all() and np.array_equal(rrows.astype(np.int64), light_rows[pick]), \
+            "light row counts differ from the reference engine"
+        for name, q in hq.items():
+            st, n = rg.run_split(q.flat(), q.nvars, cores)
+            assert st == 0 and n == heavy[name]["rows"], name
+        check = {"light_queries": len(pick), "heavy": list(hq),
+                 "how": "row counts equal the reference's CPU engine reading the exported store"}
+    line = {"metric": "scale configuration: light-query QPS, heavy-query ms, single-GPU footprint",
+            "value": len(qs) * args.steps / (sum(step_ms) / 1000.0), "unit": "light queries/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(step_ms), "higher_is_better": True, "dtype": "u32",
+            "data": "synthetic", "config": config(args), "graph": info, "heavy": heavy,
+            "parity": check, "clocks": clk.summary()}
+    print(json.dumps(line))
+    ctx.close()
+
+
 def run_profile_case(args):
     """A small, self-contained case for ncu: one heavy query (`--heavy`, resident mode) and one
     light batch, each run `--steps` times after `--warmup` runs, no oracle, no timing.  The
@@ -692,6 +769,12 @@ def main():
                     default=[1000, 10000, 50000, 100000, 125000, 150000, 175000, 200000, 500000])
     ap.add_argument("--serve-seconds", type=float, default=0.25,
                     help="arrival span of each serving rate")
+    ap.add_argument("--device-store", action="store_true",
+                    help="the scale run: store built on the device only, footprint, light batch "
+                         "and heavy queries (no host store, oracle or serving)")
+    ap.add_argument("--scale-check", type=int, default=0,
+                    help="with --device-store: light queries checked against the reference "
+                         "engine over the exported store (needs host memory for the store)")
     ap.add_argument("--serve-lanes", type=int, default=4,
                     help="serving: index-start queries running at once, one lane each")
     args = ap.parse_args()
@@ -700,6 +783,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.profile_case:
         run_profile_case(args)
+        return
+    if args.device_store:
+        run_scale(args)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)
