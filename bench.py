@@ -292,9 +292,9 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
     both = [s for s in ok if s["heavy_us"]["p99"] <= 5000.0 and
             s["heavy_completed_qps"] >= 0.95 * s["heavy_offered_qps"]]
     best2 = max(both, key=lambda s: s["offered_qps"]) if both else None
-    return {"mix": "98% light (batch shapes) / 2% heavy (star, triangle); open-loop Poisson; "
-                   "blind replies (row counts); heavy queries on %d low-priority lanes; admission "
-                   "by each query's projected bytes" % args.serve_lanes,
+    return {"mix": ("98% light (batch shapes) / 2% heavy (star, triangle); open-loop Poisson; "
+                    "blind replies (row counts); heavy queries on {} low-priority lanes; admission "
+                    "by each query's projected bytes").format(args.serve_lanes),
             "sweep": sweep,
             "sustained_qps_light_p99_le_1ms": best["light_offered_qps"] if best else None,
             "sustained_offered_qps_at_that_point": best["offered_qps"] if best else None,
