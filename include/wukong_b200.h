@@ -440,12 +440,13 @@ int wk_debug_fail_next(wk_ctx* ctx, uint32_t err_bits);
 int wk_debug_device_allocs(uint64_t* count);
 
 /* Tile-schedule knobs of the exploration launch (what the autotuner sets).
- *   knob 0: lanes per probe group of the single-query path (2, 4 or 8: 32-, 64- or 128-byte
- *           bucket slices staged per request);
+ *   knob 0: lanes per probe group of the single-query path (1: one thread per row reading its
+ *           home bucket's first 32 bytes; 2, 4 or 8: a group of lanes staging 32-, 64- or
+ *           128-byte bucket slices per request);
  *   knob 1: the same for batches and serving;
  *   knob 2: the list length above which a row's output is written as 2,048-row slices by every
  *           CTA (block-per-row) instead of by the CTA that probed it (group-per-row); 8 to
- *           2^24, default 128;
+ *           2^23, default 128;
  *   knob 3: the same for batches and serving;
  *   knob 4: single-query steps of index-start plans (and single steps) whose input has at
  *           least this many rows run as the flat count / scan / expand pipeline instead of the

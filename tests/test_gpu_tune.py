@@ -19,7 +19,7 @@ def test_knob_values_are_checked(ctx):
         assert e.value.code == wk.E_BADARG
 
 
-@pytest.mark.parametrize("lanes,slice_rows", [(2, 128), (8, 32), (4, 16384), (2, 8)])
+@pytest.mark.parametrize("lanes,slice_rows", [(2, 128), (8, 32), (4, 16384), (2, 8), (1, 128), (1, 8)])
 def test_every_setting_gives_the_oracle_results(ctx, graph20, lanes, slice_rows):
     v = graph20["vocab"]
     o = graph20["oracle"]
@@ -50,10 +50,10 @@ def test_autotune_picks_a_candidate_and_keeps_results(ctx, graph20):
     old = [ctx.tune_get(k) for k in range(6)]
     try:
         r = ctx.autotune(qs + heavy, iters=3)
-        assert r["batch_lanes"] in (2, 4, 8) and r["lanes"] in (2, 4, 8)
+        assert r["batch_lanes"] in (1, 2, 4, 8) and r["lanes"] in (1, 2, 4, 8)
         assert r["batch_slice_rows"] in (8, 16, 32, 128, 512)
         assert r["slice_rows"] in (8, 16, 32, 128, 512)
-        assert r["candidates"] == 3 * 5 + max(len(q.patterns) for q in qs) + 3 + 5
+        assert r["candidates"] == 4 * 5 + max(len(q.patterns) for q in qs) + 4 + 5
         assert 0 <= r["batch_flat"] < 64 and ctx.tune_get(wk.KNOB_BATCH_FLAT) == r["batch_flat"]
         assert ctx.tune_get(wk.KNOB_BATCH_LANES) == r["batch_lanes"]
         assert ctx.tune_get(wk.KNOB_SLICE_ROWS) == r["slice_rows"]

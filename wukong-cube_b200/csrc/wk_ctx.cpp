@@ -1416,7 +1416,8 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
     if (!ctx) return WK_E_BADARG;
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (knob == WK_KNOB_LANES || knob == WK_KNOB_BATCH_LANES) {
-        if (value != 2 && value != 4 && value != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
+        if (value != 1 && value != 2 && value != 4 && value != 8)
+            return ctx->fail(WK_E_BADARG, "lanes must be 1, 2, 4 or 8");
         if (knob == WK_KNOB_LANES) {
             ctx->default_lanes = value;
             ctx->tuned_lanes.clear();
@@ -1424,8 +1425,8 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
             ctx->batch_lanes = value;
         }
     } else if (knob == WK_KNOB_SLICE_ROWS || knob == WK_KNOB_BATCH_SLICE_ROWS) {
-        if (value < wk::kMinSliceRows || value > (1 << 24))
-            return ctx->fail(WK_E_BADARG, "slice threshold must be in [8, 2^24]");
+        if (value < wk::kMinSliceRows || value > (1 << 23))
+            return ctx->fail(WK_E_BADARG, "slice threshold must be in [8, 2^23]");
         (knob == WK_KNOB_SLICE_ROWS ? ctx->slice_rows : ctx->batch_slice_rows) = (uint32_t)value;
     } else if (knob == WK_KNOB_FLAT_ROWS) {
         if (value < 0) return ctx->fail(WK_E_BADARG, "flat threshold must be >= 0");
@@ -1447,7 +1448,7 @@ extern "C" int wk_ctx_tune_set(wk_ctx* ctx, int32_t knob, int32_t value) {
 // Lanes of one (op, input columns) step of single queries (an autotuner's per-step choice).
 int wk::tune_step_lanes(wk_ctx* ctx, int op, int cols, int lanes) {
     std::lock_guard<std::mutex> lk(ctx->mu);
-    if (lanes != 2 && lanes != 4 && lanes != 8) return ctx->fail(WK_E_BADARG, "lanes must be 2, 4 or 8");
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return ctx->fail(WK_E_BADARG, "lanes must be 1, 2, 4 or 8");
     ctx->tuned_lanes[op * 1000 + cols] = lanes;
     ctx->drop_graphs();
     return WK_SUCCESS;

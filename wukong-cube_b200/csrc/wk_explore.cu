@@ -134,6 +134,126 @@ __device__ __forceinline__ TileBuf tile_buf(uint32_t* base, int wi) {
     return b;
 }
 
+// Setup of one row of a tile: its step (descriptor), probe key, home bucket and filter target,
+// and the flag op | valid << 8 | pending << 9 | cin << 16 | cout << 24; records the row's meta.
+__device__ __forceinline__ void row_setup(const ExploreArgs& a, const TileBuf& B, int row, int wi,
+                                          uint64_t* key_out, uint32_t* bkt_out, uint32_t* tgt_out,
+                                          uint32_t* flag_out) {
+    const StepDesc* d = step_desc(a, B.q[row]);
+    const uint32_t op = d->op;
+    bool valid = op != kXDone;
+    const SegDesc* sg = &d->seg;
+    uint32_t target = d->end_const;
+    uint64_t key = 0;
+    if (op == kXStart) {
+        key = d->start_key;
+    } else if (valid && (op == kXC2K || op == kXI2K)) {
+        // const_to_known / index_to_known: every row looks up the same list
+        key = d->start_key;
+        target = B.in[row * wi + d->ce];   // shared memory: plain loads
+    } else if (valid) {
+        const uint32_t* rin = B.in + row * wi;   // shared memory: plain loads
+        const uint32_t cur = rin[d->cs];
+        if (op == kXK2K) target = rin[d->ce];
+        if (op == kXK2U && d->type_index) {
+            // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+            key = make_key(0, cur, kIn);
+            sg = &a.seg_index[kIn];
+            if (cur >= (1u << kNbitsIdx)) valid = false;
+        } else {
+            key = make_key(cur, d->pid, d->dir);
+            if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+        }
+        if (cur == kBlankId) valid = false;
+    }
+    const bool pending = valid && sg->num_buckets != 0 && key != 0;
+    const uint32_t cin = d->cin, cout = d->cout;
+    *key_out = key;
+    *bkt_out = pending ? (uint32_t)bucket_of(key, *sg) : 0;   // 32 bits (stores are refused at 2^32)
+    *tgt_out = target;
+    *flag_out = op | (valid ? 0x100u : 0u) | (pending ? 0x200u : 0u) | (cin << 16) | (cout << 24);
+    B.meta[row] = op | (cin << 8) | (cout << 16);
+}
+
+// A row's count and list offset once its pointer word is known (filters test membership of the
+// target): written to B.cnt / B.off, bytes added to the accounting.
+__device__ __forceinline__ uint32_t row_count(const ExploreArgs& a, const TileBuf& B, int row, uint32_t flag,
+                                              uint64_t p, bool found, unsigned long long& acc_alg,
+                                              unsigned long long& acc_sd) {
+    const uint32_t op = flag & 0xFFu;
+    const bool filt = is_filter_op(op);
+    const uint64_t deg = ptr_size(p);
+    const uint32_t cnt = filt ? (found ? 1u : 0u) : (uint32_t)deg;
+    B.off[row] = ptr_off(p);
+    B.cnt[row] = cnt;
+    // byte accounting, kept in registers until the CTA leaves
+    acc_sd += deg;
+    acc_alg += ((flag >> 16) & 0xFF) * 4ull + 16 + deg * 4 + (unsigned long long)cnt * (flag >> 24) * 4;
+    return cnt;
+}
+
+// One thread per row (the L = 1 launch): each thread sets up its tile rows, loads every row's
+// home sector (slots 0 and 1, 32 bytes) before comparing any, and walks on from slot 2 only
+// where that sector does not settle the key; filters then search the list themselves.  No
+// ballots or shuffles.
+__device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const TileBuf& B, int n, int wi,
+                                                unsigned long long& acc_alg, unsigned long long& acc_sd) {
+    constexpr int kRows = kTileRows / kStepThreads;
+    uint64_t key[kRows];
+    uint32_t bkt[kRows], tgt[kRows], flag[kRows];
+#pragma unroll
+    for (int k = 0; k < kRows; ++k) {
+        const int row = threadIdx.x + k * kStepThreads;
+        key[k] = 0;
+        bkt[k] = 0;
+        tgt[k] = 0;
+        flag[k] = kXDone;
+        if (row < n) row_setup(a, B, row, wi, &key[k], &bkt[k], &tgt[k], &flag[k]);
+        if ((flag[k] & 0x200u) && bkt[k] >= a.store.n_buckets) {
+            atomicOr(&a.ctl->err, kErrCorrupt);
+            flag[k] &= ~0x200u;
+        }
+    }
+    ulonglong2 s0[kRows], s1[kRows];
+#pragma unroll
+    for (int k = 0; k < kRows; ++k) {
+        s0[k] = make_ulonglong2(0, 0);
+        s1[k] = make_ulonglong2(0, 0);
+        if (flag[k] & 0x200u) {
+            const Slot* b = a.store.slots + (uint64_t)bkt[k] * kAssoc;
+            s0[k] = load_slot(b);
+            s1[k] = load_slot(b + 1);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kRows; ++k) {
+        const int row = threadIdx.x + k * kStepThreads;
+        if (row >= n || !(flag[k] & 0x100u)) continue;
+        uint64_t p = 0;
+        if (flag[k] & 0x200u) {
+            if (s0[k].x == key[k]) p = s0[k].y;
+            else if (s0[k].x == 0) p = 0;   // first empty slot: absent (insert-only store)
+            else if (s1[k].x == key[k]) p = s1[k].y;
+            else if (s1[k].x != 0) p = thread_probe(a.store, key[k], bkt[k], &a.ctl->err, 2);
+        }
+        uint64_t off = ptr_off(p), deg = ptr_size(p);
+        if (off + deg > a.store.n_edges) {
+            if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
+            deg = 0;
+        }
+        const uint32_t op = flag[k] & 0xFFu;
+        if (op == kXI2K) {   // index_to_known reads its mt slice of the list
+            uint64_t lo, hi;
+            mt_slice(step_desc(a, B.q[row])->mt, deg, &lo, &hi);
+            off += lo;
+            deg = hi - lo;
+        }
+        const bool found = is_filter_op(op) && deg &&
+                           thread_member(a.store.edges, off, deg, tgt[k], a.sorted_lists != 0);
+        row_count(a, B, row, flag[k], make_ptr(deg, off), found, acc_alg, acc_sd);
+    }
+}
+
 // Front half of a tile: start the TMA copy of its rows, probe, count, scan, publish the tile's
 // aggregate.  Nothing here waits on another CTA.
 template <int L>
@@ -142,8 +262,8 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
                                            int wi, unsigned epoch, uint64_t* s_warp,
                                            unsigned long long& acc_alg, unsigned long long& acc_sd) {
     constexpr int kGroups = kStepThreads / L;
-    constexpr int kBatches = kTileRows / (kGroups * kUnroll);
-    static_assert(kBatches * kGroups * kUnroll == kTileRows, "tile shape");
+    constexpr int kBatches = L > 1 ? kTileRows / (kGroups * kUnroll) : 1;   // L = 1: tile_probe_rows
+    static_assert(L == 1 || kBatches * kGroups * kUnroll == kTileRows, "tile shape");
     const int grp = threadIdx.x / L;
     const int h = threadIdx.x & (L - 1);
     const int gbase = (threadIdx.x & 31) & ~(L - 1);
@@ -168,13 +288,15 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     __syncthreads();
     // the rows' copy ran alongside the owner loads; read the rows from shared memory
     if (wi) mbar_wait(bar, phase, &a.ctl->err);
+    if constexpr (L == 1) {
+        tile_probe_rows(a, B, n, wi, acc_alg, acc_sd);
+    } else {
     constexpr int kOwn = (kUnroll + L - 1) / L;   // rows of a batch each lane works out
 #pragma unroll 1
     for (int b = 0; b < kBatches; ++b) {
         // Row setup, split over the group's lanes: lane h works out the rows u = h, h + L, ...
-        // of the batch (descriptor, key, home bucket, filter target), then the group shares
-        // them by shuffles, so no row's hash or descriptor is worked out twice.
-        // flag: op | valid << 8 | pending << 9 | cin << 16 | cout << 24
+        // of the batch (row_setup), then the group shares them by shuffles, so no row's hash or
+        // descriptor is worked out twice.
         uint64_t mkey[kOwn];
         uint32_t mbkt[kOwn], mtgt[kOwn], mflag[kOwn];   // buckets in 32 bits (group_probe)
 #pragma unroll
@@ -185,42 +307,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
             mbkt[j] = 0;
             mtgt[j] = 0;
             mflag[j] = kXDone;
-            if (u < kUnroll && row < n) {
-                const StepDesc* d = step_desc(a, B.q[row]);
-                const uint32_t op = d->op;
-                bool valid = op != kXDone;
-                const SegDesc* sg = &d->seg;
-                uint32_t target = d->end_const;
-                uint64_t key = 0;
-                if (op == kXStart) {
-                    key = d->start_key;
-                } else if (valid && (op == kXC2K || op == kXI2K)) {
-                    // const_to_known / index_to_known: every row looks up the same list
-                    key = d->start_key;
-                    target = B.in[row * wi + d->ce];   // shared memory: plain loads
-                } else if (valid) {
-                    const uint32_t* rin = B.in + row * wi;   // shared memory: plain loads
-                    const uint32_t cur = rin[d->cs];
-                    if (op == kXK2K) target = rin[d->ce];
-                    if (op == kXK2U && d->type_index) {
-                        // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-                        key = make_key(0, cur, kIn);
-                        sg = &a.seg_index[kIn];
-                        if (cur >= (1u << kNbitsIdx)) valid = false;
-                    } else {
-                        key = make_key(cur, d->pid, d->dir);
-                        if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
-                    }
-                    if (cur == kBlankId) valid = false;
-                }
-                const bool pending = valid && sg->num_buckets != 0 && key != 0;
-                const uint32_t cin = d->cin, cout = d->cout;
-                mkey[j] = key;
-                mbkt[j] = pending ? (uint32_t)bucket_of(key, *sg) : 0;
-                mtgt[j] = target;
-                mflag[j] = op | (valid ? 0x100u : 0u) | (pending ? 0x200u : 0u) | (cin << 16) | (cout << 24);
-                B.meta[row] = op | (cin << 8) | (cout << 16);
-            }
+            if (u < kUnroll && row < n) row_setup(a, B, row, wi, &mkey[j], &mbkt[j], &mtgt[j], &mflag[j]);
         }
         uint64_t key[kUnroll], ptr[kUnroll];
         uint32_t bucket[kUnroll];
@@ -269,18 +356,9 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         if (h == 0) {
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
-                if (valid[u]) {
-                    const uint32_t op = flag[u] & 0xFFu;
-                    const bool filt = is_filter_op(op);
-                    const uint32_t cnt = filt ? (found[u] ? 1u : 0u) : (uint32_t)deg[u];
-                    B.off[row[u]] = off[u];
-                    B.cnt[row[u]] = cnt;
-                    // byte accounting, kept in registers until the CTA leaves
-                    acc_sd += deg[u];
-                    acc_alg += ((flag[u] >> 16) & 0xFF) * 4ull + 16 + deg[u] * 4 +
-                               (unsigned long long)cnt * (flag[u] >> 24) * 4;
-                }
+                if (valid[u]) row_count(a, B, row[u], flag[u], make_ptr(deg[u], off[u]), found[u], acc_alg, acc_sd);
         }
+    }
     }
     __syncthreads();
     WK_PH(2);
@@ -609,6 +687,7 @@ size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
 cudaError_t explore_kernel_attrs() {
     const int bytes = (int)explore_smem_bytes(32, 32, nullptr);
     cudaError_t e;
+    if ((e = set_attr<1>(bytes)) != cudaSuccess) return e;
     if ((e = set_attr<2>(bytes)) != cudaSuccess) return e;
     if ((e = set_attr<4>(bytes)) != cudaSuccess) return e;
     return set_attr<8>(bytes);
@@ -618,6 +697,7 @@ CtaUse explore_cta_use(int w_in, int w_out, int lanes) {
     CtaUse u{0, 0, kStepThreads};
     cudaFuncAttributes fa{};
     cudaError_t e = cudaErrorInvalidValue;
+    if (lanes == 1) e = cudaFuncGetAttributes(&fa, explore_kernel<1>);
     if (lanes == 2) e = cudaFuncGetAttributes(&fa, explore_kernel<2>);
     if (lanes == 4) e = cudaFuncGetAttributes(&fa, explore_kernel<4>);
     if (lanes == 8) e = cudaFuncGetAttributes(&fa, explore_kernel<8>);
@@ -658,6 +738,7 @@ int explore_blocks_per_sm(int w_in, int w_out, int lanes) {
     size_t smem = explore_smem_bytes(w_in, w_out, nullptr);
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
+    if (lanes == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<1>, kStepThreads, smem);
     if (lanes == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<2>, kStepThreads, smem);
     if (lanes == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<4>, kStepThreads, smem);
     if (lanes == 8) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<8>, kStepThreads, smem);
@@ -670,6 +751,7 @@ cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s) {
     size_t smem = explore_smem_bytes(wi, a.w_out, &chunk);
     if (grid < 1) grid = 1;
     switch (a.lanes) {
+    case 1: explore_kernel<1><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
     case 2: explore_kernel<2><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
     case 8: explore_kernel<8><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
     default: explore_kernel<4><<<grid, kStepThreads, smem, s>>>(a, chunk); break;

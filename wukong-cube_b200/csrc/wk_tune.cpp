@@ -2,8 +2,8 @@
 // workload.  No counterpart in the reference (its kernels have one fixed launch shape,
 // gpu_hash.cu:96-326).
 //
-// Knobs (wk_ctx_tune_set): lanes per probe group (2 / 4 / 8 lanes, i.e. 32 / 64 / 128 bytes
-// of a bucket staged per request) and the slice threshold (lists longer than it are written
+// Knobs (wk_ctx_tune_set): lanes per probe group (1 / 2 / 4 / 8 lanes: one thread per row
+// reading the home sector, or a group reading 32 / 64 / 128 bytes of a bucket per request) and the slice threshold (lists longer than it are written
 // block-per-row as slices by every CTA, shorter ones group-per-row by the CTA that probed them),
 // and for batches the mask of levels that run as the flat passes instead of the tile launch
 // (chosen greedily level by level after the tile settings).
@@ -23,7 +23,7 @@
 
 namespace {
 
-constexpr int kLanes[] = {2, 4, 8};
+constexpr int kLanes[] = {1, 2, 4, 8};
 constexpr int kSlices[] = {8, 16, 32, 128, 512};
 
 struct Events {
@@ -187,7 +187,7 @@ extern "C" int wk_ctx_autotune(wk_ctx* ctx, const wk_query* queries, uint32_t n,
         double total = 0;
         if ((rc = time_singles(ctx, heavy, iters, nullptr, &total))) return rc;
         out->single_ms_default = total;
-        // lanes: per (op, columns) step, the fastest of the three
+        // lanes: per (op, columns) step, the fastest of the four
         std::map<int, std::map<int, double>> by_lanes;   // step key -> lanes -> ms
         std::map<int, double> sum_by_lanes;
         for (int l : kLanes) {
