@@ -146,13 +146,18 @@ __device__ __forceinline__ uint64_t count_key(const FlatArgs& a, const StepDesc&
 
 // Pointer word of `key` given its home bucket's slot 0 (already loaded): slot 1 shares slot 0's
 // 32-byte sector, so its load hits L1; the rest walk on from slot 2.
-__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0) {
+__device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key, uint64_t b, ulonglong2 s0,
+                                                unsigned* err) {
     if (s0.x == key) return s0.y;
     if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
-    const ulonglong2 s1 = load_slot(a.store.slots + b * kAssoc + 1);
+    const ulonglong2 s1 = load_slot(st.slots + b * kAssoc + 1);
     if (s1.x == key) return s1.y;
     if (s1.x == 0) return 0;
-    return thread_probe(a.store, key, b, &a.ctl->err, 2);
+    return thread_probe(st, key, b, err, 2);
+}
+
+__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0) {
+    return settle_slot(a.store, key, b, s0, &a.ctl->err);
 }
 
 // kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
@@ -402,67 +407,99 @@ __device__ void flat_level_scan_parts(const FlatLevelArgs& a, uint32_t nparts, u
     }
 }
 
-__global__ void __launch_bounds__(kFlatThreads) flat_level_count_kernel(const FlatLevelArgs a) {
+// kRowsPerThread rows per thread at a time, their home slots loaded before any is compared (as
+// in flat_count_kernel).
+__global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_kernel(const FlatLevelArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
     const uint64_t R = level_rows(a);
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
     uint64_t sum = 0, sd = 0, alg = 0;
-    for (uint64_t r = lo + threadIdx.x; r < hi; r += kFlatThreads) {
-        const StepDesc* d = a.desc + level_owner(a, r);
-        const uint32_t op = d->op;
-        uint64_t key = 0;
-        const SegDesc* sg = &d->seg;
-        bool valid = op != kXDone;
-        uint32_t target = d->end_const, cin = 0;
-        if (valid && op == kXStart) {
-            key = d->start_key;
-        } else if (valid && (op == kXC2K || op == kXI2K)) {   // one list for every row
-            cin = d->cin;
-            key = d->start_key;
-            target = __ldg(a.in + r * (uint64_t)a.w_in + d->ce);
-        } else if (valid) {
-            cin = d->cin;
-            const uint32_t* row = a.in + r * (uint64_t)a.w_in;
-            const uint32_t cur = __ldg(row + d->cs);
-            if (op == kXK2K) target = __ldg(row + d->ce);
-            if (cur == kBlankId) valid = false;
-            if (op == kXK2U && d->type_index) {
-                // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
-                key = make_key(0, cur, kIn);
-                sg = &a.seg_index[kIn];
-                if (cur >= (1u << kNbitsIdx)) valid = false;
-            } else {
-                key = make_key(cur, d->pid, d->dir);
-                if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+    constexpr int K = kRowsPerThread;
+    constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
+    for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
+        uint64_t key[K], bkt[K];
+        uint32_t target[K];
+        bool valid[K], look[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
+            key[k] = 0;
+            bkt[k] = 0;
+            target[k] = 0;
+            valid[k] = look[k] = false;
+            if (r >= hi) continue;
+            const StepDesc* d = a.desc + level_owner(a, r);
+            const uint32_t op = d->op;
+            const SegDesc* sg = &d->seg;
+            bool v = op != kXDone;
+            target[k] = d->end_const;
+            if (v && op == kXStart) {
+                key[k] = d->start_key;
+            } else if (v && (op == kXC2K || op == kXI2K)) {   // one list for every row
+                key[k] = d->start_key;
+                target[k] = __ldg(a.in + r * (uint64_t)a.w_in + d->ce);
+            } else if (v) {
+                const uint32_t* row = a.in + r * (uint64_t)a.w_in;
+                const uint32_t cur = __ldg(row + d->cs);
+                if (op == kXK2K) target[k] = __ldg(row + d->ce);
+                if (cur == kBlankId) v = false;
+                if (op == kXK2U && d->type_index) {
+                    // get_index(cur, IN) (sparql.hpp:342-345); only 17-bit ids can be keys
+                    key[k] = make_key(0, cur, kIn);
+                    sg = &a.seg_index[kIn];
+                    if (cur >= (1u << kNbitsIdx)) v = false;
+                } else {
+                    key[k] = make_key(cur, d->pid, d->dir);
+                    if (cur == 0) sg = &a.seg_index[d->dir & 1];   // vid 0 names the index
+                }
+            }
+            valid[k] = v;
+            look[k] = v && sg->num_buckets != 0 && key[k] != 0;
+            if (look[k]) bkt[k] = bucket_of(key[k], *sg);
+            if (look[k] && bkt[k] >= a.store.n_buckets) {
+                atomicOr(&a.ctl->err, kErrCorrupt);
+                look[k] = false;
             }
         }
-        uint64_t off = 0, deg = 0;
-        if (valid && sg->num_buckets != 0 && key != 0) {
-            const uint64_t p = thread_probe(a.store, key, bucket_of(key, *sg), &a.ctl->err);
-            off = ptr_off(p);
-            deg = ptr_size(p);
-            if (off + deg > a.store.n_edges) {
-                if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
-                deg = 0;
+        ulonglong2 s0[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
+            if (r >= hi) continue;
+            const StepDesc* d = a.desc + level_owner(a, r);
+            const uint32_t op = d->op;
+            uint64_t off = 0, deg = 0;
+            if (look[k]) {
+                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], &a.ctl->err);
+                off = ptr_off(p);
+                deg = ptr_size(p);
+                if (off + deg > a.store.n_edges) {
+                    if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
+                    deg = 0;
+                }
+                if (op == kXI2K) {
+                    uint64_t s_lo, s_hi;
+                    mt_slice(d->mt, deg, &s_lo, &s_hi);
+                    off += s_lo;
+                    deg = s_hi - s_lo;
+                }
             }
-            if (op == kXI2K) {
-                uint64_t lo, hi;
-                mt_slice(d->mt, deg, &lo, &hi);
-                off += lo;
-                deg = hi - lo;
+            const bool filt = is_filter_op(op);
+            uint32_t c = (uint32_t)deg;
+            if (filt) c = (valid[k] && deg && thread_member(a.store.edges, off, deg, target[k], a.sorted_lists != 0)) ? 1u : 0u;
+            if (!valid[k]) c = 0;
+            a.pos[r] = c;   // the count; flat_level_place_kernel turns it into the row's position
+            a.off[r] = off;
+            sum += c;
+            if (valid[k]) {
+                const uint32_t cin = op == kXStart ? 0u : d->cin;
+                sd += deg;
+                alg += cin * 4ull + 16 + deg * 4 + (uint64_t)c * d->cout * 4;
             }
-        }
-        const bool filt = is_filter_op(op);
-        uint32_t c = (uint32_t)deg;
-        if (filt) c = (valid && deg && thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0)) ? 1u : 0u;
-        if (!valid) c = 0;
-        a.pos[r] = c;   // the count; flat_level_place_kernel turns it into the row's position
-        a.off[r] = off;
-        sum += c;
-        if (valid) {
-            sd += deg;
-            alg += cin * 4ull + 16 + deg * 4 + (uint64_t)c * d->cout * 4;
         }
     }
     sum = block_sum(sum, s_warp);
