@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_place_kernel(const FlatArgs
     }
 }
 
-__global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArgs a, uint32_t nparts) {
+__global__ void __launch_bounds__(kFlatThreads, 8) flat_expand_kernel(const FlatArgs a, uint32_t nparts) {
     __shared__ uint64_t s_pos[kWindow + 1];
     __shared__ uint64_t s_off[kWindow];
     __shared__ uint64_t s_i0;
@@ -333,27 +333,65 @@ __global__ void __launch_bounds__(kFlatThreads) flat_expand_kernel(const FlatArg
         if (threadIdx.x == 0) s_i0 = lo;
     }
     __syncthreads();
-    const int wo = a.w_out, cin = a.w_in, ecol = a.step.cin;
+    const int wo = a.w_out, ecol = a.step.cin;
     uint64_t i = s_i0;
     uint64_t j = j0;
+    // the window's positions and offsets are loaded into registers one window ahead (a thread
+    // holds entries t = threadIdx.x and, for the end position, t = kWindow)
+    static_assert(kWindow == kFlatThreads, "one window entry per thread");
+    uint64_t nx_pos = 0, nx_off = 0, nx_end = 0;
+    {
+        const uint64_t n = min((uint64_t)kWindow, R - i);
+        if (threadIdx.x < n) {
+            nx_pos = a.pos[i + threadIdx.x];
+            nx_off = a.off[i + threadIdx.x];
+        }
+        if (threadIdx.x == 0) nx_end = a.pos[i + n];
+    }
+    constexpr int U = 4;   // output rows per thread with their neighbour loads in flight
     while (j < j1 && i < R) {
         const uint64_t n = min((uint64_t)kWindow, R - i);
-        for (int t = threadIdx.x; t <= (int)n; t += kFlatThreads) s_pos[t] = a.pos[i + t];
-        for (int t = threadIdx.x; t < (int)n; t += kFlatThreads) s_off[t] = a.off[i + t];
+        if (threadIdx.x < n) {
+            s_pos[threadIdx.x] = nx_pos;
+            s_off[threadIdx.x] = nx_off;
+        }
+        if (threadIdx.x == 0) s_pos[n] = nx_end;
         __syncthreads();
-        const uint64_t wend = min(j1, s_pos[n]);
-        for (uint64_t jj = j + threadIdx.x; jj < wend; jj += kFlatThreads) {
-            int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+        const uint64_t i2 = i + n;
+        if (i2 < R) {   // the next window's entries, while this one is written
+            const uint64_t n2 = min((uint64_t)kWindow, R - i2);
+            if (threadIdx.x < n2) {
+                nx_pos = a.pos[i2 + threadIdx.x];
+                nx_off = a.off[i2 + threadIdx.x];
             }
-            const uint64_t r = i + lo;
-            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
-            uint32_t* dst = a.out + jj * (uint64_t)wo;
-            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
-            dst[ecol] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
-            (void)cin;
+            if (threadIdx.x == 0) nx_end = a.pos[i2 + n2];
+        }
+        const uint64_t wend = min(j1, s_pos[n]);
+        for (uint64_t jb = j + threadIdx.x; jb < wend; jb += (uint64_t)U * kFlatThreads) {
+            int row[U];
+            uint32_t nb[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t jj = jb + (uint64_t)u * kFlatThreads;
+                row[u] = -1;
+                if (jj >= wend) continue;
+                int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+                }
+                row[u] = lo;
+                nb[u] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (row[u] < 0) continue;
+                const uint64_t jj = jb + (uint64_t)u * kFlatThreads;
+                const uint32_t* src = a.in + (i + row[u]) * (uint64_t)a.w_in;
+                uint32_t* dst = a.out + jj * (uint64_t)wo;
+                for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
+                dst[ecol] = nb[u];
+            }
         }
         j = max(j, wend);
         i += n;
