@@ -75,3 +75,30 @@ def test_empty_and_refused_builds():
         with pytest.raises(wk.WukongError) as e:
             ctx.build_store(np.zeros((4, 3), np.uint32), load_factor=2.0)
         assert e.value.code == wk.E_BADARG
+
+
+@pytest.mark.parametrize("load", [0.0, 1.0])
+def test_upload_then_export_gives_the_uploaded_bytes(load):
+    """The device copy keeps single-entry lists of keys alone in their bucket in the empty slot
+    1 of that bucket (an in-bucket copy the probes read instead of the edge array); the export
+    still gives back exactly the bytes that were uploaded, and queries still answer as the
+    oracle does, through the one-thread-per-row probe and the flat passes that use the copy."""
+    tr, v = wk.synth_generate(12, seed=7)
+    g, hs, he, hg = _host_arrays(tr, load, False)
+    o = oracle.OracleStore(tr)
+    with wk.Context(0) as ctx:
+        ctx.upload_gstore(g)
+        ds, de, dg = ctx.export_store()
+        assert dg == hg and np.array_equal(de, he) and np.array_equal(ds, hs)
+        inst = {t: g.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+        qs = workloads.light_queries(v, inst, 300, seed=9)
+        heavy = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+        for lanes, flat_rows in ((1, 0), (1, 1), (2, 1)):
+            ctx.tune_set(wk.KNOB_LANES, lanes)
+            ctx.tune_set(wk.KNOB_BATCH_LANES, lanes)
+            ctx.tune_set(wk.KNOB_FLAT_ROWS, flat_rows)
+            ctx.tune_set(wk.KNOB_BATCH_FLAT, 63 if flat_rows else 0)
+            for q, (t, st) in zip(qs + heavy, ctx.batch(qs) + [ctx.execute(h, wk.MODE_RESIDENT) for h in heavy]):
+                ost, want, _ = o.run(q.flat(), q.nvars)
+                assert ost == 0 and np.array_equal(oracle.sorted_rows(t), oracle.sorted_rows(want))
+    g.close()

@@ -760,6 +760,8 @@ int wk::store_adopt(wk_ctx* ctx, Slot* d_slots, uint64_t n_slots, uint32_t* d_ed
         }
         ctx->sorted_lists = (flag & 1u) ? 0 : 1;
     }
+    WK_CUDA(ctx, wk::launch_inline(ctx->dev_store(), ctx->stream));
+    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->drop_graphs();
     return WK_SUCCESS;
 }
@@ -779,8 +781,15 @@ extern "C" int wk_store_export(wk_ctx* ctx, void* slots, uint64_t slots_cap, uin
         (segs && segs_cap < ctx->segs.size()))
         return ctx->fail(WK_E_CAPACITY, "export buffers too small");
     WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (slots && ctx->n_slots)
+    if (slots && ctx->n_slots) {
         WK_CUDA(ctx, cudaMemcpy(slots, ctx->d_slots, ctx->n_slots * sizeof(wk::Slot), cudaMemcpyDeviceToHost));
+        // the pointer words of empty slots hold the device copy's in-bucket entries; the
+        // store's own layout has them zero
+        wk::Slot* h = static_cast<wk::Slot*>(slots);
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < (int64_t)ctx->n_slots; ++i)
+            if (h[i].key == 0) h[i].ptr = 0;
+    }
     if (edges && ctx->n_edges)
         WK_CUDA(ctx, cudaMemcpy(edges, ctx->d_edges, ctx->n_edges * 4, cudaMemcpyDeviceToHost));
     if (segs && !ctx->segs.empty()) std::memcpy(segs, ctx->segs.data(), ctx->segs.size() * sizeof(wk_seg_meta));

@@ -87,6 +87,28 @@ __device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
     return s.bucket_start + mod_barrett(hash_u64(key), s.num_buckets, s.magic);
 }
 
+// ---------------------------------------------------------------- single-entry lists
+// A list of one entry whose key is alone in its bucket is kept in the bucket too: the key sits
+// in slot 0, slot 1 is empty, and the device copy of the store holds the entry in slot 1's
+// pointer word, tagged with kInlineTag (inline_kernel, run at upload).  Slot 1's key word stays
+// 0, so every probe still sees an empty slot there (the reference's own probe reads key words
+// only), and the edge array is unchanged: a reader that ignores the tag still reads the list
+// from the edge array.  The readers that use it take the entry from the sector the probe already
+// loaded instead of a second random read.  Within a step, a list offset with kInlineTag set
+// carries that entry in its low 32 bits instead of an edge-array offset (list_at).
+constexpr uint64_t kInlineTag = 1ull << 63;
+
+// The tagged entry of the key found in slot 0 (pointer word p0) given slot 1 (key k1, pointer
+// word p1) of the same bucket; 0 when its list is not kept in the bucket.
+__device__ __forceinline__ uint64_t inline_entry(uint64_t p0, uint64_t k1, uint64_t p1) {
+    return (k1 == 0 && ptr_size(p0) == 1 && (p1 & kInlineTag)) ? p1 : 0;
+}
+
+// Entry k of the list at `off` (an edge-array offset, or a tagged single entry).
+__device__ __forceinline__ uint32_t list_at(const uint32_t* edges, uint64_t off, uint64_t k) {
+    return (off & kInlineTag) ? (uint32_t)off : __ldg(edges + off + k);
+}
+
 // Probe kUnroll keys per group of L lanes.  Every lane of the warp must call this (ballots and
 // shuffles are warp-wide).  On entry bucket[u] is the key's home bucket and pending[u] says
 // whether to look; on return ptr[u] is the slot's pointer word in every lane of the group, or 0
@@ -96,7 +118,8 @@ __device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
 template <int L, class BucketT>
 __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&key)[kUnroll],
                                             BucketT (&bucket)[kUnroll], bool (&pending)[kUnroll],
-                                            uint64_t (&ptr)[kUnroll], unsigned* err) {
+                                            uint64_t (&ptr)[kUnroll], unsigned* err,
+                                            uint64_t (*inl)[kUnroll] = nullptr) {
     const int lane = threadIdx.x & 31;
     const int h = lane & (L - 1);
     const int gbase = lane & ~(L - 1);
@@ -106,6 +129,7 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
     for (int u = 0; u < kUnroll; ++u) {
         ptr[u] = 0;
         round[u] = 0;
+        if (inl) (*inl)[u] = 0;
     }
     for (int it = 0;; ++it) {
         bool any = false;
@@ -139,9 +163,13 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
             const int src = hm ? gbase + __ffs(hm) - 1 : gbase + L - 1;
             const uint64_t kx = __shfl_sync(kFull, s[u].x, src);
             const uint64_t py = __shfl_sync(kFull, s[u].y, src);
+            // the home bucket's slot 1 (lane 1 of the group in the first round): a key found in
+            // slot 0 may have its single entry there
+            const uint64_t y1 = inl ? __shfl_sync(kFull, s[u].y, gbase + 1) : 0;
             if (pending[u]) {
                 if (hm) {
                     ptr[u] = py;
+                    if (inl && round[u] == 0 && hm == 1u && ((em >> 1) & 1u)) (*inl)[u] = inline_entry(py, 0, y1);
                     pending[u] = false;
                 } else if (em) {
                     pending[u] = false;           // first empty slot: the key is absent
@@ -194,9 +222,11 @@ __device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t ke
     return 0;
 }
 
-// Is `target` in the list edges[off, off + deg)?  Binary search when lists are sorted.
+// Is `target` in the list edges[off, off + deg)?  Binary search when lists are sorted.  `off`
+// may be a tagged single entry.
 __device__ __forceinline__ bool thread_member(const uint32_t* edges, uint64_t off, uint64_t deg,
                                               uint32_t target, bool sorted) {
+    if (off & kInlineTag) return deg == 1 && (uint32_t)off == target;
     const uint32_t* p = edges + off;
     if (sorted) {
         uint64_t lo = 0, hi = deg;
@@ -383,7 +413,7 @@ __device__ __forceinline__ void group_member(const uint32_t* edges, const uint64
 #pragma unroll
         for (int j = 0; j < per; ++j) {
             const uint64_t k = (uint64_t)j * L + h;
-            v[u][j] = (valid[u] && k < deg[u]) ? __ldg(edges + off[u] + k) : ~target[u];
+            v[u][j] = (valid[u] && k < deg[u]) ? list_at(edges, off[u], k) : ~target[u];
         }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {

@@ -175,16 +175,16 @@ __device__ __forceinline__ void row_setup(const ExploreArgs& a, const TileBuf& B
     B.meta[row] = op | (cin << 8) | (cout << 16);
 }
 
-// A row's count and list offset once its pointer word is known (filters test membership of the
-// target): written to B.cnt / B.off, bytes added to the accounting.
+// A row's count and list offset (an edge-array offset or a tagged single entry) once its list
+// is known (filters test membership of the target): written to B.cnt / B.off, bytes added to
+// the accounting.
 __device__ __forceinline__ uint32_t row_count(const ExploreArgs& a, const TileBuf& B, int row, uint32_t flag,
-                                              uint64_t p, bool found, unsigned long long& acc_alg,
+                                              uint64_t off, uint64_t deg, bool found, unsigned long long& acc_alg,
                                               unsigned long long& acc_sd) {
     const uint32_t op = flag & 0xFFu;
     const bool filt = is_filter_op(op);
-    const uint64_t deg = ptr_size(p);
     const uint32_t cnt = filt ? (found ? 1u : 0u) : (uint32_t)deg;
-    B.off[row] = ptr_off(p);
+    B.off[row] = off;
     B.cnt[row] = cnt;
     // byte accounting, kept in registers until the CTA leaves
     acc_sd += deg;
@@ -229,12 +229,18 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
     for (int k = 0; k < kRows; ++k) {
         const int row = threadIdx.x + k * kStepThreads;
         if (row >= n || !(flag[k] & 0x100u)) continue;
-        uint64_t p = 0;
+        uint64_t p = 0, inl = 0;
         if (flag[k] & 0x200u) {
-            if (s0[k].x == key[k]) p = s0[k].y;
-            else if (s0[k].x == 0) p = 0;   // first empty slot: absent (insert-only store)
-            else if (s1[k].x == key[k]) p = s1[k].y;
-            else if (s1[k].x != 0) p = thread_probe(a.store, key[k], bkt[k], &a.ctl->err, 2);
+            if (s0[k].x == key[k]) {
+                p = s0[k].y;
+                inl = inline_entry(p, s1[k].x, s1[k].y);
+            } else if (s0[k].x == 0) {
+                p = 0;   // first empty slot: absent (insert-only store)
+            } else if (s1[k].x == key[k]) {
+                p = s1[k].y;
+            } else if (s1[k].x != 0) {
+                p = thread_probe(a.store, key[k], bkt[k], &a.ctl->err, 2);
+            }
         }
         uint64_t off = ptr_off(p), deg = ptr_size(p);
         if (off + deg > a.store.n_edges) {
@@ -247,10 +253,12 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
             mt_slice(step_desc(a, B.q[row])->mt, deg, &lo, &hi);
             off += lo;
             deg = hi - lo;
+        } else if (deg == 1 && inl) {
+            off = inl;   // the entry was in the bucket's sector
         }
         const bool found = is_filter_op(op) && deg &&
                            thread_member(a.store.edges, off, deg, tgt[k], a.sorted_lists != 0);
-        row_count(a, B, row, flag[k], make_ptr(deg, off), found, acc_alg, acc_sd);
+        row_count(a, B, row, flag[k], off, deg, found, acc_alg, acc_sd);
     }
 }
 
@@ -356,7 +364,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         if (h == 0) {
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
-                if (valid[u]) row_count(a, B, row[u], flag[u], make_ptr(deg[u], off[u]), found[u], acc_alg, acc_sd);
+                if (valid[u]) row_count(a, B, row[u], flag[u], off[u], deg[u], found[u], acc_alg, acc_sd);
         }
     }
     }
@@ -479,7 +487,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
                 int c = 0;
                 if (opv != kXStart)
                     for (; c < cin; ++c) dst[c] = sr[c];
-                if (opv == kXStart || opv == kXK2U) dst[c++] = __ldg(a.store.edges + B.off[lo] + k);
+                if (opv == kXStart || opv == kXK2U) dst[c++] = list_at(a.store.edges, B.off[lo], k);
                 // columns past the query's own width are never read (later levels and the
                 // result gather use only the query's columns), so they are left as they are
                 const uint64_t pos = excl + B.pre[lo] + k;

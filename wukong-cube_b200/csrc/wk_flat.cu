@@ -144,20 +144,25 @@ __device__ __forceinline__ uint64_t count_key(const FlatArgs& a, const StepDesc&
     return key;
 }
 
-// Pointer word of `key` given its home bucket's slot 0 (already loaded): slot 1 shares slot 0's
-// 32-byte sector, so its load hits L1; the rest walk on from slot 2.
+// Pointer word of `key` given its home bucket's slots 0 and 1 (one 32-byte sector, already
+// loaded); the walk goes on from slot 2 only when they do not settle the key.  *inl receives the
+// key's tagged single entry when the bucket holds it (kInlineTag), else 0.
 __device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key, uint64_t b, ulonglong2 s0,
-                                                unsigned* err) {
-    if (s0.x == key) return s0.y;
+                                                ulonglong2 s1, unsigned* err, uint64_t* inl) {
+    *inl = 0;
+    if (s0.x == key) {
+        *inl = inline_entry(s0.y, s1.x, s1.y);
+        return s0.y;
+    }
     if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
-    const ulonglong2 s1 = load_slot(st.slots + b * kAssoc + 1);
     if (s1.x == key) return s1.y;
     if (s1.x == 0) return 0;
     return thread_probe(st, key, b, err, 2);
 }
 
-__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0) {
-    return settle_slot(a.store, key, b, s0, &a.ctl->err);
+__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0,
+                                           ulonglong2 s1, uint64_t* inl) {
+    return settle_slot(a.store, key, b, s0, s1, &a.ctl->err, inl);
 }
 
 // kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
@@ -166,7 +171,7 @@ __device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint
 // Registers are capped for kCountCtas CTAs per SM.  kFilter: the membership steps
 // (known_to_known, known_to_const, const_to_known, index_to_known); the other instance (starts
 // and known_to_unknown) carries no membership search.
-constexpr int kRowsPerThread = 4;
+constexpr int kRowsPerThread = 3;
 constexpr int kCountCtas = 4;
 
 template <bool kFilter>
@@ -185,9 +190,9 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
     constexpr int K = kRowsPerThread;
     constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
     for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
-        uint64_t key[K], bkt[K], p[K];
+        uint64_t key[K], bkt[K], p[K], inl[K];
         bool valid[K], look[K];
-        ulonglong2 s0[K];
+        ulonglong2 s0[K], s1[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
@@ -196,10 +201,18 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
             if (r >= hi) valid[k] = look[k] = false;
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+        for (int k = 0; k < K; ++k) {
+            s0[k] = s1[k] = make_ulonglong2(0, 0);
+            if (look[k]) {   // slots 0 and 1: one 32-byte sector
+                s0[k] = load_slot(a.store.slots + bkt[k] * kAssoc);
+                s1[k] = load_slot(a.store.slots + bkt[k] * kAssoc + 1);
+            }
+        }
 #pragma unroll
-        for (int k = 0; k < K; ++k) p[k] = look[k] ? settle(a, key[k], bkt[k], s0[k]) : 0;
+        for (int k = 0; k < K; ++k) {
+            inl[k] = 0;
+            p[k] = look[k] ? settle(a, key[k], bkt[k], s0[k], s1[k], &inl[k]) : 0;
+        }
         // counts and list offsets
         uint32_t c[K];
 #pragma unroll
@@ -215,6 +228,8 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
                 mt_slice(d.mt, deg, &s_lo, &s_hi);
                 off += s_lo;
                 deg = s_hi - s_lo;
+            } else if (deg == 1 && inl[k]) {
+                off = inl[k];   // the entry was in the bucket's sector
             }
             c[k] = (uint32_t)deg;
             if (kFilter && valid[k] && deg) {
@@ -242,7 +257,7 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
             // neighbour words are all loaded before any row is written.
             uint32_t nb[K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) nb[k] = c[k] == 1 ? __ldg(a.store.edges + p[k]) : 0;
+            for (int k = 0; k < K; ++k) nb[k] = c[k] == 1 ? list_at(a.store.edges, p[k], 0) : 0;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 if (c[k] != 1) continue;
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(kFlatThreads, 8) flat_expand_kernel(const Flat
                     if (s_pos[mid] <= jj) lo = mid; else hi = mid;
                 }
                 row[u] = lo;
-                nb[u] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
+                nb[u] = list_at(a.store.edges, s_off[lo], jj - s_pos[lo]);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -500,10 +515,15 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
                 look[k] = false;
             }
         }
-        ulonglong2 s0[K];
+        ulonglong2 s0[K], s1[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+        for (int k = 0; k < K; ++k) {
+            s0[k] = s1[k] = make_ulonglong2(0, 0);
+            if (look[k]) {   // slots 0 and 1: one 32-byte sector
+                s0[k] = load_slot(a.store.slots + bkt[k] * kAssoc);
+                s1[k] = load_slot(a.store.slots + bkt[k] * kAssoc + 1);
+            }
+        }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
@@ -512,7 +532,8 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
             const uint32_t op = d->op;
             uint64_t off = 0, deg = 0;
             if (look[k]) {
-                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], &a.ctl->err);
+                uint64_t inl = 0;
+                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err, &inl);
                 off = ptr_off(p);
                 deg = ptr_size(p);
                 if (off + deg > a.store.n_edges) {
@@ -524,6 +545,8 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
                     mt_slice(d->mt, deg, &s_lo, &s_hi);
                     off += s_lo;
                     deg = s_hi - s_lo;
+                } else if (deg == 1 && inl) {
+                    off = inl;   // the entry was in the bucket's sector
                 }
             }
             const bool filt = is_filter_op(op);
@@ -650,7 +673,7 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
             const uint32_t* src = a.in + r * (uint64_t)a.w_in;
             uint32_t* dst = a.out + jj * (uint64_t)wo;
             for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
-            dst[ecol] = __ldg(a.store.edges + s_off[lo] + (jj - s_pos[lo]));
+            dst[ecol] = list_at(a.store.edges, s_off[lo], jj - s_pos[lo]);
             a.owner_out[jj] = s_q[lo];
         }
         j = max(j, wend);

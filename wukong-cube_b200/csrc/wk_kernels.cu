@@ -83,6 +83,20 @@ __global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const u
     }
 }
 
+// The single-entry lists of keys alone in their bucket, copied into the bucket (slot 1's
+// pointer word, tagged; see kInlineTag).  Slot 1's pointer word is cleared where no entry goes
+// there, so a store adopted twice carries no stale entry.
+__global__ void inline_kernel(Slot* slots, uint64_t n_buckets, const uint32_t* edges, uint64_t n_edges) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < n_buckets; b += stride) {
+        Slot* bk = slots + b * kAssoc;
+        const uint64_t k0 = bk[0].key, p0 = bk[0].ptr, k1 = bk[1].key;
+        if (k1 != 0) continue;
+        const uint64_t off = ptr_off(p0);
+        bk[1].ptr = (k0 != 0 && ptr_size(p0) == 1 && off < n_edges) ? (kInlineTag | __ldg(edges + off)) : 0;
+    }
+}
+
 // Random-read calibration: every thread makes `per` independent 16-byte reads at pseudo-random
 // 16-byte-aligned positions of buf (the splitmix64 finaliser of thread and read index), eight in
 // flight at a time.  With buf much larger than L2 each read costs one 32-byte DRAM sector, the
@@ -121,6 +135,12 @@ cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s) {
 
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s) {
     sorted_check_kernel<<<4096, 256, 0, s>>>(st.slots, st.n_buckets * kAssoc, st.edges, st.n_edges, d_flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inline(const DevStore& st, cudaStream_t s) {
+    if (st.n_buckets)
+        inline_kernel<<<4096, 256, 0, s>>>(const_cast<Slot*>(st.slots), st.n_buckets, st.edges, st.n_edges);
     return cudaGetLastError();
 }
 

@@ -61,6 +61,9 @@ constexpr int kTileRows = 256;
 
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);
+// Copies single-entry lists of keys alone in their bucket into the bucket (kInlineTag); writes
+// the slot array.
+cudaError_t launch_inline(const DevStore& st, cudaStream_t s);
 // `grid` CTAs of 256 threads, `per` random 16-byte reads each from a `bytes`-byte buffer.
 cudaError_t launch_random_reads(const void* buf, uint64_t bytes, int per, uint64_t seed,
                                 uint32_t* sink, int grid, cudaStream_t s);
