@@ -89,9 +89,42 @@ __device__ __forceinline__ const StepDesc* step_desc(const ExploreArgs& a, uint3
     return st < a.desc_stride ? a.desc + (size_t)q * a.desc_stride + st : &c_done;
 }
 
+// How a launch's rows are cut into tiles: kTileRows-row tiles, then (when the status array has
+// room for them) the last rows in kTailTileRows-row tiles, at most kTailRowsPerCta rows per CTA
+// of the grid.  Tiles are claimed in order, so the small ones come last: they shorten the wait
+// of CTAs that run out of tiles for the last ones to finish.
+constexpr int kTailTileRows = 64;
+constexpr int kTailRowsPerCta = 128;
+struct Tiling {
+    uint64_t ntiles, nbig, big_rows;
+    __device__ __forceinline__ uint64_t r0(uint64_t t) const {
+        return t < nbig ? t * kTileRows : big_rows + (t - nbig) * kTailTileRows;
+    }
+    __device__ __forceinline__ int rows(uint64_t t, uint64_t R) const {
+        return (int)min((uint64_t)(t < nbig ? kTileRows : kTailTileRows), R - r0(t));
+    }
+};
+
+__device__ __forceinline__ Tiling make_tiling(uint64_t R, uint64_t cap_tiles) {
+    Tiling T;
+    T.nbig = (R + kTileRows - 1) / kTileRows;
+    T.big_rows = T.nbig * kTileRows;
+    T.ntiles = T.nbig;
+    const uint64_t tail = min(R, (uint64_t)kTailRowsPerCta * gridDim.x);
+    const uint64_t big = (R - tail) / kTileRows;   // whole big tiles before the tail
+    const uint64_t nt = big + (R - big * kTileRows + kTailTileRows - 1) / kTailTileRows;
+    if (nt <= cap_tiles) {
+        T.nbig = big;
+        T.big_rows = big * kTileRows;
+        T.ntiles = nt;
+    }
+    return T;
+}
+
 // Per-tile state kept in shared memory while the tile is between its front and back halves.
 struct TileState {
     unsigned long long tile;
+    unsigned long long r0;       // its first row
     unsigned long long total;    // output rows of the tile
     unsigned long long ltotal;   // output rows written by the tile itself (short lists)
     int n;
@@ -266,8 +299,8 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
 // aggregate.  Nothing here waits on another CTA.
 template <int L>
 __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& B, TileState& S,
-                                           uint64_t* bar, unsigned phase, uint64_t tile, uint64_t R,
-                                           int wi, unsigned epoch, uint64_t* s_warp,
+                                           uint64_t* bar, unsigned phase, uint64_t tile, const Tiling& T,
+                                           uint64_t R, int wi, unsigned epoch, uint64_t* s_warp,
                                            unsigned long long& acc_alg, unsigned long long& acc_sd) {
     constexpr int kGroups = kStepThreads / L;
     constexpr int kBatches = L > 1 ? kTileRows / (kGroups * kUnroll) : 1;   // L = 1: tile_probe_rows
@@ -275,8 +308,8 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
     const int grp = threadIdx.x / L;
     const int h = threadIdx.x & (L - 1);
     const int gbase = (threadIdx.x & 31) & ~(L - 1);
-    const uint64_t r0 = tile * kTileRows;
-    const int n = (int)min((uint64_t)kTileRows, R - r0);
+    const uint64_t r0 = T.r0(tile);
+    const int n = T.rows(tile, R);
     const uint32_t* src = a.in + r0 * (uint64_t)wi;
     if (threadIdx.x == 0) {
         if (wi) {
@@ -285,6 +318,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
             tma_load_1d(B.in, src, bytes, bar);
         }
         S.tile = tile;
+        S.r0 = r0;
         S.n = n;
         S.has_heavy = 0;
     }
@@ -400,7 +434,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     const uint64_t tile = S.tile;
     const int n = S.n;
     const uint64_t total = S.total, ltotal = S.ltotal;
-    const uint64_t r0 = tile * kTileRows;
+    const uint64_t r0 = S.r0;
     if (threadIdx.x < 32) {
         const uint64_t ex = resolve_prefix(a.status, a.ctl, tile, total, epoch, spin_limit(a));
         if (threadIdx.x == 0) *s_excl = ex;
@@ -514,12 +548,13 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     WK_PH(6);
 }
 
-// Resident CTAs per SM the launch is built for: registers are capped for this many, and the
-// write staging is sized so that shared memory allows as many (explore_smem_bytes).
-constexpr int kExploreMinBlocks = 7;
+// Resident CTAs per SM each launch shape is built for: registers are capped for this many, and
+// the write staging is sized so that shared memory allows as many (explore_smem_bytes).  The
+// one-thread-per-row probe holds fewer registers than the group probes.
+__host__ __device__ constexpr int explore_min_blocks(int lanes) { return lanes == 1 ? 8 : 7; }
 
 template <int L>
-__global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kernel(const ExploreArgs a, int chunk_rows) {
+__global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_kernel(const ExploreArgs a, int chunk_rows) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ unsigned long long s_claim, s_excl;
@@ -538,7 +573,8 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     // were never written, so this step does no work and reports no size of its own
     if (!a.virtual_rows && R > a.in_cap_rows) R = 0;
     const bool handed_off = !a.virtual_rows && a.max_rows && R >= a.max_rows;   // flat pipeline's
-    uint64_t ntiles = handed_off ? 0 : (R + kTileRows - 1) / kTileRows;
+    const Tiling T = make_tiling(handed_off ? 0 : R, a.ctl->status_cap);
+    uint64_t ntiles = T.ntiles;
     if (ntiles > a.ctl->status_cap) {
         if (threadIdx.x == 0) atomicOr(&a.ctl->err, kErrStatus);
         ntiles = 0;
@@ -566,7 +602,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
     int b = 0;
     WK_PH(0);
     if (cur < ntiles)
-        tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], phases & 1u, cur, R, wi, epoch, s_warp,
+        tile_front<L>(a, tile_buf(base, wi), s_ts[0], &s_bar[0], phases & 1u, cur, T, R, wi, epoch, s_warp,
                       acc_alg, acc_sd);
     while (cur < ntiles) {
         if (threadIdx.x == 0) s_claim = atomicAdd(&a.ctl->tile_counter, 1ull);
@@ -575,7 +611,7 @@ __global__ void __launch_bounds__(kStepThreads, kExploreMinBlocks) explore_kerne
         WK_PH(0);
         if (next < ntiles)
             tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1],
-                          (phases >> (b ^ 1)) & 1u, next, R, wi, epoch, s_warp, acc_alg, acc_sd);
+                          (phases >> (b ^ 1)) & 1u, next, T, R, wi, epoch, s_warp, acc_alg, acc_sd);
         tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
                      wo, chunk_rows, epoch, s_pos, s_out, &s_excl, obase);
         if (wi) phases ^= 1u << b;
@@ -673,15 +709,16 @@ cudaError_t set_attr(int bytes) {
 
 }  // namespace
 
-size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
+size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows, int lanes) {
     // two tile buffers (rows, two scans, list offsets, four per-row words) + the write staging
     const size_t bufs = 2 * tile_buf_words(w_in) * 4;
     // The staging (a position and an output row per staged row) gets what is left once
-    // kExploreMinBlocks CTAs fit in an SM's 228 KiB (1 KiB of it reserved per CTA), between 64
-    // and 512 rows.  A fixed 8 KiB staging left wide levels at 5 CTAs per SM; sizing it this way
-    // took the 16,384-query batch's two widest levels from 0.190 / 0.121 ms to 0.175 / 0.112 ms.
+    // explore_min_blocks CTAs fit in an SM's 228 KiB (1 KiB of it reserved per CTA, and the
+    // kernel's static shared memory, under 1.5 KiB), between 64 and 512 rows.  A fixed 8 KiB
+    // staging left wide levels at 5 CTAs per SM; sizing it this way took the 16,384-query
+    // batch's two widest levels from 0.190 / 0.121 ms to 0.175 / 0.112 ms.
     const size_t per_row = 8 + 4 * (size_t)(w_out > 0 ? w_out : 1);
-    const size_t budget = 233472 / kExploreMinBlocks - 1024;
+    const size_t budget = 233472 / explore_min_blocks(lanes) - 1024 - 1536;
     int chunk = kMaxChunkRows;
     if (bufs + chunk * per_row > budget)
         chunk = budget > bufs ? (int)(((budget - bufs) / per_row) & ~(size_t)31) : 64;
@@ -693,7 +730,7 @@ size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows) {
 }
 
 cudaError_t explore_kernel_attrs() {
-    const int bytes = (int)explore_smem_bytes(32, 32, nullptr);
+    const int bytes = (int)explore_smem_bytes(32, 32, nullptr, 2);   // the largest budget
     cudaError_t e;
     if ((e = set_attr<1>(bytes)) != cudaSuccess) return e;
     if ((e = set_attr<2>(bytes)) != cudaSuccess) return e;
@@ -713,7 +750,7 @@ CtaUse explore_cta_use(int w_in, int w_out, int lanes) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     if (e != cudaSuccess) fa.numRegs = 255;   // unknown: assume the worst
-    u.smem = explore_smem_bytes(w_in, w_out, nullptr) + fa.sharedSizeBytes + (size_t)reserved;
+    u.smem = explore_smem_bytes(w_in, w_out, nullptr, lanes) + fa.sharedSizeBytes + (size_t)reserved;
     // registers are allocated per warp in units of 256
     u.regs = ((fa.numRegs * 32 + 255) / 256) * 256 * (kStepThreads / 32);
     return u;
@@ -743,7 +780,7 @@ int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, i
 }
 
 int explore_blocks_per_sm(int w_in, int w_out, int lanes) {
-    size_t smem = explore_smem_bytes(w_in, w_out, nullptr);
+    size_t smem = explore_smem_bytes(w_in, w_out, nullptr, lanes);
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
     if (lanes == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<1>, kStepThreads, smem);
@@ -756,7 +793,7 @@ int explore_blocks_per_sm(int w_in, int w_out, int lanes) {
 cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s) {
     int chunk = 0;
     const int wi = a.virtual_rows ? 0 : a.w_in;
-    size_t smem = explore_smem_bytes(wi, a.w_out, &chunk);
+    size_t smem = explore_smem_bytes(wi, a.w_out, &chunk, a.lanes);
     if (grid < 1) grid = 1;
     switch (a.lanes) {
     case 1: explore_kernel<1><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
