@@ -157,47 +157,82 @@ __global__ void __launch_bounds__(1024) scan_kernel(uint32_t* v, uint32_t n, uin
     if (threadIdx.x == 0 && total) *total = (uint32_t)s_carry;
 }
 
-// Stable scatter: the CTA walks its chunk 256 elements at a time in order; an element's place
-// is its digit's running offset, plus the count of its digit in the warps before it, plus its
-// rank among the lanes of its warp with that digit.
+// Offsets of a counting pass: digit d of CTA b starts at the elements of smaller digits plus the
+// digit-d elements of CTAs before b.  One CTA of kDigits threads: thread d adds up its digit's
+// row of hist (one contiguous row of `grid` words, digit-major), then the digit totals are
+// scanned and each row is rewritten as exclusive offsets.
+__global__ void __launch_bounds__(kDigits) digit_offsets_kernel(uint32_t* hist, uint32_t grid) {
+    __shared__ uint64_t s_warp[kDigits / 32];
+    uint32_t* row = hist + (size_t)threadIdx.x * grid;
+    uint64_t tot = 0;
+    for (uint32_t b = 0; b < grid; ++b) tot += row[b];
+    const uint64_t base = block_exclusive_sum<kDigits>(tot, s_warp);
+    uint64_t run = base;
+    for (uint32_t b = 0; b < grid; ++b) {
+        const uint32_t c = row[b];
+        row[b] = (uint32_t)run;
+        run += c;
+    }
+}
+
+// Stable scatter of 2,048-element tiles: warp w of the CTA takes elements [w * 256, w * 256 + 256)
+// of the tile in 8 rounds of 32 consecutive ones, so the warp's rounds follow the elements'
+// order.  Within a round, an element's rank among the lanes with its digit comes from a match,
+// and the warp's running count of each digit (shared memory, updated by one lane per digit)
+// gives its place in the warp; one barrier then turns the warps' counts into per-warp digit
+// offsets, and the element goes to its digit's running offset + its warp's offset + its place.
+constexpr int kScatterPer = 8;                                // elements per thread per tile
+constexpr int kScatterTile = kFinThreads * kScatterPer;       // 2,048
+
 __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) {
+    constexpr int kWarps = kFinThreads / 32;
     __shared__ uint32_t s_run[kDigits];
-    __shared__ uint32_t s_cnt[kFinThreads / 32][kDigits];
-    __shared__ uint32_t s_tile[kDigits];
+    __shared__ uint32_t s_cnt[kWarps][kDigits];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     s_run[threadIdx.x] = a.hist[threadIdx.x * gridDim.x + blockIdx.x];
     uint32_t lo, hi;
     chunk(a.n, &lo, &hi);
-    for (uint32_t base = lo; base < hi; base += kFinThreads) {
-        for (int w = 0; w < kFinThreads / 32; ++w) s_cnt[w][threadIdx.x] = 0;
+    for (uint32_t base = lo; base < hi; base += kScatterTile) {
+        for (int w = 0; w < kWarps; ++w) s_cnt[w][threadIdx.x] = 0;
         __syncthreads();
-        const uint32_t i = base + threadIdx.x;
-        const bool live = i < hi;
-        const unsigned long long key = live ? a.key_in[i] : 0;
-        const uint32_t row = live ? a.idx_in[i] : 0;
-        const uint32_t dg = live ? (uint32_t)(key >> a.shift) & 0xFFu : kDigits + lane;   // lone sentinel
-        const unsigned peers = __match_any_sync(0xffffffffu, dg);
-        const int rank = __popc(peers & ((1u << lane) - 1));
-        if (live && rank == 0) s_cnt[warp][dg] = __popc(peers);
-        __syncthreads();
-        {   // per digit: exclusive prefix over the warps, and the tile's count
-            uint32_t acc = 0;
-            for (int w = 0; w < kFinThreads / 32; ++w) {
-                const uint32_t c = s_cnt[w][threadIdx.x];
-                s_cnt[w][threadIdx.x] = acc;
-                acc += c;
-            }
-            s_tile[threadIdx.x] = acc;
+        unsigned long long key[kScatterPer];
+        uint32_t row[kScatterPer], dg[kScatterPer], at[kScatterPer];
+        const uint32_t wbase = base + (uint32_t)warp * (32 * kScatterPer);
+#pragma unroll
+        for (int r = 0; r < kScatterPer; ++r) {
+            const uint32_t i = wbase + r * 32 + lane;
+            const bool live = i < hi;
+            key[r] = live ? a.key_in[i] : 0;
+            row[r] = live ? a.idx_in[i] : 0;
+            dg[r] = live ? (uint32_t)(key[r] >> a.shift) & 0xFFu : kDigits + lane;   // lone sentinel
+        }
+#pragma unroll
+        for (int r = 0; r < kScatterPer; ++r) {
+            const unsigned peers = __match_any_sync(0xffffffffu, dg[r]);
+            const int rank = __popc(peers & ((1u << lane) - 1));
+            const bool live = dg[r] < kDigits;
+            at[r] = live ? s_cnt[warp][dg[r]] + rank : 0;
+            __syncwarp();
+            if (live && rank == 0) s_cnt[warp][dg[r]] += __popc(peers);
+            __syncwarp();
         }
         __syncthreads();
-        if (live) {
-            const uint32_t at = s_run[dg] + s_cnt[warp][dg] + rank;
-            a.key_out[at] = key;
-            a.idx_out[at] = row;
+        uint32_t tile_cnt = 0;   // per digit (thread = digit): prefix over the warps
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = s_cnt[w][threadIdx.x];
+            s_cnt[w][threadIdx.x] = tile_cnt;
+            tile_cnt += c;
         }
         __syncthreads();
-        s_run[threadIdx.x] += s_tile[threadIdx.x];
+#pragma unroll
+        for (int r = 0; r < kScatterPer; ++r) {
+            if (dg[r] >= kDigits) continue;
+            const uint32_t pos = s_run[dg[r]] + s_cnt[warp][dg[r]] + at[r];
+            a.key_out[pos] = key[r];
+            a.idx_out[pos] = row[r];
+        }
         __syncthreads();
+        s_run[threadIdx.x] += tile_cnt;
     }
 }
 
@@ -466,7 +501,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             for (int shift = 0; shift < chunk_bits[k]; shift += 8) {
                 SortPass p{ka, ia, kb, ib, shift, n, hist};
                 hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
-                scan_kernel<<<1, 1024, 0, s>>>(hist, (uint32_t)(kDigits * grid), nullptr);
+                digit_offsets_kernel<<<1, kDigits, 0, s>>>(hist, (uint32_t)grid);
                 scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
                 std::swap(ka, kb);
                 std::swap(ia, ib);
