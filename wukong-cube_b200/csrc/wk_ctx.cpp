@@ -432,9 +432,9 @@ int enqueue_step(wk_ctx* ctx, const PlanStep& st, const wk_table* in, wk_table* 
         f.out_cap_rows = a.out_cap_rows;
         f.out_rows = a.out_rows;
         f.min_rows = flat_mode == kFlatAuto ? ctx->flat_min_rows : 0;
-        // a serving lane takes half of each SM (4 of 8 CTAs of 256 threads, 32 registers each),
-        // which leaves room for the iteration launches' CTAs beside it
-        const int grid = ctx->beside_ctas > 0 ? ctx->sm_count * 4 : flat_grid(ctx->sm_count);
+        // a serving lane leaves room on every SM for the iteration launches' CTAs beside it
+        const int grid = ctx->beside_ctas > 0 ? flat_grid_beside(ctx->sm_count, ctx->beside_use, ctx->beside_ctas)
+                                              : flat_grid(ctx->sm_count);
         f.pos = reinterpret_cast<uint64_t*>(ctx->d_flat);
         f.off = f.pos + ctx->flat_cap_rows + 1;
         f.part = f.off + ctx->flat_cap_rows;

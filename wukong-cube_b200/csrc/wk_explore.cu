@@ -756,10 +756,8 @@ CtaUse explore_cta_use(int w_in, int w_out, int lanes) {
     return u;
 }
 
-int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, int other_ctas) {
-    const int alone = explore_blocks_per_sm(w_in, w_out, lanes);
+int blocks_beside(const CtaUse& me, int alone, const CtaUse& other, int other_ctas) {
     if (other_ctas <= 0) return alone;
-    const CtaUse me = explore_cta_use(w_in, w_out, lanes);
     int dev = 0, smem_sm = 0, regs_sm = 0, thr_sm = 0, blk_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
@@ -777,6 +775,12 @@ int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, i
     fit(thr_sm, other.threads, me.threads);
     fit(blk_sm, 1, 1);
     return (int)std::max(1ll, n);
+}
+
+int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, int other_ctas) {
+    const int alone = explore_blocks_per_sm(w_in, w_out, lanes);
+    if (other_ctas <= 0) return alone;
+    return blocks_beside(explore_cta_use(w_in, w_out, lanes), alone, other, other_ctas);
 }
 
 int explore_blocks_per_sm(int w_in, int w_out, int lanes) {

@@ -120,6 +120,9 @@ CtaUse explore_cta_use(int w_in, int w_out, int lanes);
 // CTAs per SM of this launch that fit beside `other_ctas` resident CTAs using `other` each
 // (at least 1), so two persistent launches can be resident on every SM at once.
 int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, int other_ctas);
+// CTAs of shape `me` (at most `alone`) that fit on an SM beside other_ctas CTAs of shape
+// `other`: shared memory, registers, threads and CTA slots; at least 1.
+int blocks_beside(const CtaUse& me, int alone, const CtaUse& other, int other_ctas);
 cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s);
 
 }  // namespace wk

@@ -26,6 +26,8 @@
 // exactly one of the two writes the output.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/wukong_b200.h"
 #include "wk_device.cuh"
 #include "wk_flat.h"
@@ -685,6 +687,21 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
 }  // namespace
 
 int flat_grid(int sm_count) { return sm_count * (2048 / kFlatThreads); }
+
+int flat_grid_beside(int sm_count, const CtaUse& other, int other_ctas) {
+    cudaFuncAttributes fa{}, fb{};
+    int regs = 255;
+    if (cudaFuncGetAttributes(&fa, flat_count_kernel<true>) == cudaSuccess &&
+        cudaFuncGetAttributes(&fb, flat_count_kernel<false>) == cudaSuccess)
+        regs = std::max(fa.numRegs, fb.numRegs);
+    int dev = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    CtaUse me{(size_t)std::max(fa.sharedSizeBytes, fb.sharedSizeBytes) + (size_t)reserved,
+              ((regs * 32 + 255) / 256) * 256 * (kFlatThreads / 32), kFlatThreads};
+    const int alone = 2048 / kFlatThreads;
+    return blocks_beside(me, alone, other, other_ctas) * sm_count;
+}
 
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
     // its last CTA scans the totals

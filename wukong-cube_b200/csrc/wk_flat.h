@@ -34,6 +34,10 @@ inline size_t flat_scratch_bytes(uint64_t rows, int grid) {
     return (size_t)(rows + 1) * 8 + (size_t)rows * 8 + (size_t)(grid + 1) * 8 + 256;
 }
 int flat_grid(int sm_count);
+// The grid of a serving lane's flat passes: the CTAs per SM of the count pass (the one that holds
+// the most registers) that fit beside other_ctas CTAs of shape `other`, times the SMs (at most
+// flat_grid).
+int flat_grid_beside(int sm_count, const CtaUse& other, int other_ctas);
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s);
 cudaError_t flat_kernel_attrs();
 
