@@ -80,3 +80,16 @@ def test_packed_key_chunks(ctx, cols, span):
             got = _run(ctx, table, keep, True, offset, limit)
             want = oracle.final_process(table, keep, True, offset, limit)
             assert np.array_equal(got, want), (keep, offset, limit)
+
+
+def test_large_table_many_tiles_per_cta(ctx):
+    """3 million rows: every sort CTA scatters several 2,048-row tiles per pass, with long runs
+    of equal digits (a narrow column) and rows repeated across tiles."""
+    rng = np.random.default_rng(91)
+    rows = 3_000_000
+    table = np.stack([rng.integers(0, 1 << 20, size=rows), rng.integers(0, 4, size=rows),
+                      rng.integers(0, 1 << 26, size=rows)], axis=1).astype(np.uint32)
+    table[rng.integers(0, rows, size=rows // 4)] = table[:rows // 4]
+    got = _run(ctx, table, [0, 1], True, 0, -1)
+    want = oracle.final_process(table, [0, 1], True, 0, -1)
+    assert np.array_equal(got, want)
