@@ -30,6 +30,17 @@ __device__ __forceinline__ ulonglong2 load_slot(const Slot* p) {
     return __ldg(reinterpret_cast<const ulonglong2*>(p));
 }
 
+// Slots p[0] and p[1] (one 32-byte sector) by one 256-bit load.  p must be 32-byte aligned: an
+// even slot of a bucket (buckets are 128-byte lines of a cudaMalloc'd array).
+__device__ __forceinline__ void load_sector(const Slot* p, ulonglong2* s0, ulonglong2* s1) {
+    unsigned long long a, b, c, d;
+    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
+                 : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+                 : "l"(p));
+    *s0 = make_ulonglong2(a, b);
+    *s1 = make_ulonglong2(c, d);
+}
+
 // ---------------------------------------------------------------- mbarrier + TMA bulk copy
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -205,8 +216,8 @@ __device__ __forceinline__ uint64_t thread_probe(const DevStore& st, uint64_t ke
 #pragma unroll
         for (int s = 0; s < kAssoc - 1; s += 2) {
             if (hop == 0 && s < first) continue;
-            const ulonglong2 s0 = load_slot(b + s);   // both slots: one 32-byte sector
-            const ulonglong2 s1 = load_slot(b + s + 1);
+            ulonglong2 s0, s1;
+            load_sector(b + s, &s0, &s1);   // both slots: one 32-byte sector
             if (s0.x == key) return s0.y;
             if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
             if (s + 1 == kAssoc - 1) {   // slot 7: the chain link

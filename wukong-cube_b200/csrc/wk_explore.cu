@@ -140,8 +140,9 @@ __host__ __device__ constexpr size_t tile_buf_words(int wi) {
 }
 static_assert(tile_buf_words(1) % 4 == 0, "tile buffers start on 16 bytes");
 
-// Most rows a tile stages for its writes at once (explore_smem_bytes sizes the staging).
-constexpr int kMaxChunkRows = 512;
+// Widest input rows the launch's shared-memory attribute is set for (explore_kernel_attrs): two
+// tile buffers of 100-column rows are 221 KB of the 227 KB a CTA may have.
+constexpr int kMaxSmemCols = 100;
 
 // Shared-memory arrays of one tile buffer (tile_buf_words() words).
 struct TileBuf {
@@ -252,11 +253,7 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
     for (int k = 0; k < kRows; ++k) {
         s0[k] = make_ulonglong2(0, 0);
         s1[k] = make_ulonglong2(0, 0);
-        if (flag[k] & 0x200u) {
-            const Slot* b = a.store.slots + (uint64_t)bkt[k] * kAssoc;
-            s0[k] = load_slot(b);
-            s1[k] = load_slot(b + 1);
-        }
+        if (flag[k] & 0x200u) load_sector(a.store.slots + (uint64_t)bkt[k] * kAssoc, &s0[k], &s1[k]);
     }
 #pragma unroll
     for (int k = 0; k < kRows; ++k) {
@@ -426,11 +423,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
 template <int L>
 __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B, TileState& S,
                                           uint64_t* bar, unsigned phase, uint64_t ntiles, int wi,
-                                          int wo, int chunk_rows, unsigned epoch, uint64_t* s_pos,
-                                          uint32_t* s_out, unsigned long long* s_excl, uint64_t obase) {
-    __shared__ uint32_t s_mark[kMaxChunkRows / 32];   // first outputs of rows in the chunk
-    __shared__ uint16_t s_first[kMaxChunkRows];       // the row of each marked output
-    __shared__ int s_carry[2];                        // row of the chunk's last output
+                                          int wo, unsigned epoch, unsigned long long* s_excl, uint64_t obase) {
     const uint64_t tile = S.tile;
     const int n = S.n;
     const uint64_t total = S.total, ltotal = S.ltotal;
@@ -484,60 +477,48 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
         }
     }
     WK_PH(5);
-    // Write the short-list rows (stride w_out), chunk by chunk of the staging.  Output o of the
-    // tile's short rows belongs to the last row whose first output is at or below o: each
-    // chunk marks its rows' first outputs in a bitmap (s_mark, with the row in s_first), and an
-    // output finds its row from the highest mark at or below it, looking back at most a chunk;
-    // an output before the chunk's first mark continues the row the previous chunk ended in.
+    // Write the short-list rows (stride w_out), each warp on its own with no block barrier: warp
+    // w takes the outputs of input rows [w * 64, w * 64 + 64), 32 rows at a time, one output row
+    // per lane.  Lane l holds row l's first short output st_l; the output o belongs to the last
+    // row with st <= o (a row without outputs has the next row's st), which a 5-step search over
+    // the lanes' st values finds.  Consecutive lanes write consecutive output rows, in row-major
+    // then list order, straight to global memory.
     if (fits && ltotal) {
         const bool contiguous = !S.has_heavy;
-        int chunk = 0;
-        for (uint64_t c0 = 0; c0 < ltotal; c0 += chunk_rows, ++chunk) {
-            const int m = (int)min((uint64_t)chunk_rows, ltotal - c0);
-            for (int i = threadIdx.x; i < (m + 31) / 32; i += kStepThreads) s_mark[i] = 0;
-            __syncthreads();
-            for (int i = threadIdx.x; i < n; i += kStepThreads) {
-                const uint64_t st = contiguous ? B.pre[i] : B.lpre[i];
-                const uint64_t en = contiguous ? B.pre[i + 1] : B.lpre[i + 1];
-                if (en > st && st >= c0 && st < c0 + m) {
-                    const int j = (int)(st - c0);
-                    s_first[j] = (uint16_t)i;
-                    atomicOr(&s_mark[j >> 5], 1u << (j & 31));
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        constexpr int kWarpRows = kTileRows / (kStepThreads / 32);
+        for (int h0 = warp * kWarpRows; h0 < warp * kWarpRows + kWarpRows; h0 += 32) {
+            if (h0 >= n) break;
+            const int r = min(h0 + lane, n);   // rows past n read the end entry
+            const uint64_t st = contiguous ? B.pre[r] : (uint64_t)B.lpre[r];
+            const int last = min(h0 + 32, n);
+            const uint64_t o_begin = __shfl_sync(kFull, st, 0);
+            const uint64_t o_end = contiguous ? B.pre[last] : (uint64_t)B.lpre[last];
+            for (uint64_t o0 = o_begin; o0 < o_end; o0 += 32) {
+                const uint64_t o = o0 + lane;
+                int own = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const uint64_t sv = __shfl_sync(kFull, st, own + step);
+                    if (own + step < 32 && sv <= o) own += step;
                 }
-            }
-            __syncthreads();
-            for (int j = threadIdx.x; j < m; j += kStepThreads) {
-                int wd = j >> 5;
-                unsigned w = s_mark[wd] & (0xFFFFFFFFu >> (31 - (j & 31)));
-                while (!w && wd > 0) w = s_mark[--wd];
-                const int lo = w ? (int)s_first[wd * 32 + 31 - __clz(w)] : s_carry[chunk & 1];
-                if (j == m - 1) s_carry[(chunk + 1) & 1] = lo;
-                const uint64_t o = c0 + j;
-                const uint64_t k = o - (contiguous ? B.pre[lo] : (uint64_t)B.lpre[lo]);
-                const uint32_t meta = B.meta[lo];
+                const uint64_t st_own = __shfl_sync(kFull, st, own);
+                if (o >= o_end) continue;
+                const int row = h0 + own;
+                const uint64_t k = o - st_own;
+                const uint32_t meta = B.meta[row];
                 const int opv = meta & 0xFF, cin = (meta >> 8) & 0xFF;
-                uint32_t* dst = s_out + (size_t)j * wo;
-                const uint32_t* sr = B.in + lo * wi;
+                const uint64_t pos = excl + B.pre[row] + k;
+                uint32_t* dst = a.out + pos * wo;
+                const uint32_t* sr = B.in + row * wi;
                 int c = 0;
                 if (opv != kXStart)
                     for (; c < cin; ++c) dst[c] = sr[c];
-                if (opv == kXStart || opv == kXK2U) dst[c++] = list_at(a.store.edges, B.off[lo], k);
                 // columns past the query's own width are never read (later levels and the
                 // result gather use only the query's columns), so they are left as they are
-                const uint64_t pos = excl + B.pre[lo] + k;
-                s_pos[j] = pos;
-                if (a.owner_out) a.owner_out[pos] = B.q[lo];
+                if (opv == kXStart || opv == kXK2U) dst[c] = list_at(a.store.edges, B.off[row], k);
+                if (a.owner_out) a.owner_out[pos] = B.q[row];
             }
-            __syncthreads();
-            if (contiguous) {
-                store_words(a.out + (excl + c0) * wo, s_out, (uint64_t)m * wo);
-            } else {
-                for (int e = threadIdx.x; e < m * wo; e += kStepThreads) {
-                    const int j = e / wo, c = e - j * wo;
-                    a.out[s_pos[j] * wo + c] = s_out[e];
-                }
-            }
-            __syncthreads();
         }
     }
     __syncthreads();
@@ -548,13 +529,12 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     WK_PH(6);
 }
 
-// Resident CTAs per SM each launch shape is built for: registers are capped for this many, and
-// the write staging is sized so that shared memory allows as many (explore_smem_bytes).  The
+// Resident CTAs per SM each launch shape is built for: registers are capped for this many.  The
 // one-thread-per-row probe holds fewer registers than the group probes.
 __host__ __device__ constexpr int explore_min_blocks(int lanes) { return lanes == 1 ? 8 : 7; }
 
 template <int L>
-__global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_kernel(const ExploreArgs a, int chunk_rows) {
+__global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_kernel(const ExploreArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ unsigned long long s_claim, s_excl;
@@ -564,8 +544,6 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
     const int wi = a.virtual_rows ? 0 : a.w_in, wo = a.w_out;
     const size_t buf_words = tile_buf_words(wi);
     uint32_t* base = reinterpret_cast<uint32_t*>(smem);
-    uint64_t* s_pos = reinterpret_cast<uint64_t*>(base + 2 * buf_words);
-    uint32_t* s_out = reinterpret_cast<uint32_t*>(s_pos + chunk_rows);
 
     const unsigned epoch = *(volatile unsigned*)&a.ctl->epoch;
     uint64_t R = a.virtual_rows ? a.n_queries : *(volatile const uint64_t*)a.in_rows;
@@ -613,7 +591,7 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
             tile_front<L>(a, tile_buf(base + (b ^ 1) * buf_words, wi), s_ts[b ^ 1], &s_bar[b ^ 1],
                           (phases >> (b ^ 1)) & 1u, next, T, R, wi, epoch, s_warp, acc_alg, acc_sd);
         tile_back<L>(a, tile_buf(base + b * buf_words, wi), s_ts[b], &s_bar[b], (phases >> b) & 1u, ntiles, wi,
-                     wo, chunk_rows, epoch, s_pos, s_out, &s_excl, obase);
+                     wo, epoch, &s_excl, obase);
         if (wi) phases ^= 1u << b;
         cur = next;
         b ^= 1;
@@ -669,8 +647,7 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
         const uint32_t q = __ldcg((const unsigned int*)&it->q);
         const StepDesc* d = step_desc(a, q);
         const int opv = d->op, cin = d->cin;
-        if (opv != kXStart && threadIdx.x < cin) s_out[threadIdx.x] = __ldg(a.in + in_row * (uint64_t)a.w_in + threadIdx.x);
-        __syncthreads();
+        const uint32_t* src = a.in + in_row * (uint64_t)a.w_in;   // the row's columns: L1 hits
         const int ecol = opv == kXStart ? 0 : cin;
         const uint64_t ne = (uint64_t)count * wo;
         uint32_t* dst = a.out + out_pos * wo;
@@ -678,7 +655,7 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
             const uint64_t j = e / wo;
             const int c = (int)(e - j * wo);
             uint32_t v = 0;
-            if (c < ecol) v = s_out[c];
+            if (c < ecol) v = __ldg(src + c);
             else if (c == ecol) v = __ldg(a.store.edges + off + j);
             dst[e] = v;
         }
@@ -709,28 +686,14 @@ cudaError_t set_attr(int bytes) {
 
 }  // namespace
 
-size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows, int lanes) {
-    // two tile buffers (rows, two scans, list offsets, four per-row words) + the write staging
-    const size_t bufs = 2 * tile_buf_words(w_in) * 4;
-    // The staging (a position and an output row per staged row) gets what is left once
-    // explore_min_blocks CTAs fit in an SM's 228 KiB (1 KiB of it reserved per CTA, and the
-    // kernel's static shared memory, under 1.5 KiB), between 64 and 512 rows.  A fixed 8 KiB
-    // staging left wide levels at 5 CTAs per SM; sizing it this way took the 16,384-query
-    // batch's two widest levels from 0.190 / 0.121 ms to 0.175 / 0.112 ms.
-    const size_t per_row = 8 + 4 * (size_t)(w_out > 0 ? w_out : 1);
-    const size_t budget = 233472 / explore_min_blocks(lanes) - 1024 - 1536;
-    int chunk = kMaxChunkRows;
-    if (bufs + chunk * per_row > budget)
-        chunk = budget > bufs ? (int)(((budget - bufs) / per_row) & ~(size_t)31) : 64;
-    if (chunk > kMaxChunkRows) chunk = kMaxChunkRows;
-    if (chunk < 64) chunk = 64;
-    size_t bytes = bufs + (size_t)chunk * per_row;
-    if (chunk_rows) *chunk_rows = chunk;
-    return bytes;
+size_t explore_smem_bytes(int w_in) {
+    // two tile buffers: rows, the two scans, list offsets and three per-row words (the writes go
+    // straight to global memory, with no staging)
+    return 2 * tile_buf_words(w_in) * 4;
 }
 
 cudaError_t explore_kernel_attrs() {
-    const int bytes = (int)explore_smem_bytes(32, 32, nullptr, 2);   // the largest budget
+    const int bytes = (int)explore_smem_bytes(kMaxSmemCols);
     cudaError_t e;
     if ((e = set_attr<1>(bytes)) != cudaSuccess) return e;
     if ((e = set_attr<2>(bytes)) != cudaSuccess) return e;
@@ -750,7 +713,7 @@ CtaUse explore_cta_use(int w_in, int w_out, int lanes) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     if (e != cudaSuccess) fa.numRegs = 255;   // unknown: assume the worst
-    u.smem = explore_smem_bytes(w_in, w_out, nullptr, lanes) + fa.sharedSizeBytes + (size_t)reserved;
+    u.smem = explore_smem_bytes(w_in) + fa.sharedSizeBytes + (size_t)reserved;
     // registers are allocated per warp in units of 256
     u.regs = ((fa.numRegs * 32 + 255) / 256) * 256 * (kStepThreads / 32);
     return u;
@@ -784,7 +747,7 @@ int explore_blocks_beside(int w_in, int w_out, int lanes, const CtaUse& other, i
 }
 
 int explore_blocks_per_sm(int w_in, int w_out, int lanes) {
-    size_t smem = explore_smem_bytes(w_in, w_out, nullptr, lanes);
+    size_t smem = explore_smem_bytes(w_in);
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
     if (lanes == 1) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, explore_kernel<1>, kStepThreads, smem);
@@ -795,15 +758,14 @@ int explore_blocks_per_sm(int w_in, int w_out, int lanes) {
 }
 
 cudaError_t launch_explore(const ExploreArgs& a, int grid, cudaStream_t s) {
-    int chunk = 0;
     const int wi = a.virtual_rows ? 0 : a.w_in;
-    size_t smem = explore_smem_bytes(wi, a.w_out, &chunk, a.lanes);
+    const size_t smem = explore_smem_bytes(wi);
     if (grid < 1) grid = 1;
     switch (a.lanes) {
-    case 1: explore_kernel<1><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
-    case 2: explore_kernel<2><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
-    case 8: explore_kernel<8><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
-    default: explore_kernel<4><<<grid, kStepThreads, smem, s>>>(a, chunk); break;
+    case 1: explore_kernel<1><<<grid, kStepThreads, smem, s>>>(a); break;
+    case 2: explore_kernel<2><<<grid, kStepThreads, smem, s>>>(a); break;
+    case 8: explore_kernel<8><<<grid, kStepThreads, smem, s>>>(a); break;
+    default: explore_kernel<4><<<grid, kStepThreads, smem, s>>>(a); break;
     }
     return cudaGetLastError();
 }

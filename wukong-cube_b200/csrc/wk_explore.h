@@ -106,7 +106,7 @@ struct ExploreArgs {
 
 constexpr uint64_t kDefaultSpinLimit = 1ull << 24;
 
-size_t explore_smem_bytes(int w_in, int w_out, int* chunk_rows, int lanes);
+size_t explore_smem_bytes(int w_in);
 cudaError_t explore_kernel_attrs();
 int explore_blocks_per_sm(int w_in, int w_out, int lanes);
 

@@ -146,31 +146,20 @@ __device__ __forceinline__ uint64_t count_key(const FlatArgs& a, const StepDesc&
     return key;
 }
 
-// Pointer word of `key` given its home bucket's slot 0 (already loaded).  Slot 1 shares slot 0's
-// 32-byte sector, so its load hits L1: it is read when slot 0 holds another key, and when slot
-// 0 holds this key with a one-entry list (slot 1 may then hold the entry, kInlineTag).  The walk
-// goes on from slot 2 only when the sector does not settle the key.  *inl receives the tagged
-// entry, else 0.
+// Pointer word of `key` given its home bucket's slots 0 and 1 (one 32-byte sector, loaded
+// together); the walk goes on from slot 2 only when they do not settle the key.  *inl receives
+// the key's single entry when the bucket holds it (kInlineTag), else 0.
 __device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key, uint64_t b, ulonglong2 s0,
-                                                unsigned* err, uint64_t* inl) {
+                                                ulonglong2 s1, unsigned* err, uint64_t* inl) {
     *inl = 0;
     if (s0.x == key) {
-        if (ptr_size(s0.y) == 1) {
-            const ulonglong2 s1 = load_slot(st.slots + b * kAssoc + 1);
-            *inl = inline_entry(s0.y, s1.x, s1.y);
-        }
+        *inl = inline_entry(s0.y, s1.x, s1.y);
         return s0.y;
     }
     if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
-    const ulonglong2 s1 = load_slot(st.slots + b * kAssoc + 1);
     if (s1.x == key) return s1.y;
     if (s1.x == 0) return 0;
     return thread_probe(st, key, b, err, 2);
-}
-
-__device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint64_t b, ulonglong2 s0,
-                                           uint64_t* inl) {
-    return settle_slot(a.store, key, b, s0, &a.ctl->err, inl);
 }
 
 // kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
@@ -179,7 +168,7 @@ __device__ __forceinline__ uint64_t settle(const FlatArgs& a, uint64_t key, uint
 // Registers are capped for kCountCtas CTAs per SM.  kFilter: the membership steps
 // (known_to_known, known_to_const, const_to_known, index_to_known); the other instance (starts
 // and known_to_unknown) carries no membership search.
-constexpr int kRowsPerThread = 4;
+constexpr int kRowsPerThread = 3;
 constexpr int kCountCtas = 4;
 
 template <bool kFilter>
@@ -200,7 +189,7 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
     for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
         uint64_t key[K], bkt[K], p[K], inl[K];
         bool valid[K], look[K];
-        ulonglong2 s0[K];
+        ulonglong2 s0[K], s1[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
@@ -209,12 +198,14 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
             if (r >= hi) valid[k] = look[k] = false;
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+        for (int k = 0; k < K; ++k) {
+            s0[k] = s1[k] = make_ulonglong2(0, 0);
+            if (look[k]) load_sector(a.store.slots + bkt[k] * kAssoc, &s0[k], &s1[k]);
+        }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             inl[k] = 0;
-            p[k] = look[k] ? settle(a, key[k], bkt[k], s0[k], &inl[k]) : 0;
+            p[k] = look[k] ? settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err, &inl[k]) : 0;
         }
         // counts and list offsets
         uint32_t c[K];
@@ -518,10 +509,12 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
                 look[k] = false;
             }
         }
-        ulonglong2 s0[K];
+        ulonglong2 s0[K], s1[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k)
-            s0[k] = look[k] ? load_slot(a.store.slots + bkt[k] * kAssoc) : make_ulonglong2(0, 0);
+        for (int k = 0; k < K; ++k) {
+            s0[k] = s1[k] = make_ulonglong2(0, 0);
+            if (look[k]) load_sector(a.store.slots + bkt[k] * kAssoc, &s0[k], &s1[k]);
+        }
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
@@ -531,7 +524,7 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
             uint64_t off = 0, deg = 0;
             if (look[k]) {
                 uint64_t inl = 0;
-                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], &a.ctl->err, &inl);
+                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err, &inl);
                 off = ptr_off(p);
                 deg = ptr_size(p);
                 if (off + deg > a.store.n_edges) {
