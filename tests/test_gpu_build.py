@@ -79,10 +79,10 @@ def test_empty_and_refused_builds():
 
 @pytest.mark.parametrize("load", [0.0, 1.0])
 def test_upload_then_export_gives_the_uploaded_bytes(load):
-    """The device copy keeps single-entry lists of keys alone in their bucket in the empty slot
-    1 of that bucket (an in-bucket copy the probes read instead of the edge array); the export
-    still gives back exactly the bytes that were uploaded, and queries still answer as the
-    oracle does, through the one-thread-per-row probe and the flat passes that use the copy."""
+    """The device copy keeps every one-entry list in its key's own pointer word (the entry with
+    the pointer type 3, the original word kept aside); the export still gives back exactly the
+    bytes that were uploaded, and queries still answer as the oracle does through every probe
+    form and the flat passes."""
     tr, v = wk.synth_generate(12, seed=7)
     g, hs, he, hg = _host_arrays(tr, load, False)
     o = oracle.OracleStore(tr)
@@ -93,7 +93,7 @@ def test_upload_then_export_gives_the_uploaded_bytes(load):
         inst = {t: g.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
         qs = workloads.light_queries(v, inst, 300, seed=9)
         heavy = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
-        for lanes, flat_rows in ((1, 0), (1, 1), (2, 1)):
+        for lanes, flat_rows in ((1, 0), (1, 1), (2, 1), (8, 0)):
             ctx.tune_set(wk.KNOB_LANES, lanes)
             ctx.tune_set(wk.KNOB_BATCH_LANES, lanes)
             ctx.tune_set(wk.KNOB_FLAT_ROWS, flat_rows)

@@ -618,6 +618,7 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     if (ctx->d_slots && !ctx->borrowed_store) cudaFree(ctx->d_slots);
     if (ctx->d_edges && !ctx->borrowed_store) cudaFree(ctx->d_edges);
     if (ctx->d_pseg && !ctx->borrowed_store) cudaFree(ctx->d_pseg);
+    if (ctx->d_inline_orig && !ctx->borrowed_store) cudaFree(ctx->d_inline_orig);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_heavy) cudaFree(ctx->d_heavy);
     if (ctx->d_flat) cudaFree(ctx->d_flat);
@@ -760,8 +761,46 @@ int wk::store_adopt(wk_ctx* ctx, Slot* d_slots, uint64_t n_slots, uint32_t* d_ed
         }
         ctx->sorted_lists = (flag & 1u) ? 0 : 1;
     }
-    WK_CUDA(ctx, wk::launch_inline(ctx->dev_store(), ctx->stream));
-    WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    {
+        // one-entry lists into their keys' pointer words, the original words kept aside: count,
+        // then convert
+        if (ctx->d_inline_orig) cudaFree(ctx->d_inline_orig);
+        ctx->d_inline_orig = nullptr;
+        ctx->n_inline = 0;
+        struct Counts {
+            unsigned long long n;
+            unsigned clash, pad;
+        };
+        Counts* d_c = nullptr;
+        Counts h_c{};
+        WK_CUDA(ctx, wk::dev_malloc(&d_c, sizeof(Counts)));
+        cudaError_t e = cudaMemsetAsync(d_c, 0, sizeof(Counts), ctx->stream);
+        if (e == cudaSuccess) e = wk::launch_inline(ctx->dev_store(), &d_c->n, &d_c->clash, nullptr, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_c, d_c, sizeof(Counts), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e == cudaSuccess && !h_c.clash && h_c.n) {
+            if (wk::dev_malloc(&ctx->d_inline_orig, h_c.n * 16) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(d_c);
+                ctx->has_store = false;
+                return ctx->fail(WK_E_OOM, "one-entry list table");
+            }
+            e = cudaMemsetAsync(d_c, 0, sizeof(Counts), ctx->stream);
+            if (e == cudaSuccess)
+                e = wk::launch_inline(ctx->dev_store(), &d_c->n, &d_c->clash, ctx->d_inline_orig, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            ctx->n_inline = h_c.n;
+        }
+        cudaFree(d_c);
+        if (e != cudaSuccess) {
+            ctx->has_store = false;
+            return ctx->cuda_fail(e, "one-entry lists");
+        }
+        if (h_c.clash) {
+            ctx->has_store = false;
+            return ctx->fail(WK_E_UNSUPPORTED, "a pointer word of type 3 (attribute values are not served)");
+        }
+    }
     ctx->drop_graphs();
     return WK_SUCCESS;
 }
@@ -783,12 +822,15 @@ extern "C" int wk_store_export(wk_ctx* ctx, void* slots, uint64_t slots_cap, uin
     WK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (slots && ctx->n_slots) {
         WK_CUDA(ctx, cudaMemcpy(slots, ctx->d_slots, ctx->n_slots * sizeof(wk::Slot), cudaMemcpyDeviceToHost));
-        // the pointer words of empty slots hold the device copy's in-bucket entries; the
-        // store's own layout has them zero
-        wk::Slot* h = static_cast<wk::Slot*>(slots);
+        // the device copy keeps one-entry lists in their keys' pointer words; put the original
+        // words back
+        if (ctx->n_inline) {
+            std::vector<uint64_t> orig(ctx->n_inline * 2);
+            WK_CUDA(ctx, cudaMemcpy(orig.data(), ctx->d_inline_orig, orig.size() * 8, cudaMemcpyDeviceToHost));
+            wk::Slot* h = static_cast<wk::Slot*>(slots);
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < (int64_t)ctx->n_slots; ++i)
-            if (h[i].key == 0) h[i].ptr = 0;
+            for (int64_t i = 0; i < (int64_t)ctx->n_inline; ++i) h[orig[2 * i]].ptr = orig[2 * i + 1];
+        }
     }
     if (edges && ctx->n_edges)
         WK_CUDA(ctx, cudaMemcpy(edges, ctx->d_edges, ctx->n_edges * 4, cudaMemcpyDeviceToHost));

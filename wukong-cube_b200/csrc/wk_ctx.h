@@ -93,6 +93,8 @@ struct wk_ctx {
     wk::PredSeg* d_pseg = nullptr;    // predicate segments by pid * 2 + dir (versatile steps)
     uint32_t n_pseg = 0;
     std::map<uint32_t, uint64_t> index_len;   // tpid * 2 + dir -> length of its index list
+    uint64_t* d_inline_orig = nullptr;   // (slot index, original pointer word) of every slot
+    uint64_t n_inline = 0;               // whose one-entry list is kept in the slot itself
     bool borrowed_store = false;   // a serving lane: the store belongs to its parent context
     wk::CtaUse beside_use{0, 0, 0};   // a serving lane leaves room on every SM for this many
     int beside_ctas = 0;              // resident CTAs of this size (the iteration launches)

@@ -99,20 +99,34 @@ __device__ __forceinline__ uint64_t bucket_of(uint64_t key, const SegDesc& s) {
 }
 
 // ---------------------------------------------------------------- single-entry lists
-// A list of one entry whose key is alone in its bucket is kept in the bucket too: the key sits
-// in slot 0, slot 1 is empty, and the device copy of the store holds the entry in slot 1's
-// pointer word, tagged with kInlineTag (inline_kernel, run at upload).  Slot 1's key word stays
-// 0, so every probe still sees an empty slot there (the reference's own probe reads key words
-// only), and the edge array is unchanged: a reader that ignores the tag still reads the list
-// from the edge array.  The readers that use it take the entry from the sector the probe already
-// loaded instead of a second random read.  Within a step, a list offset with kInlineTag set
+// The device copy of the store keeps a one-entry list in its key's own pointer word: iptr_t's
+// type field (bits 62-63, 0 for the ids this path reads) is set to 3, the size stays 1 and the
+// offset field holds the entry itself (inline_kernel, run at upload; the original pointer words
+// are kept aside for wk_store_export).  A probe that finds the key then has the entry without a
+// second random read of the edge array.  Within a step, a list offset with kInlineTag set
 // carries that entry in its low 32 bits instead of an edge-array offset (list_at).
 constexpr uint64_t kInlineTag = 1ull << 63;
+constexpr uint64_t kInlinePtrType = 3ull << 62;
 
-// The tagged entry of the key found in slot 0 (pointer word p0) given slot 1 (key k1, pointer
-// word p1) of the same bucket; 0 when its list is not kept in the bucket.
-__device__ __forceinline__ uint64_t inline_entry(uint64_t p0, uint64_t k1, uint64_t p1) {
-    return (k1 == 0 && ptr_size(p0) == 1 && (p1 & kInlineTag)) ? p1 : 0;
+__host__ __device__ __forceinline__ bool ptr_is_inline(uint64_t p) { return (p >> 62) == 3; }
+__host__ __device__ __forceinline__ uint64_t make_inline_ptr(uint32_t entry) {
+    return kInlinePtrType | ((uint64_t)entry << kNbitsSize) | 1;
+}
+
+// The list a pointer word names: *off an edge-array offset or a tagged entry, *deg its length;
+// an offset past the edge array sets kErrCorrupt and an empty list.
+__device__ __forceinline__ void list_of_ptr(uint64_t p, uint64_t n_edges, unsigned* err, uint64_t* off,
+                                            uint64_t* deg) {
+    *deg = ptr_size(p);
+    if (ptr_is_inline(p)) {
+        *off = kInlineTag | (uint32_t)(p >> kNbitsSize);
+        return;
+    }
+    *off = ptr_off(p);
+    if (*off + *deg > n_edges) {
+        if (*deg) atomicOr(err, kErrCorrupt);
+        *deg = 0;
+    }
 }
 
 // Entry k of the list at `off` (an edge-array offset, or a tagged single entry).
@@ -129,8 +143,7 @@ __device__ __forceinline__ uint32_t list_at(const uint32_t* edges, uint64_t off,
 template <int L, class BucketT>
 __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (&key)[kUnroll],
                                             BucketT (&bucket)[kUnroll], bool (&pending)[kUnroll],
-                                            uint64_t (&ptr)[kUnroll], unsigned* err,
-                                            uint64_t (*inl)[kUnroll] = nullptr) {
+                                            uint64_t (&ptr)[kUnroll], unsigned* err) {
     const int lane = threadIdx.x & 31;
     const int h = lane & (L - 1);
     const int gbase = lane & ~(L - 1);
@@ -140,7 +153,6 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
     for (int u = 0; u < kUnroll; ++u) {
         ptr[u] = 0;
         round[u] = 0;
-        if (inl) (*inl)[u] = 0;
     }
     for (int it = 0;; ++it) {
         bool any = false;
@@ -174,13 +186,9 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
             const int src = hm ? gbase + __ffs(hm) - 1 : gbase + L - 1;
             const uint64_t kx = __shfl_sync(kFull, s[u].x, src);
             const uint64_t py = __shfl_sync(kFull, s[u].y, src);
-            // the home bucket's slot 1 (lane 1 of the group in the first round): a key found in
-            // slot 0 may have its single entry there
-            const uint64_t y1 = inl ? __shfl_sync(kFull, s[u].y, gbase + 1) : 0;
             if (pending[u]) {
                 if (hm) {
                     ptr[u] = py;
-                    if (inl && round[u] == 0 && hm == 1u && ((em >> 1) & 1u)) (*inl)[u] = inline_entry(py, 0, y1);
                     pending[u] = false;
                 } else if (em) {
                     pending[u] = false;           // first empty slot: the key is absent

@@ -259,32 +259,21 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
     for (int k = 0; k < kRows; ++k) {
         const int row = threadIdx.x + k * kStepThreads;
         if (row >= n || !(flag[k] & 0x100u)) continue;
-        uint64_t p = 0, inl = 0;
+        uint64_t p = 0;
         if (flag[k] & 0x200u) {
-            if (s0[k].x == key[k]) {
-                p = s0[k].y;
-                inl = inline_entry(p, s1[k].x, s1[k].y);
-            } else if (s0[k].x == 0) {
-                p = 0;   // first empty slot: absent (insert-only store)
-            } else if (s1[k].x == key[k]) {
-                p = s1[k].y;
-            } else if (s1[k].x != 0) {
-                p = thread_probe(a.store, key[k], bkt[k], &a.ctl->err, 2);
-            }
+            if (s0[k].x == key[k]) p = s0[k].y;
+            else if (s0[k].x == 0) p = 0;   // first empty slot: absent (insert-only store)
+            else if (s1[k].x == key[k]) p = s1[k].y;
+            else if (s1[k].x != 0) p = thread_probe(a.store, key[k], bkt[k], &a.ctl->err, 2);
         }
-        uint64_t off = ptr_off(p), deg = ptr_size(p);
-        if (off + deg > a.store.n_edges) {
-            if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
-            deg = 0;
-        }
+        uint64_t off, deg;
+        list_of_ptr(p, a.store.n_edges, &a.ctl->err, &off, &deg);
         const uint32_t op = flag[k] & 0xFFu;
-        if (op == kXI2K) {   // index_to_known reads its mt slice of the list
-            uint64_t lo, hi;
+        if (op == kXI2K) {   // index_to_known reads its mt slice of the list (a one-entry list
+            uint64_t lo, hi;   // keeps its entry: its slice starts at 0)
             mt_slice(step_desc(a, B.q[row])->mt, deg, &lo, &hi);
             off += lo;
             deg = hi - lo;
-        } else if (deg == 1 && inl) {
-            off = inl;   // the entry was in the bucket's sector
         }
         const bool found = is_filter_op(op) && deg &&
                            thread_member(a.store.edges, off, deg, tgt[k], a.sorted_lists != 0);
@@ -372,12 +361,7 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
 #pragma unroll
         for (int u = 0; u < kUnroll; ++u) {
             const uint32_t op = flag[u] & 0xFFu;
-            off[u] = ptr_off(ptr[u]);
-            deg[u] = ptr_size(ptr[u]);
-            if (off[u] + deg[u] > a.store.n_edges) {
-                if (h == 0 && deg[u]) atomicOr(&a.ctl->err, kErrCorrupt);
-                deg[u] = 0;
-            }
+            list_of_ptr(ptr[u], a.store.n_edges, &a.ctl->err, &off[u], &deg[u]);
             if (op == kXI2K && valid[u]) {   // index_to_known reads its mt slice of the list
                 uint64_t lo, hi;
                 mt_slice(step_desc(a, B.q[row[u]])->mt, deg[u], &lo, &hi);

@@ -147,15 +147,10 @@ __device__ __forceinline__ uint64_t count_key(const FlatArgs& a, const StepDesc&
 }
 
 // Pointer word of `key` given its home bucket's slots 0 and 1 (one 32-byte sector, loaded
-// together); the walk goes on from slot 2 only when they do not settle the key.  *inl receives
-// the key's single entry when the bucket holds it (kInlineTag), else 0.
+// together); the walk goes on from slot 2 only when they do not settle the key.
 __device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key, uint64_t b, ulonglong2 s0,
-                                                ulonglong2 s1, unsigned* err, uint64_t* inl) {
-    *inl = 0;
-    if (s0.x == key) {
-        *inl = inline_entry(s0.y, s1.x, s1.y);
-        return s0.y;
-    }
+                                                ulonglong2 s1, unsigned* err) {
+    if (s0.x == key) return s0.y;
     if (s0.x == 0) return 0;   // first empty slot: absent (insert-only store)
     if (s1.x == key) return s1.y;
     if (s1.x == 0) return 0;
@@ -187,7 +182,7 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
     constexpr int K = kRowsPerThread;
     constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
     for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
-        uint64_t key[K], bkt[K], p[K], inl[K];
+        uint64_t key[K], bkt[K], p[K];
         bool valid[K], look[K];
         ulonglong2 s0[K], s1[K];
 #pragma unroll
@@ -203,27 +198,20 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
             if (look[k]) load_sector(a.store.slots + bkt[k] * kAssoc, &s0[k], &s1[k]);
         }
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            inl[k] = 0;
-            p[k] = look[k] ? settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err, &inl[k]) : 0;
-        }
+        for (int k = 0; k < K; ++k)
+            p[k] = look[k] ? settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err) : 0;
         // counts and list offsets
         uint32_t c[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
-            uint64_t off = ptr_off(p[k]), deg = ptr_size(p[k]);
-            if (off + deg > a.store.n_edges) {
-                if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
-                deg = 0;
-            }
+            uint64_t off, deg;
+            list_of_ptr(p[k], a.store.n_edges, &a.ctl->err, &off, &deg);
             if (d.op == kXI2K && valid[k]) {   // index_to_known reads its mt slice of the list
                 uint64_t s_lo, s_hi;
                 mt_slice(d.mt, deg, &s_lo, &s_hi);
                 off += s_lo;
                 deg = s_hi - s_lo;
-            } else if (deg == 1 && inl[k]) {
-                off = inl[k];   // the entry was in the bucket's sector
             }
             c[k] = (uint32_t)deg;
             if (kFilter && valid[k] && deg) {
@@ -523,21 +511,13 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_ker
             const uint32_t op = d->op;
             uint64_t off = 0, deg = 0;
             if (look[k]) {
-                uint64_t inl = 0;
-                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err, &inl);
-                off = ptr_off(p);
-                deg = ptr_size(p);
-                if (off + deg > a.store.n_edges) {
-                    if (deg) atomicOr(&a.ctl->err, kErrCorrupt);
-                    deg = 0;
-                }
+                const uint64_t p = settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err);
+                list_of_ptr(p, a.store.n_edges, &a.ctl->err, &off, &deg);
                 if (op == kXI2K) {
                     uint64_t s_lo, s_hi;
                     mt_slice(d->mt, deg, &s_lo, &s_hi);
                     off += s_lo;
                     deg = s_hi - s_lo;
-                } else if (deg == 1 && inl) {
-                    off = inl;   // the entry was in the bucket's sector
                 }
             }
             const bool filt = is_filter_op(op);

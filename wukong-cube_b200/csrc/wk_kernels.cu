@@ -23,12 +23,8 @@ __global__ void list_kernel(const ListArgs a) {
         if (threadIdx.x == 0) s_ptr = ptr[0];
     }
     __syncthreads();
-    const uint64_t off = ptr_off(s_ptr);
-    uint64_t sz = ptr_size(s_ptr);
-    if (off + sz > a.store.n_edges) {
-        if (blockIdx.x == 0 && threadIdx.x == 0 && sz) atomicOr(&a.ctl->err, kErrCorrupt);
-        sz = 0;
-    }
+    uint64_t off, sz;
+    list_of_ptr(s_ptr, a.store.n_edges, &a.ctl->err, &off, &sz);
     // mt_factor slice (sparql.hpp:213-224)
     const uint64_t f = a.mt_factor > 0 ? (uint64_t)a.mt_factor : 1;
     const uint64_t start = (uint64_t)a.mt_tid % f, len = sz / f;
@@ -45,6 +41,10 @@ __global__ void list_kernel(const ListArgs a) {
         }
     }
     if (n > a.out_cap) return;
+    if (off & kInlineTag) {   // a one-entry list kept in its key's slot
+        if (n && blockIdx.x == 0 && threadIdx.x == 0) a.out[0] = (uint32_t)off;
+        return;
+    }
     // grid-stride copy, eight loads in flight per thread before their stores (the list starts
     // at any word, so the words are moved one by one; each warp access is 128 contiguous bytes)
     const uint32_t* srcp = a.store.edges + off + b;
@@ -72,6 +72,7 @@ __global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const u
         if ((i & (kAssoc - 1)) == kAssoc - 1) continue;   // chain link
         const Slot s = slots[i];
         if (s.key == 0) continue;
+        if (ptr_is_inline(s.ptr)) continue;   // a one-entry list (none before inline_kernel)
         const uint64_t off = ptr_off(s.ptr), sz = ptr_size(s.ptr);
         if (off + sz > n_edges) {
             if (lane == 0) atomicOr(unsorted, 2u);
@@ -83,17 +84,26 @@ __global__ void sorted_check_kernel(const Slot* slots, uint64_t n_slots, const u
     }
 }
 
-// The single-entry lists of keys alone in their bucket, copied into the bucket (slot 1's
-// pointer word, tagged; see kInlineTag).  Slot 1's pointer word is cleared where no entry goes
-// there, so a store adopted twice carries no stale entry.
-__global__ void inline_kernel(Slot* slots, uint64_t n_buckets, const uint32_t* edges, uint64_t n_edges) {
+// One-entry lists into their keys' own pointer words (see kInlinePtrType): for every data slot
+// (slots 0-6) whose list has one entry, the original pointer word goes to the side table
+// `orig` (slot index, pointer word; wk_store_export puts them back) and the slot's pointer word
+// becomes the entry with the inline type.  With orig null the kernel only counts such slots
+// (into *n) and whether any pointer word already carries type 3 (into *clash; the store is then
+// refused, since that type cannot be told apart).
+__global__ void inline_kernel(Slot* slots, uint64_t n_slots, const uint32_t* edges, uint64_t n_edges,
+                              unsigned long long* n, unsigned* clash, uint64_t* orig) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < n_buckets; b += stride) {
-        Slot* bk = slots + b * kAssoc;
-        const uint64_t k0 = bk[0].key, p0 = bk[0].ptr, k1 = bk[1].key;
-        if (k1 != 0) continue;
-        const uint64_t off = ptr_off(p0);
-        bk[1].ptr = (k0 != 0 && ptr_size(p0) == 1 && off < n_edges) ? (kInlineTag | __ldg(edges + off)) : 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_slots; i += stride) {
+        if ((i & (kAssoc - 1)) == kAssoc - 1) continue;   // chain link
+        const Slot sl = slots[i];
+        if (sl.key == 0) continue;
+        if (!orig && ptr_is_inline(sl.ptr)) atomicOr(clash, 1u);
+        if ((sl.ptr >> 62) != 0 || ptr_size(sl.ptr) != 1 || ptr_off(sl.ptr) >= n_edges) continue;
+        const unsigned long long at = atomicAdd(n, 1ull);
+        if (!orig) continue;
+        orig[2 * at] = i;
+        orig[2 * at + 1] = sl.ptr;
+        slots[i].ptr = make_inline_ptr(__ldg(edges + ptr_off(sl.ptr)));
     }
 }
 
@@ -138,9 +148,11 @@ cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream
     return cudaGetLastError();
 }
 
-cudaError_t launch_inline(const DevStore& st, cudaStream_t s) {
+cudaError_t launch_inline(const DevStore& st, unsigned long long* n, unsigned* clash, uint64_t* orig,
+                          cudaStream_t s) {
     if (st.n_buckets)
-        inline_kernel<<<4096, 256, 0, s>>>(const_cast<Slot*>(st.slots), st.n_buckets, st.edges, st.n_edges);
+        inline_kernel<<<4096, 256, 0, s>>>(const_cast<Slot*>(st.slots), st.n_buckets * kAssoc, st.edges, st.n_edges,
+                                           n, clash, orig);
     return cudaGetLastError();
 }
 

@@ -61,9 +61,12 @@ constexpr int kTileRows = 256;
 
 cudaError_t launch_list(const ListArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_sorted_check(const DevStore& st, unsigned* d_flag, cudaStream_t s);
-// Copies single-entry lists of keys alone in their bucket into the bucket (kInlineTag); writes
-// the slot array.
-cudaError_t launch_inline(const DevStore& st, cudaStream_t s);
+// One-entry lists into their keys' pointer words (inline_kernel): with orig null, counts them
+// into *n and flags pointer words that already carry the inline type in *clash; with orig (two
+// words per counted slot), converts them and keeps the original pointer words there.  *n must
+// be 0 on entry.
+cudaError_t launch_inline(const DevStore& st, unsigned long long* n, unsigned* clash, uint64_t* orig,
+                          cudaStream_t s);
 // `grid` CTAs of 256 threads, `per` random 16-byte reads each from a `bytes`-byte buffer.
 cudaError_t launch_random_reads(const void* buf, uint64_t bytes, int per, uint64_t seed,
                                 uint32_t* sink, int grid, cudaStream_t s);

@@ -56,12 +56,7 @@ __device__ __forceinline__ void list_of(const VersArgs& a, uint64_t vid, uint32_
     const uint64_t key = make_key(vid, pid, a.dir);
     if (sg.num_buckets == 0 || key == 0) return;
     const uint64_t p = thread_probe(a.store, key, bucket_of(key, sg), &a.ctl->err);
-    *off = ptr_off(p);
-    *deg = ptr_size(p);
-    if (*off + *deg > a.store.n_edges) {
-        if (*deg) atomicOr(&a.ctl->err, kErrCorrupt);
-        *deg = 0;
-    }
+    list_of_ptr(p, a.store.n_edges, &a.ctl->err, off, deg);   // *off may be a tagged entry
 }
 
 __device__ __forceinline__ uint32_t row_start(const VersArgs& a, uint64_t r) {
@@ -76,7 +71,7 @@ __device__ uint64_t walk_row(const VersArgs& a, uint64_t r, uint32_t cur, bool w
     list_of(a, cur, kPredicateId, a.vp_seg, &poff, &npred);
     uint64_t n = 0;
     for (uint64_t k = 0; k < npred; ++k) {
-        const uint32_t p = __ldg(a.store.edges + poff + k);
+        const uint32_t p = list_at(a.store.edges, poff, k);
         SegDesc sg;
         if (!pred_seg(a, p, a.dir, &sg)) continue;
         uint64_t off, deg;
@@ -97,7 +92,7 @@ __device__ uint64_t walk_row(const VersArgs& a, uint64_t r, uint32_t cur, bool w
                     uint32_t* dst = a.out + (at + n + j) * (uint64_t)a.w_out;
                     for (int c = 0; c < a.cin; ++c) dst[c] = __ldg(src + c);
                     dst[a.cin] = p;
-                    dst[a.cin + 1] = __ldg(a.store.edges + off + j);
+                    dst[a.cin + 1] = list_at(a.store.edges, off, j);
                 }
             }
             n += deg;
