@@ -490,18 +490,20 @@ def run_ours(args, world, rank, local_rank):
     pin = wk.Table(ctx, max(star_table.size, 1))
     pin.upload(star_table)
     keep = [star_v2c[1], star_v2c[0]]
+    pout = pin.final_process(keep, distinct=True)   # warm: the output table and scratch grow once
     pp_ms = []
-    for _ in range(3):
+    for _ in range(5):
         t0 = time.perf_counter()
-        pout = pin.final_process(keep, distinct=True)
+        pin.final_process(keep, distinct=True, out=pout)
         pp_ms.append((time.perf_counter() - t0) * 1000)
-        pp_rows = pout.shape()[0]
-        pout.free()
+    pp_rows = pout.shape()[0]
+    pout.free()
     pin.free()
     post_pattern = {"op": "DISTINCT on two of the heavy star's three columns (wk_table_final_process)",
                     "rows_in": int(star_table.shape[0]), "cols_in": int(star_table.shape[1]),
                     "rows_out": int(pp_rows), "ms": statistics.median(pp_ms),
-                    "timing": "host clock around the call, which ends with a device sync"}
+                    "timing": "host clock around the call (it ends with a device sync), median of 5 "
+                              "after a warm call, output table reused"}
 
     # ---- serving: open-loop Poisson sweep, 98 % light / 2 % heavy, blind replies
     serving = None

@@ -117,6 +117,21 @@ int wk_ctx::ensure_flat(uint64_t in_rows_cap) {
     return WK_SUCCESS;
 }
 
+int wk_ctx::final_scratch_reserve(size_t bytes) {
+    if (bytes <= final_scratch_bytes) return WK_SUCCESS;
+    WK_CUDA(this, cudaStreamSynchronize(stream));
+    if (d_final_scratch) cudaFree(d_final_scratch);
+    d_final_scratch = nullptr;
+    final_scratch_bytes = 0;
+    const size_t cap = bytes + bytes / 4;
+    if (wk::dev_malloc(&d_final_scratch, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WK_E_OOM, "post-pattern scratch");
+    }
+    final_scratch_bytes = cap;
+    return WK_SUCCESS;
+}
+
 int wk_ctx::ensure_status(uint64_t tiles) {
     if (tiles <= status_cap) return WK_SUCCESS;
     uint64_t cap = std::max<uint64_t>(tiles + tiles / 2, 1 << 14);
@@ -622,6 +637,7 @@ extern "C" int wk_ctx_destroy(wk_ctx* ctx) {
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_heavy) cudaFree(ctx->d_heavy);
     if (ctx->d_flat) cudaFree(ctx->d_flat);
+    if (ctx->d_final_scratch) cudaFree(ctx->d_final_scratch);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_rows) cudaFreeHost(ctx->h_rows);

@@ -110,6 +110,8 @@ struct wk_ctx {
     uint64_t flat_min_rows = 65536;
     void* d_flat = nullptr;          // its scratch (wk_flat.h)
     uint64_t flat_cap_rows = 0;
+    void* d_final_scratch = nullptr;   // scratch of the post-pattern stage and the BOUND filter
+    size_t final_scratch_bytes = 0;
 
     // scan control of the context stream
     wk::StepCtl* d_ctl = nullptr;
@@ -176,6 +178,7 @@ struct wk_ctx {
     int ensure_status(uint64_t tiles);
     int ensure_heavy(uint64_t out_rows_cap);
     int ensure_flat(uint64_t in_rows_cap);
+    int final_scratch_reserve(size_t bytes);
     int table_reserve(wk_table* t, uint64_t elems);
     int read_ctl(uint32_t* err, uint64_t* need);
     int clear_ctl_err();

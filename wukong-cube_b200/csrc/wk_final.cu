@@ -424,14 +424,13 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     const size_t key_bytes = sort ? 2 * (size_t)n * 8 : 0;
     const size_t bytes = keep_bytes + idx_bytes + key_bytes + (size_t)kDigits * grid * 4 +
                          ((size_t)grid + 2) * 4 + (size_t)cols * 8 + 64;
-    char* scratch = nullptr;
-    if (wk::dev_malloc(&scratch, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return ctx->fail(WK_E_OOM, "post-pattern scratch");
-    }
+    // the context keeps the scratch between calls (grown, never shrunk): an allocation and a
+    // cudaFree per call would cost more than the stage's own kernels
+    int src = ctx->final_scratch_reserve(bytes);
+    if (src) return src;
+    char* scratch = static_cast<char*>(ctx->d_final_scratch);
     auto done = [&](int rc) {
         cudaStreamSynchronize(s);
-        cudaFree(scratch);
         return rc;
     };
     int32_t* d_keep = reinterpret_cast<int32_t*>(scratch);
@@ -566,14 +565,11 @@ extern "C" int wk_table_filter_bound(wk_ctx* ctx, const wk_table* in, const int3
     const uint32_t n = (uint32_t)R;
     const int grid = std::max(1, std::min<int>(ctx->sm_count * 4, (int)((n + 2047) / 2048)));
     const size_t bytes = 256 + ((size_t)grid + 2) * 4 + 64;
-    char* scratch = nullptr;
-    if (wk::dev_malloc(&scratch, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return ctx->fail(WK_E_OOM, "filter scratch");
-    }
+    int src = ctx->final_scratch_reserve(bytes);
+    if (src) return src;
+    char* scratch = static_cast<char*>(ctx->d_final_scratch);
     auto done = [&](int code) {
         cudaStreamSynchronize(s);
-        cudaFree(scratch);
         return code;
     };
     int32_t* d_cols = reinterpret_cast<int32_t*>(scratch);

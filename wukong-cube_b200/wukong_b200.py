@@ -451,9 +451,10 @@ class Table:
         _check(lib().wk_table_download(self.ctx.h, self.h, _ptr(out), out.size), self.ctx.h)
         return out[:rows * cols].reshape(rows, cols)
 
-    def final_process(self, keep_cols, distinct=False, offset=0, limit=-1):
-        """The post-pattern stage on the device (wk_table_final_process) into a new Table."""
-        out = Table(self.ctx)
+    def final_process(self, keep_cols, distinct=False, offset=0, limit=-1, out=None):
+        """The post-pattern stage on the device (wk_table_final_process) into `out` (a new Table
+        when None; an existing one is reused, grown when needed)."""
+        out = out if out is not None else Table(self.ctx)
         keep = (C.c_int32 * max(len(keep_cols), 1))(*[int(c) for c in keep_cols])
         _check(lib().wk_table_final_process(self.ctx.h, self.h, keep, len(keep_cols),
                                             1 if distinct else 0, offset, limit, out.h), self.ctx.h)
