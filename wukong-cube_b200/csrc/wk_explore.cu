@@ -212,14 +212,15 @@ __device__ __forceinline__ void row_setup(const ExploreArgs& a, const TileBuf& B
 // A row's count and list offset (an edge-array offset or a tagged single entry) once its list
 // is known (filters test membership of the target): written to B.cnt / B.off, bytes added to
 // the accounting.
-__device__ __forceinline__ uint32_t row_count(const ExploreArgs& a, const TileBuf& B, int row, uint32_t flag,
-                                              uint64_t off, uint64_t deg, bool found, unsigned long long& acc_alg,
-                                              unsigned long long& acc_sd) {
+__device__ __forceinline__ uint32_t row_count(const ExploreArgs& a, const TileBuf& B, TileState& S, int row,
+                                              uint32_t flag, uint64_t off, uint64_t deg, bool found,
+                                              unsigned long long& acc_alg, unsigned long long& acc_sd) {
     const uint32_t op = flag & 0xFFu;
     const bool filt = is_filter_op(op);
     const uint32_t cnt = filt ? (found ? 1u : 0u) : (uint32_t)deg;
     B.off[row] = off;
     B.cnt[row] = cnt;
+    if (cnt > slice_threshold(a)) S.has_heavy = 1;   // its rows go to the slice queue
     // byte accounting, kept in registers until the CTA leaves
     acc_sd += deg;
     acc_alg += ((flag >> 16) & 0xFF) * 4ull + 16 + deg * 4 + (unsigned long long)cnt * (flag >> 24) * 4;
@@ -230,7 +231,7 @@ __device__ __forceinline__ uint32_t row_count(const ExploreArgs& a, const TileBu
 // home sector (slots 0 and 1, 32 bytes) before comparing any, and walks on from slot 2 only
 // where that sector does not settle the key; filters then search the list themselves.  No
 // ballots or shuffles.
-__device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const TileBuf& B, int n, int wi,
+__device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const TileBuf& B, TileState& S, int n, int wi,
                                                 unsigned long long& acc_alg, unsigned long long& acc_sd) {
     constexpr int kRows = kTileRows / kStepThreads;
     uint64_t key[kRows];
@@ -277,7 +278,7 @@ __device__ __forceinline__ void tile_probe_rows(const ExploreArgs& a, const Tile
         }
         const bool found = is_filter_op(op) && deg &&
                            thread_member(a.store.edges, off, deg, tgt[k], a.sorted_lists != 0);
-        row_count(a, B, row, flag[k], off, deg, found, acc_alg, acc_sd);
+        row_count(a, B, S, row, flag[k], off, deg, found, acc_alg, acc_sd);
     }
 }
 
@@ -306,18 +307,19 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         S.tile = tile;
         S.r0 = r0;
         S.n = n;
-        S.has_heavy = 0;
     }
     for (int i = threadIdx.x; i < n; i += kStepThreads) {
         B.q[i] = a.virtual_rows ? (a.virt_owner ? __ldg(a.virt_owner + r0 + i) : (uint32_t)(r0 + i))
                                 : (a.owner_in ? __ldg(a.owner_in + r0 + i) : 0u);
         B.cnt[i] = 0;
     }
-    __syncthreads();
+    // the one-thread-per-row probe reads only the rows this thread just set up; the group probes
+    // share rows across threads
+    if constexpr (L > 1) __syncthreads();
     // the rows' copy ran alongside the owner loads; read the rows from shared memory
     if (wi) mbar_wait(bar, phase, &a.ctl->err);
     if constexpr (L == 1) {
-        tile_probe_rows(a, B, n, wi, acc_alg, acc_sd);
+        tile_probe_rows(a, B, S, n, wi, acc_alg, acc_sd);
     } else {
     constexpr int kOwn = (kUnroll + L - 1) / L;   // rows of a batch each lane works out
 #pragma unroll 1
@@ -379,16 +381,13 @@ __device__ __forceinline__ void tile_front(const ExploreArgs& a, const TileBuf& 
         if (h == 0) {
 #pragma unroll
             for (int u = 0; u < kUnroll; ++u)
-                if (valid[u]) row_count(a, B, row[u], flag[u], off[u], deg[u], found[u], acc_alg, acc_sd);
+                if (valid[u]) row_count(a, B, S, row[u], flag[u], off[u], deg[u], found[u], acc_alg, acc_sd);
         }
     }
     }
     __syncthreads();
     WK_PH(2);
-    const uint32_t thr = slice_threshold(a);
-    for (int i = threadIdx.x; i < n; i += kStepThreads)
-        if (B.cnt[i] > thr) S.has_heavy = 1;
-    __syncthreads();
+    const uint32_t thr = slice_threshold(a);   // S.has_heavy was set by row_count
     const uint64_t total = block_scan(B.cnt, B.pre, n, s_warp);
     const uint64_t ltotal =
         S.has_heavy ? block_scan(B.cnt, B.lpre, n, s_warp, [thr](uint32_t c) { return (uint64_t)(c > thr ? 0u : c); })
@@ -509,6 +508,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
     if (threadIdx.x == 0) {   // this tile's slices are all reserved
         __threadfence();
         atomicAdd(&a.ctl->tiles_done, 1ull);
+        S.has_heavy = 0;      // the buffer's next tile starts without long lists
     }
     WK_PH(6);
 }
@@ -552,6 +552,7 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
     if (threadIdx.x == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
+        s_ts[0].has_heavy = s_ts[1].has_heavy = 0;   // row_count sets them; tile_back clears them
     }
     unsigned phases = 0;   // mbarrier phase bit of each tile buffer
     unsigned long long acc_alg = 0, acc_sd = 0;   // this thread's share of the byte accounting
