@@ -632,20 +632,35 @@ __global__ void __launch_bounds__(kFlatThreads) flat_level_expand_kernel(const F
         }
         __syncthreads();
         const uint64_t wend = min(j1, s_pos[n]);
-        for (uint64_t jj = j + threadIdx.x; jj < wend; jj += kFlatThreads) {
-            int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+        constexpr int U = 4;   // output rows per thread with their neighbour loads in flight
+        for (uint64_t jb = j + threadIdx.x; jb < wend; jb += (uint64_t)U * kFlatThreads) {
+            int row[U];
+            uint32_t nb[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t jj = jb + (uint64_t)u * kFlatThreads;
+                row[u] = -1;
+                if (jj >= wend) continue;
+                int lo = 0, hi = (int)n;   // last t with s_pos[t] <= jj
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_pos[mid] <= jj) lo = mid; else hi = mid;
+                }
+                if (s_ecol[lo] < 0) continue;   // filters wrote their rows already
+                row[u] = lo;
+                nb[u] = list_at(a.store.edges, s_off[lo], jj - s_pos[lo]);
             }
-            const int ecol = s_ecol[lo];
-            if (ecol < 0) continue;   // filters wrote their rows already
-            const uint64_t r = i + lo;
-            const uint32_t* src = a.in + r * (uint64_t)a.w_in;
-            uint32_t* dst = a.out + jj * (uint64_t)wo;
-            for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
-            dst[ecol] = list_at(a.store.edges, s_off[lo], jj - s_pos[lo]);
-            a.owner_out[jj] = s_q[lo];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (row[u] < 0) continue;
+                const uint64_t jj = jb + (uint64_t)u * kFlatThreads;
+                const int lo = row[u], ecol = s_ecol[lo];
+                const uint32_t* src = a.in + (i + lo) * (uint64_t)a.w_in;
+                uint32_t* dst = a.out + jj * (uint64_t)wo;
+                for (int k = 0; k < ecol; ++k) dst[k] = __ldg(src + k);
+                dst[ecol] = nb[u];
+                a.owner_out[jj] = s_q[lo];
+            }
         }
         j = max(j, wend);
         i += n;
