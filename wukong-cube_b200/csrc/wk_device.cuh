@@ -41,21 +41,6 @@ __device__ __forceinline__ void load_sector(const Slot* p, ulonglong2* s0, ulong
     *s1 = make_ulonglong2(c, d);
 }
 
-// ---------------------------------------------------------------- cp.async gathers
-// One home sector (slots 0 and 1, 32 bytes) copied into shared memory without a register: two
-// 16-byte asynchronous copies.  The copies of a thread are grouped with cp_async_commit and
-// waited for with cp_async_wait<N> (all but the N most recent groups complete).
-__device__ __forceinline__ void cp_async_sector(void* smem_dst, const Slot* src) {
-    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16), "l"(src + 1) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // ---------------------------------------------------------------- mbarrier + TMA bulk copy
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);

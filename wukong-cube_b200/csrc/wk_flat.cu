@@ -157,28 +157,18 @@ __device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key
     return thread_probe(st, key, b, err, 2);
 }
 
-// The count pass gathers home sectors into shared memory with asynchronous copies, so the
-// reads in flight are not bounded by registers: each thread works in rounds of kAsyncRows
-// rows, and the copies of the next round are issued before the current round is compared, so
-// two rounds (2 * kAsyncRows sectors per thread, 6,144 per SM at 2 CTAs of 256 threads) are in
-// flight.  The landing buffers take kCountSmem bytes of dynamic shared memory.  kFilter: the
-// membership steps (known_to_known, known_to_const, const_to_known, index_to_known); the other
-// instance (starts and known_to_unknown) carries no membership search.
-constexpr int kAsyncRows = 6;
-constexpr int kCountCtas = 2;
-constexpr size_t kCountSmem = 2ull * kAsyncRows * kFlatThreads * 32;
-
-// The rows of one round of a count thread: key, home bucket, and valid / look bits.
-struct CountRound {
-    uint64_t key[kAsyncRows];
-    uint64_t bkt[kAsyncRows];
-    uint32_t bits;   // bit k: row k valid; bit 16 + k: row k probed
-};
+// kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
+// loaded before any is compared, and the neighbour words of their one-to-one rows are loaded
+// before any output row is written, so a thread has that many random reads in flight.
+// Registers are capped for kCountCtas CTAs per SM.  kFilter: the membership steps
+// (known_to_known, known_to_const, const_to_known, index_to_known); the other instance (starts
+// and known_to_unknown) carries no membership search.
+constexpr int kRowsPerThread = 3;
+constexpr int kCountCtas = 4;
 
 template <bool kFilter>
 __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(const FlatArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
-    extern __shared__ __align__(16) unsigned char s_land[];
     const uint64_t R = flat_rows(a);
     if (R < a.min_rows) return;
     uint64_t lo, hi;
@@ -189,73 +179,55 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
     uint64_t sum = 0, sd = 0, nvalid = 0;
     bool ones = true;   // every row of this thread has exactly one output row
     const bool spec = R <= a.out_cap_rows;   // output row r exists: one-to-one rows written here
-    constexpr int K = kAsyncRows;
-    constexpr uint64_t kRound = (uint64_t)K * kFlatThreads;
-    const uint64_t rbase = lo + threadIdx.x;   // row k of round i: rbase + i * kRound + k * threads
-    // landing place of row k of a round in buffer `buf`: this thread's 32 bytes
-    auto land = [&](int buf, int k) {
-        return reinterpret_cast<ulonglong2*>(s_land) + ((size_t)(buf * K + k) * kFlatThreads + threadIdx.x) * 2;
-    };
-    // work out a round's keys and start its sector copies
-    auto issue = [&](CountRound& st, uint64_t round, int buf) {
-        st.bits = 0;
+    constexpr int K = kRowsPerThread;
+    constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
+    for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
+        uint64_t key[K], bkt[K], p[K];
+        bool valid[K], look[K];
+        ulonglong2 s0[K], s1[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const uint64_t r = rbase + round * kRound + (uint64_t)k * kFlatThreads;
-            st.key[k] = 0;
-            st.bkt[k] = 0;
-            if (r >= hi) continue;
-            bool valid, look;
-            const uint32_t cur = __ldg(a.in + r * (uint64_t)a.w_in + d.cs);
-            st.key[k] = count_key(a, d, from_const, cur, &valid, &look, &st.bkt[k]);
-            st.bits |= (valid ? 1u << k : 0u) | (look ? 1u << (16 + k) : 0u);
-            if (look) cp_async_sector(land(buf, k), a.store.slots + st.bkt[k] * kAssoc);
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
+            const uint32_t cur = r < hi ? __ldg(a.in + r * (uint64_t)a.w_in + d.cs) : kBlankId;
+            key[k] = count_key(a, d, from_const, cur, &valid[k], &look[k], &bkt[k]);
+            if (r >= hi) valid[k] = look[k] = false;
         }
-    };
-    CountRound cur;
-    if (rbase < hi) issue(cur, 0, 0);
-    cp_async_commit();
-    for (uint64_t round = 0; rbase + round * kRound < hi; ++round) {
-        CountRound nxt;
-        nxt.bits = 0;
-        if (rbase + (round + 1) * kRound < hi) issue(nxt, round + 1, (int)((round + 1) & 1));
-        cp_async_commit();
-        cp_async_wait<1>();   // this round's copies have landed
-        const int buf = (int)(round & 1);
-        uint32_t c[K];
-        uint64_t loff[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const uint64_t r = rbase + round * kRound + (uint64_t)k * kFlatThreads;
-            const bool valid = (cur.bits >> k) & 1u, look = (cur.bits >> (16 + k)) & 1u;
-            uint64_t p = 0;
-            if (look) {
-                const ulonglong2* l = land(buf, k);
-                p = settle_slot(a.store, cur.key[k], cur.bkt[k], l[0], l[1], &a.ctl->err);
-            }
+            s0[k] = s1[k] = make_ulonglong2(0, 0);
+            if (look[k]) load_sector(a.store.slots + bkt[k] * kAssoc, &s0[k], &s1[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            p[k] = look[k] ? settle_slot(a.store, key[k], bkt[k], s0[k], s1[k], &a.ctl->err) : 0;
+        // counts and list offsets
+        uint32_t c[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
             uint64_t off, deg;
-            list_of_ptr(p, a.store.n_edges, &a.ctl->err, &off, &deg);
-            if (d.op == kXI2K && valid) {   // index_to_known reads its mt slice of the list
+            list_of_ptr(p[k], a.store.n_edges, &a.ctl->err, &off, &deg);
+            if (d.op == kXI2K && valid[k]) {   // index_to_known reads its mt slice of the list
                 uint64_t s_lo, s_hi;
                 mt_slice(d.mt, deg, &s_lo, &s_hi);
                 off += s_lo;
                 deg = s_hi - s_lo;
             }
             c[k] = (uint32_t)deg;
-            if (kFilter && valid && deg) {
+            if (kFilter && valid[k] && deg) {
                 // the membership target shares the row's sector with its start column
                 const uint32_t target = tcol >= 0 ? __ldg(a.in + r * (uint64_t)a.w_in + tcol) : d.end_const;
                 c[k] = thread_member(a.store.edges, off, deg, target, a.sorted_lists != 0) ? 1u : 0u;
             }
-            if (!valid) c[k] = 0;
-            loff[k] = off;
+            if (!valid[k]) c[k] = 0;
+            p[k] = off;   // from here on p holds the list offset
             if (r < hi) {
                 a.pos[r] = c[k];   // the count; flat_place_kernel turns it into the row's position
                 if (!kFilter) a.off[r] = off;
                 if (c[k] != 1) ones = false;
                 sum += c[k];
             }
-            if (valid) {
+            if (valid[k]) {
                 sd += deg;
                 ++nvalid;
             }
@@ -264,23 +236,21 @@ __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(co
             // A row with exactly one output row writes it now, at output row r: when every row
             // has one (a functional predicate), that is the step's output and the place and
             // expand passes return at once; otherwise expand overwrites these rows.  The rows'
-            // neighbour words are all loaded (or taken from their slots) before any is written.
+            // neighbour words are all loaded before any row is written.
             uint32_t nb[K];
 #pragma unroll
-            for (int k = 0; k < K; ++k) nb[k] = c[k] == 1 ? list_at(a.store.edges, loff[k], 0) : 0;
+            for (int k = 0; k < K; ++k) nb[k] = c[k] == 1 ? list_at(a.store.edges, p[k], 0) : 0;
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 if (c[k] != 1) continue;
-                const uint64_t r = rbase + round * kRound + (uint64_t)k * kFlatThreads;
+                const uint64_t r = r0 + (uint64_t)k * kFlatThreads;
                 const uint32_t* src = a.in + r * (uint64_t)a.w_in;
                 uint32_t* dst = a.out + r * (uint64_t)a.w_out;
                 for (int j = 0; j < d.cin; ++j) dst[j] = __ldg(src + j);
                 dst[d.cin] = nb[k];
             }
         }
-        cur = nxt;
     }
-    cp_async_wait<0>();
     const bool all_ones = __syncthreads_and(ones);
     sum = block_sum(sum, s_warp);
     sd = block_sum(sd, s_warp);
@@ -472,16 +442,15 @@ __device__ void flat_level_scan_parts(const FlatLevelArgs& a, uint32_t nparts, u
     }
 }
 
-// kLevelRows rows per thread at a time, their home sectors loaded before any is compared.
-constexpr int kLevelRows = 3;
-constexpr int kLevelCountCtas = 4;
-__global__ void __launch_bounds__(kFlatThreads, kLevelCountCtas) flat_level_count_kernel(const FlatLevelArgs a) {
+// kRowsPerThread rows per thread at a time, their home slots loaded before any is compared (as
+// in flat_count_kernel).
+__global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_level_count_kernel(const FlatLevelArgs a) {
     __shared__ uint64_t s_warp[kFlatThreads / 32];
     const uint64_t R = level_rows(a);
     uint64_t lo, hi;
     chunk_of(R, &lo, &hi);
     uint64_t sum = 0, sd = 0, alg = 0;
-    constexpr int K = kLevelRows;
+    constexpr int K = kRowsPerThread;
     constexpr uint64_t kStride = (uint64_t)K * kFlatThreads;
     for (uint64_t r0 = lo + threadIdx.x; r0 < hi; r0 += kStride) {
         uint64_t key[K], bkt[K];
@@ -712,16 +681,16 @@ int flat_grid_beside(int sm_count, const CtaUse& other, int other_ctas) {
     int dev = 0, reserved = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-    CtaUse me{(size_t)std::max(fa.sharedSizeBytes, fb.sharedSizeBytes) + kCountSmem + (size_t)reserved,
+    CtaUse me{(size_t)std::max(fa.sharedSizeBytes, fb.sharedSizeBytes) + (size_t)reserved,
               ((regs * 32 + 255) / 256) * 256 * (kFlatThreads / 32), kFlatThreads};
-    const int alone = kCountCtas;
+    const int alone = 2048 / kFlatThreads;
     return blocks_beside(me, alone, other, other_ctas) * sm_count;
 }
 
 cudaError_t launch_flat(const FlatArgs& a, int grid, cudaStream_t s) {
     // its last CTA scans the totals
-    if (is_filter_op(a.step.op)) flat_count_kernel<true><<<grid, kFlatThreads, kCountSmem, s>>>(a);
-    else flat_count_kernel<false><<<grid, kFlatThreads, kCountSmem, s>>>(a);
+    if (is_filter_op(a.step.op)) flat_count_kernel<true><<<grid, kFlatThreads, 0, s>>>(a);
+    else flat_count_kernel<false><<<grid, kFlatThreads, 0, s>>>(a);
     flat_place_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     if (a.step.op == kXK2U) flat_expand_kernel<<<grid, kFlatThreads, 0, s>>>(a, (uint32_t)grid);
     return cudaGetLastError();
@@ -738,12 +707,6 @@ cudaError_t flat_kernel_attrs() {
     cudaError_t e;
     if ((e = use_max_shared_carveout(flat_count_kernel<true>)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_count_kernel<false>)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(flat_count_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kCountSmem)) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(flat_count_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kCountSmem)) != cudaSuccess)
-        return e;
     if ((e = use_max_shared_carveout(flat_place_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_expand_kernel)) != cudaSuccess) return e;
     if ((e = use_max_shared_carveout(flat_level_count_kernel)) != cudaSuccess) return e;
