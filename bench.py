@@ -777,7 +777,7 @@ def main():
     ap.add_argument("--scale-check", type=int, default=0,
                     help="with --device-store: light queries checked against the reference "
                          "engine over the exported store (needs host memory for the store)")
-    ap.add_argument("--serve-lanes", type=int, default=4,
+    ap.add_argument("--serve-lanes", type=int, default=1,
                     help="serving: index-start queries running at once, one lane each")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -146,7 +146,7 @@ typedef struct wk_serve_config {
                                          (0: the largest projection among the run's index-start
                                          queries, at most 1 GiB) */
     uint32_t max_inflight;            /* constant-start queries resident at once (default 65536) */
-    uint32_t max_heavy_inflight;      /* index-start queries running at once (default 4); each
+    uint32_t max_heavy_inflight;      /* index-start queries running at once (default 1); each
                                          runs whole on its own lane: a stream of the lowest
                                          priority with its own tables, beside the iterations */
     int32_t light_ctas_per_sm;        /* exploration CTAs per SM of the iteration launches; the

@@ -471,7 +471,7 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
     if (!S.cfg.arena_bytes) S.cfg.arena_bytes = 1ull << 30;
     if (!S.cfg.min_proj_bytes) S.cfg.min_proj_bytes = 64ull << 10;
     if (!S.cfg.max_inflight) S.cfg.max_inflight = 65536;
-    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 4;
+    if (!S.cfg.max_heavy_inflight) S.cfg.max_heavy_inflight = 1;
     if (S.cfg.light_ctas_per_sm <= 0) S.cfg.light_ctas_per_sm = 2;
 
     // Resolve every plan once (the same dispatch as a single query).
