@@ -45,10 +45,11 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
-# 16,384-query batch on the 10,000-organisation graph: 110,025,216 B + 9,299,456 B for
-# 2,560,041 input rows, with the knobs the autotuner picks here (2 lanes, 32-row slices, flat
-# passes for levels 0 and 1).
-LEVEL_TRAFFIC_PER_ROW = (110025216 + 9299456) / 2560041
+# 16,384-query batch on the 1,000-organisation graph: 102,455,040 B + 18,419,712 B for
+# 2,617,493 input rows, with the knobs the autotuner picks (one thread per row, 32-row slices,
+# flat passes for levels 0 and 1).  Scaled by the dominant level's input rows; on the larger
+# graph fewer sectors hit in L2, so the scaled figure is a lower bound there.
+LEVEL_TRAFFIC_PER_ROW = (102455040 + 18419712) / 2617493
 
 
 def peaks():
@@ -571,8 +572,8 @@ def run_ours(args, world, rank, local_rank):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                                           "this level in a replay of the same batch (1 pass; "
-                                           "46.6 B per input row) x this launch's input rows",
+                                           "batch level 3 on the 1,000-organisation graph (1 pass; "
+                                           "46.2 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": dom_kernel,
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
