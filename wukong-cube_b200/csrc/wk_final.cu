@@ -180,7 +180,9 @@ __global__ void __launch_bounds__(kDigits) digit_offsets_kernel(uint32_t* hist, 
 // order.  Within a round, an element's rank among the lanes with its digit comes from a match,
 // and the warp's running count of each digit (shared memory, updated by one lane per digit)
 // gives its place in the warp; one barrier then turns the warps' counts into per-warp digit
-// offsets, and the element goes to its digit's running offset + its warp's offset + its place.
+// offsets.  The tile is placed in shared memory sorted by digit (stable), and then written out
+// in that order, consecutive threads on consecutive elements, so each digit's run goes to
+// global memory in contiguous, coalesced stores.
 constexpr int kScatterPer = 8;                                // elements per thread per tile
 constexpr int kScatterTile = kFinThreads * kScatterPer;       // 2,048
 
@@ -188,6 +190,10 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
     constexpr int kWarps = kFinThreads / 32;
     __shared__ uint32_t s_run[kDigits];
     __shared__ uint32_t s_cnt[kWarps][kDigits];
+    __shared__ uint32_t s_tbase[kDigits];
+    __shared__ unsigned long long s_key[kScatterTile];
+    __shared__ uint32_t s_idx[kScatterTile];
+    __shared__ uint64_t s_warp[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     s_run[threadIdx.x] = a.hist[threadIdx.x * gridDim.x + blockIdx.x];
     uint32_t lo, hi;
@@ -223,13 +229,26 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
             s_cnt[w][threadIdx.x] = tile_cnt;
             tile_cnt += c;
         }
+        // the tile sorted by digit in shared memory: digit d's elements start at s_tbase[d]
+        const uint32_t tbase = (uint32_t)block_exclusive_sum<kFinThreads>(tile_cnt, s_warp);
+        s_tbase[threadIdx.x] = tbase;
         __syncthreads();
 #pragma unroll
         for (int r = 0; r < kScatterPer; ++r) {
             if (dg[r] >= kDigits) continue;
-            const uint32_t pos = s_run[dg[r]] + s_cnt[warp][dg[r]] + at[r];
-            a.key_out[pos] = key[r];
-            a.idx_out[pos] = row[r];
+            const uint32_t lp = s_tbase[dg[r]] + s_cnt[warp][dg[r]] + at[r];
+            s_key[lp] = key[r];
+            s_idx[lp] = row[r];
+        }
+        __syncthreads();
+        // consecutive threads write consecutive elements: each digit's run goes out contiguous
+        const uint32_t m = min((uint32_t)kScatterTile, hi - base);
+        for (uint32_t j = threadIdx.x; j < m; j += kFinThreads) {
+            const unsigned long long k = s_key[j];
+            const uint32_t d = (uint32_t)(k >> a.shift) & 0xFFu;
+            const uint32_t pos = s_run[d] + (j - s_tbase[d]);
+            a.key_out[pos] = k;
+            a.idx_out[pos] = s_idx[j];
         }
         __syncthreads();
         s_run[threadIdx.x] += tile_cnt;
