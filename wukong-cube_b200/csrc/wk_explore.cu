@@ -583,74 +583,71 @@ __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_k
     }
 
     // Out of tiles: write queued long-list slices until every tile is done and the queue is
-    // drained, each warp on its own (a slice is often a few dozen rows, too few for a whole
-    // CTA).  A claimed index either gets reserved by a tile still running (wait for its tag)
-    // or lies past the final count (stop).  Every wait is bounded.
-    {
-        const int lane = threadIdx.x & 31;
-        for (;;) {
-            unsigned long long idx = 0;
+    // drained.  A claimed index either gets reserved by a tile still running (wait for its
+    // tag) or lies past the final count (stop).  Every wait is bounded.
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long idx = atomicAdd(&a.ctl->heavy_claim, 1ull);
             int state = 0;
-            if (lane == 0) {
-                idx = atomicAdd(&a.ctl->heavy_claim, 1ull);
-                unsigned long long spins = 0;
-                for (;;) {
-                    unsigned long long hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
-                    if (idx < hn) {
-                        if (idx >= a.heavy_cap) {
-                            state = 2;   // the queue overflowed; kErrOverflow is already set
-                            break;
-                        }
-                        if (*(volatile uint32_t*)&a.heavy[idx].tag == epoch) {
-                            __threadfence();
-                            state = 1;
-                            break;
-                        }
-                    } else if (*(volatile unsigned long long*)&a.ctl->tiles_done >= ntiles) {
-                        __threadfence();
-                        hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
-                        if (idx >= hn) {
-                            state = 2;
-                            break;
-                        }
-                        continue;
+            unsigned long long spins = 0;
+            for (;;) {
+                unsigned long long hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
+                if (idx < hn) {
+                    if (idx >= a.heavy_cap) {
+                        state = 2;   // the queue overflowed; kErrOverflow is already set
+                        break;
                     }
-                    if (++spins > spin_limit(a)) {
-                        atomicOr(&a.ctl->err, kErrTimeout);
+                    if (*(volatile uint32_t*)&a.heavy[idx].tag == epoch) {
+                        __threadfence();
+                        state = 1;
+                        break;
+                    }
+                } else if (*(volatile unsigned long long*)&a.ctl->tiles_done >= ntiles) {
+                    __threadfence();
+                    hn = *(volatile unsigned long long*)&a.ctl->heavy_n;
+                    if (idx >= hn) {
                         state = 2;
                         break;
                     }
-                    if (spins > 32) __nanosleep(64);
+                    continue;
                 }
+                if (++spins > spin_limit(a)) {
+                    atomicOr(&a.ctl->err, kErrTimeout);
+                    state = 2;
+                    break;
+                }
+                if (spins > 32) __nanosleep(64);
             }
-            state = __shfl_sync(kFull, state, 0);
-            idx = __shfl_sync(kFull, idx, 0);
-            if (state != 1) break;
-            const HeavyItem* it = a.heavy + idx;
-            const uint64_t in_row = __ldcg((const unsigned long long*)&it->in_row);
-            const uint64_t off = __ldcg((const unsigned long long*)&it->off);
-            const uint64_t out_pos = __ldcg((const unsigned long long*)&it->out_pos);
-            const uint32_t count = __ldcg((const unsigned int*)&it->count);
-            const uint32_t q = __ldcg((const unsigned int*)&it->q);
-            const StepDesc* d = step_desc(a, q);
-            const int opv = d->op, cin = d->cin;
-            const uint32_t* src = a.in + in_row * (uint64_t)a.w_in;   // the row's columns: L1 hits
-            const int ecol = opv == kXStart ? 0 : cin;
-            const uint64_t ne = (uint64_t)count * wo;
-            uint32_t* dst = a.out + out_pos * wo;
-            for (uint64_t e = lane; e < ne; e += 32) {
-                const uint64_t j = e / wo;
-                const int c = (int)(e - j * wo);
-                uint32_t v = 0;
-                if (c < ecol) v = __ldg(src + c);
-                else if (c == ecol) v = __ldg(a.store.edges + off + j);
-                dst[e] = v;
-            }
-            if (a.owner_out)
-                for (uint32_t j = lane; j < count; j += 32) a.owner_out[out_pos + j] = q;
+            s_claim = state == 1 ? idx : ~0ull;
         }
+        __syncthreads();
+        const unsigned long long idx = s_claim;
+        if (idx == ~0ull) break;
+        const HeavyItem* it = a.heavy + idx;
+        const uint64_t in_row = __ldcg((const unsigned long long*)&it->in_row);
+        const uint64_t off = __ldcg((const unsigned long long*)&it->off);
+        const uint64_t out_pos = __ldcg((const unsigned long long*)&it->out_pos);
+        const uint32_t count = __ldcg((const unsigned int*)&it->count);
+        const uint32_t q = __ldcg((const unsigned int*)&it->q);
+        const StepDesc* d = step_desc(a, q);
+        const int opv = d->op, cin = d->cin;
+        const uint32_t* src = a.in + in_row * (uint64_t)a.w_in;   // the row's columns: L1 hits
+        const int ecol = opv == kXStart ? 0 : cin;
+        const uint64_t ne = (uint64_t)count * wo;
+        uint32_t* dst = a.out + out_pos * wo;
+        for (uint64_t e = threadIdx.x; e < ne; e += kStepThreads) {
+            const uint64_t j = e / wo;
+            const int c = (int)(e - j * wo);
+            uint32_t v = 0;
+            if (c < ecol) v = __ldg(src + c);
+            else if (c == ecol) v = __ldg(a.store.edges + off + j);
+            dst[e] = v;
+        }
+        if (a.owner_out)
+            for (uint32_t j = threadIdx.x; j < count; j += kStepThreads) a.owner_out[out_pos + j] = q;
+        __syncthreads();
     }
-    __syncthreads();
     WK_PH(7);
     WK_PH_FLUSH;
 #pragma unroll
