@@ -488,11 +488,22 @@ using wk::KeyRec;
         if (e_ != cudaSuccess) return (ctx)->cuda_fail(e_, #call); \
     } while (0)
 
-// Device buffers of one build, freed together.
+// Device buffers of one build, freed together at the end, or one by one (release) as soon as
+// nothing reads them any more, so the build's peak stays within the device at a billion keys.
 struct Bufs {
     std::vector<void*> ptrs;
     ~Bufs() {
         for (void* p : ptrs) cudaFree(p);
+    }
+    // Frees p (one of this set's buffers; cudaFree waits for the work that may still read it).
+    void release(const void* p) {
+        if (!p) return;
+        for (size_t i = 0; i < ptrs.size(); ++i)
+            if (ptrs[i] == p) {
+                cudaFree(ptrs[i]);
+                ptrs.erase(ptrs.begin() + i);
+                return;
+            }
     }
     template <class T>
     bool get(T** p, uint64_t n) {
@@ -600,8 +611,8 @@ int group_starts(Builder& bd, unsigned long long* key, uint32_t* pred, uint64_t 
     if (rc) return rc;
     item_lo.resize(g);
     cudaError_t e = cudaMemcpyAsync(item_lo.data(), pos, g * 8, cudaMemcpyDeviceToHost, bd.s);
+    uint64_t* kk = nullptr;
     if (e == cudaSuccess && kstart) {
-        uint64_t* kk = nullptr;
         if (!bd.B.get(&kk, g)) return bd.ctx->fail(WK_E_OOM, "store build groups");
         wk::key_of_item_kernel<<<(int)std::min<uint64_t>((g + 255) / 256, 1024), 256, 0, bd.s>>>(kstart, nkeys, pos,
                                                                                              g, kk);
@@ -609,7 +620,24 @@ int group_starts(Builder& bd, unsigned long long* key, uint32_t* pred, uint64_t 
         e = cudaMemcpyAsync(key_lo.data(), kk, g * 8, cudaMemcpyDeviceToHost, bd.s);
     }
     if (e != cudaSuccess) return bd.ctx->cuda_fail(e, "store build groups");
-    return bd.sync();
+    rc = bd.sync();
+    bd.B.release(pos);   // room for every item, of which a few were used
+    bd.B.release(kk);
+    return rc;
+}
+
+// The first n words of `p` (a buffer of this build) moved to a buffer of exactly n words; p is
+// freed.  For the arrays whose length is only known once a compaction has filled them.
+template <class T>
+int shrink_to(Builder& bd, T** p, uint64_t n, const char* what) {
+    T* q = nullptr;
+    if (!bd.B.get(&q, n)) return bd.ctx->fail(WK_E_OOM, what);
+    cudaError_t e = cudaMemcpyAsync(q, *p, std::max<uint64_t>(n, 1) * sizeof(T), cudaMemcpyDeviceToDevice, bd.s);
+    if (e != cudaSuccess) return bd.ctx->cuda_fail(e, what);
+    const int rc = bd.sync();
+    bd.B.release(*p);
+    *p = q;
+    return rc;
 }
 
 struct SegPlan {
@@ -630,13 +658,21 @@ struct IdxEntry {
 
 // Steps 3 and 4 once each direction's items are sorted: vertex-predicate lists, type instances,
 // the segment table, lists and key records, placement.
-int gbuild_segments(wk_ctx* ctx, Builder& bd, DirItems* D, double load, bool versatile, uint32_t* hist,
-                    uint32_t* part, wk::Slot** out_slots, uint64_t* out_n_slots, uint32_t** out_edges,
-                    uint64_t* out_n_edges, std::vector<wk_seg_meta>& segs) {
+// spare_k / spare_v: the sort's free pair of buffers (room for every item), reused by the type
+// index.  Every buffer of the sorted items is freed once the lists and key records are made.
+int gbuild_segments(wk_ctx* ctx, Builder& bd, DirItems* D, unsigned long long* spare_k, uint32_t* spare_v,
+                    double load, bool versatile, uint32_t* hist, uint32_t* part, wk::Slot** out_slots,
+                    uint64_t* out_n_slots, uint32_t** out_edges, uint64_t* out_n_edges,
+                    std::vector<wk_seg_meta>& segs) {
     using namespace wk;
     Bufs& B = bd.B;
     cudaStream_t s = bd.s;
     int rc;
+
+    std::vector<const void*> dead;   // freed once the lists and key records are made
+    for (int di = 0; di < 2; ++di)
+        for (const void* q : {(const void*)D[di].key, (const void*)D[di].pred, (const void*)D[di].kstart})
+            dead.push_back(q);
 
     // ---- vertex-predicate lists: each direction's key runs as (vid << 32 | predicate) pairs,
     // stably re-sorted by vid (each vertex's predicates stay ascending), then runs by vertex
@@ -649,6 +685,9 @@ int gbuild_segments(wk_ctx* ctx, Builder& bd, DirItems* D, double load, bool ver
             uint32_t *v = nullptr, *vv = nullptr;
             if (!B.get(&k, nk) || !B.get(&v, nk) || !B.get(&kk, nk) || !B.get(&vv, nk) || !B.get(&V.kstart, nk + 1))
                 return ctx->fail(WK_E_OOM, "store build vertex predicates");
+            for (const void* q : {(const void*)k, (const void*)v, (const void*)kk, (const void*)vv,
+                                  (const void*)V.kstart})
+                dead.push_back(q);
             if (nk)
                 vp_pairs_kernel<<<bd.grid_for(nk), kT, 0, s>>>(D[di].key, D[di].pred, D[di].kstart, nk, k, v);
             int where = 0;
@@ -675,13 +714,15 @@ int gbuild_segments(wk_ctx* ctx, Builder& bd, DirItems* D, double load, bool ver
     std::vector<uint64_t> trun;
     std::vector<uint32_t> tids;
     {
-        unsigned long long *k = nullptr, *kk = nullptr;
-        uint32_t *v = nullptr, *vv = nullptr;
+        // the spare pair has room for every item; the ping-pong pair is sized once the type
+        // items are counted
+        unsigned long long *k = spare_k, *kk = nullptr;
+        uint32_t *v = spare_v, *vv = nullptr;
         const uint64_t n0 = D[0].n;
-        if (!B.get(&k, n0) || !B.get(&v, n0) || !B.get(&kk, n0) || !B.get(&vv, n0))
-            return ctx->fail(WK_E_OOM, "store build type index");
         Compact c{D[0].key, D[0].pred, n0, 2, (uint32_t)kTypeId, nullptr, k, v};
         if ((rc = bd.compact(c, part, &ntype))) return rc;
+        if (!B.get(&kk, ntype) || !B.get(&vv, ntype)) return ctx->fail(WK_E_OOM, "store build type index");
+        for (const void* q : {(const void*)k, (const void*)v, (const void*)kk, (const void*)vv}) dead.push_back(q);
         int where = 0;
         if ((rc = bd.sort(k, v, kk, vv, ntype, kNbitsIdx, 0, hist, &where))) return rc;
         tk = where ? kk : k;
@@ -838,6 +879,9 @@ int gbuild_segments(wk_ctx* ctx, Builder& bd, DirItems* D, double load, bool ver
         if ((rc = bd.sync())) return rc;   // hr lives until the copy is done
     }
 
+    // the items, key runs and type instances are all in the edges and key records now
+    for (const void* q : dead) B.release(q);
+
     // ---- placement
     unsigned long long *bk = nullptr, *bk2 = nullptr;
     uint32_t *ins = nullptr, *ins2 = nullptr, *ext = nullptr;
@@ -915,23 +959,29 @@ int gbuild(wk_ctx* ctx, const uint32_t* d_tr, uint64_t n, double load, bool vers
         !B.get(&d_mm, 8))
         return ctx->fail(WK_E_OOM, "store build scratch");
 
-    // ---- 1-2: items of each direction, sorted and deduplicated
+    // ---- 1-2: items of each direction, sorted and deduplicated.  Both directions are packed
+    // first, so the triples are freed before the sort's second pair of buffers is needed.
     DirItems D[2];   // [0] OUT, [1] IN
+    unsigned long long* pk[2] = {nullptr, nullptr};
+    uint32_t* pv[2] = {nullptr, nullptr};
+    unsigned long long pcnt[2] = {0, 0};
+    int rc;
+    for (int di = 0; di < 2; ++di) {
+        if (!B.get(&pk[di], n) || !B.get(&pv[di], n)) return ctx->fail(WK_E_OOM, "store build items");
+        WKG_CUDA(ctx, cudaMemsetAsync(d_count, 0, 8, s));
+        if (n) pack_kernel<<<bd.grid_for(n), kT, 0, s>>>(d_tr, n, di == 0 ? kOut : kIn, pk[di], pv[di], d_count);
+        WKG_CUDA(ctx, cudaMemcpyAsync(&pcnt[di], d_count, 8, cudaMemcpyDeviceToHost, s));
+        if ((rc = bd.sync())) return rc;
+    }
+    B.release(d_tr);
     unsigned long long* k2 = nullptr;
     uint32_t* v2 = nullptr;
     if (!B.get(&k2, n) || !B.get(&v2, n)) return ctx->fail(WK_E_OOM, "store build sort buffers");
-    int rc;
     for (int di = 0; di < 2; ++di) {
-        const int dir = di == 0 ? kOut : kIn;
         DirItems& Dd = D[di];
-        unsigned long long* k = nullptr;
-        uint32_t* v = nullptr;
-        if (!B.get(&k, n) || !B.get(&v, n)) return ctx->fail(WK_E_OOM, "store build items");
-        WKG_CUDA(ctx, cudaMemsetAsync(d_count, 0, 8, s));
-        if (n) pack_kernel<<<bd.grid_for(n), kT, 0, s>>>(d_tr, n, dir, k, v, d_count);
-        unsigned long long cnt = 0;
-        WKG_CUDA(ctx, cudaMemcpyAsync(&cnt, d_count, 8, cudaMemcpyDeviceToHost, s));
-        if ((rc = bd.sync())) return rc;
+        unsigned long long* k = pk[di];
+        uint32_t* v = pv[di];
+        const unsigned long long cnt = pcnt[di];
         uint32_t mm[6] = {0xFFFFFFFFu, 0, 0xFFFFFFFFu, 0, 0xFFFFFFFFu, 0};
         if (cnt) {
             WKG_CUDA(ctx, cudaMemcpyAsync(d_mm, mm, sizeof(mm), cudaMemcpyHostToDevice, s));
@@ -965,6 +1015,7 @@ int gbuild(wk_ctx* ctx, const uint32_t* d_tr, uint64_t n, double load, bool vers
         Compact kc{Dd.key, Dd.pred, nd, 1, 0, nullptr, reinterpret_cast<unsigned long long*>(Dd.kstart), nullptr};
         if ((rc = bd.compact(kc, part, &nk))) return rc;
         Dd.nkeys = nk;
+        if ((rc = shrink_to(bd, &Dd.kstart, nk + 1, "store build keys"))) return rc;
         WKG_CUDA(ctx, cudaMemcpyAsync(Dd.kstart + nk, &Dd.n, 8, cudaMemcpyHostToDevice, s));
         // groups: where the predicate changes (few), and the key run each one opens
         if ((rc = group_starts(bd, Dd.key, Dd.pred, Dd.n, 3, Dd.kstart, Dd.nkeys, part, Dd.item_lo, Dd.key_lo)))
@@ -974,8 +1025,8 @@ int gbuild(wk_ctx* ctx, const uint32_t* d_tr, uint64_t n, double load, bool vers
             WKG_CUDA(ctx, cudaMemcpyAsync(&Dd.preds[gi], Dd.pred + Dd.item_lo[gi], 4, cudaMemcpyDeviceToHost, s));
         if ((rc = bd.sync())) return rc;
     }
-    return gbuild_segments(ctx, bd, D, load, versatile, hist, part, out_slots, out_n_slots, out_edges, out_n_edges,
-                           segs);
+    return gbuild_segments(ctx, bd, D, k2, v2, load, versatile, hist, part, out_slots, out_n_slots, out_edges,
+                           out_n_edges, segs);
 }
 
 }  // namespace
