@@ -172,7 +172,8 @@ __device__ __forceinline__ void group_probe(const DevStore& st, const uint64_t (
                     pending[u] = false;
                     if (h == 0) atomicOr(err, kErrCorrupt);
                 } else {
-                    s[u] = load_slot(st.slots + bucket[u] * kAssoc + round[u] * L + h);
+                    // 64-bit index: slot numbers pass 2^32 from bucket 2^29 on
+                    s[u] = load_slot(st.slots + (uint64_t)bucket[u] * kAssoc + round[u] * L + h);
                 }
             }
         }
