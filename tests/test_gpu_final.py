@@ -93,3 +93,32 @@ def test_large_table_many_tiles_per_cta(ctx):
     got = _run(ctx, table, [0, 1], True, 0, -1)
     want = oracle.final_process(table, [0, 1], True, 0, -1)
     assert np.array_equal(got, want)
+
+
+def _signed_sorted(table):
+    """The rows in the reference's order: every column as a signed 32-bit value, first column
+    most significant."""
+    s = table.view(np.int32)
+    order = np.lexsort([s[:, c] for c in range(table.shape[1] - 1, -1, -1)])
+    return table[order]
+
+
+@pytest.mark.parametrize("case", ["in_order", "last_pair_swapped", "descending"])
+def test_tables_already_in_order(ctx, case):
+    """A table already in the sort's order skips the sort; one that is out of order by a single
+    pair at its very end, or reversed, does not."""
+    rng = np.random.default_rng(11)
+    rows = 50000
+    pool = np.array([0, 3, 9, 2**17, 2**31 - 1, 2**31, 2**32 - 2, 2**32 - 1], dtype=np.uint64)
+    table = _signed_sorted(pool[rng.integers(0, len(pool), size=(rows, 3))].astype(np.uint32))
+    if case == "last_pair_swapped":
+        k = rows - 2
+        while np.array_equal(table[k], table[k + 1]):
+            k -= 1
+        table[[k, k + 1]] = table[[k + 1, k]]
+    elif case == "descending":
+        table = np.ascontiguousarray(table[::-1])
+    for keep in ([0, 1], [1, 2], [2], [2, 0, 1]):
+        got = _run(ctx, table, keep, True, 0, -1)
+        want = oracle.final_process(table, keep, True, 0, -1)
+        assert np.array_equal(got, want), (case, keep)

@@ -8,7 +8,8 @@
 // of each run of neighbours equal on the required columns the first is kept.  The sort is an
 // LSD radix sort of (packed key, row index) pairs over only the bits in which the rows differ
 // (see "DISTINCT sort" below); rows equal in every column are interchangeable, so the result
-// does not depend on how the reference's std::sort orders them.
+// does not depend on how the reference's std::sort orders them.  A table found to be in that
+// order already (one pass over it, rows_sorted_kernel) skips the sort.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -104,6 +105,27 @@ __global__ void __launch_bounds__(kFinThreads) key_kernel(const uint32_t* table,
         keys[i] = k;
         idx_out[i] = r;
     }
+}
+
+// *flag = 1 when some row is greater than the next one, every column compared as a signed 32-bit
+// value in column order (ReduceCmp).  A table already in that order is what the sort would
+// return (rows equal in every column are interchangeable), so the sort is skipped for it: the
+// exploration writes rows in input order and each row's new column from a sorted list, so a
+// table started from an index or a constant with unique rows comes out in this order.
+__global__ void __launch_bounds__(kFinThreads) rows_sorted_kernel(const uint32_t* table, int cols, uint32_t n,
+                                                                  unsigned* flag) {
+    bool bad = false;
+    for (uint32_t i = blockIdx.x * kFinThreads + threadIdx.x; i + 1 < n && !bad; i += gridDim.x * kFinThreads) {
+        const uint32_t* r = table + (uint64_t)i * cols;
+        for (int c = 0; c < cols; ++c) {
+            const int32_t x = (int32_t)__ldg(r + c), y = (int32_t)__ldg(r + cols + c);
+            if (x != y) {
+                bad = x > y;
+                break;
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
 struct SortPass {
@@ -266,10 +288,13 @@ struct UniqueArgs {
     uint32_t* out;         // kept row indices
 };
 
+// Row i of the sorted order (idx null: the table was in order already).
+__device__ __forceinline__ uint32_t sorted_row(const UniqueArgs& a, uint32_t i) { return a.idx ? a.idx[i] : i; }
+
 __device__ __forceinline__ bool starts_run(const UniqueArgs& a, uint32_t i) {
     if (i == 0) return true;
-    const uint32_t* r = a.table + (uint64_t)a.idx[i] * a.cols;
-    const uint32_t* p = a.table + (uint64_t)a.idx[i - 1] * a.cols;
+    const uint32_t* r = a.table + (uint64_t)sorted_row(a, i) * a.cols;
+    const uint32_t* p = a.table + (uint64_t)sorted_row(a, i - 1) * a.cols;
     for (int k = 0; k < a.n_keep; ++k)
         if (r[a.keep[k]] != p[a.keep[k]]) return true;
     return false;
@@ -297,7 +322,7 @@ __global__ void __launch_bounds__(kFinThreads) unique_place_kernel(const UniqueA
         const uint64_t m = i < hi ? starts_run(a, i) : 0;
         const uint64_t ex = block_exclusive_sum<kFinThreads>(m, s_warp);
         const uint64_t carry = s_carry;
-        if (m) a.out[carry + ex] = a.idx[i];
+        if (m) a.out[carry + ex] = sorted_row(a, i);
         __syncthreads();
         if (threadIdx.x == kFinThreads - 1) s_carry = carry + ex + m;
         __syncthreads();
@@ -465,71 +490,86 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     if (e != cudaSuccess) return done(ctx->cuda_fail(e, "post-pattern columns"));
     const uint32_t* idx = nullptr;   // null: rows in table order
     uint64_t m = n;
+    bool in_order = false;
+    if (sort) {   // a table already in the sort's order keeps it (d_total is free until the scan)
+        unsigned h_flag = 1;
+        if ((e = cudaMemsetAsync(d_total, 0, 4, s)) == cudaSuccess) {
+            rows_sorted_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)((n + kFinThreads - 1) / kFinThreads))),
+                                 kFinThreads, 0, s>>>(in->d, cols, n, d_total);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flag, d_total, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return done(ctx->cuda_fail(e, "order check"));
+        in_order = h_flag == 0;
+    }
     if (sort) {
-        // each column's range, in signed order
-        std::vector<uint32_t> mm(2 * (size_t)cols);
-        for (int c = 0; c < cols; ++c) {
-            mm[2 * c] = 0xFFFFFFFFu;
-            mm[2 * c + 1] = 0;
-        }
-        if ((e = cudaMemcpyAsync(d_mm, mm.data(), mm.size() * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-            return done(ctx->cuda_fail(e, "column ranges"));
-        minmax_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256))),
-                        kFinThreads, 0, s>>>(in->d, (uint64_t)n * cols, cols, d_mm);
-        if ((e = cudaGetLastError()) != cudaSuccess ||
-            (e = cudaMemcpyAsync(mm.data(), d_mm, mm.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-            (e = cudaStreamSynchronize(s)) != cudaSuccess)
-            return done(ctx->cuda_fail(e, "column ranges"));
-        // chunks of columns, last column first; a constant column orders nothing and is left out
-        std::vector<ChunkDesc> chunks;
-        std::vector<int> chunk_bits;
-        ChunkDesc cur{};
-        int cur_bits = 0;
-        auto flush = [&]() {
-            if (!cur.nc) return;
-            // columns were added least significant first; the key wants the most significant first
-            std::reverse(cur.ccol, cur.ccol + cur.nc);
-            std::reverse(cur.cbits, cur.cbits + cur.nc);
-            std::reverse(cur.cmin, cur.cmin + cur.nc);
-            chunks.push_back(cur);
-            chunk_bits.push_back(cur_bits);
-            cur = ChunkDesc{};
-            cur_bits = 0;
-        };
-        for (int c = cols - 1; c >= 0; --c) {
-            const uint32_t lo = mm[2 * c], hi = mm[2 * c + 1];
-            if (lo >= hi) continue;
-            const int b = 32 - __builtin_clz(hi - lo);
-            if (cur_bits + b > 64) flush();
-            cur.ccol[cur.nc] = c;
-            cur.cbits[cur.nc] = b;
-            cur.cmin[cur.nc] = lo;
-            cur.nc++;
-            cur_bits += b;
-        }
-        flush();
-        const int kgrid = std::max(1, std::min(ctx->sm_count * 8, (int)((n + 255) / 256)));
-        uint32_t* ia = idx0;
-        uint32_t* ib = idx1;
-        unsigned long long* ka = key0;
-        unsigned long long* kb = key1;
-        const uint32_t* sorted = nullptr;
-        for (size_t k = 0; k < chunks.size(); ++k) {
-            key_kernel<<<kgrid, kFinThreads, 0, s>>>(in->d, cols, chunks[k], sorted, n, ka, ia);
-            for (int shift = 0; shift < chunk_bits[k]; shift += 8) {
-                SortPass p{ka, ia, kb, ib, shift, n, hist};
-                hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
-                digit_offsets_kernel<<<1, kDigits, 0, s>>>(hist, (uint32_t)grid);
-                scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
-                std::swap(ka, kb);
-                std::swap(ia, ib);
+        const uint32_t* sorted = nullptr;   // the sorted row order (null: the table's own)
+        if (!in_order) {
+            // each column's range, in signed order
+            std::vector<uint32_t> mm(2 * (size_t)cols);
+            for (int c = 0; c < cols; ++c) {
+                mm[2 * c] = 0xFFFFFFFFu;
+                mm[2 * c + 1] = 0;
             }
-            sorted = ia;
-            std::swap(ia, ib);   // the next chunk's keys go to the other index array
-        }
-        if (!sorted) {   // every column constant: every row is equal, the table order stands
-            iota_kernel<<<kgrid, kFinThreads, 0, s>>>(idx0, n);
-            sorted = idx0;
+            if ((e = cudaMemcpyAsync(d_mm, mm.data(), mm.size() * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                return done(ctx->cuda_fail(e, "column ranges"));
+            minmax_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256))),
+                            kFinThreads, 0, s>>>(in->d, (uint64_t)n * cols, cols, d_mm);
+            if ((e = cudaGetLastError()) != cudaSuccess ||
+                (e = cudaMemcpyAsync(mm.data(), d_mm, mm.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess)
+                return done(ctx->cuda_fail(e, "column ranges"));
+            // chunks of columns, last column first; a constant column orders nothing and is left out
+            std::vector<ChunkDesc> chunks;
+            std::vector<int> chunk_bits;
+            ChunkDesc cur{};
+            int cur_bits = 0;
+            auto flush = [&]() {
+                if (!cur.nc) return;
+                // columns were added least significant first; the key wants the most significant first
+                std::reverse(cur.ccol, cur.ccol + cur.nc);
+                std::reverse(cur.cbits, cur.cbits + cur.nc);
+                std::reverse(cur.cmin, cur.cmin + cur.nc);
+                chunks.push_back(cur);
+                chunk_bits.push_back(cur_bits);
+                cur = ChunkDesc{};
+                cur_bits = 0;
+            };
+            for (int c = cols - 1; c >= 0; --c) {
+                const uint32_t lo = mm[2 * c], hi = mm[2 * c + 1];
+                if (lo >= hi) continue;
+                const int b = 32 - __builtin_clz(hi - lo);
+                if (cur_bits + b > 64) flush();
+                cur.ccol[cur.nc] = c;
+                cur.cbits[cur.nc] = b;
+                cur.cmin[cur.nc] = lo;
+                cur.nc++;
+                cur_bits += b;
+            }
+            flush();
+            const int kgrid = std::max(1, std::min(ctx->sm_count * 8, (int)((n + 255) / 256)));
+            uint32_t* ia = idx0;
+            uint32_t* ib = idx1;
+            unsigned long long* ka = key0;
+            unsigned long long* kb = key1;
+            for (size_t k = 0; k < chunks.size(); ++k) {
+                key_kernel<<<kgrid, kFinThreads, 0, s>>>(in->d, cols, chunks[k], sorted, n, ka, ia);
+                for (int shift = 0; shift < chunk_bits[k]; shift += 8) {
+                    SortPass p{ka, ia, kb, ib, shift, n, hist};
+                    hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
+                    digit_offsets_kernel<<<1, kDigits, 0, s>>>(hist, (uint32_t)grid);
+                    scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
+                    std::swap(ka, kb);
+                    std::swap(ia, ib);
+                }
+                sorted = ia;
+                std::swap(ia, ib);   // the next chunk's keys go to the other index array
+            }
+            if (!sorted) {   // every column constant: every row is equal, the table order stands
+                iota_kernel<<<kgrid, kFinThreads, 0, s>>>(idx0, n);
+                sorted = idx0;
+            }
         }
         uint32_t* kept = sorted == idx0 ? idx1 : idx0;
         UniqueArgs u{in->d, cols, d_keep, n_keep, sorted, n, part, kept};
