@@ -160,11 +160,13 @@ __device__ __forceinline__ uint64_t settle_slot(const DevStore& st, uint64_t key
 // kRowsPerThread rows per thread at a time: their keys are worked out and their home slots
 // loaded before any is compared, and the neighbour words of their one-to-one rows are loaded
 // before any output row is written, so a thread has that many random reads in flight.
-// Registers are capped for kCountCtas CTAs per SM.  kFilter: the membership steps
-// (known_to_known, known_to_const, const_to_known, index_to_known); the other instance (starts
-// and known_to_unknown) carries no membership search.
-constexpr int kRowsPerThread = 3;
-constexpr int kCountCtas = 4;
+// Registers are capped for kCountCtas CTAs per SM.  One row per thread at 8 CTAs (2,048 threads
+// per SM) measured best: more rows per thread at fewer CTAs (2-8 rows, 2-6 CTAs) ran 1-35%
+// slower on the heavy star and triangle, so resident warps, not reads per thread, set the rate.
+// kFilter: the membership steps (known_to_known, known_to_const, const_to_known,
+// index_to_known); the other instance (starts and known_to_unknown) carries no membership search.
+constexpr int kRowsPerThread = 1;
+constexpr int kCountCtas = 8;
 
 template <bool kFilter>
 __global__ void __launch_bounds__(kFlatThreads, kCountCtas) flat_count_kernel(const FlatArgs a) {
