@@ -50,6 +50,15 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 # flat passes for levels 0 and 1).  Scaled by the dominant level's input rows; on the larger
 # graph fewer sectors hit in L2, so the scaled figure is a lower bound there.
 LEVEL_TRAFFIC_PER_ROW = (102455040 + 18419712) / 2617493
+# DRAM bytes (read + write) per input row of the heavy triangle's flat steps, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of its launches on the
+# 2,000-organisation graph (4.2 GB store, 1,821,743 input rows per step), the count launch plus
+# place and expand: the known_to_known step (degreeFrom) and the one-to-one known_to_unknown step
+# (memberOf).  Scaled by the dominant heavy step's input rows.
+HEAVY_TRAFFIC_PER_ROW = {
+    "known_to_known": (216070400 + 13536000 + 7780864) / 1821743,
+    "known_to_unknown": (202016000 + 32311808 + 11264 + 25344) / 1821743,
+}
 
 
 def peaks():
@@ -486,25 +495,39 @@ def run_ours(args, world, rank, local_rank):
         if heavy_cpu.get(name):
             heavy[name]["speedup_vs_cpu"] = heavy_cpu[name] / heavy[name]["ms"]
 
-    # ---- post-pattern stage on the device: DISTINCT ?x2 ?x1 over the heavy star's table
+    # ---- post-pattern stage on the device: DISTINCT ?x2 ?x1 over the heavy star's table, as the
+    # star leaves it (already in the sort's order, so the sort is skipped) and with its rows
+    # shuffled (the radix sort runs); the sort's order is canonical, so both give the same rows
     star_table, star_v2c = ctx.execute(hq[0], wk.MODE_RESIDENT)
-    pin = wk.Table(ctx, max(star_table.size, 1))
-    pin.upload(star_table)
     keep = [star_v2c[1], star_v2c[0]]
-    pout = pin.final_process(keep, distinct=True)   # warm: the output table and scratch grow once
-    pp_ms = []
-    for _ in range(5):
-        t0 = time.perf_counter()
-        pin.final_process(keep, distinct=True, out=pout)
-        pp_ms.append((time.perf_counter() - t0) * 1000)
-    pp_rows = pout.shape()[0]
-    pout.free()
-    pin.free()
+
+    def time_distinct(table):
+        pin = wk.Table(ctx, max(table.size, 1))
+        pin.upload(table)
+        pout = pin.final_process(keep, distinct=True)   # warm: the output table and scratch grow once
+        ms = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            pin.final_process(keep, distinct=True, out=pout)
+            ms.append((time.perf_counter() - t0) * 1000)
+        rows = pout.download()
+        pout.free()
+        pin.free()
+        return statistics.median(ms), rows
+
+    pp_ms, pp_out = time_distinct(star_table)
+    shuffled = star_table[np.random.default_rng(args.seed).permutation(star_table.shape[0])]
+    pp_sh_ms, pp_sh_out = time_distinct(shuffled)
+    assert np.array_equal(pp_out, pp_sh_out), "DISTINCT differs on the shuffled rows"
+    del shuffled, pp_sh_out
     post_pattern = {"op": "DISTINCT on two of the heavy star's three columns (wk_table_final_process)",
                     "rows_in": int(star_table.shape[0]), "cols_in": int(star_table.shape[1]),
-                    "rows_out": int(pp_rows), "ms": statistics.median(pp_ms),
+                    "rows_out": int(pp_out.shape[0]), "ms": pp_ms,
+                    "ms_rows_shuffled": pp_sh_ms,
                     "timing": "host clock around the call (it ends with a device sync), median of 5 "
-                              "after a warm call, output table reused"}
+                              "after a warm call, output table reused; ms: the table as the star "
+                              "leaves it (in the sort's order: the sort is skipped), "
+                              "ms_rows_shuffled: the same rows shuffled (radix sort), same result"}
 
     # ---- serving: open-loop Poisson sweep, 98 % light / 2 % heavy, blind replies
     serving = None
@@ -582,7 +605,13 @@ def run_ours(args, world, rank, local_rank):
                                             dom["rows_in"] / (dom["ms"] / 1000.0) / rr_peak,
                                         "note": "one probe per input row"}},
             "roofline_heavy": {"bound": "hbm", "achieved": hach, "peak": peak, "unit": "GB/s",
-                               "frac": hach / peak, "traffic": None,
+                               "frac": hach / peak,
+                               "traffic": (HEAVY_TRAFFIC_PER_ROW[hdom["kind"]] * hdom["rows_in"]
+                                           if hdom["kind"] in HEAVY_TRAFFIC_PER_ROW else None),
+                               "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                                 "the triangle's flat launches on the 2,000-organisation "
+                                                 "graph (1 pass; B per input row of this step's kind) x "
+                                                 "this step's input rows",
                                "kernel": "single-query " + hdom["kind"] + " step (tile launch or "
                                          "flat pipeline, whichever the device picked)",
                                "algorithmic_bytes": hdom["alg_bytes"], "kernel_ms": hdom["ms"],
@@ -769,7 +798,7 @@ def main():
     ap.add_argument("--heavy-cpu-reps", type=int, default=3,
                     help="timed CPU-engine runs of each heavy query (median reported)")
     ap.add_argument("--serve-rates", type=lambda s: [int(x) for x in s.split(",")],
-                    default=[1000, 10000, 50000, 100000, 125000, 150000, 175000, 200000, 500000])
+                    default=[1000, 10000, 25000, 50000, 65000, 80000, 100000, 125000, 150000, 200000, 500000])
     ap.add_argument("--serve-seconds", type=float, default=0.25,
                     help="arrival span of each serving rate")
     ap.add_argument("--device-store", action="store_true",

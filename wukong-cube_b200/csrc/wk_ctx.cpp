@@ -1330,8 +1330,8 @@ extern "C" int wk_query_execute_host(wk_ctx* ctx, const wk_query* q, int32_t mod
     return table_download(ctx, t, host_out, cap_elems, rows);
 }
 
-int wk::query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows) {
-    int rc = query_run(ctx, q, WK_MODE_RESIDENT, t, nullptr, nullptr);
+int wk::query_run_rows(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_table** t, uint64_t* rows) {
+    int rc = query_run(ctx, q, mode, t, nullptr, nullptr);
     if (rc) return rc;
     rc = table_rows(ctx, *t, rows);
     if (rc) return rc;

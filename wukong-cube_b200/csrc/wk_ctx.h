@@ -203,8 +203,9 @@ StepDesc make_step_desc(const wk_ctx* ctx, const PlanStep& s);
 // leave room on every SM for `beside_ctas` CTAs of size `beside_use`.  Released with
 // wk_ctx_destroy, before the parent.
 int ctx_make_child(wk_ctx* parent, const CtaUse& beside_use, int beside_ctas, wk_ctx** out);
-// Run a whole query in RESIDENT mode and report its final table and row count (host sync).
-int query_run_rows(wk_ctx* ctx, const wk_query* q, const wk_table** t, uint64_t* rows);
+// Run a whole query (mode: WK_MODE_RESIDENT or WK_MODE_GRAPH) and report its final table and row
+// count (host sync).
+int query_run_rows(wk_ctx* ctx, const wk_query* q, int32_t mode, const wk_table** t, uint64_t* rows);
 // Copy `elems` elements of a device table to host memory (host sync).
 int table_copy_out(wk_ctx* ctx, const wk_table* t, uint64_t elems, uint32_t* host);
 // Size a serving lane's tables and scan scratch for `elems`-element tables up front.

@@ -549,7 +549,9 @@ extern "C" int wk_serve_run_open_loop(wk_ctx* ctx, const wk_serve_config* cfg_in
                          const wk_table* t = nullptr;
                          uint64_t rows = 0, off = 0;
                          wk_qresult& r = results[q];
-                         int qrc = wk::query_run_rows(lane, &queries[q], &t, &rows);
+                         // a graph per plan, captured by the lane's first query of that plan:
+                         // one launch instead of one per step pass
+                         int qrc = wk::query_run_rows(lane, &queries[q], WK_MODE_GRAPH, &t, &rows);
                          if (qrc == WK_SUCCESS && S.cfg.blind) {
                              r.rows = rows;
                              r.cols = t->cols;
