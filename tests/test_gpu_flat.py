@@ -96,3 +96,32 @@ def test_small_tables_overflow_and_rerun_in_flat(knobs, graph20):
             for mode in (wk.MODE_RESIDENT, wk.MODE_GRAPH):
                 got, _ = c2.execute(q, mode)
                 assert np.array_equal(oracle.sorted_rows(got), oracle.sorted_rows(want))
+
+
+@pytest.mark.parametrize("cols", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("rows", [1, 3, 1021, 6000])
+def test_flat_expand_widths(knobs, graph20, cols, rows):
+    """known_to_unknown through the flat passes at output widths 2-6: short lists (the courses
+    a person takes) and long ones (the persons of a unit), blank rows, at row counts below, at
+    and well past one expand window, the table equal to the oracle's row for row."""
+    ctx = knobs
+    v = graph20["vocab"]
+    o = graph20["oracle"]
+    ctx.tune_set(wk.KNOB_FLAT_ROWS, 1)
+    rng = np.random.default_rng(100 * cols + rows)
+    persons = np.asarray(graph20["instances"][v["t_person_a"]], np.uint32)
+    units = np.asarray(graph20["instances"][v["t_unit"]], np.uint32)
+    for start, pid, d in ((persons, v["p_takes"], wk.OUT), (units, v["p_member_of"], wk.IN)):
+        tab = rng.integers(1 << 17, 1 << 20, size=(rows, cols), dtype=np.uint64).astype(np.uint32)
+        cs = int(rng.integers(0, cols))
+        tab[:, cs] = rng.choice(start, rows)
+        tab[::13, cs] = 0xFFFFFFFF
+        tin = ctx.table(tab, capacity=tab.size)
+        out = ctx.table(capacity=16)
+        ctx.known_to_unknown(tin, cs, pid, d, out)
+        want = o.step(0, tab, cs, pid, d)
+        got = out.download()
+        tin.free()
+        out.free()
+        assert got.shape == want.shape, (cols, rows, pid)
+        assert np.array_equal(got, want), (cols, rows, pid)
