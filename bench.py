@@ -61,6 +61,23 @@ HEAVY_TRAFFIC_PER_ROW = {
 }
 
 
+def dram_rate(traffic_bytes, ms, peak_gbs):
+    """DRAM bytes actually moved (the ncu-derived traffic) per second of the launch, beside the
+    algorithmic-byte rate: a random probe moves a whole DRAM line for its 16 algorithmic bytes,
+    so this is the rate at which the memory itself is kept busy."""
+    gbs = traffic_bytes / (ms / 1000.0) / 1e9
+    return {"gbs": gbs, "frac_of_peak": gbs / peak_gbs}
+
+
+def call_latency(seconds):
+    """p50 / p99 / max of host-clock call durations, in ms: every query of a call has its result
+    on the host when the call returns, so this is its host-visible latency (plans in, tables
+    out, copies included)."""
+    ms = sorted(t * 1000.0 for t in seconds)
+    return {"p50": ms[len(ms) // 2], "p99": ms[min(len(ms) - 1, int(0.99 * len(ms)))], "max": ms[-1],
+            "calls": len(ms)}
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -583,8 +600,10 @@ def run_ours(args, world, rank, local_rank):
                     "d2h_bytes_per_step": d2h,
                     "step": "one wk_batch_execute_stream call: %d batches of %d light queries"
                             % (args.e2e_batches, args.light),
+                    "latency_ms_per_call": call_latency(e2e_t),
                     "single_batch_call": {"value": e2e_single, "unit": "light queries/s",
-                                          "api": "wk_batch_execute, one batch per call"}},
+                                          "api": "wk_batch_execute, one batch per call",
+                                          "latency_ms_per_call": call_latency(one_t)}},
             "plain_path": {"value": plain, "unit": "light queries/s", "sample": len(sample)},
             "single_query_resident": {"value": single_resident, "unit": "light queries/s"},
             "speedup_vs_plain": value / plain,
@@ -594,6 +613,7 @@ def run_ours(args, world, rank, local_rank):
             "post_pattern": post_pattern,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": LEVEL_TRAFFIC_PER_ROW * dom["rows_in"],
+                         "traffic_rate": dram_rate(LEVEL_TRAFFIC_PER_ROW * dom["rows_in"], dom["ms"], peak),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "batch level 3 on the 1,000-organisation graph (1 pass; "
                                            "46.2 B per input row) x this launch's input rows",
@@ -608,6 +628,9 @@ def run_ours(args, world, rank, local_rank):
                                "frac": hach / peak,
                                "traffic": (HEAVY_TRAFFIC_PER_ROW[hdom["kind"]] * hdom["rows_in"]
                                            if hdom["kind"] in HEAVY_TRAFFIC_PER_ROW else None),
+                               "traffic_rate": (dram_rate(HEAVY_TRAFFIC_PER_ROW[hdom["kind"]] * hdom["rows_in"],
+                                                          hdom["ms"], peak)
+                                                if hdom["kind"] in HEAVY_TRAFFIC_PER_ROW else None),
                                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                                  "the triangle's flat launches on the 2,000-organisation "
                                                  "graph (1 pass; B per input row of this step's kind) x "
