@@ -272,7 +272,8 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
     # warm-up run (untimed): loads every kernel of the serving path and builds the lanes
     wq = workloads.light_queries(v, inst, 1000, seed=args.seed + 4999)
     wq[::50] = [hq[j % 2] for j in range(len(wq[::50]))]
-    ctx.serve(wq, np.linspace(0, 50000, len(wq)), blind=1, max_heavy_inflight=args.serve_lanes)
+    ctx.serve(wq, np.linspace(0, 50000, len(wq)), blind=1, max_heavy_inflight=args.serve_lanes,
+              light_ctas_per_sm=args.serve_light_ctas)
     sweep = []
     for k, qps in enumerate(args.serve_rates):
         rng = np.random.default_rng(args.seed + 7000 + k)
@@ -284,7 +285,8 @@ def serving_sweep(ctx, v, inst, o, args, plain_qps, heavy_rows):
             qs[i] = hq[j % 2]
             is_heavy[i] = True
         arrivals = np.cumsum(rng.exponential(1e6 / qps, size=n))
-        res = ctx.serve(qs, arrivals, blind=1, max_heavy_inflight=args.serve_lanes)
+        res = ctx.serve(qs, arrivals, blind=1, max_heavy_inflight=args.serve_lanes,
+                        light_ctas_per_sm=args.serve_light_ctas)
         st = np.array([r[1] for r in res])
         rows = np.array([r[4] for r in res], np.int64)
         lat = np.array([r[3] - r[2] for r in res])
@@ -832,6 +834,9 @@ def main():
                          "engine over the exported store (needs host memory for the store)")
     ap.add_argument("--serve-lanes", type=int, default=1,
                     help="serving: index-start queries running at once, one lane each")
+    ap.add_argument("--serve-light-ctas", type=int, default=0,
+                    help="serving: exploration CTAs per SM of the iteration launches (0: the library's "
+                         "default); the lanes' launches are sized to leave room for one more")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
