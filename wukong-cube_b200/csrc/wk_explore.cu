@@ -515,7 +515,7 @@ __device__ __forceinline__ void tile_back(const ExploreArgs& a, const TileBuf& B
 
 // Resident CTAs per SM each launch shape is built for: registers are capped for this many.  The
 // one-thread-per-row probe holds fewer registers than the group probes.
-__host__ __device__ constexpr int explore_min_blocks(int lanes) { return lanes == 1 ? 8 : 7; }
+__host__ __device__ constexpr int explore_min_blocks(int lanes) { return lanes == 1 ? 9 : 7; }
 
 template <int L>
 __global__ void __launch_bounds__(kStepThreads, explore_min_blocks(L)) explore_kernel(const ExploreArgs a) {
