@@ -45,11 +45,11 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
-# 16,384-query batch on the 1,000-organisation graph: 102,455,040 B + 18,419,712 B for
+# 16,384-query batch on the 1,000-organisation graph: 102,522,624 B + 18,580,480 B for
 # 2,617,493 input rows, with the knobs the autotuner picks (one thread per row, 32-row slices,
 # flat passes for levels 0 and 1).  Scaled by the dominant level's input rows; on the larger
 # graph fewer sectors hit in L2, so the scaled figure is a lower bound there.
-LEVEL_TRAFFIC_PER_ROW = (102455040 + 18419712) / 2617493
+LEVEL_TRAFFIC_PER_ROW = (102522624 + 18580480) / 2617493
 # DRAM bytes (read + write) per input row of the heavy triangle's flat steps, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of its launches on the
 # 2,000-organisation graph (4.2 GB store, 1,821,743 input rows per step), the count launch plus
@@ -618,7 +618,7 @@ def run_ours(args, world, rank, local_rank):
                          "traffic_rate": dram_rate(LEVEL_TRAFFIC_PER_ROW * dom["rows_in"], dom["ms"], peak),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "batch level 3 on the 1,000-organisation graph (1 pass; "
-                                           "46.2 B per input row) x this launch's input rows",
+                                           "46.3 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": dom_kernel,
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
