@@ -277,6 +277,20 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
     }
 }
 
+// out row i = table row idx[i]: the table in sorted order, so the run compaction and the
+// projection read consecutive rows instead of gathering each row (and its neighbour) through
+// the index array.  One thread per element, consecutive threads on consecutive elements.
+__global__ void __launch_bounds__(kFinThreads) gather_rows_kernel(const uint32_t* table, int cols,
+                                                                  const uint32_t* idx, uint32_t n, uint32_t* out) {
+    const uint64_t total = (uint64_t)n * cols;
+    for (uint64_t e = blockIdx.x * (uint64_t)kFinThreads + threadIdx.x; e < total;
+         e += (uint64_t)gridDim.x * kFinThreads) {
+        const uint64_t i = e / cols;
+        const int c = (int)(e - i * cols);
+        out[e] = __ldg(table + (uint64_t)__ldg(idx + i) * cols + c);
+    }
+}
+
 struct UniqueArgs {
     const uint32_t* table;
     int cols;
@@ -465,7 +479,8 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     const bool sort = distinct && n > 1;
     const size_t keep_bytes = ((size_t)n_keep * 4 + 255) & ~(size_t)255;
     const size_t idx_bytes = ((2 * (size_t)n * 4) + 255) & ~(size_t)255;
-    const size_t key_bytes = sort ? 2 * (size_t)n * 8 : 0;
+    // the two key arrays; once the sort is done the same room holds the table in sorted order
+    const size_t key_bytes = sort ? std::max(2 * (size_t)n * 8, (size_t)n * cols * 4) : 0;
     const size_t bytes = keep_bytes + idx_bytes + key_bytes + (size_t)kDigits * grid * 4 +
                          ((size_t)grid + 2) * 4 + (size_t)cols * 8 + 64;
     // the context keeps the scratch between calls (grown, never shrunk): an allocation and a
@@ -489,6 +504,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     cudaError_t e = cudaMemcpyAsync(d_keep, keep_cols, (size_t)n_keep * 4, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return done(ctx->cuda_fail(e, "post-pattern columns"));
     const uint32_t* idx = nullptr;   // null: rows in table order
+    const uint32_t* table_src = in->d;   // the rows idx refers to (the sorted copy after a sort)
     uint64_t m = n;
     bool in_order = false;
     if (sort) {   // a table already in the sort's order keeps it (d_total is free until the scan)
@@ -572,7 +588,17 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             }
         }
         uint32_t* kept = sorted == idx0 ? idx1 : idx0;
-        UniqueArgs u{in->d, cols, d_keep, n_keep, sorted, n, part, kept};
+        // rows gathered into sorted order once (into the key arrays' room): the compaction then
+        // compares consecutive rows and the projection reads the kept ones from this copy
+        const uint32_t* rows_src = in->d;
+        if (sorted) {
+            uint32_t* sorted_rows = reinterpret_cast<uint32_t*>(key0);
+            const int ggrid = std::max(1, std::min<int>(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256)));
+            gather_rows_kernel<<<ggrid, kFinThreads, 0, s>>>(in->d, cols, sorted, n, sorted_rows);
+            rows_src = sorted_rows;
+            sorted = nullptr;
+        }
+        UniqueArgs u{rows_src, cols, d_keep, n_keep, sorted, n, part, kept};
         unique_count_kernel<<<grid, kFinThreads, 0, s>>>(u);
         scan_kernel<<<1, 1024, 0, s>>>(part, (uint32_t)grid, d_total);
         unique_place_kernel<<<grid, kFinThreads, 0, s>>>(u);
@@ -583,6 +609,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             return done(ctx->cuda_fail(e, "distinct count"));
         m = h_total;
         idx = kept;
+        table_src = rows_src;
     }
     const uint64_t start = std::min<uint64_t>((uint64_t)offset, m);
     const uint64_t count = limit < 0 ? m - start : std::min<uint64_t>((uint64_t)limit, m - start);
@@ -590,7 +617,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     if (rc) return done(rc);
     out->cols = n_keep;
     const int pgrid = std::max(1, std::min<int>(ctx->sm_count * 8, (int)((count * n_keep + 255) / 256)));
-    project_kernel<<<pgrid, kFinThreads, 0, s>>>(in->d, cols, d_keep, n_keep, idx, start, count, out->d,
+    project_kernel<<<pgrid, kFinThreads, 0, s>>>(table_src, cols, d_keep, n_keep, idx, start, count, out->d,
                                                  out->d_rows);
     if ((e = cudaGetLastError()) != cudaSuccess) return done(ctx->cuda_fail(e, "projection launch"));
     return done(WK_SUCCESS);
