@@ -34,9 +34,13 @@ __device__ __forceinline__ ulonglong2 load_slot(const Slot* p) {
 // even slot of a bucket (buckets are 128-byte lines of a cudaMalloc'd array).
 __device__ __forceinline__ void load_sector(const Slot* p, ulonglong2* s0, ulonglong2* s1) {
     unsigned long long a, b, c, d;
-    asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];"
-                 : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
-                 : "l"(p));
+    // a probe's line is seldom read again: no L1 allocation, first out of L2
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
+        "ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u64 {%0, %1, %2, %3}, [%4], pol;\n\t}"
+        : "=l"(a), "=l"(b), "=l"(c), "=l"(d)
+        : "l"(p));
     *s0 = make_ulonglong2(a, b);
     *s1 = make_ulonglong2(c, d);
 }
