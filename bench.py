@@ -45,19 +45,19 @@ METRIC = "light-query QPS at p99 latency; heavy-query ms; vs plain per-query GPU
 
 # DRAM bytes (read + write) per input row of the dominant batch level, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of level 3 of a replay of the
-# 16,384-query batch on the 1,000-organisation graph: 102,522,624 B + 18,580,480 B for
+# 16,384-query batch on the 1,000-organisation graph: 103,307,264 B + 18,270,720 B for
 # 2,617,493 input rows, with the knobs the autotuner picks (one thread per row, 32-row slices,
 # flat passes for levels 0 and 1).  Scaled by the dominant level's input rows; on the larger
 # graph fewer sectors hit in L2, so the scaled figure is a lower bound there.
-LEVEL_TRAFFIC_PER_ROW = (102522624 + 18580480) / 2617493
+LEVEL_TRAFFIC_PER_ROW = (103307264 + 18270720) / 2617493
 # DRAM bytes (read + write) per input row of the heavy triangle's flat steps, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of its launches on the
 # 2,000-organisation graph (4.2 GB store, 1,821,743 input rows per step), the count launch plus
 # place and expand: the known_to_known step (degreeFrom) and the one-to-one known_to_unknown step
 # (memberOf).  Scaled by the dominant heavy step's input rows.
 HEAVY_TRAFFIC_PER_ROW = {
-    "known_to_known": (216070400 + 13536000 + 7780864) / 1821743,
-    "known_to_unknown": (202016000 + 32311808 + 11264 + 25344) / 1821743,
+    "known_to_known": (221116672 + 3919872 + 7783168) / 1821743,
+    "known_to_unknown": (207086336 + 8665088 + 11008 + 23040) / 1821743,
 }
 
 
@@ -618,7 +618,7 @@ def run_ours(args, world, rank, local_rank):
                          "traffic_rate": dram_rate(LEVEL_TRAFFIC_PER_ROW * dom["rows_in"], dom["ms"], peak),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                                            "batch level 3 on the 1,000-organisation graph (1 pass; "
-                                           "46.3 B per input row) x this launch's input rows",
+                                           "46.4 B per input row) x this launch's input rows",
                          "peak_source": src,
                          "kernel": dom_kernel,
                          "algorithmic_bytes": dom["alg_bytes"], "kernel_ms": dom["ms"],
