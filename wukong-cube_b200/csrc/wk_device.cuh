@@ -26,8 +26,22 @@ __device__ __forceinline__ unsigned long long pack_status(unsigned epoch, unsign
     return ((unsigned long long)epoch << 48) | (flag << 46) | (v & kValMask);
 }
 
+// 16 bytes from a random place in a large array, read once: no L1 allocation, first out of L2
+// (the probes' lines would otherwise push out the lines the streaming reads and writes reuse).
+__device__ __forceinline__ uint4 load16_once(const void* p) {
+    uint4 v;
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_first.b64 pol, 1.0;\n\t"
+        "ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], pol;\n\t}"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ ulonglong2 load_slot(const Slot* p) {
-    return __ldg(reinterpret_cast<const ulonglong2*>(p));
+    const uint4 v = load16_once(p);
+    return make_ulonglong2((unsigned long long)v.y << 32 | v.x, (unsigned long long)v.w << 32 | v.z);
 }
 
 // Slots p[0] and p[1] (one 32-byte sector) by one 256-bit load.  p must be 32-byte aligned: an

@@ -109,9 +109,10 @@ __global__ void inline_kernel(Slot* slots, uint64_t n_slots, const uint32_t* edg
 
 // Random-read calibration: every thread makes `per` independent 16-byte reads at pseudo-random
 // 16-byte-aligned positions of buf (the splitmix64 finaliser of thread and read index), eight in
-// flight at a time.  With buf much larger than L2 each read costs one 32-byte DRAM sector, the
-// unit the probes and short list reads of the exploration step pay.  The words read are summed
-// and stored only if the sum is one the fill cannot produce, which keeps the reads live.
+// flight at a time, in the probes' own load form (no L1 allocation, first out of L2).  With buf
+// much larger than L2 each read moves a whole DRAM line (about 123 B measured), as a probe of a
+// distinct key does.  The words read are summed and stored only if the sum is one the fill
+// cannot produce, which keeps the reads live.
 __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(256) random_read_kernel(const uint4* __restric
     uint32_t acc = 0;
 #pragma unroll 8
     for (int i = 0; i < per; ++i) {
-        const uint4 v = __ldg(buf + mix64(seed + t * 0x9e3779b97f4a7c15ull + (uint64_t)i) % n16);
+        const uint4 v = dev::load16_once(buf + mix64(seed + t * 0x9e3779b97f4a7c15ull + (uint64_t)i) % n16);
         acc += v.x + v.y + v.z + v.w;
     }
     if (acc == 1u) sink[0] = acc;
