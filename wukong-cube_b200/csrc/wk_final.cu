@@ -136,7 +136,9 @@ struct SortPass {
     int shift;
     uint32_t n;
     uint32_t* hist;          // [kDigits][grid]: digit-major, so one scan gives the offsets
+    uint32_t* dtot;          // [kDigits]: elements of each digit
 };
+static_assert(kFinThreads == kDigits, "the counting passes give each digit one thread");
 
 __device__ __forceinline__ void chunk(uint32_t n, uint32_t* lo, uint32_t* hi) {
     const uint32_t c = (n + gridDim.x - 1) / gridDim.x;
@@ -148,14 +150,24 @@ __global__ void __launch_bounds__(kFinThreads) iota_kernel(uint32_t* idx, uint32
     for (uint32_t i = blockIdx.x * kFinThreads + threadIdx.x; i < n; i += gridDim.x * kFinThreads) idx[i] = i;
 }
 
+// Digit counts of each CTA's chunk.  A thread loads eight keys before it counts any of them, so
+// eight loads per thread are in flight instead of one.
 __global__ void __launch_bounds__(kFinThreads) hist_kernel(const SortPass a) {
+    constexpr int kPer = 8;
     __shared__ uint32_t s_h[kDigits];
     s_h[threadIdx.x] = 0;
     __syncthreads();
     uint32_t lo, hi;
     chunk(a.n, &lo, &hi);
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += kFinThreads)
-        atomicAdd(&s_h[(uint32_t)(a.key_in[i] >> a.shift) & 0xFFu], 1u);
+    uint64_t i = lo + threadIdx.x;
+    for (; i + (kPer - 1) * kFinThreads < hi; i += kPer * kFinThreads) {
+        unsigned long long k[kPer];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) k[r] = a.key_in[i + r * kFinThreads];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) atomicAdd(&s_h[(uint32_t)(k[r] >> a.shift) & 0xFFu], 1u);
+    }
+    for (; i < hi; i += kFinThreads) atomicAdd(&s_h[(uint32_t)(a.key_in[i] >> a.shift) & 0xFFu], 1u);
     __syncthreads();
     a.hist[threadIdx.x * gridDim.x + blockIdx.x] = s_h[threadIdx.x];
 }
@@ -180,21 +192,27 @@ __global__ void __launch_bounds__(1024) scan_kernel(uint32_t* v, uint32_t n, uin
 }
 
 // Offsets of a counting pass: digit d of CTA b starts at the elements of smaller digits plus the
-// digit-d elements of CTAs before b.  One CTA of kDigits threads: thread d adds up its digit's
-// row of hist (one contiguous row of `grid` words, digit-major), then the digit totals are
-// scanned and each row is rewritten as exclusive offsets.
-__global__ void __launch_bounds__(kDigits) digit_offsets_kernel(uint32_t* hist, uint32_t grid) {
-    __shared__ uint64_t s_warp[kDigits / 32];
-    uint32_t* row = hist + (size_t)threadIdx.x * grid;
-    uint64_t tot = 0;
-    for (uint32_t b = 0; b < grid; ++b) tot += row[b];
-    const uint64_t base = block_exclusive_sum<kDigits>(tot, s_warp);
-    uint64_t run = base;
-    for (uint32_t b = 0; b < grid; ++b) {
-        const uint32_t c = row[b];
-        row[b] = (uint32_t)run;
-        run += c;
+// digit-d elements of CTAs before b.  CTA d of this launch scans digit d's row of hist (one
+// contiguous row of `grid` words, digit-major) in place into exclusive offsets within the digit,
+// with coalesced loads, and writes the digit's total to dtot[d]; each scatter CTA then adds the
+// elements of smaller digits (an exclusive scan of dtot) itself.
+__global__ void __launch_bounds__(kFinThreads) digit_rows_kernel(uint32_t* hist, uint32_t grid, uint32_t* dtot) {
+    __shared__ uint64_t s_warp[kFinThreads / 32];
+    __shared__ uint64_t s_carry;
+    uint32_t* row = hist + (size_t)blockIdx.x * grid;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (uint32_t b0 = 0; b0 < grid; b0 += kFinThreads) {
+        const uint32_t b = b0 + threadIdx.x;
+        const uint64_t x = b < grid ? row[b] : 0;
+        const uint64_t ex = block_exclusive_sum<kFinThreads>(x, s_warp);
+        const uint64_t carry = s_carry;
+        if (b < grid) row[b] = (uint32_t)(carry + ex);
+        __syncthreads();
+        if (threadIdx.x == kFinThreads - 1) s_carry = carry + ex + x;
+        __syncthreads();
     }
+    if (threadIdx.x == 0) dtot[blockIdx.x] = (uint32_t)s_carry;
 }
 
 // Stable scatter of 2,048-element tiles: warp w of the CTA takes elements [w * 256, w * 256 + 256)
@@ -204,11 +222,12 @@ __global__ void __launch_bounds__(kDigits) digit_offsets_kernel(uint32_t* hist, 
 // gives its place in the warp; one barrier then turns the warps' counts into per-warp digit
 // offsets.  The tile is placed in shared memory sorted by digit (stable), and then written out
 // in that order, consecutive threads on consecutive elements, so each digit's run goes to
-// global memory in contiguous, coalesced stores.
+// global memory in contiguous, coalesced stores.  Built for 4 CTAs per SM (64 registers, no
+// spills; 34.9 KB of shared memory each), so the pass's 4 CTAs per SM run in one wave.
 constexpr int kScatterPer = 8;                                // elements per thread per tile
 constexpr int kScatterTile = kFinThreads * kScatterPer;       // 2,048
 
-__global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) {
+__global__ void __launch_bounds__(kFinThreads, 4) scatter_kernel(const SortPass a) {
     constexpr int kWarps = kFinThreads / 32;
     __shared__ uint32_t s_run[kDigits];
     __shared__ uint32_t s_cnt[kWarps][kDigits];
@@ -217,7 +236,10 @@ __global__ void __launch_bounds__(kFinThreads) scatter_kernel(const SortPass a) 
     __shared__ uint32_t s_idx[kScatterTile];
     __shared__ uint64_t s_warp[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    s_run[threadIdx.x] = a.hist[threadIdx.x * gridDim.x + blockIdx.x];
+    // thread d: digit d's first place for this CTA = the elements of smaller digits plus the
+    // digit-d elements of the CTAs before this one
+    const uint32_t smaller = (uint32_t)block_exclusive_sum<kFinThreads>(a.dtot[threadIdx.x], s_warp);
+    s_run[threadIdx.x] = smaller + a.hist[threadIdx.x * gridDim.x + blockIdx.x];
     uint32_t lo, hi;
     chunk(a.n, &lo, &hi);
     for (uint32_t base = lo; base < hi; base += kScatterTile) {
@@ -432,6 +454,7 @@ cudaError_t final_kernel_attrs() {
     if (e == cudaSuccess) e = use_max_shared_carveout(key_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(hist_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scan_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(digit_rows_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scatter_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_count_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_place_kernel);
@@ -475,14 +498,14 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     const uint32_t n = (uint32_t)R;
     const int grid = std::max(1, std::min<int>(ctx->sm_count * 4, (int)((n + 2047) / 2048)));
     // scratch: the required columns, two index arrays, two key arrays (DISTINCT only), the
-    // digit histogram, the CTA counts and the distinct total, the column ranges
+    // digit histogram, the CTA counts and the distinct total, the column ranges, the digit totals
     const bool sort = distinct && n > 1;
     const size_t keep_bytes = ((size_t)n_keep * 4 + 255) & ~(size_t)255;
     const size_t idx_bytes = ((2 * (size_t)n * 4) + 255) & ~(size_t)255;
     // the two key arrays; once the sort is done the same room holds the table in sorted order
     const size_t key_bytes = sort ? std::max(2 * (size_t)n * 8, (size_t)n * cols * 4) : 0;
     const size_t bytes = keep_bytes + idx_bytes + key_bytes + (size_t)kDigits * grid * 4 +
-                         ((size_t)grid + 2) * 4 + (size_t)cols * 8 + 64;
+                         ((size_t)grid + 2) * 4 + (size_t)cols * 8 + (size_t)kDigits * 4 + 64;
     // the context keeps the scratch between calls (grown, never shrunk): an allocation and a
     // cudaFree per call would cost more than the stage's own kernels
     int src = ctx->final_scratch_reserve(bytes);
@@ -501,6 +524,7 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     uint32_t* part = hist + (size_t)kDigits * grid;
     uint32_t* d_total = part + grid + 1;
     uint32_t* d_mm = d_total + 1;
+    uint32_t* dtot = d_mm + 2 * (size_t)cols;
     cudaError_t e = cudaMemcpyAsync(d_keep, keep_cols, (size_t)n_keep * 4, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return done(ctx->cuda_fail(e, "post-pattern columns"));
     const uint32_t* idx = nullptr;   // null: rows in table order
@@ -572,9 +596,9 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             for (size_t k = 0; k < chunks.size(); ++k) {
                 key_kernel<<<kgrid, kFinThreads, 0, s>>>(in->d, cols, chunks[k], sorted, n, ka, ia);
                 for (int shift = 0; shift < chunk_bits[k]; shift += 8) {
-                    SortPass p{ka, ia, kb, ib, shift, n, hist};
+                    SortPass p{ka, ia, kb, ib, shift, n, hist, dtot};
                     hist_kernel<<<grid, kFinThreads, 0, s>>>(p);
-                    digit_offsets_kernel<<<1, kDigits, 0, s>>>(hist, (uint32_t)grid);
+                    digit_rows_kernel<<<kDigits, kFinThreads, 0, s>>>(hist, (uint32_t)grid, dtot);
                     scatter_kernel<<<grid, kFinThreads, 0, s>>>(p);
                     std::swap(ka, kb);
                     std::swap(ia, ib);
