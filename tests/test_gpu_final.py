@@ -122,3 +122,21 @@ def test_tables_already_in_order(ctx, case):
         got = _run(ctx, table, keep, True, 0, -1)
         want = oracle.final_process(table, keep, True, 0, -1)
         assert np.array_equal(got, want), (case, keep)
+
+
+@pytest.mark.parametrize("cols", [3, 4])
+@pytest.mark.parametrize("edge", [-1, 0, 1])
+def test_order_check_at_tile_edges(ctx, cols, edge):
+    """The order check stages rows in tiles of 8,192 // cols - 1 row pairs (plus the row after
+    them): a table in order but for one pair of distinct rows swapped where a tile ends, where
+    the next begins, or one further in, must still go through the sort."""
+    rng = np.random.default_rng(12 + cols)
+    rows = 30000
+    table = _signed_sorted(rng.integers(0, 2**32, size=(rows, cols), dtype=np.uint64).astype(np.uint32))
+    k = 3 * (8192 // cols - 1) + edge   # the swapped pair: rows k and k + 1
+    assert not np.array_equal(table[k], table[k + 1])
+    table[[k, k + 1]] = table[[k + 1, k]]
+    keep = [cols - 1, 0]
+    got = _run(ctx, table, keep, True, 0, -1)
+    want = oracle.final_process(table, keep, True, 0, -1)
+    assert np.array_equal(got, want), (cols, edge)

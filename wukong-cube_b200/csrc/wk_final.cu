@@ -56,6 +56,28 @@ __global__ void __launch_bounds__(kFinThreads) minmax_kernel(const uint32_t* tab
     const int step = (int)(stride % cols);
     uint32_t lo = 0xFFFFFFFFu, hi = 0;
     int cur = c;
+    // eight loads in flight per thread; the host makes the grid's stride a multiple of cols where
+    // it can, so a thread's elements stay in one column and the fold below never runs in the loop
+    constexpr int kPer = 8;
+    for (; e + (kPer - 1) * stride < elems; e += kPer * stride) {
+        uint32_t v[kPer];
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) v[r] = __ldg(table + e + r * stride) ^ 0x80000000u;
+#pragma unroll
+        for (int r = 0; r < kPer; ++r) {
+            if (c != cur) {
+                atomicMin(&s_lo[cur], lo);
+                atomicMax(&s_hi[cur], hi);
+                lo = 0xFFFFFFFFu;
+                hi = 0;
+                cur = c;
+            }
+            lo = min(lo, v[r]);
+            hi = max(hi, v[r]);
+            c += step;
+            if (c >= cols) c -= cols;
+        }
+    }
     for (; e < elems; e += stride) {
         const uint32_t v = __ldg(table + e) ^ 0x80000000u;
         if (c != cur) {   // column changed: fold the run so far into shared memory
@@ -112,20 +134,47 @@ __global__ void __launch_bounds__(kFinThreads) key_kernel(const uint32_t* table,
 // return (rows equal in every column are interchangeable), so the sort is skipped for it: the
 // exploration writes rows in input order and each row's new column from a sorted list, so a
 // table started from an index or a constant with unique rows comes out in this order.
+// A CTA stages `tile_rows` consecutive rows and the row after them in shared memory with
+// coalesced loads, eight in flight per thread, then each thread compares one row with the next
+// out of shared memory; a CTA that finds a pair out of order stops.
+constexpr int kCheckWords = 8192;   // 32 KiB of rows per tile
+
 __global__ void __launch_bounds__(kFinThreads) rows_sorted_kernel(const uint32_t* table, int cols, uint32_t n,
-                                                                  unsigned* flag) {
-    bool bad = false;
-    for (uint32_t i = blockIdx.x * kFinThreads + threadIdx.x; i + 1 < n && !bad; i += gridDim.x * kFinThreads) {
-        const uint32_t* r = table + (uint64_t)i * cols;
-        for (int c = 0; c < cols; ++c) {
-            const int32_t x = (int32_t)__ldg(r + c), y = (int32_t)__ldg(r + cols + c);
-            if (x != y) {
-                bad = x > y;
-                break;
+                                                                  uint32_t tile_rows, unsigned* flag) {
+    __shared__ uint32_t s_t[kCheckWords];
+    const uint32_t pairs = n - 1;   // pair i is rows (i, i + 1); n >= 2
+    for (uint64_t t0 = (uint64_t)blockIdx.x * tile_rows; t0 < pairs; t0 += (uint64_t)gridDim.x * tile_rows) {
+        const uint32_t here = (uint32_t)min((uint64_t)tile_rows, pairs - t0);   // pairs of this tile
+        const uint32_t words = (here + 1) * (uint32_t)cols;                     // <= kCheckWords
+        const uint32_t* src = table + t0 * cols;
+        constexpr int kPer = 8;
+        uint32_t w = threadIdx.x;
+        for (; w + (kPer - 1) * kFinThreads < words; w += kPer * kFinThreads) {
+            uint32_t v[kPer];
+#pragma unroll
+            for (int r = 0; r < kPer; ++r) v[r] = __ldg(src + w + r * kFinThreads);
+#pragma unroll
+            for (int r = 0; r < kPer; ++r) s_t[w + r * kFinThreads] = v[r];
+        }
+        for (; w < words; w += kFinThreads) s_t[w] = __ldg(src + w);
+        __syncthreads();
+        bool bad = false;
+        for (uint32_t i = threadIdx.x; i < here && !bad; i += kFinThreads) {
+            const uint32_t* r = s_t + i * cols;
+            for (int c = 0; c < cols; ++c) {
+                const int32_t x = (int32_t)r[c], y = (int32_t)r[cols + c];
+                if (x != y) {
+                    bad = x > y;
+                    break;
+                }
             }
         }
+        // also the barrier before the next tile overwrites s_t
+        if (__syncthreads_or(bad)) {
+            if (threadIdx.x == 0) atomicOr(flag, 1u);
+            return;
+        }
     }
-    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
 struct SortPass {
@@ -455,6 +504,7 @@ cudaError_t final_kernel_attrs() {
     if (e == cudaSuccess) e = use_max_shared_carveout(hist_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scan_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(digit_rows_kernel);
+    if (e == cudaSuccess) e = use_max_shared_carveout(rows_sorted_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(scatter_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_count_kernel);
     if (e == cudaSuccess) e = use_max_shared_carveout(unique_place_kernel);
@@ -492,6 +542,9 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
         return WK_SUCCESS;
     }
     if (n_keep == 0) return ctx->fail(WK_NO_REQUIRED_VAR, "no required variable");
+    // tables hold at most 32 columns (the context's column limit); the sort's chunk layout and
+    // the order check's row tiles are sized for that
+    if (cols > 32) return ctx->fail(WK_E_CAPACITY, "more than 32 columns");
     for (int k = 0; k < n_keep; ++k)
         if (keep_cols[k] < 0 || keep_cols[k] >= cols) return ctx->fail(WK_E_BADARG, "required column out of range");
     if (R >= (1ull << 32)) return ctx->fail(WK_E_CAPACITY, "table too long for the post-pattern stage");
@@ -534,8 +587,10 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
     if (sort) {   // a table already in the sort's order keeps it (d_total is free until the scan)
         unsigned h_flag = 1;
         if ((e = cudaMemsetAsync(d_total, 0, 4, s)) == cudaSuccess) {
-            rows_sorted_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)((n + kFinThreads - 1) / kFinThreads))),
-                                 kFinThreads, 0, s>>>(in->d, cols, n, d_total);
+            const uint32_t tile_rows = (uint32_t)(kCheckWords / cols - 1);   // cols <= 32: >= 255 rows
+            const int cgrid = (int)std::max<uint64_t>(
+                1, std::min<uint64_t>((uint64_t)ctx->sm_count * 6, ((uint64_t)n - 1 + tile_rows - 1) / tile_rows));
+            rows_sorted_kernel<<<cgrid, kFinThreads, 0, s>>>(in->d, cols, n, tile_rows, d_total);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaMemcpyAsync(&h_flag, d_total, 4, cudaMemcpyDeviceToHost, s);
@@ -554,8 +609,9 @@ extern "C" int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int
             }
             if ((e = cudaMemcpyAsync(d_mm, mm.data(), mm.size() * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
                 return done(ctx->cuda_fail(e, "column ranges"));
-            minmax_kernel<<<std::max(1, std::min(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256))),
-                            kFinThreads, 0, s>>>(in->d, (uint64_t)n * cols, cols, d_mm);
+            int mgrid = std::max(1, std::min(ctx->sm_count * 8, (int)(((uint64_t)n * cols + 255) / 256)));
+            if (mgrid >= cols) mgrid -= mgrid % cols;   // stride a multiple of cols: one column per thread
+            minmax_kernel<<<mgrid, kFinThreads, 0, s>>>(in->d, (uint64_t)n * cols, cols, d_mm);
             if ((e = cudaGetLastError()) != cudaSuccess ||
                 (e = cudaMemcpyAsync(mm.data(), d_mm, mm.size() * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
                 (e = cudaStreamSynchronize(s)) != cudaSuccess)
