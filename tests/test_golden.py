@@ -239,6 +239,45 @@ def test_non_versatile_store_refuses_unknown_predicates(graph20, golden):
             assert st == wk.UNKNOWN_PATTERN, g["name"]
 
 
+def test_reference_final_stage_live(graph20):
+    """Where the reference engine library was built: the reference's own final stage
+    (execute_sparql_query with required variables, DISTINCT, LIMIT and OFFSET) equals the
+    oracle's restatement row for row, in order, on the heavy star, the heavy triangle and light
+    queries, for seeded random choices of required variables (any subset, any order) and of
+    DISTINCT / OFFSET / LIMIT. The device stage is checked against the same restatement."""
+    import oracle
+    import refengine
+    import workloads
+    if not refengine.available():
+        pytest.skip("the reference engine library was not built here")
+    o, tr, v = graph20["oracle"], graph20["triples"], graph20["vocab"]
+    g = refengine.graph_from_store(o, tr, v)
+    qs = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+    qs += workloads.light_queries(v, graph20["instances"], 40, seed=23)
+    rng = np.random.default_rng(31)
+    checked = 0
+    for q in qs:
+        st, rows, v2c = o.run(q.flat(), q.nvars)
+        if st != 0:
+            continue
+        bound = refengine.bound_vars(q.flat())
+        for _ in range(4):
+            req = [int(x) for x in rng.permutation(bound)[:int(rng.integers(1, len(bound) + 1))]]
+            distinct = bool(rng.integers(0, 2))
+            n = rows.shape[0]
+            offset = int(rng.choice([0, 0, 1, 3, n // 2, n + 2]))
+            limit = int(rng.choice([-1, -1, 0, 1, 5, n]))
+            rst, rtab, _ = g.run(q.flat(), q.nvars, required=req, distinct=distinct, limit=limit,
+                                 offset=offset)
+            assert rst == 0
+            keep = [v2c[-r - 1] for r in req]
+            want = oracle.final_process(rows, keep, distinct=distinct, offset=offset, limit=limit)
+            assert rtab.shape == want.shape, (req, distinct, offset, limit)
+            assert np.array_equal(rtab, want), (req, distinct, offset, limit)
+            checked += 1
+    assert checked >= 100
+
+
 @pytest.mark.parametrize("versatile", [False, True])
 def test_reference_engine_dispatch_live(built, versatile):
     """Where the reference engine library was built: seeded random plans (the dispatch test's
