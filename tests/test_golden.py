@@ -239,6 +239,35 @@ def test_non_versatile_store_refuses_unknown_predicates(graph20, golden):
             assert st == wk.UNKNOWN_PATTERN, g["name"]
 
 
+def test_reference_engine_live_zipf(built):
+    """Where the reference engine library was built: on a 30-organisation graph whose
+    degreeFrom targets and course choices follow Zipf (s = 1.1), the skewed shape of the scale
+    configuration, the reference engine gives the oracle's status, rows and column map for the
+    heavy star, the heavy triangle and 150 light queries."""
+    import oracle
+    import refengine
+    import workloads
+    import wukong_b200 as wk
+    if not refengine.available():
+        pytest.skip("the reference engine library was not built here")
+    tr, v = wk.synth_generate(30, seed=5, zipf=True, zipf_s=1.1)
+    o = oracle.OracleStore(tr)
+    g = refengine.graph_from_store(o, tr, v)
+    inst = {t: o.get_index(t, wk.IN) for t in range(v["t_org"], v["t_doc"] + 1)}
+    qs = [workloads.heavy_star(v), workloads.heavy_triangle(v)]
+    qs += workloads.light_queries(v, inst, 150, seed=41)
+    nonempty = 0
+    for q in qs:
+        st, rows, v2c = g.run(q.flat(), q.nvars, required=refengine.bound_vars(q.flat()) or [-1])
+        ost, orows, ov2c = o.run(q.flat(), q.nvars)
+        assert st == ost
+        if st == 0:
+            assert np.array_equal(oracle.sorted_rows(rows), oracle.sorted_rows(orows))
+            assert list(v2c) == list(ov2c)
+            nonempty += rows.shape[0] > 0
+    assert nonempty >= 100
+
+
 def test_reference_final_stage_live(graph20):
     """Where the reference engine library was built: the reference's own final stage
     (execute_sparql_query with required variables, DISTINCT, LIMIT and OFFSET) equals the
