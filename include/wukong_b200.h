@@ -281,8 +281,10 @@ int wk_table_shape(wk_ctx* ctx, const wk_table* t, uint64_t* rows, int32_t* cols
  * kept; then `offset` rows dropped and at most `limit` kept (limit < 0: all); then the
  * projection onto keep_cols, the required variables' columns in their order.  The result goes
  * to `out` (grown as needed; not `in`).  An empty input comes back empty with its columns
- * unchanged, as the reference leaves it; WK_NO_REQUIRED_VAR if n_keep == 0.  ORDER BY compares
- * the ids' strings in the reference and is not offered. */
+ * unchanged, as the reference leaves it; WK_NO_REQUIRED_VAR if n_keep == 0; WK_E_CAPACITY for a
+ * table of more than 32 columns (the context's column limit) or of 2^32 rows or more;
+ * WK_E_CORRUPT for an input whose row count is past its capacity.  ORDER BY compares the ids'
+ * strings in the reference and is not offered. */
 int wk_table_final_process(wk_ctx* ctx, const wk_table* in, const int32_t* keep_cols, int32_t n_keep,
                            int32_t distinct, int64_t offset, int64_t limit, wk_table* out);
 /* The BOUND filters of a query on the device: SPARQLEngine::bound_filter (sparql.hpp:1222-1234)
